@@ -1,0 +1,166 @@
+/* ising_b200.h — C ABI of the B200 Metropolis / parallel-tempering engine.
+ *
+ * Drop-in for the CPU sweep of EldosZhupanov/ising_engine (the "S1" path):
+ * the 64-replica Metropolis sweep over CSR couplings, the dE / local-field
+ * update and the DEO parallel-tempering replica exchange. Plain pointers and
+ * sizes only; no C++ or torch types cross this boundary.
+ *
+ * Conventions
+ *  - Every call returns an ie_status; no exception or abort crosses the ABI.
+ *    After a non-zero status, ie_last_error() returns a message for the thread.
+ *  - The caller owns every host buffer; the library copies what it needs and
+ *    owns all device memory. A handle is not thread-safe; one CUDA stream per
+ *    handle.
+ *  - Spin words use the reference's init-word layout (ultimate.rs:272-275):
+ *    bit r of word [cell][site] is replica r, cell = t + num_temps * p.
+ *  - Integer mode (all linear terms and couplings integral, |value| <= 127 per
+ *    coupling, local fields bounded by 127) is bit-exact with the reference for
+ *    spins, energies, swap decisions and master-RNG position. Otherwise the f64
+ *    mode runs the reference's f64 arithmetic in the reference's order.
+ */
+#ifndef ISING_B200_H
+#define ISING_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IE_NUM_REPLICAS 64 /* NUM_REPLICAS, src/solver/types.rs:17 */
+
+typedef enum ie_status {
+    IE_OK = 0,
+    IE_ERR_INVALID = 1,     /* bad shape, index out of range, bad config */
+    IE_ERR_UNSUPPORTED = 2, /* e.g. num_slices != 1 or num_pops != 1 */
+    IE_ERR_OOM = 3,         /* device allocation failed */
+    IE_ERR_CUDA = 4,        /* CUDA runtime error */
+    IE_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+    IE_ERR_DEVICE = 6       /* device-side error word set (bounds check) */
+} ie_status;
+
+/* Mirrors QuboModel + CsrMatrix (src/core/hubo.rs:165-173,
+ * src/core/csr_matrix.rs:6-10): both triangles stored, usize -> uint64. */
+typedef struct ie_problem {
+    uint64_t num_vars;
+    const double* linear;        /* [num_vars] */
+    const uint64_t* row_offsets; /* [num_vars + 1] */
+    const uint64_t* col_indices; /* [nnz] */
+    const double* values;        /* [nnz] */
+    double energy_offset;
+} ie_problem;
+
+/* Mirrors the UltimateSolver fields the PT path reads (ultimate.rs:18-57).
+ * exchange_interval is an extension: phase 2 of engine::step runs after every
+ * k-th step (k = 1, the default when 0 is passed, is the reference). */
+typedef struct ie_config {
+    double temp_max;
+    double temp_min;
+    uint64_t sweeps_per_exchange;
+    uint64_t total_exchanges;
+    uint64_t seed;
+    uint32_t num_temps;  /* default 10 (ultimate.rs:75) */
+    uint32_t num_pops;   /* must be 1 (PA-PT is not on this path) */
+    uint32_t num_slices; /* must be 1 (the Trotter branch is not on this path) */
+    uint32_t exchange_interval;
+    int32_t force_f64;   /* nonzero: use the f64 mode even for integral input */
+    int32_t device;      /* CUDA device ordinal */
+} ie_config;
+
+typedef struct ie_handle ie_handle;
+typedef struct ie_batch ie_batch;
+
+const char* ie_last_error(void);
+int ie_abi_version(void);
+
+/* ---- single instance (engine::step seam and the UltimateSolver PT loop) ---- */
+
+/* Replaces QuantumField::new + StepScratch::for_field + ChaCha8Rng::seed_from_u64
+ * (ultimate.rs:152,235,299). Copies the problem to the device. */
+ie_status ie_create(const ie_problem* problem, const ie_config* config, ie_handle** out);
+ie_status ie_destroy(ie_handle* h);
+
+/* is_clamped/clamp_val [num_vars] (engine.rs:567-571, ultimate.rs:154-159).
+ * Call before ie_init_random. NULL clears all clamps. */
+ie_status ie_set_clamps(ie_handle* h, const uint8_t* is_clamped, const int8_t* clamp_val);
+
+/* ultimate.rs:248-290: one gen::<u64>() word per (t, v) from the master stream
+ * (clamped sites take their value and draw nothing), then
+ * calculate_replica_energies for every cell. */
+ie_status ie_init_random(ie_handle* h);
+
+/* Sets spin words [num_temps][num_vars] directly (no master-stream draws) and
+ * recomputes the tracked energies. */
+ie_status ie_set_spins(ie_handle* h, const uint64_t* words);
+
+/* engine::step (engine.rs:573-819) n_steps times with a constant temperature
+ * ladder temps[num_temps]: base_seed draw, index-order sweep of every cell,
+ * DEO exchange (every exchange_interval-th step), phase toggle. Energies are
+ * re-synced every 1000 steps as ultimate.rs:316-324 does. */
+ie_status ie_step(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t n_steps);
+
+/* Per-step temperature schedule temps[n_steps][num_temps] (SA schedules). */
+ie_status ie_run_schedule(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t n_steps);
+
+/* The UltimateSolver PT loop (ultimate.rs:234-336) with the geometric ladder
+ * of the config: total_exchanges x sweeps_per_exchange steps, resync every
+ * 1000 steps, update_incumbent after every exchange block (ultimate.rs:397-430).
+ * Requires ie_init_random (or ie_set_spins) first. */
+ie_status ie_run_pt(ie_handle* h);
+
+ie_status ie_read_spins(ie_handle* h, uint64_t* words /* [num_temps][num_vars] */);
+ie_status ie_read_energies(ie_handle* h, double* energies /* [num_temps][64] */);
+/* swap attempts / accepts per adjacent pair [num_temps - 1] (engine.rs:545-551). */
+ie_status ie_read_swap_stats(ie_handle* h, uint64_t* attempts, uint64_t* accepts);
+/* Master-stream position (number of u64 draws so far) and DEO phase. */
+ie_status ie_read_rng_state(ie_handle* h, uint64_t* draws, int32_t* deo_odd_phase);
+/* Incumbent of ie_run_pt: energy (model energy incl. offset) and state [num_vars]. */
+ie_status ie_read_incumbent(ie_handle* h, double* energy, int8_t* state);
+/* Best replica of the final field in (t, r) order with strict < on the model
+ * energy (ultimate.rs:345-368), merged with the incumbent (ultimate.rs:371-373). */
+ie_status ie_read_best(ie_handle* h, double* energy, int8_t* state);
+
+/* geometric ladder temps[i] = T_max * f^i, f = (T_min/T_max)^(1/(nt-1)),
+ * computed with pow and powi exactly as ultimate.rs:238-246. */
+ie_status ie_geometric_temps(double temp_max, double temp_min, uint32_t num_temps, double* out);
+/* suggested_temp_range (src/solver/schedule.rs:21-43). */
+ie_status ie_suggested_temp_range(const ie_problem* problem, double* temp_max, double* temp_min);
+
+/* ---- batched: many single-cell SA instances in one persistent launch ---- */
+
+typedef struct ie_batch_config {
+    int32_t device;
+    int32_t force_f64;
+    uint32_t threads_per_block; /* 0 = autotune */
+    uint32_t blocks_per_sm;     /* 0 = autotune */
+} ie_batch_config;
+
+/* count problems, each run as one cell of 64 replicas with its own seed. */
+ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint64_t* seeds,
+                          const ie_batch_config* config, ie_batch** out);
+ie_status ie_batch_destroy(ie_batch* b);
+/* Random init of every instance (ultimate.rs:248-290 with num_temps = 1). */
+ie_status ie_batch_init_random(ie_batch* b);
+/* Runs temps[n_steps] (one temperature per step, shared by all instances) on
+ * every instance: engine::step with num_temps = 1, resync every 1000 steps. */
+ie_status ie_batch_run_schedule(ie_batch* b, const double* temps, uint64_t n_steps);
+/* Same schedule, one launch per instance in sequence (the plain method). */
+ie_status ie_batch_run_schedule_plain(ie_batch* b, const double* temps, uint64_t n_steps,
+                                      uint32_t first, uint32_t count);
+/* Spin words of instance i at words + offsets[i] (offsets = prefix sums of n). */
+ie_status ie_batch_read_spins(ie_batch* b, uint64_t* words);
+ie_status ie_batch_read_energies(ie_batch* b, double* energies /* [count][64] */);
+ie_status ie_batch_read_draws(ie_batch* b, uint64_t* draws /* [count] */);
+/* FP64 recompute of every instance's energies on the device, reference order. */
+ie_status ie_batch_recompute_energies(ie_batch* b, double* energies /* [count][64] */);
+/* Device time of the last run call in milliseconds (CUDA events on its stream). */
+ie_status ie_batch_last_run_ms(ie_batch* b, double* ms);
+/* Number of kernel launches the last run call issued. */
+ie_status ie_batch_last_launches(ie_batch* b, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ISING_B200_H */

@@ -1,0 +1,998 @@
+// Host side of the B200 engine: problem ingestion, device memory, launch
+// orchestration and the C ABI declared in include/ising_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/ising_b200.h"
+#include "ie_device.cuh"
+#include "ie_launch.h"
+
+using namespace ie;
+
+namespace {
+
+thread_local std::string g_err;
+
+ie_status fail(ie_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+#define IE_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(e_ == cudaErrorMemoryAllocation ? IE_ERR_OOM : IE_ERR_CUDA,        \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+#define IE_TRY(expr)                   \
+    do {                               \
+        ie_status s_ = (expr);         \
+        if (s_ != IE_OK) return s_;    \
+    } while (0)
+
+// rand_core 0.6.4 SeedableRng::seed_from_u64: PCG32 outputs fill the 32-byte
+// ChaCha8 key (little-endian), as ChaCha8Rng::seed_from_u64 (ultimate.rs:152).
+void chacha_key_from_u64(uint64_t state, uint32_t key[8]) {
+    const uint64_t mul = 6364136223846793005ULL, inc = 11634580027462260723ULL;
+    for (int i = 0; i < 8; i++) {
+        state = state * mul + inc;
+        const uint32_t xs = (uint32_t)(((state >> 18) ^ state) >> 27);
+        const uint32_t rot = (uint32_t)(state >> 59);
+        key[i] = (xs >> rot) | (xs << ((32 - rot) & 31));
+    }
+}
+
+// f64::powi for a runtime exponent lowers to compiler-rt's __powidf2.
+double powi_rt(double a, int b) {
+    const bool recip = b < 0;
+    double r = 1.0;
+    for (;;) {
+        if (b & 1) r *= a;
+        b /= 2;
+        if (b == 0) break;
+        a *= a;
+    }
+    return recip ? 1.0 / r : r;
+}
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    ie_status alloc(size_t count) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = count;
+        if (count == 0) return IE_OK;
+        IE_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        return IE_OK;
+    }
+    ie_status upload(const std::vector<T>& h, cudaStream_t st) {
+        IE_TRY(alloc(h.size()));
+        if (!h.empty()) IE_CUDA(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        return IE_OK;
+    }
+};
+
+// One ingested problem (both triangles, reference row order).
+struct HostInst {
+    uint32_t n = 0;
+    int32_t H = 0;
+    uint32_t mode = kModeF64;
+    double offset = 0.0;
+    std::vector<uint32_t> rows;   // n + 1
+    std::vector<uint32_t> ents;   // integer mode packed entries
+    std::vector<int32_t> linp;
+    std::vector<uint32_t> cols;
+    std::vector<double> vals;
+    std::vector<double> lin;
+};
+
+ie_status ingest(const ie_problem* p, bool force_f64, HostInst& out) {
+    if (!p) return fail(IE_ERR_INVALID, "problem is NULL");
+    const uint64_t n = p->num_vars;
+    if (n >= (1ULL << 31)) return fail(IE_ERR_INVALID, "num_vars too large");
+    if (n > 0 && (!p->linear || !p->row_offsets))
+        return fail(IE_ERR_INVALID, "linear/row_offsets must be non-NULL");
+    const uint64_t nnz = n ? p->row_offsets[n] : 0;
+    if (n && p->row_offsets[0] != 0) return fail(IE_ERR_INVALID, "row_offsets[0] must be 0");
+    if (nnz >= (1ULL << 32)) return fail(IE_ERR_INVALID, "too many couplings");
+    if (nnz && (!p->col_indices || !p->values)) return fail(IE_ERR_INVALID, "col_indices/values must be non-NULL");
+    out.n = (uint32_t)n;
+    out.offset = p->energy_offset;
+    out.rows.resize(n + 1);
+    out.lin.assign(p->linear, p->linear + n);
+    out.cols.resize(nnz);
+    out.vals.assign(p->values, p->values + nnz);
+    for (uint64_t i = 0; i <= n; i++) {
+        if (i && p->row_offsets[i] < p->row_offsets[i - 1])
+            return fail(IE_ERR_INVALID, "row_offsets must be non-decreasing");
+        out.rows[i] = (uint32_t)p->row_offsets[i];
+    }
+    for (uint64_t k = 0; k < nnz; k++) {
+        if (p->col_indices[k] >= n) return fail(IE_ERR_INVALID, "column index out of range");
+        if (!std::isfinite(p->values[k])) return fail(IE_ERR_INVALID, "non-finite coupling");
+        out.cols[k] = (uint32_t)p->col_indices[k];
+    }
+    for (uint64_t i = 0; i < n; i++)
+        if (!std::isfinite(p->linear[i])) return fail(IE_ERR_INVALID, "non-finite linear term");
+
+    // Integer mode: integral values, |w| <= 127, |local field| <= 127 at every
+    // site, tracked energies within int32 and columns within 24 bits.
+    bool integral = !force_f64 && n < (1u << 24);
+    double ebound = 0.0;
+    int32_t H = 0;
+    std::vector<int32_t> linp(n);
+    for (uint64_t i = 0; integral && i < n; i++) {
+        const double l = p->linear[i];
+        if (l != std::trunc(l) || std::fabs(l) > 127.0) {
+            integral = false;
+            break;
+        }
+        double neg = 0.0, pos = 0.0;
+        for (uint64_t k = p->row_offsets[i]; k < p->row_offsets[i + 1]; k++) {
+            const double w = p->values[k];
+            if (w != std::trunc(w) || std::fabs(w) > 127.0) {
+                integral = false;
+                break;
+            }
+            if (w < 0) neg += w;
+            else pos += w;
+            if (p->col_indices[k] > i) ebound += std::fabs(w);
+        }
+        if (!integral) break;
+        const double hlo = l + neg, hhi = l + pos;
+        const double hv = std::max(std::fabs(hlo), std::fabs(hhi));
+        if (hv > (double)kMaxH) {
+            integral = false;
+            break;
+        }
+        H = std::max(H, (int32_t)hv);
+        linp[i] = (int32_t)hlo;
+        ebound += std::fabs(l);
+    }
+    if (integral && ebound >= 2147483647.0) integral = false;
+    if (integral) {
+        out.mode = kModeInt;
+        out.H = H;
+        out.linp = std::move(linp);
+        out.ents.resize(nnz);
+        for (uint64_t k = 0; k < nnz; k++) {
+            const double w = p->values[k];
+            const uint32_t aw = (uint32_t)std::fabs(w);
+            out.ents[k] = (uint32_t)p->col_indices[k] | (aw << 24) | (w < 0 ? 0x80000000u : 0u);
+        }
+    } else {
+        out.mode = kModeF64;
+        out.H = 0;
+    }
+    return IE_OK;
+}
+
+// Exchange thresholds for the integer mode (engine.rs:725-727): for the pair
+// (t, t+1) with db = 1/T_t - 1/T_{t+1}, a swap with exponent db*de < 0 is
+// accepted iff gen::<f64>() < exp(db*de), i.e. iff (draw >> 11) <
+// ceil(exp(db*de) * 2^53), which depends only on |de|. Built with the host
+// libm exp, the same function the reference calls.
+struct XTables {
+    std::vector<uint64_t> tab, off, dmax, dund;
+    std::vector<double> dbeta;
+};
+
+ie_status build_xtables(const double* temps, uint32_t nt, XTables& X) {
+    X = XTables();
+    const uint32_t np = nt > 1 ? nt - 1 : 0;
+    X.off.resize(std::max<uint32_t>(np, 1));
+    X.dmax.resize(std::max<uint32_t>(np, 1));
+    X.dund.resize(std::max<uint32_t>(np, 1));
+    X.dbeta.resize(std::max<uint32_t>(np, 1));
+    for (uint32_t t = 0; t < np; t++) {
+        const double b1 = 1.0 / temps[t], b2 = 1.0 / temps[t + 1];
+        const double db = b1 - b2;
+        X.dbeta[t] = db;
+        X.off[t] = X.tab.size();
+        const double adb = std::fabs(db);
+        if (!(adb > 0.0) || !std::isfinite(adb)) {
+            X.dmax[t] = 0;
+            X.dund[t] = 0;
+            continue;
+        }
+        uint64_t a = 1;
+        for (;; a++) {
+            const double ex = -(adb * (double)a);
+            const double T = std::ceil(std::ldexp(std::exp(ex), 53));
+            if (T <= 1.0) break;
+            X.tab.push_back((uint64_t)T);
+            if (X.tab.size() > (1u << 24))
+                return fail(IE_ERR_UNSUPPORTED, "temperature ladder too fine for the integer exchange tables");
+        }
+        X.dmax[t] = a - 1;
+        // largest |de| with exp(-adb*|de|) > 0 (monotone), by bisection
+        uint64_t lo = a - 1, hi = (uint64_t)std::min(1e18, std::ceil(800.0 / adb) + 2.0);
+        while (hi - lo > 1) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (std::exp(-(adb * (double)mid)) > 0.0) lo = mid;
+            else hi = mid;
+        }
+        X.dund[t] = lo;
+    }
+    return IE_OK;
+}
+
+int g_sm_count = -1;
+
+struct Engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t count = 0;
+    uint32_t nt = 1;
+    std::vector<InstDesc> desc;
+    std::vector<HostInst> insts;
+    std::vector<uint8_t> clampf;
+    std::vector<int8_t> clampv;
+    std::vector<uint32_t> keys;
+    size_t total_sites = 0, total_nnz = 0, total_words = 0, total_energy = 0;
+    int32_t maxH = 0;
+
+    DevBuf<InstDesc> d_desc;
+    DevBuf<uint32_t> d_rows, d_ents, d_cols, d_keys, d_quads, d_queue, d_draw_idx, d_unclamped;
+    DevBuf<int32_t> d_linp, d_Ei, d_deo, d_err;
+    DevBuf<double> d_vals, d_lin, d_Ef, d_temps, d_dbeta, d_scratch;
+    DevBuf<uint8_t> d_clampf;
+    DevBuf<int8_t> d_clampv;
+    DevBuf<uint64_t> d_spins, d_pos, d_att, d_acc, d_xtab, d_xoff, d_xdmax, d_xdund;
+
+    uint64_t steps_done = 0;
+    uint32_t nquads = 0;
+    double last_ms = 0.0;
+    uint64_t last_launches = 0;
+    uint32_t threads_per_block = 0, blocks_per_sm = 0;
+    std::vector<double> xtemps;  // ladder the exchange tables were built for
+    bool initialized = false;
+
+    ~Engine() {
+        if (device >= 0) cudaSetDevice(device);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    DevArrays arrays() const {
+        DevArrays A;
+        A.desc = d_desc.p;
+        A.rows = d_rows.p;
+        A.ents = d_ents.p;
+        A.linp = d_linp.p;
+        A.cols = d_cols.p;
+        A.vals = d_vals.p;
+        A.lin = d_lin.p;
+        A.clampf = d_clampf.p;
+        A.clampv = d_clampv.p;
+        A.keys = d_keys.p;
+        A.spins = d_spins.p;
+        A.Ei = d_Ei.p;
+        A.Ef = d_Ef.p;
+        A.pos = d_pos.p;
+        A.deo = d_deo.p;
+        A.att = d_att.p;
+        A.acc = d_acc.p;
+        A.err = d_err.p;
+        return A;
+    }
+
+    ie_status setup_device(int dev) {
+        device = dev;
+        int ndev = 0;
+        IE_CUDA(cudaGetDeviceCount(&ndev));
+        if (dev < 0 || dev >= ndev) return fail(IE_ERR_INVALID, "invalid CUDA device ordinal");
+        IE_CUDA(cudaSetDevice(dev));
+        IE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        IE_CUDA(cudaEventCreate(&ev0));
+        IE_CUDA(cudaEventCreate(&ev1));
+        if (g_sm_count < 0) IE_CUDA(cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev));
+        return IE_OK;
+    }
+
+    // Lays out `problems` (each with `cells` temperature cells) and uploads.
+    ie_status build(const ie_problem* problems, uint32_t n_problems, uint32_t cells, const uint64_t* seeds,
+                    bool force_f64) {
+        count = n_problems;
+        nt = cells;
+        insts.resize(count);
+        desc.resize(count);
+        keys.resize((size_t)count * 8);
+        for (uint32_t i = 0; i < count; i++) {
+            IE_TRY(ingest(&problems[i], force_f64, insts[i]));
+            chacha_key_from_u64(seeds[i], &keys[(size_t)8 * i]);
+        }
+        size_t site = 0, ent = 0, spin = 0, energy = 0, stat = 0;
+        for (uint32_t i = 0; i < count; i++) {
+            const HostInst& h = insts[i];
+            InstDesc& d = desc[i];
+            d.n = h.n;
+            d.H = h.H;
+            d.mode = h.mode;
+            d.nt = nt;
+            d.row = site + i;  // rows are n+1 per instance
+            d.ent = ent;
+            d.site = site;
+            d.spin = spin;
+            d.energy = energy;
+            d.stat = stat;
+            site += h.n;
+            ent += h.cols.size();
+            spin += (size_t)nt * h.n;
+            energy += (size_t)nt * kReplicas;
+            stat += nt > 1 ? nt - 1 : 1;
+            maxH = std::max(maxH, h.H);
+        }
+        total_sites = site;
+        total_nnz = ent;
+        total_words = spin;
+        total_energy = energy;
+        std::vector<uint32_t> rows(site + count), ents(ent), cols(ent);
+        std::vector<int32_t> linp(site, 0);
+        std::vector<double> vals(ent), lin(site);
+        for (uint32_t i = 0; i < count; i++) {
+            const HostInst& h = insts[i];
+            const InstDesc& d = desc[i];
+            std::copy(h.rows.begin(), h.rows.end(), rows.begin() + d.row);
+            std::copy(h.cols.begin(), h.cols.end(), cols.begin() + d.ent);
+            std::copy(h.vals.begin(), h.vals.end(), vals.begin() + d.ent);
+            std::copy(h.lin.begin(), h.lin.end(), lin.begin() + d.site);
+            if (h.mode == kModeInt) {
+                std::copy(h.ents.begin(), h.ents.end(), ents.begin() + d.ent);
+                std::copy(h.linp.begin(), h.linp.end(), linp.begin() + d.site);
+            }
+        }
+        clampf.assign(site, 0);
+        clampv.assign(site, 0);
+        IE_TRY(d_desc.upload(desc, stream));
+        IE_TRY(d_rows.upload(rows, stream));
+        IE_TRY(d_ents.upload(ents, stream));
+        IE_TRY(d_linp.upload(linp, stream));
+        IE_TRY(d_cols.upload(cols, stream));
+        IE_TRY(d_vals.upload(vals, stream));
+        IE_TRY(d_lin.upload(lin, stream));
+        IE_TRY(d_keys.upload(keys, stream));
+        IE_TRY(d_clampf.upload(clampf, stream));
+        IE_TRY(d_clampv.upload(clampv, stream));
+        IE_TRY(d_spins.alloc(std::max<size_t>(spin, 1)));
+        IE_CUDA(cudaMemsetAsync(d_spins.p, 0, std::max<size_t>(spin, 1) * sizeof(uint64_t), stream));
+        IE_TRY(d_Ei.alloc(std::max<size_t>(energy, 1)));
+        IE_TRY(d_Ef.alloc(std::max<size_t>(energy, 1)));
+        IE_CUDA(cudaMemsetAsync(d_Ei.p, 0, std::max<size_t>(energy, 1) * sizeof(int32_t), stream));
+        IE_CUDA(cudaMemsetAsync(d_Ef.p, 0, std::max<size_t>(energy, 1) * sizeof(double), stream));
+        std::vector<uint64_t> zeros64(count, 0);
+        std::vector<int32_t> zeros32(count, 0);
+        IE_TRY(d_pos.upload(zeros64, stream));
+        IE_TRY(d_deo.upload(zeros32, stream));
+        std::vector<uint64_t> zstat(std::max<size_t>(stat, 1), 0);
+        IE_TRY(d_att.upload(zstat, stream));
+        IE_TRY(d_acc.upload(zstat, stream));
+        IE_TRY(d_err.upload(std::vector<int32_t>(1, 0), stream));
+        IE_TRY(d_queue.alloc(1));
+        IE_TRY(d_scratch.alloc(std::max<size_t>((size_t)nt * kReplicas, 1)));
+        IE_TRY(upload_draw_idx());
+        IE_CUDA(cudaStreamSynchronize(stream));
+        return IE_OK;
+    }
+
+    ie_status upload_draw_idx() {
+        std::vector<uint32_t> idx(std::max<size_t>(total_sites, 1), 0), unc(count, 0);
+        for (uint32_t i = 0; i < count; i++) {
+            uint32_t c = 0;
+            for (uint32_t v = 0; v < desc[i].n; v++) {
+                idx[desc[i].site + v] = c;
+                if (!clampf[desc[i].site + v]) c++;
+            }
+            unc[i] = c;
+        }
+        IE_TRY(d_draw_idx.upload(idx, stream));
+        IE_TRY(d_unclamped.upload(unc, stream));
+        return IE_OK;
+    }
+
+    ie_status set_clamps(uint32_t inst, const uint8_t* f, const int8_t* v) {
+        const InstDesc& d = desc[inst];
+        for (uint32_t i = 0; i < d.n; i++) {
+            clampf[d.site + i] = f ? (f[i] ? 1 : 0) : 0;
+            clampv[d.site + i] = (f && f[i] && v) ? (v[i] == 1 ? 1 : 0) : 0;
+        }
+        IE_CUDA(cudaMemcpyAsync(d_clampf.p, clampf.data(), clampf.size(), cudaMemcpyHostToDevice, stream));
+        IE_CUDA(cudaMemcpyAsync(d_clampv.p, clampv.data(), clampv.size(), cudaMemcpyHostToDevice, stream));
+        IE_TRY(upload_draw_idx());
+        IE_CUDA(cudaStreamSynchronize(stream));
+        return IE_OK;
+    }
+
+    ie_status init_random() {
+        const DevArrays A = arrays();
+        IE_CUDA(launch_init(A, 0, count, d_draw_idx.p, d_unclamped.p, stream));
+        IE_CUDA(launch_energy(A, 0, count, stream));
+        IE_CUDA(cudaStreamSynchronize(stream));
+        initialized = true;
+        return IE_OK;
+    }
+
+    size_t batch_smem(int block) const { return (size_t)(block / 8) * (2 * maxH + 1) * sizeof(uint64_t); }
+
+    // Orders instances longest-first into quads of similar size and degree
+    // (same mode) so the four groups of a warp stay in step.
+    void build_quads() {
+        std::vector<uint32_t> order(count);
+        std::iota(order.begin(), order.end(), 0u);
+        auto degree = [&](uint32_t i) {
+            return insts[i].n ? (uint32_t)((insts[i].cols.size() + insts[i].n / 2) / insts[i].n) : 0u;
+        };
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+            if (desc[a].mode != desc[b].mode) return desc[a].mode > desc[b].mode;
+            if (degree(a) != degree(b)) return degree(a) > degree(b);
+            return desc[a].n > desc[b].n;
+        });
+        std::vector<std::vector<uint32_t>> quads;
+        for (size_t i = 0; i < order.size();) {
+            std::vector<uint32_t> q;
+            const uint32_t m = desc[order[i]].mode, dg = degree(order[i]);
+            while (q.size() < 4 && i < order.size() && desc[order[i]].mode == m && degree(order[i]) == dg)
+                q.push_back(order[i++]);
+            quads.push_back(q);
+        }
+        auto work = [&](const std::vector<uint32_t>& q) {
+            double w = 0;
+            for (uint32_t i : q) {
+                const double c = (double)insts[i].n * ((double)insts[i].cols.size() / std::max(1u, insts[i].n) + 8.0) *
+                                 (desc[i].mode == kModeF64 ? 3.0 : 1.0);
+                w = std::max(w, c);
+            }
+            return w;
+        };
+        std::stable_sort(quads.begin(), quads.end(),
+                         [&](const std::vector<uint32_t>& a, const std::vector<uint32_t>& b) { return work(a) > work(b); });
+        std::vector<uint32_t> flat;
+        for (auto& q : quads)
+            for (int k = 0; k < 4; k++) flat.push_back(k < (int)q.size() ? q[k] : 0xffffffffu);
+        nquads = (uint32_t)quads.size();
+        d_quads.upload(flat, stream);
+    }
+
+    // Runs temps[steps] on every single-cell instance in one persistent launch.
+    ie_status run_batch(const double* temps, uint64_t steps) {
+        if (nt != 1) return fail(IE_ERR_INVALID, "batched runs need single-cell instances");
+        if (!initialized) return fail(IE_ERR_INVALID, "call init_random before running");
+        if (steps == 0) return IE_OK;
+        if (steps > 0xffffffffULL) return fail(IE_ERR_INVALID, "too many steps in one call");
+        if (!nquads) build_quads();
+        std::vector<double> t(temps, temps + steps);
+        for (double x : t)
+            if (!(x > 0.0) || !std::isfinite(x)) return fail(IE_ERR_INVALID, "temperatures must be positive");
+        IE_TRY(d_temps.upload(t, stream));
+        int block = threads_per_block ? (int)threads_per_block : 128;
+        const size_t smem = batch_smem(block);
+        IE_CUDA(set_smem_limits(std::max<size_t>(smem, 48 * 1024), pt_smem_cap()));
+        int occ = batch_occupancy(block, smem);
+        if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
+        if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
+        const int warps_per_block = block / 32;
+        const int want = (int)((nquads + warps_per_block - 1) / warps_per_block);
+        const int grid = std::max(1, std::min(want, occ * g_sm_count));
+        RunArgs R{};
+        R.temps = d_temps.p;
+        R.temps_per_step = 1;
+        R.steps = (uint32_t)steps;
+        R.step_base = steps_done;
+        R.exchange_interval = 1;
+        R.quads = d_quads.p;
+        R.nquads = nquads;
+        R.queue = d_queue.p;
+        IE_CUDA(cudaMemsetAsync(d_queue.p, 0, sizeof(uint32_t), stream));
+        IE_CUDA(cudaEventRecord(ev0, stream));
+        IE_CUDA(launch_batch_sa(arrays(), R, grid, block, 2 * maxH + 1, smem, stream));
+        IE_CUDA(cudaEventRecord(ev1, stream));
+        IE_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0;
+        IE_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        last_ms = ms;
+        last_launches = 1;
+        steps_done += steps;
+        return IE_OK;
+    }
+
+    // The plain method: one launch per instance, in sequence.
+    ie_status run_plain(const double* temps, uint64_t steps, uint32_t first, uint32_t n_inst) {
+        if (nt != 1) return fail(IE_ERR_INVALID, "plain runs need single-cell instances");
+        if (!initialized) return fail(IE_ERR_INVALID, "call init_random before running");
+        if ((uint64_t)first + n_inst > count) return fail(IE_ERR_INVALID, "instance range out of bounds");
+        if (steps == 0 || n_inst == 0) return IE_OK;
+        std::vector<double> t(temps, temps + steps);
+        IE_TRY(d_temps.upload(t, stream));
+        std::vector<uint32_t> quads((size_t)4 * n_inst, 0xffffffffu);
+        for (uint32_t i = 0; i < n_inst; i++) quads[4 * (size_t)i] = first + i;
+        DevBuf<uint32_t> dq;
+        IE_TRY(dq.upload(quads, stream));
+        const size_t smem = batch_smem(32);
+        IE_CUDA(set_smem_limits(std::max<size_t>(smem, 48 * 1024), pt_smem_cap()));
+        RunArgs R{};
+        R.temps = d_temps.p;
+        R.temps_per_step = 1;
+        R.steps = (uint32_t)steps;
+        R.step_base = steps_done;
+        R.exchange_interval = 1;
+        R.nquads = 1;
+        R.queue = d_queue.p;
+        IE_CUDA(cudaEventRecord(ev0, stream));
+        for (uint32_t i = 0; i < n_inst; i++) {
+            R.quads = dq.p + 4 * (size_t)i;
+            IE_CUDA(cudaMemsetAsync(d_queue.p, 0, sizeof(uint32_t), stream));
+            IE_CUDA(launch_batch_sa(arrays(), R, 1, 32, 2 * maxH + 1, smem, stream));
+        }
+        IE_CUDA(cudaEventRecord(ev1, stream));
+        IE_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0;
+        IE_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        last_ms = ms;
+        last_launches = n_inst;
+        return IE_OK;
+    }
+
+    size_t pt_smem(uint32_t cells, int32_t H, uint32_t mode) const {
+        const size_t tab = mode == kModeInt ? (size_t)cells * (2 * H + 1) : 0;
+        return (tab + (size_t)cells * kReplicas + cells + 2) * sizeof(uint64_t);
+    }
+    size_t pt_smem_cap() const {
+        size_t m = 48 * 1024;
+        for (uint32_t i = 0; i < count; i++) m = std::max(m, pt_smem(nt, desc[i].H, desc[i].mode));
+        return std::min<size_t>(m, 227 * 1024);
+    }
+
+    // engine::step n_steps times on instance 0 (all nt cells) with a constant
+    // ladder (temps_per_step = 0) or a per-step ladder.
+    ie_status run_pt(const double* temps, uint64_t steps, bool per_step, uint32_t exchange_interval) {
+        if (!initialized) return fail(IE_ERR_INVALID, "call init_random or set_spins before stepping");
+        if (steps == 0) return IE_OK;
+        const uint32_t rows = per_step ? (uint32_t)steps : 1u;
+        std::vector<double> t(temps, temps + (size_t)rows * nt);
+        for (double x : t)
+            if (!(x > 0.0) || !std::isfinite(x)) return fail(IE_ERR_INVALID, "temperatures must be positive");
+        const InstDesc& d = desc[0];
+        if (per_step && nt > 1 && d.mode == kModeInt) {
+            // exchange tables are per ladder: one launch per step
+            for (uint64_t s = 0; s < steps; s++) IE_TRY(run_pt(temps + s * nt, 1, false, exchange_interval));
+            return IE_OK;
+        }
+        if (nt > 1 && d.mode == kModeInt && (xtemps.size() != nt || !std::equal(xtemps.begin(), xtemps.end(), t.begin()))) {
+            XTables X;
+            IE_TRY(build_xtables(t.data(), nt, X));
+            IE_TRY(d_xtab.upload(X.tab.empty() ? std::vector<uint64_t>(1, 0) : X.tab, stream));
+            IE_TRY(d_xoff.upload(X.off, stream));
+            IE_TRY(d_xdmax.upload(X.dmax, stream));
+            IE_TRY(d_xdund.upload(X.dund, stream));
+            IE_TRY(d_dbeta.upload(X.dbeta, stream));
+            xtemps.assign(t.begin(), t.begin() + nt);
+        } else if (nt > 1 && d.mode == kModeF64) {
+            std::vector<double> db(nt - 1);
+            for (uint32_t k = 0; k + 1 < nt; k++) db[k] = 1.0 / t[k] - 1.0 / t[k + 1];
+            if (per_step) {
+                // f64 exchange reads dbeta of the current ladder: one launch per step
+                for (uint64_t s = 0; s < steps; s++) IE_TRY(run_pt(temps + s * nt, 1, false, exchange_interval));
+                return IE_OK;
+            }
+            IE_TRY(d_dbeta.upload(db, stream));
+        }
+        IE_TRY(d_temps.upload(t, stream));
+        const int block = (int)(((nt * 8) + 31) / 32 * 32);
+        if (block > 1024) return fail(IE_ERR_UNSUPPORTED, "at most 128 temperatures per instance");
+        const size_t smem = pt_smem(nt, d.H, d.mode);
+        if (smem > 227 * 1024) return fail(IE_ERR_UNSUPPORTED, "temperature ladder too large for shared memory");
+        IE_CUDA(set_smem_limits(48 * 1024, std::max<size_t>(smem, 48 * 1024)));
+        RunArgs R{};
+        R.temps = d_temps.p;
+        R.temps_per_step = per_step ? 1 : 0;
+        R.step_base = steps_done;
+        R.exchange_interval = exchange_interval ? exchange_interval : 1;
+        R.xtab = d_xtab.p;
+        R.xoff = d_xoff.p;
+        R.xdmax = d_xdmax.p;
+        R.xdund = d_xdund.p;
+        R.dbeta = d_dbeta.p;
+        IE_CUDA(cudaEventRecord(ev0, stream));
+        uint64_t launches = 0;
+        // f64 resync points and very long runs split into launches of at most
+        // 2^30 steps; each launch continues the same trajectory.
+        uint64_t done = 0;
+        while (done < steps) {
+            const uint64_t chunk = std::min<uint64_t>(steps - done, 1ULL << 30);
+            R.steps = (uint32_t)chunk;
+            R.step_base = steps_done + done;
+            R.temps = d_temps.p + (per_step ? done * nt : 0);
+            IE_CUDA(launch_pt(arrays(), R, 0, 1, d.mode, block, d.mode == kModeInt ? 2 * d.H + 1 : 0, smem, stream));
+            launches++;
+            done += chunk;
+        }
+        IE_CUDA(cudaEventRecord(ev1, stream));
+        IE_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0;
+        IE_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        last_ms = ms;
+        last_launches = launches;
+        steps_done += steps;
+        return IE_OK;
+    }
+
+    ie_status read_words(uint32_t inst0, uint32_t ninst, uint64_t* out) {
+        const size_t w0 = desc[inst0].spin;
+        const size_t w1 = (inst0 + ninst < count) ? desc[inst0 + ninst].spin : total_words;
+        std::vector<uint64_t> h(w1 - w0);
+        if (!h.empty())
+            IE_CUDA(cudaMemcpyAsync(h.data(), d_spins.p + w0, h.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+        IE_CUDA(cudaStreamSynchronize(stream));
+        for (size_t i = 0; i < h.size(); i++) out[i] = transpose8x8(h[i]);
+        return IE_OK;
+    }
+
+    ie_status write_words(uint32_t inst, const uint64_t* in) {
+        const InstDesc& d = desc[inst];
+        std::vector<uint64_t> h((size_t)d.nt * d.n);
+        for (size_t i = 0; i < h.size(); i++) h[i] = transpose8x8(in[i]);
+        if (!h.empty())
+            IE_CUDA(cudaMemcpyAsync(d_spins.p + d.spin, h.data(), h.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
+        IE_CUDA(launch_energy(arrays(), inst, 1, stream));
+        IE_CUDA(cudaStreamSynchronize(stream));
+        initialized = true;
+        return IE_OK;
+    }
+
+    ie_status read_energies(double* out) {
+        std::vector<int32_t> ei(total_energy);
+        std::vector<double> ef(total_energy);
+        IE_CUDA(cudaMemcpyAsync(ei.data(), d_Ei.p, total_energy * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+        IE_CUDA(cudaMemcpyAsync(ef.data(), d_Ef.p, total_energy * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        IE_CUDA(cudaStreamSynchronize(stream));
+        for (uint32_t i = 0; i < count; i++) {
+            const InstDesc& d = desc[i];
+            for (size_t k = 0; k < (size_t)d.nt * kReplicas; k++)
+                out[d.energy + k] = d.mode == kModeInt ? (double)ei[d.energy + k] : ef[d.energy + k];
+        }
+        return IE_OK;
+    }
+
+    ie_status recompute_energies(double* out) {
+        DevBuf<double> tmp;
+        IE_TRY(tmp.alloc(std::max<size_t>(total_energy, 1)));
+        IE_CUDA(launch_energy_check(arrays(), 0, count, tmp.p, stream));
+        IE_CUDA(cudaMemcpyAsync(out, tmp.p, total_energy * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        IE_CUDA(cudaStreamSynchronize(stream));
+        return IE_OK;
+    }
+
+    ie_status check_err() {
+        int32_t e = 0;
+        IE_CUDA(cudaMemcpy(&e, d_err.p, sizeof(e), cudaMemcpyDeviceToHost));
+        if (e) return fail(IE_ERR_DEVICE, "device-side check failed (code " + std::to_string(e) + ")");
+        return IE_OK;
+    }
+};
+
+bool cfg_valid(const ie_config* c, std::string& why) {
+    if (!c) {
+        why = "config is NULL";
+        return false;
+    }
+    if (c->num_pops != 0 && c->num_pops != 1) {
+        why = "num_pops must be 1 (population annealing is not on this path)";
+        return false;
+    }
+    if (c->num_slices != 0 && c->num_slices != 1) {
+        why = "num_slices must be 1 (the Trotter branch is not on this path)";
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+struct ie_handle {
+    Engine eng;
+    ie_config cfg{};
+    double offset = 0.0;
+    DevBuf<double> d_inc_e;
+    DevBuf<uint64_t> d_inc_state;
+    bool have_incumbent = false;
+};
+
+struct ie_batch {
+    Engine eng;
+};
+
+extern "C" {
+
+const char* ie_last_error(void) { return g_err.c_str(); }
+int ie_abi_version(void) { return 1; }
+
+ie_status ie_geometric_temps(double temp_max, double temp_min, uint32_t num_temps, double* out) {
+    if (!out || num_temps == 0) return fail(IE_ERR_INVALID, "num_temps must be >= 1");
+    const double f = num_temps > 1 ? std::pow(temp_min / temp_max, 1.0 / (double)(num_temps - 1)) : 1.0;
+    for (uint32_t i = 0; i < num_temps; i++) out[i] = temp_max * powi_rt(f, (int)i);
+    return IE_OK;
+}
+
+ie_status ie_suggested_temp_range(const ie_problem* p, double* tmax, double* tmin) {
+    if (!p || !tmax || !tmin) return fail(IE_ERR_INVALID, "NULL argument");
+    double max_local = 0.0, min_nz = std::numeric_limits<double>::infinity();
+    for (uint64_t i = 0; i < p->num_vars; i++) {
+        double local = std::fabs(p->linear[i]);
+        if (p->linear[i] != 0.0) min_nz = std::min(min_nz, std::fabs(p->linear[i]));
+        for (uint64_t k = p->row_offsets[i]; k < p->row_offsets[i + 1]; k++) {
+            const double w = p->values[k];
+            local += std::fabs(w);
+            if (w != 0.0) min_nz = std::min(min_nz, std::fabs(w));
+        }
+        max_local = std::max(max_local, local);
+    }
+    if (max_local == 0.0 || !std::isfinite(min_nz)) {
+        *tmax = 1.0;
+        *tmin = 0.1;
+        return IE_OK;
+    }
+    const double t_max = max_local / 0.693147180559945309417232121458176568;  // LN_2
+    const double t_min = std::min(min_nz / std::log(100.0), t_max * 0.5);
+    *tmax = t_max;
+    *tmin = t_min;
+    return IE_OK;
+}
+
+ie_status ie_create(const ie_problem* problem, const ie_config* config, ie_handle** out) {
+    if (!out) return fail(IE_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    std::string why;
+    if (!cfg_valid(config, why)) return fail(config ? IE_ERR_UNSUPPORTED : IE_ERR_INVALID, why);
+    std::unique_ptr<ie_handle> h(new ie_handle());
+    h->cfg = *config;
+    if (h->cfg.num_temps == 0) h->cfg.num_temps = 10;
+    if (h->cfg.exchange_interval == 0) h->cfg.exchange_interval = 1;
+    if (h->cfg.num_temps > 128) return fail(IE_ERR_UNSUPPORTED, "at most 128 temperatures");
+    IE_TRY(h->eng.setup_device(config->device));
+    IE_TRY(h->eng.build(problem, 1, h->cfg.num_temps, &config->seed, config->force_f64 != 0));
+    h->offset = problem->energy_offset;
+    IE_TRY(h->d_inc_e.upload(std::vector<double>(1, std::numeric_limits<double>::infinity()), h->eng.stream));
+    IE_TRY(h->d_inc_state.alloc(std::max<uint64_t>((problem->num_vars + 63) / 64, 1)));
+    IE_CUDA(cudaMemsetAsync(h->d_inc_state.p, 0, h->d_inc_state.n * sizeof(uint64_t), h->eng.stream));
+    IE_CUDA(cudaStreamSynchronize(h->eng.stream));
+    *out = h.release();
+    return IE_OK;
+}
+
+ie_status ie_destroy(ie_handle* h) {
+    delete h;
+    return IE_OK;
+}
+
+ie_status ie_set_clamps(ie_handle* h, const uint8_t* is_clamped, const int8_t* clamp_val) {
+    if (!h) return fail(IE_ERR_INVALID, "handle is NULL");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    return h->eng.set_clamps(0, is_clamped, clamp_val);
+}
+
+ie_status ie_init_random(ie_handle* h) {
+    if (!h) return fail(IE_ERR_INVALID, "handle is NULL");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    return h->eng.init_random();
+}
+
+ie_status ie_set_spins(ie_handle* h, const uint64_t* words) {
+    if (!h || !words) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    return h->eng.write_words(0, words);
+}
+
+ie_status ie_step(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t n_steps) {
+    if (!h || !temps) return fail(IE_ERR_INVALID, "NULL argument");
+    if (n_temps != h->eng.nt) return fail(IE_ERR_INVALID, "n_temps must equal the handle's num_temps");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    return h->eng.run_pt(temps, n_steps, false, h->cfg.exchange_interval);
+}
+
+ie_status ie_run_schedule(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t n_steps) {
+    if (!h || !temps) return fail(IE_ERR_INVALID, "NULL argument");
+    if (n_temps != h->eng.nt) return fail(IE_ERR_INVALID, "n_temps must equal the handle's num_temps");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    return h->eng.run_pt(temps, n_steps, true, h->cfg.exchange_interval);
+}
+
+ie_status ie_run_pt(ie_handle* h) {
+    if (!h) return fail(IE_ERR_INVALID, "handle is NULL");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    std::vector<double> temps(h->eng.nt);
+    IE_TRY(ie_geometric_temps(h->cfg.temp_max, h->cfg.temp_min, h->eng.nt, temps.data()));
+    const uint32_t n_words = (uint32_t)h->d_inc_state.n;
+    for (uint64_t ex = 0; ex < h->cfg.total_exchanges; ex++) {
+        IE_TRY(h->eng.run_pt(temps.data(), h->cfg.sweeps_per_exchange, false, h->cfg.exchange_interval));
+        IE_CUDA(launch_incumbent(h->eng.arrays(), 0, h->offset, h->d_inc_e.p, h->d_inc_state.p, n_words,
+                                 h->eng.stream));
+    }
+    IE_CUDA(cudaStreamSynchronize(h->eng.stream));
+    h->have_incumbent = true;
+    return IE_OK;
+}
+
+ie_status ie_read_spins(ie_handle* h, uint64_t* words) {
+    if (!h || !words) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    return h->eng.read_words(0, 1, words);
+}
+
+ie_status ie_read_energies(ie_handle* h, double* energies) {
+    if (!h || !energies) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    return h->eng.read_energies(energies);
+}
+
+ie_status ie_read_swap_stats(ie_handle* h, uint64_t* attempts, uint64_t* accepts) {
+    if (!h || !attempts || !accepts) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    const uint32_t np = h->eng.nt > 1 ? h->eng.nt - 1 : 0;
+    if (np) {
+        IE_CUDA(cudaMemcpy(attempts, h->eng.d_att.p, np * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        IE_CUDA(cudaMemcpy(accepts, h->eng.d_acc.p, np * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    }
+    return IE_OK;
+}
+
+ie_status ie_read_rng_state(ie_handle* h, uint64_t* draws, int32_t* deo) {
+    if (!h || !draws || !deo) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    IE_CUDA(cudaMemcpy(draws, h->eng.d_pos.p, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    IE_CUDA(cudaMemcpy(deo, h->eng.d_deo.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return IE_OK;
+}
+
+ie_status ie_read_incumbent(ie_handle* h, double* energy, int8_t* state) {
+    if (!h || !energy || !state) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    const uint64_t n = h->eng.desc[0].n;
+    std::vector<uint64_t> w(h->d_inc_state.n);
+    IE_CUDA(cudaMemcpy(energy, h->d_inc_e.p, sizeof(double), cudaMemcpyDeviceToHost));
+    IE_CUDA(cudaMemcpy(w.data(), h->d_inc_state.p, w.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < n; i++) state[i] = (int8_t)((w[i / 64] >> (i % 64)) & 1);
+    return IE_OK;
+}
+
+ie_status ie_read_best(ie_handle* h, double* energy, int8_t* state) {
+    if (!h || !energy || !state) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    Engine& E = h->eng;
+    const uint32_t nt = E.nt;
+    const uint64_t n = E.desc[0].n;
+    DevBuf<double> es;
+    IE_TRY(es.alloc((size_t)nt * kReplicas));
+    IE_CUDA(launch_model_energy(E.arrays(), 0, nt, h->offset, es.p, E.stream));
+    std::vector<double> he((size_t)nt * kReplicas);
+    IE_CUDA(cudaMemcpyAsync(he.data(), es.p, he.size() * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    IE_CUDA(cudaStreamSynchronize(E.stream));
+    double best = std::numeric_limits<double>::infinity();
+    size_t arg = 0;
+    bool found = false;
+    for (size_t i = 0; i < he.size(); i++)
+        if (he[i] < best) {
+            best = he[i];
+            arg = i;
+            found = true;
+        }
+    std::vector<uint64_t> words((size_t)nt * n);
+    IE_TRY(E.read_words(0, 1, words.data()));
+    for (uint64_t v = 0; v < n; v++)
+        state[v] = found ? (int8_t)((words[(arg / kReplicas) * n + v] >> (arg % kReplicas)) & 1) : 0;
+    *energy = best;
+    if (h->have_incumbent) {
+        double ie_ = 0;
+        std::vector<int8_t> inc(n);
+        IE_TRY(ie_read_incumbent(h, &ie_, inc.data()));
+        if (ie_ < best) {
+            *energy = ie_;
+            std::copy(inc.begin(), inc.end(), state);
+        }
+    }
+    return IE_OK;
+}
+
+// ---- batch ----
+
+ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint64_t* seeds,
+                          const ie_batch_config* config, ie_batch** out) {
+    if (!out || !problems || !seeds) return fail(IE_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    if (count == 0) return fail(IE_ERR_INVALID, "count must be >= 1");
+    std::unique_ptr<ie_batch> b(new ie_batch());
+    ie_batch_config cfg{};
+    if (config) cfg = *config;
+    IE_TRY(b->eng.setup_device(cfg.device));
+    b->eng.threads_per_block = cfg.threads_per_block;
+    b->eng.blocks_per_sm = cfg.blocks_per_sm;
+    if (cfg.threads_per_block && (cfg.threads_per_block % 32 || cfg.threads_per_block > 256))
+        return fail(IE_ERR_INVALID, "threads_per_block must be a multiple of 32, at most 256");
+    IE_TRY(b->eng.build(problems, count, 1, seeds, cfg.force_f64 != 0));
+    *out = b.release();
+    return IE_OK;
+}
+
+ie_status ie_batch_destroy(ie_batch* b) {
+    delete b;
+    return IE_OK;
+}
+
+ie_status ie_batch_init_random(ie_batch* b) {
+    if (!b) return fail(IE_ERR_INVALID, "batch is NULL");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    return b->eng.init_random();
+}
+
+ie_status ie_batch_run_schedule(ie_batch* b, const double* temps, uint64_t n_steps) {
+    if (!b || !temps) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    IE_TRY(b->eng.run_batch(temps, n_steps));
+    return b->eng.check_err();
+}
+
+ie_status ie_batch_run_schedule_plain(ie_batch* b, const double* temps, uint64_t n_steps, uint32_t first,
+                                      uint32_t count) {
+    if (!b || !temps) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    return b->eng.run_plain(temps, n_steps, first, count);
+}
+
+ie_status ie_batch_read_spins(ie_batch* b, uint64_t* words) {
+    if (!b || !words) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    return b->eng.read_words(0, b->eng.count, words);
+}
+
+ie_status ie_batch_read_energies(ie_batch* b, double* energies) {
+    if (!b || !energies) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    return b->eng.read_energies(energies);
+}
+
+ie_status ie_batch_read_draws(ie_batch* b, uint64_t* draws) {
+    if (!b || !draws) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    IE_CUDA(cudaMemcpy(draws, b->eng.d_pos.p, b->eng.count * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    return IE_OK;
+}
+
+ie_status ie_batch_recompute_energies(ie_batch* b, double* energies) {
+    if (!b || !energies) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    return b->eng.recompute_energies(energies);
+}
+
+ie_status ie_batch_last_run_ms(ie_batch* b, double* ms) {
+    if (!b || !ms) return fail(IE_ERR_INVALID, "NULL argument");
+    *ms = b->eng.last_ms;
+    return IE_OK;
+}
+
+ie_status ie_batch_last_launches(ie_batch* b, uint64_t* launches) {
+    if (!b || !launches) return fail(IE_ERR_INVALID, "NULL argument");
+    *launches = b->eng.last_launches;
+    return IE_OK;
+}
+
+}  // extern "C"

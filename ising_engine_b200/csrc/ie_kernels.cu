@@ -1,0 +1,633 @@
+// CUDA kernels of the B200 Metropolis / PT engine (sm_100a).
+//
+// Work decomposition. The reference sweeps each cell (temperature) in site
+// order v = 0..n-1 and draws the 64 uniforms of site v from an 8-lane
+// Xoshiro256++ generator: lane l produces the uniforms of replicas
+// l, l+8, ..., l+56 (engine.rs:145-151). Replicas are independent Markov
+// chains, so the natural unit of parallel work is (cell, lane): one thread
+// runs one lane's generator and owns exactly the 8 replicas it drives. The 8
+// threads of a cell never communicate during a sweep. Spin words are stored
+// lane-major: byte l of word [cell][v] holds replicas l+8k at bit k, so a
+// thread reads and writes only its own byte and no two threads ever write the
+// same byte.
+//
+// Integer mode (bit-exact): the local field of the thread's 8 replicas is
+// accumulated SWAR-style, one byte per replica, from non-negative weight
+// magnitudes (negative couplings contribute |w| * (1 - x_j) and are folded
+// into a per-site constant). The Metropolis decision is one 64-bit compare of
+// the raw Xoshiro output against a per-temperature threshold table indexed by
+// dE (metropolis_threshold), which reproduces u < fast_exp(-dE*beta) exactly.
+//
+// f64 mode: the reference's f64 arithmetic in the reference's order
+// (engine.rs:218-271, 663-670) with every operation explicitly rounded.
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "ie_device.cuh"
+#include "ie_kernels.cuh"
+
+namespace ie {
+
+// ---------------------------------------------------------------------------
+// One cell sweep by one (cell, lane) thread, integer mode.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sweep_int(const DevArrays& A, const InstDesc& d, uint64_t* words,
+                                          int lane, const uint64_t* __restrict__ tab,
+                                          uint64_t cell_seed, int32_t (&E)[8]) {
+    Xoshiro x;
+    x.seed_lane(cell_seed, lane);
+    uint8_t* sp = reinterpret_cast<uint8_t*>(words) + lane;
+    const uint32_t* __restrict__ rows = A.rows + d.row;
+    const uint32_t* __restrict__ ents = A.ents + d.ent;
+    const int32_t* __restrict__ linp = A.linp + d.site;
+    const uint8_t* __restrict__ clampf = A.clampf + d.site;
+    const int H = d.H;
+    uint32_t beg = __ldg(rows);
+    for (uint32_t v = 0; v < d.n; v++) {
+        const uint32_t end = __ldg(rows + v + 1);
+        if (__ldg(clampf + v)) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) x.advance();
+            beg = end;
+            continue;
+        }
+        uint64_t res[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) res[k] = x.next();
+        uint32_t aL = 0, aH = 0;
+        for (uint32_t e = beg; e < end; e++) {
+            const uint32_t en = __ldg(ents + e);
+            const uint32_t b = sp[8u * (en & 0xFFFFFFu)];
+            const uint32_t w = (en >> 24) & 0x7Fu;
+            const uint32_t nm = (0u - (en >> 31)) & 0x01010101u;
+            aL += w * (spread4(b) ^ nm);
+            aH += w * (spread4(b >> 4) ^ nm);
+        }
+        beg = end;
+        const uint32_t xb = sp[8u * v];
+        const int lp = __ldg(linp + v);
+        const uint32_t cA = (uint32_t)(H + lp) * 0x01010101u;
+        const uint32_t cB = (uint32_t)(H - lp) * 0x01010101u;
+        const uint32_t xL = spread4(xb) * 0xFFu;
+        const uint32_t xH = spread4(xb >> 4) * 0xFFu;
+        // byte k of iL/iH = dE_k + H for replica lane + 8k
+        const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
+        const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
+        uint32_t flips = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
+            if (res[k] <= tab[idx]) {
+                flips |= 1u << k;
+                E[k] += (int32_t)idx - H;
+            }
+        }
+        sp[8u * v] = (uint8_t)(xb ^ flips);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One cell sweep by one (cell, lane) thread, f64 mode (engine.rs:218-271 and
+// 663-670 in order; adding w * 0.0 is skipped, which changes no value).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sweep_f64(const DevArrays& A, const InstDesc& d, uint64_t* words,
+                                          int lane, double beta, uint64_t cell_seed,
+                                          double (&E)[8]) {
+    Xoshiro x;
+    x.seed_lane(cell_seed, lane);
+    uint8_t* sp = reinterpret_cast<uint8_t*>(words) + lane;
+    const uint32_t* __restrict__ rows = A.rows + d.row;
+    const uint32_t* __restrict__ cols = A.cols + d.ent;
+    const double* __restrict__ vals = A.vals + d.ent;
+    const double* __restrict__ lin = A.lin + d.site;
+    const uint8_t* __restrict__ clampf = A.clampf + d.site;
+    uint32_t beg = __ldg(rows);
+    for (uint32_t v = 0; v < d.n; v++) {
+        const uint32_t end = __ldg(rows + v + 1);
+        if (__ldg(clampf + v)) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) x.advance();
+            beg = end;
+            continue;
+        }
+        uint64_t res[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) res[k] = x.next();
+        const uint32_t xb = sp[8u * v];
+        const double wl = __ldg(lin + v);
+        double dl[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) dl[k] = ((xb >> k) & 1u) ? -wl : wl;
+        for (uint32_t e = beg; e < end; e++) {
+            const uint32_t j = __ldg(cols + e);
+            const double w = __ldg(vals + e);
+            const uint32_t bj = sp[8u * j];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                if ((bj >> k) & 1u) dl[k] = __dadd_rn(dl[k], ((xb >> k) & 1u) ? -w : w);
+            }
+        }
+        beg = end;
+        uint32_t flips = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const double ev = fast_exp_rn(__dmul_rn(-dl[k], beta));
+            const double u = __dmul_rn((double)(res[k] >> 12), 2.220446049250313e-16);  // 2^-52
+            if (dl[k] <= 0.0 || u < ev) {
+                flips |= 1u << k;
+                E[k] = __dadd_rn(E[k], dl[k]);
+            }
+        }
+        sp[8u * v] = (uint8_t)(xb ^ flips);
+    }
+}
+
+// calculate_replica_energies_local (engine.rs:333-368) for the thread's 8
+// replicas, f64 in reference order (site order, CSR order, v < j edges).
+__device__ void energies_f64(const DevArrays& A, const InstDesc& d, const uint64_t* words, int lane,
+                             double (&E)[8]) {
+    const uint8_t* sp = reinterpret_cast<const uint8_t*>(words) + lane;
+    const uint32_t* rows = A.rows + d.row;
+    const uint32_t* cols = A.cols + d.ent;
+    const double* vals = A.vals + d.ent;
+    const double* lin = A.lin + d.site;
+#pragma unroll
+    for (int k = 0; k < 8; k++) E[k] = 0.0;
+    for (uint32_t v = 0; v < d.n; v++) {
+        const uint32_t xb = sp[8u * v];
+        const double wl = lin[v];
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if ((xb >> k) & 1u) E[k] = __dadd_rn(E[k], wl);
+        for (uint32_t e = rows[v]; e < rows[v + 1]; e++) {
+            const uint32_t j = cols[e];
+            if (v < j) {
+                const uint32_t m = xb & sp[8u * j];
+                if (m) {
+                    const double w = vals[e];
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        if ((m >> k) & 1u) E[k] = __dadd_rn(E[k], w);
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned group_mask(int tid) { return 0xFFu << (8 * ((tid >> 3) & 3)); }
+
+// Number of exchange phases executed in global steps (base, base + steps].
+__device__ __forceinline__ uint32_t exchanges_in(uint64_t base, uint32_t steps, uint32_t k) {
+    return (uint32_t)((base + steps) / k - base / k);
+}
+
+// ---------------------------------------------------------------------------
+// Batched single-cell kernel: persistent; each warp pulls a quad of up to 4
+// instances (same mode, similar size and degree) from a global queue ordered
+// longest-first, and its four 8-thread groups run one instance each through
+// the whole temperature schedule. Shared memory: one threshold table per group.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) batch_sa_kernel(DevArrays A, RunArgs R, int tab_stride) {
+    extern __shared__ uint64_t smem[];
+    const int tid = threadIdx.x;
+    const int lane = tid & 7;
+    const int gw = (tid >> 3) & 3;
+    const unsigned gmask = group_mask(tid);
+    uint64_t* tab = smem + (size_t)(tid >> 3) * tab_stride;
+    for (;;) {
+        uint32_t q = 0;
+        if ((tid & 31) == 0) q = atomicAdd(R.queue, 1u);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= R.nquads) break;
+        const uint32_t inst = R.quads[4 * q + gw];
+        if (inst == 0xffffffffu) continue;
+        const InstDesc d = A.desc[inst];
+        uint64_t* words = A.spins + d.spin;
+        uint32_t key[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
+        const uint64_t pos0 = A.pos[inst];
+        if (d.mode == kModeInt) {
+            int32_t E[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) E[k] = A.Ei[d.energy + lane + 8 * k];
+            const int ts = 2 * d.H + 1;
+            for (uint32_t s = 0; s < R.steps; s++) {
+                const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
+                __syncwarp(gmask);
+                for (int i = lane; i < ts; i += 8) tab[i] = metropolis_threshold(i - d.H, beta);
+                __syncwarp(gmask);
+                const uint64_t base = chacha8_draw(key, pos0 + s);
+                sweep_int(A, d, words, lane, tab, base, E);
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) A.Ei[d.energy + lane + 8 * k] = E[k];
+        } else {
+            double E[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) E[k] = A.Ef[d.energy + lane + 8 * k];
+            for (uint32_t s = 0; s < R.steps; s++) {
+                const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
+                const uint64_t base = chacha8_draw(key, pos0 + s);
+                sweep_f64(A, d, words, lane, beta, base, E);
+                if ((R.step_base + s + 1) % kResyncEvery == 0) energies_f64(A, d, words, lane, E);
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) A.Ef[d.energy + lane + 8 * k] = E[k];
+        }
+        __syncwarp(gmask);
+        if (lane == 0) {
+            A.pos[inst] = pos0 + R.steps;
+            A.deo[inst] ^= (int32_t)(exchanges_in(R.step_base, R.steps, R.exchange_interval) & 1u);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// PT kernel: one CTA per instance, thread (cell c, lane l) = threadIdx.x.
+// Runs R.steps steps of engine::step: base_seed draw, sweep of every cell,
+// and every exchange_interval-th step the DEO exchange (engine.rs:713-789)
+// decided by warp 0 with ballots for the draw positions and applied as a
+// masked XOR swap of whole configurations by the whole CTA.
+// Shared memory: [nt][tab_stride] thresholds | [nt][64] energies (f64) |
+// [nt] swap masks | master position.
+// ---------------------------------------------------------------------------
+template <uint32_t MODE>
+__global__ void __launch_bounds__(1024) pt_kernel(DevArrays A, RunArgs R, uint32_t inst0, int tab_stride) {
+    extern __shared__ uint64_t smem[];
+    const uint32_t inst = inst0 + blockIdx.x;
+    const InstDesc d = A.desc[inst];
+    const int nt = (int)d.nt;
+    const int tid = threadIdx.x;
+    const int lane = tid & 7;
+    const int c = tid >> 3;
+    const bool active = c < nt;
+    const unsigned gmask = group_mask(tid);
+    uint64_t* tab = smem + (size_t)c * tab_stride;
+    double* Es = reinterpret_cast<double*>(smem + (size_t)nt * tab_stride);
+    uint64_t* masks = reinterpret_cast<uint64_t*>(Es + (size_t)nt * kReplicas);
+    uint64_t* spos = masks + nt;
+    uint64_t* words = A.spins + d.spin;
+    uint32_t key[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
+    uint64_t pos = A.pos[inst];
+    int deo = A.deo[inst];
+    typedef typename std::conditional<MODE == kModeInt, int32_t, double>::type EType;
+    EType E[8];
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if constexpr (MODE == kModeInt) E[k] = A.Ei[d.energy + (size_t)c * kReplicas + lane + 8 * k];
+            else E[k] = A.Ef[d.energy + (size_t)c * kReplicas + lane + 8 * k];
+        }
+    }
+    const int ts = 2 * d.H + 1;
+    for (uint32_t s = 0; s < R.steps; s++) {
+        const double* T = R.temps + (R.temps_per_step ? (size_t)s * nt : 0);
+        const uint64_t base = chacha8_draw(key, pos);
+        pos += 1;
+        if (active) {
+            const double beta = __ddiv_rn(1.0, T[c]);
+            uint64_t* cw = words + (size_t)c * d.n;
+            if constexpr (MODE == kModeInt) {
+                __syncwarp(gmask);
+                for (int i = lane; i < ts; i += 8) tab[i] = metropolis_threshold(i - d.H, beta);
+                __syncwarp(gmask);
+                sweep_int(A, d, cw, lane, tab, base + (uint64_t)c, E);
+            } else {
+                sweep_f64(A, d, cw, lane, beta, base + (uint64_t)c, E);
+            }
+        }
+        const uint64_t g = R.step_base + s + 1;
+        if (g % R.exchange_interval == 0) {
+            if (nt > 1) {
+                __syncthreads();
+                if (active) {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) Es[c * kReplicas + lane + 8 * k] = (double)E[k];
+                }
+                for (int t = tid; t < nt; t += blockDim.x) masks[t] = 0;
+                __syncthreads();
+                if (tid < 32) {
+                    uint64_t p = pos;
+                    const unsigned lt = (1u << tid) - 1u;
+                    for (int t = deo; t + 1 < nt; t += 2) {
+                        const double db = R.dbeta[t];
+                        const double dea = __dsub_rn(Es[t * kReplicas + tid], Es[(t + 1) * kReplicas + tid]);
+                        const double deb = __dsub_rn(Es[t * kReplicas + tid + 32], Es[(t + 1) * kReplicas + tid + 32]);
+                        const double exa = __dmul_rn(db, dea);
+                        const double exb = __dmul_rn(db, deb);
+                        const bool na = exa < 0.0, nb = exb < 0.0;
+                        const unsigned ma = __ballot_sync(0xffffffffu, na);
+                        const unsigned mb = __ballot_sync(0xffffffffu, nb);
+                        bool aa = !na, ab = !nb;
+                        if (na) {
+                            const uint64_t m = chacha8_draw(key, p + __popc(ma & lt)) >> 11;
+                            if constexpr (MODE == kModeInt) {
+                                const uint64_t ad = (uint64_t)fabs(dea);
+                                const uint64_t th = ad <= R.xdmax[t] ? R.xtab[R.xoff[t] + ad - 1]
+                                                                     : (ad <= R.xdund[t] ? 1ULL : 0ULL);
+                                aa = m < th;
+                            } else {
+                                aa = __dmul_rn((double)m, 1.1102230246251565e-16) < exp(exa);
+                            }
+                        }
+                        if (nb) {
+                            const uint64_t m = chacha8_draw(key, p + __popc(ma) + __popc(mb & lt)) >> 11;
+                            if constexpr (MODE == kModeInt) {
+                                const uint64_t ad = (uint64_t)fabs(deb);
+                                const uint64_t th = ad <= R.xdmax[t] ? R.xtab[R.xoff[t] + ad - 1]
+                                                                     : (ad <= R.xdund[t] ? 1ULL : 0ULL);
+                                ab = m < th;
+                            } else {
+                                ab = __dmul_rn((double)m, 1.1102230246251565e-16) < exp(exb);
+                            }
+                        }
+                        p += (uint64_t)(__popc(ma) + __popc(mb));
+                        const unsigned Aa = __ballot_sync(0xffffffffu, aa);
+                        const unsigned Ab = __ballot_sync(0xffffffffu, ab);
+                        if (aa) {
+                            const double tmp = Es[t * kReplicas + tid];
+                            Es[t * kReplicas + tid] = Es[(t + 1) * kReplicas + tid];
+                            Es[(t + 1) * kReplicas + tid] = tmp;
+                        }
+                        if (ab) {
+                            const double tmp = Es[t * kReplicas + tid + 32];
+                            Es[t * kReplicas + tid + 32] = Es[(t + 1) * kReplicas + tid + 32];
+                            Es[(t + 1) * kReplicas + tid + 32] = tmp;
+                        }
+                        if (tid == 0) {
+                            masks[t] = (uint64_t)Aa | ((uint64_t)Ab << 32);
+                            A.att[d.stat + t] += kReplicas;
+                            A.acc[d.stat + t] += (uint64_t)(__popc(Aa) + __popc(Ab));
+                        }
+                    }
+                    if (tid == 0) *spos = p;
+                }
+                __syncthreads();
+                pos = *spos;
+                for (int t = deo; t + 1 < nt; t += 2) {
+                    const uint64_t M = masks[t];
+                    if (M == 0) continue;
+                    const uint64_t LM = transpose8x8(M);
+                    uint64_t* w1 = words + (size_t)t * d.n;
+                    uint64_t* w2 = words + (size_t)(t + 1) * d.n;
+                    for (uint32_t v = tid; v < d.n; v += blockDim.x) {
+                        const uint64_t a = w1[v], b = w2[v];
+                        const uint64_t dd = (a ^ b) & LM;
+                        w1[v] = a ^ dd;
+                        w2[v] = b ^ dd;
+                    }
+                }
+                __syncthreads();
+                if (active) {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) E[k] = (EType)Es[c * kReplicas + lane + 8 * k];
+                }
+            }
+            deo ^= 1;
+        }
+        if constexpr (MODE == kModeF64) {
+            if (g % kResyncEvery == 0) {
+                if (nt > 1) __syncthreads();  // swaps by other threads are visible
+                if (active) energies_f64(A, d, words + (size_t)c * d.n, lane, E);
+            }
+        }
+    }
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if constexpr (MODE == kModeInt) A.Ei[d.energy + (size_t)c * kReplicas + lane + 8 * k] = E[k];
+            else A.Ef[d.energy + (size_t)c * kReplicas + lane + 8 * k] = E[k];
+        }
+    }
+    if (tid == 0) {
+        A.pos[inst] = pos;
+        A.deo[inst] = deo;
+    }
+}
+
+template __global__ void pt_kernel<kModeInt>(DevArrays, RunArgs, uint32_t, int);
+template __global__ void pt_kernel<kModeF64>(DevArrays, RunArgs, uint32_t, int);
+
+// ---------------------------------------------------------------------------
+// Random init (ultimate.rs:248-280): one gen::<u64>() word per unclamped
+// (cell, site) in cell-major, site-minor order; clamped sites take their value
+// in every replica. One CTA per instance. draw_idx[site] = number of unclamped
+// sites before it; unclamped = their total.
+// ---------------------------------------------------------------------------
+__global__ void init_spins_kernel(DevArrays A, uint32_t inst0, const uint32_t* draw_idx,
+                                  const uint32_t* unclamped) {
+    const uint32_t inst = inst0 + blockIdx.x;
+    const InstDesc d = A.desc[inst];
+    uint32_t key[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
+    const uint64_t pos0 = A.pos[inst];
+    const uint64_t U = unclamped[inst];
+    const uint64_t total = (uint64_t)d.nt * d.n;
+    for (uint64_t i = threadIdx.x; i < total; i += blockDim.x) {
+        const uint32_t c = (uint32_t)(i / d.n);
+        const uint32_t v = (uint32_t)(i % d.n);
+        uint64_t w;
+        if (A.clampf[d.site + v]) {
+            w = A.clampv[d.site + v] == 1 ? ~0ULL : 0ULL;
+        } else {
+            w = transpose8x8(chacha8_draw(key, pos0 + (uint64_t)c * U + draw_idx[d.site + v]));
+        }
+        A.spins[d.spin + i] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) A.pos[inst] = pos0 + (uint64_t)d.nt * U;
+}
+
+// Tracked energies from scratch: one (cell, lane) thread per 8 replicas,
+// reference order. Integer mode stores the exact integer value.
+__global__ void energy_kernel(DevArrays A, uint32_t inst0) {
+    const uint32_t inst = inst0 + blockIdx.x;
+    const InstDesc d = A.desc[inst];
+    for (uint32_t t = threadIdx.x; t < d.nt * 8u; t += blockDim.x) {
+        const uint32_t c = t >> 3, lane = t & 7;
+        double E[8];
+        energies_f64(A, d, A.spins + d.spin + (size_t)c * d.n, (int)lane, E);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const size_t o = d.energy + (size_t)c * kReplicas + lane + 8 * k;
+            if (d.mode == kModeInt) A.Ei[o] = (int32_t)E[k];
+            else A.Ef[o] = E[k];
+        }
+    }
+}
+
+// Same recompute into a separate f64 buffer [inst][cell][64] without touching
+// the tracked energies (FP64 verification of any mode).
+__global__ void energy_check_kernel(DevArrays A, uint32_t inst0, double* out) {
+    const uint32_t inst = inst0 + blockIdx.x;
+    const InstDesc d = A.desc[inst];
+    for (uint32_t t = threadIdx.x; t < d.nt * 8u; t += blockDim.x) {
+        const uint32_t c = t >> 3, lane = t & 7;
+        double E[8];
+        energies_f64(A, d, A.spins + d.spin + (size_t)c * d.n, (int)lane, E);
+#pragma unroll
+        for (int k = 0; k < 8; k++) out[d.energy + (size_t)c * kReplicas + lane + 8 * k] = E[k];
+    }
+}
+
+// Model energy (hubo.rs:176-189: offset, then per set variable its linear
+// term and half of each set neighbour's coupling, CSR order) of one replica's
+// configuration. One thread per (cell, replica); used for the incumbent and
+// the final best-replica extraction (ultimate.rs:345-368, 397-430).
+__global__ void model_energy_kernel(DevArrays A, uint32_t inst, double offset, double* out) {
+    const InstDesc d = A.desc[inst];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.nt * (uint32_t)kReplicas) return;
+    const uint32_t c = t >> 6, r = t & 63;
+    const uint8_t* sp = reinterpret_cast<const uint8_t*>(A.spins + d.spin + (size_t)c * d.n) + (r & 7);
+    const uint32_t bit = r >> 3;
+    const uint32_t* rows = A.rows + d.row;
+    const uint32_t* cols = A.cols + d.ent;
+    const double* vals = A.vals + d.ent;
+    const double* lin = A.lin + d.site;
+    double e = offset;
+    for (uint32_t i = 0; i < d.n; i++) {
+        if ((sp[8u * i] >> bit) & 1u) {
+            e = __dadd_rn(e, lin[i]);
+            for (uint32_t k = rows[i]; k < rows[i + 1]; k++)
+                if ((sp[8u * cols[k]] >> bit) & 1u) e = __dadd_rn(e, __dmul_rn(vals[k], 0.5));
+        }
+    }
+    out[t] = e;
+}
+
+// update_incumbent (ultimate.rs:397-430): argmin of the tracked energies in
+// (cell, replica) order with strict <, re-scored with the model energy; the
+// incumbent changes only on a strict improvement. Single CTA of 64 threads.
+__global__ void incumbent_kernel(DevArrays A, uint32_t inst, double offset, double* inc_e,
+                                 uint64_t* inc_state, uint32_t n_words) {
+    __shared__ double sv[64];
+    __shared__ int si[64];
+    __shared__ double score;
+    __shared__ int argc, argr;
+    const InstDesc d = A.desc[inst];
+    const int tid = threadIdx.x;
+    double best = __longlong_as_double(0x7ff0000000000000LL);
+    int bi = 0x7fffffff;
+    for (uint32_t t = tid; t < d.nt * (uint32_t)kReplicas; t += 64) {
+        const double e = d.mode == kModeInt ? (double)A.Ei[d.energy + t] : A.Ef[d.energy + t];
+        if (e < best) {
+            best = e;
+            bi = (int)t;
+        }
+    }
+    sv[tid] = best;
+    si[tid] = bi;
+    __syncthreads();
+    if (tid == 0) {
+        double b = sv[0];
+        int i0 = si[0];
+        for (int i = 1; i < 64; i++)
+            if (sv[i] < b || (sv[i] == b && si[i] < i0)) {
+                b = sv[i];
+                i0 = si[i];
+            }
+        argc = -1;
+        if (b < __longlong_as_double(0x7ff0000000000000LL)) {
+            argc = i0 >> 6;
+            argr = i0 & 63;
+        }
+    }
+    __syncthreads();
+    if (argc < 0) return;
+    const uint8_t* sp = reinterpret_cast<const uint8_t*>(A.spins + d.spin + (size_t)argc * d.n) + (argr & 7);
+    const uint32_t bit = argr >> 3;
+    if (tid == 0) {
+        const uint32_t* rows = A.rows + d.row;
+        const uint32_t* cols = A.cols + d.ent;
+        const double* vals = A.vals + d.ent;
+        const double* lin = A.lin + d.site;
+        double e = offset;
+        for (uint32_t i = 0; i < d.n; i++) {
+            if ((sp[8u * i] >> bit) & 1u) {
+                e = __dadd_rn(e, lin[i]);
+                for (uint32_t k = rows[i]; k < rows[i + 1]; k++)
+                    if ((sp[8u * cols[k]] >> bit) & 1u) e = __dadd_rn(e, __dmul_rn(vals[k], 0.5));
+            }
+        }
+        score = e;
+    }
+    __syncthreads();
+    if (score < *inc_e) {
+        // packed incumbent state: bit i%64 of word i/64
+        for (uint32_t w = tid; w < n_words; w += 64) {
+            uint64_t acc = 0;
+            for (uint32_t b = 0; b < 64 && 64 * w + b < d.n; b++)
+                acc |= (uint64_t)((sp[8u * (64 * w + b)] >> bit) & 1u) << b;
+            inc_state[w] = acc;
+        }
+        __syncthreads();
+        if (tid == 0) *inc_e = score;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launch wrappers (declared in ie_launch.h).
+// ---------------------------------------------------------------------------
+cudaError_t set_smem_limits(size_t batch_bytes, size_t pt_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(batch_sa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(pt_kernel<kModeInt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pt_bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(pt_kernel<kModeF64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pt_bytes);
+}
+
+int batch_occupancy(int block, size_t smem) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_sa_kernel, block, smem) != cudaSuccess) return 0;
+    return n;
+}
+
+cudaError_t launch_batch_sa(const DevArrays& A, const RunArgs& R, int grid, int block, int tab_stride,
+                            size_t smem, cudaStream_t st) {
+    batch_sa_kernel<<<grid, block, smem, st>>>(A, R, tab_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pt(const DevArrays& A, const RunArgs& R, uint32_t inst0, uint32_t ninst, uint32_t mode,
+                      int block, int tab_stride, size_t smem, cudaStream_t st) {
+    if (mode == kModeInt) pt_kernel<kModeInt><<<ninst, block, smem, st>>>(A, R, inst0, tab_stride);
+    else pt_kernel<kModeF64><<<ninst, block, smem, st>>>(A, R, inst0, tab_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init(const DevArrays& A, uint32_t inst0, uint32_t ninst, const uint32_t* draw_idx,
+                        const uint32_t* unclamped, cudaStream_t st) {
+    init_spins_kernel<<<ninst, 256, 0, st>>>(A, inst0, draw_idx, unclamped);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy(const DevArrays& A, uint32_t inst0, uint32_t ninst, cudaStream_t st) {
+    energy_kernel<<<ninst, 128, 0, st>>>(A, inst0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy_check(const DevArrays& A, uint32_t inst0, uint32_t ninst, double* out, cudaStream_t st) {
+    energy_check_kernel<<<ninst, 128, 0, st>>>(A, inst0, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_model_energy(const DevArrays& A, uint32_t inst, uint32_t nt, double offset, double* out,
+                                cudaStream_t st) {
+    const uint32_t total = nt * (uint32_t)kReplicas;
+    model_energy_kernel<<<(total + 127) / 128, 128, 0, st>>>(A, inst, offset, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_incumbent(const DevArrays& A, uint32_t inst, double offset, double* inc_e, uint64_t* inc_state,
+                             uint32_t n_words, cudaStream_t st) {
+    incumbent_kernel<<<1, 64, 0, st>>>(A, inst, offset, inc_e, inc_state, n_words);
+    return cudaGetLastError();
+}
+
+}  // namespace ie

@@ -1,0 +1,69 @@
+// Kernel-side data model shared by the host code (ie_engine.cu) and kernels.
+#pragma once
+#include <cstdint>
+
+namespace ie {
+
+constexpr int kReplicas = 64;
+constexpr int kLanes = 8;     // Xoshiro lanes per cell; thread (cell, lane) owns 8 replicas
+constexpr int kMaxH = 127;    // integer mode: local fields within [-127, 127]
+constexpr int kTabMax = 2 * kMaxH + 1;
+constexpr int kResyncEvery = 1000;  // ultimate.rs:316-324
+
+enum Mode : uint32_t { kModeInt = 0, kModeF64 = 1 };
+
+// One instance (problem + its cells). All offsets index the engine-wide arrays.
+struct InstDesc {
+    uint32_t n;      // sites
+    int32_t H;       // integer-mode bound on |local field|
+    uint32_t mode;   // Mode
+    uint32_t nt;     // cells (temperatures); num_pops = 1
+    uint64_t row;    // rows[row .. row+n]: entry offsets relative to `ent`
+    uint64_t ent;    // ents[] (int mode) and cols[]/vals[] base
+    uint64_t site;   // linp[], lin[], clampf[] base
+    uint64_t spin;   // spins[]: cell c word v at spin + c*n + v (lane-major bytes)
+    uint64_t energy; // Ei[] / Ef[]: cell c replica r at energy + c*64 + r
+    uint64_t stat;   // swap stats base ([nt-1] per instance)
+};
+
+struct DevArrays {
+    const InstDesc* desc;
+    const uint32_t* rows;
+    const uint32_t* ents;    // int mode: col | (|w| << 24) | (w < 0) << 31
+    const int32_t* linp;     // int mode: lin + sum of negative weights of the row
+    const uint32_t* cols;    // original CSR (both modes), reference order
+    const double* vals;
+    const double* lin;
+    const uint8_t* clampf;   // 1 = clamped site
+    const int8_t* clampv;    // clamp value (0/1)
+    const uint32_t* keys;    // master ChaCha8 key [inst][8]
+    uint64_t* spins;
+    int32_t* Ei;
+    double* Ef;
+    uint64_t* pos;           // master-stream position (u64 draws) [inst]
+    int32_t* deo;            // DEO phase [inst]
+    uint64_t* att;           // swap attempts [stat + pair]
+    uint64_t* acc;           // swap accepts
+    int32_t* err;            // device error word
+};
+
+// Run parameters of one launch.
+struct RunArgs {
+    const double* temps;      // [steps][nt] temperatures, or [nt] when temps_per_step == 0
+    uint32_t temps_per_step;  // 1: temps advance with the step, 0: constant ladder
+    uint32_t steps;
+    uint64_t step_base;       // steps already executed (resync and exchange cadence)
+    uint32_t exchange_interval;
+    // exchange thresholds (int mode): per pair t of the ladder
+    const uint64_t* xtab;     // thresholds ceil(exp(db*de) * 2^53) for |de| = 1..dmax[t]
+    const uint64_t* xoff;     // [nt-1] offsets into xtab
+    const uint64_t* xdmax;    // [nt-1]
+    const uint64_t* xdund;    // [nt-1] largest |de| with exp > 0
+    const double* dbeta;      // [nt-1] 1/T_t - 1/T_{t+1}
+    // batched work queue
+    const uint32_t* quads;    // [nquads][4] instance ids (0xffffffff = empty)
+    uint32_t nquads;
+    uint32_t* queue;          // atomic counter
+};
+
+}  // namespace ie

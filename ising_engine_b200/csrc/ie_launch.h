@@ -1,0 +1,22 @@
+// Host-side launch wrappers of the kernels in ie_kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ie_kernels.cuh"
+
+namespace ie {
+cudaError_t set_smem_limits(size_t batch_bytes, size_t pt_bytes);
+int batch_occupancy(int block, size_t smem);
+cudaError_t launch_batch_sa(const DevArrays& A, const RunArgs& R, int grid, int block, int tab_stride,
+                            size_t smem, cudaStream_t st);
+cudaError_t launch_pt(const DevArrays& A, const RunArgs& R, uint32_t inst0, uint32_t ninst, uint32_t mode,
+                      int block, int tab_stride, size_t smem, cudaStream_t st);
+cudaError_t launch_init(const DevArrays& A, uint32_t inst0, uint32_t ninst, const uint32_t* draw_idx,
+                        const uint32_t* unclamped, cudaStream_t st);
+cudaError_t launch_energy(const DevArrays& A, uint32_t inst0, uint32_t ninst, cudaStream_t st);
+cudaError_t launch_energy_check(const DevArrays& A, uint32_t inst0, uint32_t ninst, double* out, cudaStream_t st);
+cudaError_t launch_model_energy(const DevArrays& A, uint32_t inst, uint32_t nt, double offset, double* out,
+                                cudaStream_t st);
+cudaError_t launch_incumbent(const DevArrays& A, uint32_t inst, double offset, double* inc_e, uint64_t* inc_state,
+                             uint32_t n_words, cudaStream_t st);
+}  // namespace ie

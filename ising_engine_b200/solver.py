@@ -1,0 +1,105 @@
+"""UltimateSolver's parallel-tempering path on the device.
+
+Mirrors the reference's solver configuration (src/solver/ultimate.rs:18-87)
+and its PT path (ultimate.rs:234-387): random init from the master stream,
+total_exchanges x sweeps_per_exchange calls of engine::step with energy
+resync every 1000 steps, update_incumbent after every exchange block, best
+replica extraction, then the 1-opt polish of src/solver/local_search.rs:19-57.
+
+Presolve and component decomposition (ultimate.rs:161-218) are host-side
+reductions before this path; ``solve`` accepts their result as clamps.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .core import QuboModel
+from .engine import Engine
+
+NUM_REPLICAS = 64
+
+
+def steepest_descent_1opt(model: QuboModel, state, is_clamped=None) -> float:
+    """local_search.rs:19-57 (steepest improving flip, lowest index on ties),
+    in the same f64 evaluation order. Polishes ``state`` in place."""
+    n = model.num_vars
+    state = np.asarray(state)
+    clamped = np.zeros(n, dtype=bool) if is_clamped is None else np.asarray(is_clamped, dtype=bool)
+    ro = model.row_offsets.astype(np.int64)
+    ci = model.col_indices.astype(np.int64)
+    va = model.values
+    lin = model.linear
+    gains = np.zeros(n)
+    for i in range(n):
+        field = float(lin[i])
+        for k in range(ro[i], ro[i + 1]):
+            field += float(va[k]) * float(state[ci[k]])
+        gains[i] = (1.0 - 2.0 * float(state[i])) * field
+    total = 0.0
+    while True:
+        best_i, best_g = -1, -1e-12
+        for i in range(n):
+            if not clamped[i] and gains[i] < best_g:
+                best_i, best_g = i, float(gains[i])
+        if best_i < 0:
+            return total
+        total -= best_g
+        dirn = 1.0 - 2.0 * float(state[best_i])
+        state[best_i] = 1 - state[best_i]
+        gains[best_i] = -best_g
+        for k in range(ro[best_i], ro[best_i + 1]):
+            j = ci[k]
+            gains[j] += (1.0 - 2.0 * float(state[j])) * float(va[k]) * dirn
+
+
+class UltimateSolver:
+    """Configuration of the reference's UltimateSolver (ultimate.rs:18-57) for
+    the PT path: num_pops = num_slices = 1."""
+
+    def __init__(self, temp_max: float, temp_min: float, sweeps: int, exchanges: int,
+                 seed: int | None, num_temps: int = 10, exchange_interval: int = 1,
+                 device: int = 0):
+        self.num_replicas = NUM_REPLICAS
+        self.temp_max = float(temp_max)
+        self.temp_min = float(temp_min)
+        self.sweeps_per_exchange = int(sweeps)
+        self.total_exchanges = int(exchanges)
+        self.seed = int(np.random.SeedSequence().entropy % (1 << 64)) if seed is None else int(seed)
+        self.num_slices = 1
+        self.num_temps = int(num_temps)
+        self.num_pops = 1
+        self.exchange_interval = int(exchange_interval)
+        self.device = device
+
+    @staticmethod
+    def new(temp_max, temp_min, sweeps, exchanges, seed):
+        return UltimateSolver(temp_max, temp_min, sweeps, exchanges, seed)
+
+    def with_quantum_dims(self, slices: int, temps: int, pops: int) -> "UltimateSolver":
+        if slices != 1 or pops != 1:
+            raise NotImplementedError("only num_slices = num_pops = 1 is on the device path")
+        self.num_temps = int(temps)
+        return self
+
+    def engine(self, model: QuboModel) -> Engine:
+        return Engine(model, num_temps=self.num_temps, seed=self.seed,
+                      exchange_interval=self.exchange_interval, temp_max=self.temp_max,
+                      temp_min=self.temp_min, sweeps_per_exchange=self.sweeps_per_exchange,
+                      total_exchanges=self.total_exchanges, device=self.device)
+
+    def solve(self, model: QuboModel, clamped=()) -> np.ndarray:
+        """PT path of UltimateSolver::solve for `model` with `clamped` fixings."""
+        n = model.num_vars
+        is_clamped = np.zeros(n, dtype=np.uint8)
+        cval = np.zeros(n, dtype=np.int8)
+        for idx, val in clamped:
+            is_clamped[idx] = 1
+            cval[idx] = val
+        with self.engine(model) as eng:
+            if len(clamped):
+                eng.set_clamps(is_clamped, cval)
+            eng.init_random()
+            eng.run_pt()
+            _, best = eng.best()
+        steepest_descent_1opt(model, best, is_clamped.astype(bool))
+        return best

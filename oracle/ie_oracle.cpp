@@ -1,0 +1,1124 @@
+// CPU oracle: a plain C++ restatement of the reference's S1 Metropolis/PT path.
+//
+// TEST INFRASTRUCTURE ONLY. Nothing in the product (the ising_engine_b200 package
+// and its CUDA library) links, imports or calls this file. It is used by tests/,
+// by __graft_entry__.smoke() as the checker, and by bench.py's cpu_baseline /
+// --impl reference leg as the timed CPU restatement of the reference's Rayon path.
+//
+// Parity pin: the end-to-end golden of tests/test_regression_golden.rs:87-111
+// (UltimateSolver::new(50,0.05,30,40,Some(2024)) on the seeded n=32 instance)
+// is reproduced by or_solve(); tests/test_oracle_golden.py asserts it.
+//
+// Every function cites the reference file:line it restates. Compile with
+// -ffp-contract=off and no fast-math: the reference's f64 arithmetic is
+// uncontracted (Rust never fuses a*b+c on its own).
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <functional>
+#include <limits>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr int NR = 64;  // NUM_REPLICAS, src/solver/types.rs:17
+
+// ---------------------------------------------------------------------------
+// Master RNG: rand_chacha 0.3.1 ChaCha8Rng, seeded by rand_core 0.6.4
+// SeedableRng::seed_from_u64, drawn through rand 0.8.5 (gen::<u64>, gen::<f64>,
+// gen_range::<f64>). Third-party crates (Cargo.lock:2656-2705), restated from
+// their published algorithms; call sites ultimate.rs:151-152,272 and
+// engine.rs:596,727.
+// ---------------------------------------------------------------------------
+static inline uint32_t rotl32(uint32_t x, int k) { return (x << k) | (x >> (32 - k)); }
+
+// One ChaCha block with 8 rounds (4 double rounds). Input layout: constants,
+// 8 key words, 64-bit block counter (words 12-13), 64-bit stream id (14-15).
+static void chacha8_block(const uint32_t key[8], uint64_t counter, uint32_t out[16]) {
+    uint32_t in[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u,
+                       key[0], key[1], key[2], key[3], key[4], key[5], key[6], key[7],
+                       (uint32_t)counter, (uint32_t)(counter >> 32), 0u, 0u};
+    uint32_t x[16];
+    std::memcpy(x, in, sizeof(x));
+#define QR(a, b, c, d)                      \
+    x[a] += x[b]; x[d] ^= x[a]; x[d] = rotl32(x[d], 16); \
+    x[c] += x[d]; x[b] ^= x[c]; x[b] = rotl32(x[b], 12); \
+    x[a] += x[b]; x[d] ^= x[a]; x[d] = rotl32(x[d], 8);  \
+    x[c] += x[d]; x[b] ^= x[c]; x[b] = rotl32(x[b], 7);
+    for (int i = 0; i < 4; i++) {
+        QR(0, 4, 8, 12) QR(1, 5, 9, 13) QR(2, 6, 10, 14) QR(3, 7, 11, 15)
+        QR(0, 5, 10, 15) QR(1, 6, 11, 12) QR(2, 7, 8, 13) QR(3, 4, 9, 14)
+    }
+#undef QR
+    for (int i = 0; i < 16; i++) out[i] = x[i] + in[i];
+}
+
+struct ChaCha8Rng {
+    uint32_t key[8];
+    uint64_t counter = 0;  // next block to generate
+    uint32_t buf[64];      // rand_chacha buffers 4 blocks
+    int idx = 64;
+    uint64_t draws = 0;    // number of u64 draws so far (stream position)
+
+    // rand_core 0.6.4 seed_from_u64: PCG32 output fills the 32-byte seed.
+    explicit ChaCha8Rng(uint64_t state) {
+        const uint64_t MUL = 6364136223846793005ULL, INC = 11634580027462260723ULL;
+        for (int i = 0; i < 8; i++) {
+            state = state * MUL + INC;
+            uint32_t xs = (uint32_t)(((state >> 18) ^ state) >> 27);
+            uint32_t rot = (uint32_t)(state >> 59);
+            key[i] = (xs >> rot) | (xs << ((32 - rot) & 31));  // little-endian bytes = word
+        }
+    }
+    void refill() {
+        for (int b = 0; b < 4; b++) chacha8_block(key, counter + b, buf + 16 * b);
+        counter += 4;
+        idx = 0;
+    }
+    // BlockRng::next_u64: two consecutive u32 words, low first. Every draw on
+    // this path is 64-bit, so the index is always even.
+    uint64_t next_u64() {
+        if (idx >= 64) refill();
+        uint64_t v = (uint64_t)buf[idx] | ((uint64_t)buf[idx + 1] << 32);
+        idx += 2;
+        draws++;
+        return v;
+    }
+    // rand 0.8.5 Standard for f64: 53 high bits times 2^-53.
+    double gen_f64() { return (double)(next_u64() >> 11) * (1.0 / 9007199254740992.0); }
+    // rand 0.8.5 UniformFloat::<f64>::sample_single (gen_range(low..high)).
+    double gen_range(double low, double high) {
+        double scale = high - low;
+        for (;;) {
+            uint64_t bits = (next_u64() >> 12) | 0x3FF0000000000000ULL;
+            double v12;
+            std::memcpy(&v12, &bits, 8);
+            double v01 = v12 - 1.0;
+            double res = v01 * scale + low;
+            if (res < high) return res;
+            uint64_t sb;
+            std::memcpy(&sb, &scale, 8);
+            sb -= 1;
+            std::memcpy(&scale, &sb, 8);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Xoshiro256PlusPlusX8, src/solver/engine.rs:81-172.
+// ---------------------------------------------------------------------------
+static inline uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+struct XoshiroX8 {
+    uint64_t s[4][8];
+    // engine.rs:87-103: SplitMix64 sequence, lane-major fill.
+    explicit XoshiroX8(uint64_t seed) {
+        uint64_t state = seed;
+        auto next = [&]() {
+            state += 0x9e3779b97f4a7c15ULL;
+            uint64_t z = state;
+            z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+            z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+            return z ^ (z >> 31);
+        };
+        for (int lane = 0; lane < 8; lane++)
+            for (int w = 0; w < 4; w++) s[w][lane] = next();
+    }
+    inline void advance() {
+        for (int l = 0; l < 8; l++) {
+            uint64_t t = s[1][l] << 17;
+            s[2][l] ^= s[0][l];
+            s[3][l] ^= s[1][l];
+            s[1][l] ^= s[2][l];
+            s[0][l] ^= s[3][l];
+            s[2][l] ^= t;
+            s[3][l] = rotl64(s[3][l], 45);
+        }
+    }
+    // engine.rs:107-125: uniform = (result >> 12) * 2^-52 via the mantissa trick.
+    inline void next_f64x8(double* out) {
+        for (int l = 0; l < 8; l++) {
+            uint64_t result = rotl64(s[0][l] + s[3][l], 23) + s[0][l];
+            uint64_t bits = 0x3FF0000000000000ULL | (result >> 12);
+            double d;
+            std::memcpy(&d, &bits, 8);
+            out[l] = d - 1.0;
+        }
+        advance();
+    }
+    // engine.rs:145-151: 64 uniforms, replica r = 8*call + lane.
+    inline void next_f64x64(double* out) {
+        for (int c = 0; c < 8; c++) next_f64x8(out + 8 * c);
+    }
+    // engine.rs:159-171
+    inline void skip_f64x64() {
+        for (int c = 0; c < 8; c++) advance();
+    }
+};
+
+// engine.rs:181-205 (f64::clamp semantics, left-to-right sums, no contraction).
+static inline double fast_exp(double x) {
+    if (x < -20.0) x = -20.0;
+    if (x > 0.0) x = 0.0;
+    double r = x * 0.0625;
+    double r2 = r * r;
+    double r3 = r2 * r;
+    double p = 1.0 + r + 0.5 * r2 + (1.0 / 6.0) * r3 + (1.0 / 24.0) * r2 * r2 +
+               (1.0 / 120.0) * r2 * r3 + (1.0 / 720.0) * r3 * r3;
+    double p2 = p * p;
+    double p4 = p2 * p2;
+    double p8 = p4 * p4;
+    return p8 * p8;
+}
+
+// compiler-rt __powidf2, which Rust's f64::powi lowers to for a runtime exponent.
+static double powi(double a, int b) {
+    const bool recip = b < 0;
+    double r = 1.0;
+    for (;;) {
+        if (b & 1) r *= a;
+        b /= 2;
+        if (b == 0) break;
+        a *= a;
+    }
+    return recip ? 1.0 / r : r;
+}
+
+// ---------------------------------------------------------------------------
+// Problem: QuboModel + CsrMatrix (src/core/hubo.rs:165-189, csr_matrix.rs:6-30).
+// Both triangles stored; E = offset + sum lin*x + 1/2 sum_csr w x_i x_j.
+// FlatHuboModel::from_hubo (hubo.rs:94-158) keeps the rows in the same order, so
+// the edge2 CSR equals the quadratic CSR (ultimate.rs:140-148).
+// ---------------------------------------------------------------------------
+struct Qubo {
+    int64_t n = 0;
+    std::vector<double> linear;
+    std::vector<int64_t> row;
+    std::vector<int64_t> col;
+    std::vector<double> val;
+    double offset = 0.0;
+};
+
+static Qubo make_qubo(int64_t n, const double* lin, const int64_t* row, const int64_t* col,
+                      const double* val, double offset) {
+    Qubo q;
+    q.n = n;
+    q.linear.assign(lin, lin + n);
+    q.row.assign(row, row + n + 1);
+    int64_t nnz = q.row[n];
+    q.col.assign(col, col + nnz);
+    q.val.assign(val, val + nnz);
+    q.offset = offset;
+    return q;
+}
+
+// hubo.rs:176-189
+static double total_energy(const Qubo& m, const int8_t* state) {
+    double e = m.offset;
+    for (int64_t i = 0; i < m.n; i++) {
+        if (state[i] == 1) {
+            e += m.linear[i];
+            for (int64_t k = m.row[i]; k < m.row[i + 1]; k++)
+                if (state[m.col[k]] == 1) e += m.val[k] * 0.5;
+        }
+    }
+    return e;
+}
+
+// ---------------------------------------------------------------------------
+// QuantumField with num_slices = 1 (src/solver/types.rs:17-58). Spins are one
+// byte per replica: spins[(v + n*cell)*64 + r], cell = t + nt*p.
+// ---------------------------------------------------------------------------
+struct Field {
+    int64_t n;
+    int nt, np;
+    std::vector<int8_t> spins;
+    std::vector<std::array<double, NR>> energies;
+    Field(int64_t n_, int nt_, int np_) : n(n_), nt(nt_), np(np_),
+        spins((size_t)n_ * nt_ * np_ * NR, 0), energies((size_t)nt_ * np_) {
+        for (auto& e : energies) e.fill(0.0);
+    }
+    int8_t* cell(int c) { return spins.data() + (size_t)c * n * NR; }
+};
+
+// engine.rs:218-271 (edge2 only: QUBO input has no edge3/edge4 terms).
+static inline void delta_e_local(const Qubo& m, const int8_t* spins, int64_t v, double* delta) {
+    const int8_t* xv = spins + v * NR;
+    int8_t sign[NR];
+    for (int r = 0; r < NR; r++) sign[r] = (int8_t)(1 - 2 * xv[r]);
+    const double wl = m.linear[v];
+    for (int r = 0; r < NR; r++) delta[r] = wl * (double)sign[r];
+    for (int64_t k = m.row[v]; k < m.row[v + 1]; k++) {
+        const int8_t* xj = spins + m.col[k] * NR;
+        const double w = m.val[k];
+        for (int r = 0; r < NR; r++) {
+            int8_t t = (int8_t)((xj[r] ^ xv[r]) - xv[r]);
+            delta[r] += w * (double)t;
+        }
+    }
+}
+
+// engine.rs:333-368 (num_slices = 1: the Trotter term is j_tau = 0 and adds 0).
+static void replica_energies(const Qubo& m, const int8_t* spins, double* en) {
+    for (int r = 0; r < NR; r++) en[r] = 0.0;
+    for (int64_t v = 0; v < m.n; v++) {
+        const int8_t* xv = spins + v * NR;
+        const double wl = m.linear[v];
+        for (int r = 0; r < NR; r++) en[r] += wl * (double)xv[r];
+        for (int64_t k = m.row[v]; k < m.row[v + 1]; k++) {
+            int64_t j = m.col[k];
+            if (v < j) {
+                const double w = m.val[k];
+                const int8_t* xj = spins + j * NR;
+                for (int r = 0; r < NR; r++) en[r] += w * (double)(xv[r] & xj[r]);
+            }
+        }
+    }
+}
+
+struct StepScratch {
+    std::vector<uint64_t> attempts, accepts;
+    bool deo_odd = false;
+};
+
+// A tiny fork/join pool standing in for Rayon's par_chunks_mut (engine.rs:603-608).
+static void parallel_for(int count, int threads, const std::function<void(int)>& fn) {
+    if (threads <= 1 || count <= 1) {
+        for (int i = 0; i < count; i++) fn(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    int nthr = std::min(threads, count);
+    for (int t = 0; t < nthr; t++)
+        pool.emplace_back([&]() {
+            for (int i; (i = next.fetch_add(1)) < count;) fn(i);
+        });
+    for (auto& th : pool) th.join();
+}
+
+// Phase 1 of engine.rs:573-703 for one cell: index-order Metropolis sweep.
+static void sweep_cell(const Qubo& m, int8_t* spins, double* es, double beta, uint64_t seed,
+                       const std::vector<uint8_t>& clamped) {
+    XoshiroX8 rng(seed);
+    double u[NR], d[NR];
+    for (int64_t v = 0; v < m.n; v++) {
+        if (clamped[v]) {
+            rng.skip_f64x64();
+            continue;
+        }
+        rng.next_f64x64(u);
+        delta_e_local(m, spins, v, d);
+        int8_t* xv = spins + v * NR;
+        for (int r = 0; r < NR; r++) {
+            double td = d[r];
+            double ev = fast_exp(-td * beta);
+            bool accept = (td <= 0.0) | (u[r] < ev);
+            int8_t flip = (int8_t)accept;
+            xv[r] ^= flip;
+            es[r] += td * (double)flip;
+        }
+    }
+}
+
+// Phase 2 of engine.rs:713-789: DEO replica exchange on the master RNG.
+static void exchange(Field& f, const double* temps, StepScratch& sc, ChaCha8Rng& rng,
+                     bool stats) {
+    const int nt = f.nt;
+    const int parity = sc.deo_odd ? 1 : 0;
+    for (int p = 0; p < f.np; p++) {
+        for (int t = parity; t + 1 < nt; t += 2) {
+            auto& e1 = f.energies[t + nt * p];
+            auto& e2 = f.energies[t + 1 + nt * p];
+            double b1 = 1.0 / temps[t], b2 = 1.0 / temps[t + 1];
+            double db = b1 - b2;
+            bool mask[NR];
+            bool any = false;
+            int acc = 0;
+            for (int r = 0; r < NR; r++) {
+                double de = e1[r] - e2[r];
+                double ex = db * de;
+                mask[r] = ex >= 0.0 || rng.gen_f64() < std::exp(ex);
+                any |= mask[r];
+                acc += mask[r];
+            }
+            if (stats) {
+                sc.attempts[t] += NR;
+                sc.accepts[t] += (uint64_t)acc;
+            }
+            if (any) {
+                int8_t* c1 = f.cell(t + nt * p);
+                int8_t* c2 = f.cell(t + 1 + nt * p);
+                int8_t lm[NR];
+                for (int r = 0; r < NR; r++) lm[r] = (int8_t)(-(int8_t)mask[r]);
+                for (int64_t v = 0; v < f.n; v++)
+                    for (int r = 0; r < NR; r++) {
+                        int8_t dd = (int8_t)((c1[v * NR + r] ^ c2[v * NR + r]) & lm[r]);
+                        c1[v * NR + r] ^= dd;
+                        c2[v * NR + r] ^= dd;
+                    }
+                for (int r = 0; r < NR; r++)
+                    if (mask[r]) std::swap(e1[r], e2[r]);
+            }
+        }
+    }
+}
+
+// engine::step (engine.rs:573-819) with an optional exchange skip: the
+// exchange-interval extension runs phase 2 only when do_exchange is set, and
+// the DEO phase toggles per executed exchange (interval 1 is the reference).
+static void step(Field& f, const Qubo& m, const double* temps, const std::vector<uint8_t>& clamped,
+                 StepScratch& sc, ChaCha8Rng& rng, bool do_exchange, bool stats, int threads,
+                 uint64_t* base_seed_out) {
+    const uint64_t base_seed = rng.next_u64();
+    if (base_seed_out) *base_seed_out = base_seed;
+    const int cells = f.nt * f.np;
+    parallel_for(cells, threads, [&](int c) {
+        int t = c % f.nt;
+        double beta = 1.0 / temps[t];
+        sweep_cell(m, f.cell(c), f.energies[c].data(), beta, base_seed + (uint64_t)c, clamped);
+    });
+    if (do_exchange) {
+        exchange(f, temps, sc, rng, stats);
+        sc.deo_odd = !sc.deo_odd;
+    }
+}
+
+// ultimate.rs:248-280 (random branch; the GNN warm start is not on the path).
+static void init_field(Field& f, const std::vector<uint8_t>& clamped,
+                       const std::vector<int8_t>& cval, ChaCha8Rng& rng) {
+    for (int p = 0; p < f.np; p++)
+        for (int t = 0; t < f.nt; t++) {
+            int8_t* s = f.cell(t + f.nt * p);
+            for (int64_t v = 0; v < f.n; v++) {
+                if (clamped[v]) {
+                    int8_t val = cval[v] == 1 ? 1 : 0;
+                    for (int r = 0; r < NR; r++) s[v * NR + r] = val;
+                } else {
+                    uint64_t w = rng.next_u64();
+                    for (int r = 0; r < NR; r++) s[v * NR + r] = (int8_t)((w >> r) & 1);
+                }
+            }
+        }
+}
+
+// ultimate.rs:237-246
+static std::vector<double> geometric_temps(double tmax, double tmin, int nt) {
+    double f = nt > 1 ? std::pow(tmin / tmax, 1.0 / (double)(nt - 1)) : 1.0;
+    std::vector<double> t(nt);
+    for (int i = 0; i < nt; i++) t[i] = tmax * powi(f, i);
+    return t;
+}
+
+// ultimate.rs:397-430 (num_slices = 1)
+static void update_incumbent(const Qubo& m, Field& f, double& best_e, std::vector<int8_t>& best,
+                             std::vector<int8_t>& buf) {
+    int arg_c = 0, arg_r = 0;
+    double mn = std::numeric_limits<double>::infinity();
+    for (size_t c = 0; c < f.energies.size(); c++)
+        for (int r = 0; r < NR; r++)
+            if (f.energies[c][r] < mn) {
+                mn = f.energies[c][r];
+                arg_c = (int)c;
+                arg_r = r;
+            }
+    if (!std::isfinite(mn)) return;
+    const int8_t* s = f.cell(arg_c);
+    for (int64_t v = 0; v < f.n; v++) buf[v] = s[v * NR + arg_r];
+    double e = total_energy(m, buf.data());
+    if (e < best_e) {
+        best_e = e;
+        best = buf;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Presolve (src/presolve/mod.rs, src/presolve/qpbo.rs) and 1-opt polish
+// (src/solver/local_search.rs:19-57): needed only to reproduce the end-to-end
+// golden through UltimateSolver::solve.
+// ---------------------------------------------------------------------------
+using Assign = std::vector<std::pair<int64_t, int8_t>>;
+
+// presolve/mod.rs:54-105
+static std::vector<int8_t> first_order_fixpoint(const Qubo& m, const Assign& assumptions) {
+    const int64_t n = m.n;
+    std::vector<double> h = m.linear;
+    std::vector<int8_t> status(n, -1);
+    for (auto& a : assumptions) status[a.first] = a.second;
+    for (auto& a : assumptions)
+        if (a.second == 1)
+            for (int64_t k = m.row[a.first]; k < m.row[a.first + 1]; k++) h[m.col[k]] += m.val[k];
+    for (;;) {
+        bool changed = false;
+        for (int64_t i = 0; i < n; i++) {
+            if (status[i] >= 0) continue;
+            double lo = h[i], hi = h[i];
+            for (int64_t k = m.row[i]; k < m.row[i + 1]; k++)
+                if (status[m.col[k]] < 0) {
+                    double w = m.val[k];
+                    if (w < 0.0) lo += w;
+                    else hi += w;
+                }
+            if (lo >= 0.0) {
+                status[i] = 0;
+                changed = true;
+            } else if (hi <= 0.0) {
+                status[i] = 1;
+                for (int64_t k = m.row[i]; k < m.row[i + 1]; k++) h[m.col[k]] += m.val[k];
+                changed = true;
+            }
+        }
+        if (!changed) break;
+    }
+    return status;
+}
+
+static bool has_index(const Assign& a, int64_t i) {
+    for (auto& x : a)
+        if (x.first == i) return true;
+    return false;
+}
+
+// presolve/mod.rs:126-183
+static Assign probing(const Qubo& m, const Assign& clamped) {
+    const int64_t n = m.n;
+    std::vector<uint8_t> user(n, 0);
+    Assign assumptions = clamped;
+    for (auto& c : clamped) user[c.first] = 1;
+    for (;;) {
+        auto base = first_order_fixpoint(m, assumptions);
+        Assign newly;
+        Assign assumed;
+        for (int64_t i = 0; i < n; i++)
+            if (base[i] >= 0) assumed.push_back({i, base[i]});
+        for (int64_t i = 0; i < n; i++) {
+            if (base[i] >= 0) continue;
+            Assign a0 = assumed;
+            a0.push_back({i, 0});
+            auto b0 = first_order_fixpoint(m, a0);
+            Assign a1 = assumed;
+            a1.push_back({i, 1});
+            auto b1 = first_order_fixpoint(m, a1);
+            for (int64_t j = 0; j < n; j++) {
+                if (j == i || base[j] >= 0) continue;
+                if (b0[j] >= 0 && b1[j] >= 0 && b0[j] == b1[j] && !has_index(newly, j))
+                    newly.push_back({j, b0[j]});
+            }
+        }
+        size_t before = assumptions.size();
+        for (auto& x : assumed)
+            if (!has_index(assumptions, x.first)) assumptions.push_back(x);
+        for (auto& x : newly)
+            if (!has_index(assumptions, x.first)) assumptions.push_back(x);
+        if (assumptions.size() == before) break;
+    }
+    Assign out;
+    for (auto& x : assumptions)
+        if (!user[x.first]) out.push_back(x);
+    return out;
+}
+
+// qpbo.rs:43-140: Dinic max-flow on f64 capacities.
+struct Dinic {
+    int n;
+    std::vector<std::vector<int>> head;
+    std::vector<int> to;
+    std::vector<double> cap;
+    std::vector<int> level, it;
+    static constexpr double EPS = 1e-9;
+    explicit Dinic(int n_) : n(n_), head(n_), level(n_, 0), it(n_, 0) {}
+    void add_edge(int u, int v, double c) {
+        int e = (int)to.size();
+        to.push_back(v);
+        cap.push_back(c);
+        head[u].push_back(e);
+        to.push_back(u);
+        cap.push_back(0.0);
+        head[v].push_back(e + 1);
+    }
+    bool bfs(int s, int t) {
+        std::fill(level.begin(), level.end(), -1);
+        std::deque<int> q;
+        level[s] = 0;
+        q.push_back(s);
+        while (!q.empty()) {
+            int u = q.front();
+            q.pop_front();
+            for (int e : head[u])
+                if (cap[e] > EPS && level[to[e]] < 0) {
+                    level[to[e]] = level[u] + 1;
+                    q.push_back(to[e]);
+                }
+        }
+        return level[t] >= 0;
+    }
+    double dfs(int u, int t, double f) {
+        if (u == t) return f;
+        while (it[u] < (int)head[u].size()) {
+            int e = head[u][it[u]];
+            int v = to[e];
+            if (cap[e] > EPS && level[v] == level[u] + 1) {
+                double d = dfs(v, t, std::min(f, cap[e]));
+                if (d > EPS) {
+                    cap[e] -= d;
+                    cap[e ^ 1] += d;
+                    return d;
+                }
+            }
+            it[u]++;
+        }
+        return 0.0;
+    }
+    double max_flow(int s, int t) {
+        double flow = 0.0;
+        while (bfs(s, t)) {
+            std::fill(it.begin(), it.end(), 0);
+            for (;;) {
+                double f = dfs(s, t, std::numeric_limits<double>::infinity());
+                if (f <= EPS) break;
+                flow += f;
+            }
+        }
+        return flow;
+    }
+};
+
+static std::vector<uint8_t> bfs_reach(const std::vector<std::vector<int>>& adj, int s) {
+    std::vector<uint8_t> seen(adj.size(), 0);
+    std::deque<int> q;
+    seen[s] = 1;
+    q.push_back(s);
+    while (!q.empty()) {
+        int u = q.front();
+        q.pop_front();
+        for (int v : adj[u])
+            if (!seen[v]) {
+                seen[v] = 1;
+                q.push_back(v);
+            }
+    }
+    return seen;
+}
+
+// qpbo.rs:160-266
+static std::vector<int8_t> roof_duality(const Qubo& m) {
+    const int64_t n = m.n;
+    if (n == 0) return {};
+    const int src = (int)(2 * n), sink = (int)(2 * n + 1);
+    auto node_comp = [&](int lit) { return lit == src ? sink : (lit == sink ? src : (lit ^ 1)); };
+    Dinic g((int)(2 * n + 2));
+    double scale = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+        scale = std::max(scale, std::fabs(m.linear[i]));
+        for (int64_t k = m.row[i]; k < m.row[i + 1]; k++) scale = std::max(scale, std::fabs(m.val[k]));
+    }
+    if (!(scale > 0.0)) scale = 1.0;
+    const double EPS = Dinic::EPS;
+    auto add_quad = [&](int u, int v, double c) {
+        if (c > EPS) {
+            g.add_edge(u, node_comp(v), c);
+            g.add_edge(v, node_comp(u), c);
+        }
+    };
+    auto add_linear = [&](int u, double c) {
+        if (c >= 0.0) {
+            if (c > EPS) {
+                g.add_edge(u, sink, c);
+                g.add_edge(src, node_comp(u), c);
+            }
+        } else {
+            double cc = -c;
+            int ubar = node_comp(u);
+            g.add_edge(ubar, sink, cc);
+            g.add_edge(src, u, cc);
+        }
+    };
+    for (int64_t i = 0; i < n; i++) add_linear((int)(2 * i), m.linear[i] / scale);
+    for (int64_t i = 0; i < n; i++)
+        for (int64_t k = m.row[i]; k < m.row[i + 1]; k++) {
+            int64_t j = m.col[k];
+            if (i < j) {
+                double w = m.val[k] / scale;
+                if (w >= 0.0) {
+                    add_quad((int)(2 * i), (int)(2 * j), w);
+                } else {
+                    add_linear((int)(2 * i), w);
+                    add_quad((int)(2 * i), (int)(2 * j + 1), -w);
+                }
+            }
+        }
+    g.max_flow(src, sink);
+    std::vector<std::vector<int>> adj(g.n), radj(g.n);
+    for (int u = 0; u < g.n; u++)
+        for (int e : g.head[u])
+            if (g.cap[e] > EPS) adj[u].push_back(g.to[e]);
+    for (int u = 0; u < g.n; u++)
+        for (int v : adj[u]) radj[v].push_back(u);
+    auto in_s = bfs_reach(adj, src);
+    auto in_t = bfs_reach(radj, sink);
+    std::vector<int8_t> out(n, -1);
+    for (int64_t i = 0; i < n; i++) {
+        int p = (int)(2 * i), q = (int)(2 * i + 1);
+        if (in_s[p] && in_t[q]) out[i] = 1;
+        else if (in_t[p] && in_s[q]) out[i] = 0;
+    }
+    return out;
+}
+
+// presolve/mod.rs:328-381
+static Qubo reduce_by_clamps(const Qubo& m, const Assign& clamped, std::vector<int64_t>& free_map) {
+    const int64_t n = m.n;
+    std::vector<int8_t> cv(n, -1);
+    for (auto& c : clamped) cv[c.first] = c.second;
+    free_map.clear();
+    for (int64_t i = 0; i < n; i++)
+        if (cv[i] < 0) free_map.push_back(i);
+    std::vector<int64_t> g2l(n, -1);
+    for (size_t li = 0; li < free_map.size(); li++) g2l[free_map[li]] = (int64_t)li;
+    const int64_t mm = (int64_t)free_map.size();
+    Qubo r;
+    r.n = mm;
+    r.linear.assign(mm, 0.0);
+    std::vector<std::vector<std::pair<int64_t, double>>> rows(mm);
+    for (int64_t li = 0; li < mm; li++) {
+        int64_t gi = free_map[li];
+        double h = m.linear[gi];
+        for (int64_t k = m.row[gi]; k < m.row[gi + 1]; k++) {
+            int64_t j = m.col[k];
+            if (cv[j] < 0) {
+                if (g2l[j] >= 0) rows[li].push_back({g2l[j], m.val[k]});
+            } else if (cv[j] == 1) {
+                h += m.val[k];
+            }
+        }
+        r.linear[li] = h;
+    }
+    r.row.push_back(0);
+    for (auto& rw : rows) {
+        std::stable_sort(rw.begin(), rw.end(),
+                         [](const std::pair<int64_t, double>& a, const std::pair<int64_t, double>& b) {
+                             return a.first < b.first;
+                         });
+        for (auto& e : rw) {
+            r.col.push_back(e.first);
+            r.val.push_back(e.second);
+        }
+        r.row.push_back((int64_t)r.col.size());
+    }
+    return r;
+}
+
+// presolve/mod.rs:283-321
+static Assign full_presolve(const Qubo& m, const Assign& clamped) {
+    const int64_t n = m.n;
+    std::vector<uint8_t> user(n, 0);
+    for (auto& c : clamped) user[c.first] = 1;
+    Assign assumptions = clamped;
+    std::vector<int64_t> free_map;
+    Qubo red = reduce_by_clamps(m, clamped, free_map);
+    auto rd = roof_duality(red);
+    for (size_t li = 0; li < rd.size(); li++) {
+        if (rd[li] < 0) continue;
+        int64_t gi = free_map[li];
+        if (!user[gi] && !has_index(assumptions, gi)) assumptions.push_back({gi, rd[li]});
+    }
+    auto probed = probing(m, assumptions);
+    for (auto& x : probed)
+        if (!user[x.first] && !has_index(assumptions, x.first)) assumptions.push_back(x);
+    Assign out;
+    for (auto& x : assumptions)
+        if (!user[x.first]) out.push_back(x);
+    return out;
+}
+
+// presolve/mod.rs:194-219
+static std::vector<std::vector<int64_t>> connected_components(const Qubo& m,
+                                                              const std::vector<uint8_t>& active) {
+    const int64_t n = m.n;
+    std::vector<uint8_t> visited(n, 0);
+    std::vector<std::vector<int64_t>> comps;
+    std::vector<int64_t> stack;
+    for (int64_t s = 0; s < n; s++) {
+        if (!active[s] || visited[s]) continue;
+        std::vector<int64_t> comp;
+        visited[s] = 1;
+        stack.push_back(s);
+        while (!stack.empty()) {
+            int64_t v = stack.back();
+            stack.pop_back();
+            comp.push_back(v);
+            for (int64_t k = m.row[v]; k < m.row[v + 1]; k++) {
+                int64_t j = m.col[k];
+                if (m.val[k] != 0.0 && active[j] && !visited[j]) {
+                    visited[j] = 1;
+                    stack.push_back(j);
+                }
+            }
+        }
+        std::sort(comp.begin(), comp.end());
+        comps.push_back(comp);
+    }
+    return comps;
+}
+
+// presolve/mod.rs:228-270
+static Qubo extract_component(const Qubo& m, const std::vector<int64_t>& comp,
+                              const std::vector<uint8_t>& fixed_one) {
+    std::vector<int64_t> g2l(m.n, -1);
+    for (size_t li = 0; li < comp.size(); li++) g2l[comp[li]] = (int64_t)li;
+    Qubo r;
+    r.n = (int64_t)comp.size();
+    r.row.push_back(0);
+    for (int64_t gi : comp) {
+        double h = m.linear[gi];
+        for (int64_t k = m.row[gi]; k < m.row[gi + 1]; k++) {
+            int64_t j = m.col[k];
+            if (g2l[j] >= 0) {
+                r.col.push_back(g2l[j]);
+                r.val.push_back(m.val[k]);
+            } else if (fixed_one[j]) {
+                h += m.val[k];
+            }
+        }
+        r.linear.push_back(h);
+        r.row.push_back((int64_t)r.col.size());
+    }
+    r.offset = 0.0;
+    return r;
+}
+
+// local_search.rs:19-57
+static double one_opt(const Qubo& m, int8_t* state, const std::vector<uint8_t>& clamped) {
+    const int64_t n = m.n;
+    std::vector<double> gains(n);
+    for (int64_t i = 0; i < n; i++) {
+        double field = m.linear[i];
+        for (int64_t k = m.row[i]; k < m.row[i + 1]; k++) field += m.val[k] * (double)state[m.col[k]];
+        gains[i] = (1.0 - 2.0 * (double)state[i]) * field;
+    }
+    double total = 0.0;
+    for (;;) {
+        int64_t bi = -1;
+        double bg = -1e-12;
+        for (int64_t i = 0; i < n; i++)
+            if (!clamped[i] && gains[i] < bg) {
+                bi = i;
+                bg = gains[i];
+            }
+        if (bi < 0) return total;
+        total -= bg;
+        double dir = 1.0 - 2.0 * (double)state[bi];
+        state[bi] = (int8_t)(1 - state[bi]);
+        gains[bi] = -bg;
+        for (int64_t k = m.row[bi]; k < m.row[bi + 1]; k++) {
+            int64_t j = m.col[k];
+            gains[j] += (1.0 - 2.0 * (double)state[j]) * m.val[k] * dir;
+        }
+    }
+}
+
+struct SolverCfg {
+    double tmax, tmin;
+    int64_t sweeps, exchanges;
+    uint64_t seed;
+    int nt;
+    int threads;
+};
+
+// UltimateSolver::solve, ultimate.rs:138-387, PT path (num_pops = 1,
+// num_slices = 1, no GNN warm start, ICM / 2-opt / path relinking off as in
+// UltimateSolver::new).
+static std::vector<int8_t> solve(const Qubo& m, const Assign& clamped, const SolverCfg& cfg) {
+    const int64_t n = m.n;
+    ChaCha8Rng rng(cfg.seed);
+    std::vector<uint8_t> is_clamped(n, 0);
+    std::vector<int8_t> cval(n, 0);
+    for (auto& c : clamped) {
+        is_clamped[c.first] = 1;
+        cval[c.first] = c.second;
+    }
+    auto derived = full_presolve(m, clamped);
+    for (auto& d : derived) {
+        is_clamped[d.first] = 1;
+        cval[d.first] = d.second;
+    }
+    std::vector<uint8_t> free(n);
+    for (int64_t i = 0; i < n; i++) free[i] = !is_clamped[i];
+    auto comps = connected_components(m, free);
+    if (comps.size() > 1) {
+        std::vector<uint8_t> fixed_one(n, 0);
+        std::vector<int8_t> result(n, 0);
+        for (int64_t v = 0; v < n; v++)
+            if (is_clamped[v]) {
+                result[v] = cval[v];
+                fixed_one[v] = cval[v] == 1;
+            }
+        for (size_t ci = 0; ci < comps.size(); ci++) {
+            Qubo sub = extract_component(m, comps[ci], fixed_one);
+            SolverCfg sc = cfg;
+            sc.seed = cfg.seed + (uint64_t)ci + 1;
+            auto ss = solve(sub, {}, sc);
+            for (size_t li = 0; li < comps[ci].size(); li++) result[comps[ci][li]] = ss[li];
+        }
+        return result;
+    }
+    Field f(n, cfg.nt, 1);
+    auto temps = geometric_temps(cfg.tmax, cfg.tmin, cfg.nt);
+    init_field(f, is_clamped, cval, rng);
+    for (int t = 0; t < cfg.nt; t++) replica_energies(m, f.cell(t), f.energies[t].data());
+    StepScratch sc;
+    sc.attempts.assign(std::max(cfg.nt - 1, 0), 0);
+    sc.accepts.assign(std::max(cfg.nt - 1, 0), 0);
+    double inc_e = std::numeric_limits<double>::infinity();
+    std::vector<int8_t> inc(n, 0), buf(n, 0);
+    uint64_t counter = 0;
+    for (int64_t ex = 0; ex < cfg.exchanges; ex++) {
+        for (int64_t sw = 0; sw < cfg.sweeps; sw++) {
+            step(f, m, temps.data(), is_clamped, sc, rng, true, false, cfg.threads, nullptr);
+            counter++;
+            if (counter % 1000 == 0)
+                for (int t = 0; t < cfg.nt; t++) replica_energies(m, f.cell(t), f.energies[t].data());
+        }
+        update_incumbent(m, f, inc_e, inc, buf);
+    }
+    std::vector<int8_t> best(n, 0), rb((size_t)NR * n);
+    double best_e = std::numeric_limits<double>::infinity();
+    for (int t = 0; t < cfg.nt; t++) {
+        const int8_t* s = f.cell(t);
+        for (int64_t v = 0; v < n; v++)
+            for (int r = 0; r < NR; r++) rb[(size_t)r * n + v] = s[v * NR + r];
+        for (int r = 0; r < NR; r++) {
+            double e = total_energy(m, rb.data() + (size_t)r * n);
+            if (e < best_e) {
+                best_e = e;
+                std::copy(rb.begin() + (size_t)r * n, rb.begin() + (size_t)(r + 1) * n, best.begin());
+            }
+        }
+    }
+    if (inc_e < best_e) best = inc;
+    one_opt(m, best.data(), is_clamped);
+    return best;
+}
+
+static void pack_words(const Field& f, uint64_t* words) {
+    const int cells = f.nt * f.np;
+    for (int c = 0; c < cells; c++)
+        for (int64_t v = 0; v < f.n; v++) {
+            uint64_t w = 0;
+            const int8_t* s = f.spins.data() + ((size_t)c * f.n + v) * NR;
+            for (int r = 0; r < NR; r++) w |= (uint64_t)(s[r] & 1) << r;
+            words[(size_t)c * f.n + v] = w;
+        }
+}
+
+static void unpack_words(Field& f, const uint64_t* words) {
+    const int cells = f.nt * f.np;
+    for (int c = 0; c < cells; c++)
+        for (int64_t v = 0; v < f.n; v++) {
+            uint64_t w = words[(size_t)c * f.n + v];
+            int8_t* s = f.spins.data() + ((size_t)c * f.n + v) * NR;
+            for (int r = 0; r < NR; r++) s[r] = (int8_t)((w >> r) & 1);
+        }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C API (ctypes). Problems are passed as (n, linear, row_offsets, cols, vals,
+// offset) with int64 CSR indices, mirroring QuboModel/CsrMatrix.
+// ===========================================================================
+extern "C" {
+
+int or_abi_version() { return 3; }
+
+void or_chacha8_u64(uint64_t seed, uint64_t skip, uint64_t count, uint64_t* out) {
+    ChaCha8Rng r(seed);
+    for (uint64_t i = 0; i < skip; i++) r.next_u64();
+    for (uint64_t i = 0; i < count; i++) out[i] = r.next_u64();
+}
+
+void or_chacha8_block(const uint32_t* key, uint64_t counter, uint32_t* out) {
+    chacha8_block(key, counter, out);
+}
+
+void or_xoshiro_x8_f64(uint64_t seed, uint64_t calls, double* out) {
+    XoshiroX8 r(seed);
+    for (uint64_t c = 0; c < calls; c++) r.next_f64x8(out + 8 * c);
+}
+
+double or_fast_exp(double x) { return fast_exp(x); }
+
+void or_geometric_temps(double tmax, double tmin, int nt, double* out) {
+    auto t = geometric_temps(tmax, tmin, nt);
+    std::copy(t.begin(), t.end(), out);
+}
+
+// The seeded n=32 dense instance of tests/test_regression_golden.rs:25-57.
+// Writes 992 CSR entries (rows of 31) and 32 linear terms.
+void or_golden_instance(int64_t* row, int64_t* col, double* val, double* lin) {
+    const int n = 32;
+    ChaCha8Rng rng(0xC0FFEEULL);
+    std::vector<double> upper((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) upper[(size_t)i * n + j] = rng.gen_range(-1.0, 1.0);
+    int64_t k = 0;
+    row[0] = 0;
+    for (int i = 0; i < n; i++) {
+        for (int j = 0; j < n; j++)
+            if (i != j) {
+                col[k] = j;
+                val[k] = i < j ? upper[(size_t)i * n + j] : upper[(size_t)j * n + i];
+                k++;
+            }
+        row[i + 1] = k;
+    }
+    for (int i = 0; i < n; i++) lin[i] = rng.gen_range(-1.0, 1.0);
+}
+
+double or_total_energy(int64_t n, const double* lin, const int64_t* row, const int64_t* col,
+                       const double* val, double offset, const int8_t* state) {
+    Qubo m = make_qubo(n, lin, row, col, val, offset);
+    return total_energy(m, state);
+}
+
+// UltimateSolver::new(tmax, tmin, sweeps, exchanges, Some(seed)) with num_temps
+// = nt, then .solve(model, clamped). Writes n states; returns 0.
+int or_solve(int64_t n, const double* lin, const int64_t* row, const int64_t* col,
+             const double* val, double offset, double tmax, double tmin, int64_t sweeps,
+             int64_t exchanges, uint64_t seed, int nt, const int64_t* clamp_idx,
+             const int8_t* clamp_val, int64_t n_clamps, int threads, int8_t* state_out) {
+    Qubo m = make_qubo(n, lin, row, col, val, offset);
+    Assign cl;
+    for (int64_t i = 0; i < n_clamps; i++) cl.push_back({clamp_idx[i], clamp_val[i]});
+    SolverCfg cfg{tmax, tmin, sweeps, exchanges, seed, nt, threads};
+    auto s = solve(m, cl, cfg);
+    std::copy(s.begin(), s.end(), state_out);
+    return 0;
+}
+
+// full_presolve: writes derived (idx, val) fixings; returns their count.
+int64_t or_full_presolve(int64_t n, const double* lin, const int64_t* row, const int64_t* col,
+                         const double* val, const int64_t* clamp_idx, const int8_t* clamp_val,
+                         int64_t n_clamps, int64_t* out_idx, int8_t* out_val) {
+    Qubo m = make_qubo(n, lin, row, col, val, 0.0);
+    Assign cl;
+    for (int64_t i = 0; i < n_clamps; i++) cl.push_back({clamp_idx[i], clamp_val[i]});
+    auto d = full_presolve(m, cl);
+    for (size_t i = 0; i < d.size(); i++) {
+        out_idx[i] = d[i].first;
+        out_val[i] = d[i].second;
+    }
+    return (int64_t)d.size();
+}
+
+double or_one_opt(int64_t n, const double* lin, const int64_t* row, const int64_t* col,
+                  const double* val, int8_t* state, const uint8_t* clamped) {
+    Qubo m = make_qubo(n, lin, row, col, val, 0.0);
+    std::vector<uint8_t> cl(clamped, clamped + n);
+    return one_opt(m, state, cl);
+}
+
+// The PT/SA step loop of ultimate.rs:248-336 under a caller-given per-step
+// temperature schedule temps[step][nt] (a constant ladder repeated = the
+// reference's PT run; one temperature per step = an SA schedule).
+//   init_words: if non-null, [nt][n] u64 spin words used instead of the random
+//               init (the master stream then draws nothing for the init).
+//   exchange_interval: phase 2 runs after every k-th step (k = 1 is the reference).
+//   incumbent_every: if > 0, update_incumbent after every that many steps.
+// Outputs: words [nt][n], energies [nt][64] (tracked), swap attempts/accepts
+// [nt-1], draws = master-stream u64 position, base_seeds [steps] (optional),
+// incumbent energy and state (optional).
+int or_run_schedule(int64_t n, const double* lin, const int64_t* row, const int64_t* col,
+                    const double* val, int nt, const double* temps, int64_t steps, uint64_t seed,
+                    const uint64_t* init_words, const uint8_t* clamped, const int8_t* clamp_val,
+                    int64_t exchange_interval, int collect_stats, int64_t incumbent_every,
+                    int threads, uint64_t* words_out, double* energies_out, uint64_t* attempts_out,
+                    uint64_t* accepts_out, uint64_t* draws_out, uint64_t* base_seeds_out,
+                    double* inc_energy_out, int8_t* inc_state_out) {
+    Qubo m = make_qubo(n, lin, row, col, val, 0.0);
+    std::vector<uint8_t> isc(n, 0);
+    std::vector<int8_t> cv(n, 0);
+    if (clamped) {
+        for (int64_t i = 0; i < n; i++) {
+            isc[i] = clamped[i];
+            cv[i] = clamp_val ? clamp_val[i] : 0;
+        }
+    }
+    ChaCha8Rng rng(seed);
+    Field f(n, nt, 1);
+    if (init_words) unpack_words(f, init_words);
+    else init_field(f, isc, cv, rng);
+    for (int t = 0; t < nt; t++) replica_energies(m, f.cell(t), f.energies[t].data());
+    StepScratch sc;
+    sc.attempts.assign(std::max(nt - 1, 0), 0);
+    sc.accepts.assign(std::max(nt - 1, 0), 0);
+    if (exchange_interval < 1) exchange_interval = 1;
+    double inc_e = std::numeric_limits<double>::infinity();
+    std::vector<int8_t> inc(n, 0), buf(n, 0);
+    for (int64_t s = 0; s < steps; s++) {
+        bool ex = ((s + 1) % exchange_interval) == 0;
+        step(f, m, temps + (size_t)s * nt, isc, sc, rng, ex, collect_stats != 0, threads,
+             base_seeds_out ? base_seeds_out + s : nullptr);
+        if ((uint64_t)(s + 1) % 1000 == 0)
+            for (int t = 0; t < nt; t++) replica_energies(m, f.cell(t), f.energies[t].data());
+        if (incumbent_every > 0 && (s + 1) % incumbent_every == 0) update_incumbent(m, f, inc_e, inc, buf);
+    }
+    if (words_out) pack_words(f, words_out);
+    if (energies_out)
+        for (int t = 0; t < nt; t++)
+            for (int r = 0; r < NR; r++) energies_out[(size_t)t * NR + r] = f.energies[t][r];
+    if (attempts_out)
+        for (int t = 0; t + 1 < nt; t++) {
+            attempts_out[t] = sc.attempts[t];
+            accepts_out[t] = sc.accepts[t];
+        }
+    if (draws_out) *draws_out = rng.draws;
+    if (inc_energy_out) *inc_energy_out = inc_e;
+    if (inc_state_out) std::copy(inc.begin(), inc.end(), inc_state_out);
+    return 0;
+}
+
+// Recomputes per-replica energies of spin words [cells][n] (engine.rs:333-418).
+void or_replica_energies(int64_t n, const double* lin, const int64_t* row, const int64_t* col,
+                         const double* val, int cells, const uint64_t* words, double* out) {
+    Qubo m = make_qubo(n, lin, row, col, val, 0.0);
+    Field f(n, cells, 1);
+    unpack_words(f, words);
+    for (int c = 0; c < cells; c++) replica_energies(m, f.cell(c), out + (size_t)c * NR);
+}
+
+// Many independent single-cell SA runs in parallel over instances (the CPU
+// baseline for the batched configuration). Instance i has its CSR at
+// row_ptrs[i] etc. All share the temps schedule temps[steps]. Words out at
+// words_out + word_off[i]; energies at energies_out + 64*i.
+int or_run_sa_batch(int64_t count, const int64_t* ns, const double* const* lins,
+                    const int64_t* const* rows, const int64_t* const* cols,
+                    const double* const* vals, const uint64_t* seeds, const double* temps,
+                    int64_t steps, int threads, uint64_t* words_out, const int64_t* word_off,
+                    double* energies_out) {
+    parallel_for((int)count, threads, [&](int i) {
+        Qubo m = make_qubo(ns[i], lins[i], rows[i], cols[i], vals[i], 0.0);
+        std::vector<uint8_t> isc(m.n, 0);
+        std::vector<int8_t> cv(m.n, 0);
+        ChaCha8Rng rng(seeds[i]);
+        Field f(m.n, 1, 1);
+        init_field(f, isc, cv, rng);
+        replica_energies(m, f.cell(0), f.energies[0].data());
+        StepScratch sc;
+        for (int64_t s = 0; s < steps; s++) {
+            step(f, m, temps + s, isc, sc, rng, true, false, 1, nullptr);
+            if ((uint64_t)(s + 1) % 1000 == 0) replica_energies(m, f.cell(0), f.energies[0].data());
+        }
+        if (words_out) pack_words(f, words_out + word_off[i]);
+        if (energies_out)
+            for (int r = 0; r < NR; r++) energies_out[(size_t)i * NR + r] = f.energies[0][r];
+    });
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,42 @@
+"""The C-ABI library builds, loads and exports every function the header
+declares; host-only entry points behave without a GPU."""
+import ctypes as C
+
+import numpy as np
+
+from ising_engine_b200 import _build, _ffi
+from ising_engine_b200 import instances as I
+from ising_engine_b200.engine import _problem
+
+
+def test_library_exports_every_header_symbol():
+    L = _ffi.lib()
+    syms = _ffi.header_symbols()
+    assert len(syms) >= 25
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+    assert set(syms) == set(_ffi._SIGS), "bindings and header disagree"
+    assert L.ie_abi_version() == 1
+
+
+def test_library_is_in_tree():
+    assert _build.LIB_PATH.startswith(_build.HERE)
+
+
+def test_invalid_arguments_return_status_not_abort():
+    L = _ffi.lib()
+    assert L.ie_create(None, None, None) == 1  # IE_ERR_INVALID
+    assert b"NULL" in L.ie_last_error()
+    assert L.ie_geometric_temps(1.0, 0.1, 0, None) == 1
+
+
+def test_suggested_temp_range_matches_definition():
+    """src/solver/schedule.rs:21-43."""
+    m = I.maxcut_gnm(50, 200, 3)
+    from ising_engine_b200.engine import suggested_temp_range
+    tmax, tmin = suggested_temp_range(m)
+    ro, va, lin = m.row_offsets.astype(int), m.values, m.linear
+    ml = max(abs(lin[i]) + np.abs(va[ro[i]:ro[i + 1]]).sum() for i in range(m.num_vars))
+    mn = min(np.abs(lin[lin != 0]).min(), np.abs(va[va != 0]).min())
+    assert tmax == ml / np.log(2.0)
+    assert tmin == min(mn / np.log(100.0), tmax * 0.5)

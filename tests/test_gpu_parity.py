@@ -1,0 +1,202 @@
+"""Parity of the CUDA path with the CPU oracle, through the C ABI.
+
+Integer couplings: spin words, tracked energies, swap statistics, DEO phase
+and master-stream position must be bit-identical after k steps. The f64 mode
+runs the reference's f64 arithmetic in the reference's order, so the same
+bit-identity is asserted there too on these cases; the FP64 recompute check
+uses the stated relative tolerance 1e-6.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from ising_engine_b200 import instances as I
+from ising_engine_b200.core import CsrMatrix, QuboModel
+from ising_engine_b200.engine import BatchEngine, Engine, geometric_temps
+from ising_engine_b200.solver import UltimateSolver
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FP64_REL_TOL = 1e-6
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "regression_golden.json")))
+
+
+def assert_same_run(eng: Engine, ref, check_stats=True):
+    w = eng.spins()
+    assert w.shape == ref.words.shape
+    bad = np.nonzero((w != ref.words).any(axis=1))[0]
+    assert len(bad) == 0, f"spin words differ in cells {bad[:8]}"
+    e = eng.energies()
+    assert e.tobytes() == ref.energies.tobytes(), np.argwhere(e != ref.energies)[:8]
+    draws, _ = eng.rng_state()
+    assert draws == ref.draws
+    if check_stats and eng.num_temps > 1:
+        att, acc = eng.swap_stats()
+        assert (att == ref.swap_attempts).all()
+        assert (acc == ref.swap_accepts).all()
+
+
+def test_lattice_2d_single_cell_1000_sweeps():
+    """2D periodic +-J, L=32, one cell at beta=1, random init, 1000 sweeps."""
+    m = I.pm_j_lattice(32, 2, seed=2024)
+    ref = O.run_schedule(m, np.ones((1000, 1)), 11)
+    with Engine(m, num_temps=1, seed=11) as eng:
+        eng.init_random()
+        eng.step([1.0], 1000)
+        assert_same_run(eng, ref)
+    b = BatchEngine([m], [11])
+    b.init_random()
+    b.run_schedule(np.ones(1000))
+    assert (b.spins() == ref.words.reshape(-1)).all()
+    assert b.energies().tobytes() == ref.energies.tobytes()
+    assert int(b.draws()[0]) == ref.draws
+    b.close()
+
+
+@pytest.mark.parametrize("interval", [1, 3])
+def test_pt_maxcut_exchange(interval):
+    m = I.maxcut_gnm(96, 700, seed=3)
+    temps = I.geometric_beta_ladder(8, 0.1, 3.0)
+    steps = 61
+    ref = O.run_schedule(m, np.tile(temps, (steps, 1)), 77, exchange_interval=interval,
+                         collect_stats=True)
+    with Engine(m, num_temps=8, seed=77, exchange_interval=interval) as eng:
+        eng.init_random()
+        eng.step(temps, 20)
+        eng.step(temps, steps - 20)  # split calls continue the same trajectory
+        assert_same_run(eng, ref)
+        _, deo = eng.rng_state()
+        assert deo == (steps // interval) % 2
+
+
+def test_maxcut_800_pt32_interval10():
+    """The G(n=800, m=19176) Max-Cut ladder: 32 temperatures, beta geometric
+    0.1..3.0, exchange every 10 sweeps (a shortened run)."""
+    m = I.maxcut_gnm(800, 19176, seed=42)
+    temps = I.geometric_beta_ladder(32, 0.1, 3.0)
+    steps = 100
+    ref = O.run_schedule(m, np.tile(temps, (steps, 1)), 1337, exchange_interval=10,
+                         collect_stats=True, threads=8)
+    with Engine(m, num_temps=32, seed=1337, exchange_interval=10) as eng:
+        eng.init_random()
+        eng.step(temps, steps)
+        assert_same_run(eng, ref)
+
+
+def test_clamped_sites_int_and_f64():
+    rng = np.random.default_rng(9)
+    for integer in (True, False):
+        m = I.random_regular_qubo(60, 4, rng, integer=integer)
+        clamped = np.zeros(60, np.uint8)
+        clamped[[0, 7, 31, 59]] = 1
+        cval = np.zeros(60, np.int8)
+        cval[[0, 31]] = 1
+        temps = [2.0, 1.0, 0.5, 0.25]
+        ref = O.run_schedule(m, np.tile(temps, (40, 1)), 5, clamped=clamped, clamp_val=cval,
+                             collect_stats=True)
+        with Engine(m, num_temps=4, seed=5) as eng:
+            eng.set_clamps(clamped, cval)
+            eng.init_random()
+            eng.step(temps, 40)
+            assert_same_run(eng, ref)
+
+
+@pytest.mark.parametrize("hot,cold,seed,favourable", [(0, 1, 1, True), (1, 0, 2, False)])
+def test_swap_statistics_known_answers(hot, cold, seed, favourable):
+    """test_population_annealing.rs:354-420 on the device."""
+    m = QuboModel(1, np.array([10.0]), CsrMatrix(np.zeros(0), np.zeros(0, np.uint64),
+                                                 np.zeros(2, np.uint64)))
+    with Engine(m, num_temps=2, seed=seed) as eng:
+        eng.set_clamps(np.ones(1, np.uint8), np.array([hot], np.int8))
+        eng.set_spins(np.array([[~np.uint64(0) if hot else 0], [~np.uint64(0) if cold else 0]],
+                               dtype=np.uint64))
+        eng.step([2.0, 0.5], 1)
+        rate = eng.swap_acceptance_rates()[0]
+        draws, _ = eng.rng_state()
+    if favourable:
+        assert rate == 1.0 and draws == 1
+    else:
+        assert rate < 0.01 and draws == 65
+
+
+def test_uneven_batch_bit_exact_and_plain_equal():
+    models, seeds = I.uneven_batch(24, seed=7, n_max=600)
+    temps = I.sa_temps(60)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
+    b = BatchEngine(models, seeds)
+    b.init_random()
+    b.run_schedule(temps)
+    w = b.spins()
+    e = b.energies()
+    assert (w == words_ref).all()
+    assert e.tobytes() == ref_e.tobytes()
+    assert (b.draws() == np.array([m.num_vars + 60 for m in models], np.uint64)).all()
+    rec = b.recompute_energies()
+    rel = np.abs(rec - e) / np.maximum(np.abs(rec), 1.0)
+    assert rel.max() <= FP64_REL_TOL
+    b.close()
+    p = BatchEngine(models, seeds)
+    p.init_random()
+    p.run_schedule_plain(temps)
+    assert p.last_launches() == len(models)
+    assert (p.spins() == w).all()
+    assert p.energies().tobytes() == e.tobytes()
+    p.close()
+
+
+def test_f64_resync_across_1000_steps():
+    rng = np.random.default_rng(21)
+    m = I.random_regular_qubo(48, 6, rng, integer=False)
+    temps = I.sa_temps(1003, 0.2, 2.0)
+    ref = O.run_schedule(m, temps, 31)
+    with Engine(m, num_temps=1, seed=31) as eng:
+        eng.init_random()
+        eng.run_schedule(temps)
+        assert_same_run(eng, ref)
+    b = BatchEngine([m], [31])
+    b.init_random()
+    b.run_schedule(temps)
+    assert b.energies().tobytes() == ref.energies.tobytes()
+    b.close()
+
+
+def test_forced_f64_equals_integer_mode():
+    m = I.pm_j_lattice(8, 2, seed=4)
+    temps = I.geometric_beta_ladder(4, 0.3, 1.5)
+    out = []
+    for f in (False, True):
+        with Engine(m, num_temps=4, seed=8, force_f64=f) as eng:
+            eng.init_random()
+            eng.step(temps, 50)
+            out.append((eng.spins(), eng.energies(), eng.rng_state(), eng.swap_stats()))
+    assert (out[0][0] == out[1][0]).all()
+    assert out[0][1].tobytes() == out[1][1].tobytes()
+    assert out[0][2] == out[1][2]
+    assert all((a == b).all() for a, b in zip(out[0][3], out[1][3]))
+
+
+def test_golden_pt_trajectory_and_solve():
+    """UltimateSolver(50, 0.05, 30, 40, 2024) on the golden n=32 float
+    instance: the device PT loop matches the oracle step for step, and the
+    full solve returns the reference's golden state."""
+    lin, row, col, val = O.golden_instance()
+    m = QuboModel(32, lin, CsrMatrix(val, col.astype(np.uint64), row.astype(np.uint64)))
+    s = GOLDEN["solver"]
+    temps = geometric_temps(s["temp_max"], s["temp_min"], s["num_temps"])
+    steps = s["sweeps"] * s["exchanges"]
+    ref = O.run_schedule(m, np.tile(temps, (steps, 1)), s["seed"], incumbent_every=s["sweeps"],
+                         collect_stats=True)
+    solver = UltimateSolver(s["temp_max"], s["temp_min"], s["sweeps"], s["exchanges"], s["seed"])
+    with solver.engine(m) as eng:
+        eng.init_random()
+        eng.run_pt()
+        assert_same_run(eng, ref)
+        inc_e, inc_s = eng.incumbent()
+        assert inc_e == ref.incumbent_energy
+        assert (inc_s == ref.incumbent_state).all()
+    state = solver.solve(m)
+    assert state.tolist() == GOLDEN["golden_state"]
+    assert abs(m.calculate_total_energy(state) - GOLDEN["golden_energy"]) < GOLDEN["energy_tolerance"]
