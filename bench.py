@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Spin-flip attempts/s of the batched uneven-instance workload on B200.
+
+Workload (one "step"): 4096 random-regular QUBO instances, N log-uniform in
+[64, 4096], degree uniform in {3..16}, even-indexed instances with integer
+couplings in [-8, 8] (bit-exact integer mode), odd-indexed with float32
+N(0, 1) couplings widened to f64 (f64 mode), each run as one cell of 64
+replicas through an SA schedule with beta linear 0.1 -> 5.0 over 2000 sweeps,
+all in one persistent launch. Attempts = sum_i N_i * 64 * sweeps.
+
+  value : attempts/s with the problems resident in HBM (device time, CUDA
+          events on the library's stream, max over ranks).
+  e2e   : the same metric through the public API from host buffers: create
+          (host->device copy of the problems), init, run, read spins and
+          energies back (device->host), wall clock.
+  --impl reference : the CPU restatement of the reference's Rayon path (the
+          oracle), all host threads, on a bounded sample of the workload.
+
+Multi-GPU: replicas only; every rank runs its own batch (weak scaling), no
+collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "spin-flip attempts/s: batched vs plain GPU, same energies; serve p50/p99 ms"
+UNIT = "attempts/s"
+OPS_PER_ATTEMPT = 22  # algorithmic int32 ops per attempt: Xoshiro256++ step (20) + 64-bit compare (2)
+WORKLOAD = ("uneven batch: 4096 random-regular QUBO instances, N log-uniform [64,4096], degree "
+            "3..16, half integer couplings [-8,8], half float32 N(0,1); SA beta 0.1->5.0 over 2000 "
+            "sweeps; 64 replicas per instance")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--count", type=int, default=4096)
+    p.add_argument("--sweeps", type=int, default=2000)
+    p.add_argument("--seed", type=int, default=20260)
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--threads-per-block", type=int, default=0)
+    p.add_argument("--blocks-per-sm", type=int, default=0)
+    return p.parse_args()
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    def __init__(self, ws, rank, backend):
+        self.ws, self.rank = ws, rank
+        self.pg = None
+        if ws > 1:
+            import datetime
+
+            import torch.distributed as td
+            td.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+            self.td = td
+
+    def barrier(self):
+        if self.ws > 1:
+            self.td.barrier()
+
+    def max(self, x: float) -> float:
+        if self.ws == 1:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if self.ws == 1:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.ws > 1:
+            self.td.destroy_process_group()
+
+
+def make_workload(count, seed, sweeps):
+    """The seeded batch; cached as a pickle under $BENCH_CACHE when set."""
+    import pickle
+
+    from ising_engine_b200 import instances as I
+    cache = os.environ.get("BENCH_CACHE")
+    path = os.path.join(cache, f"batch_{count}_{seed}.pkl") if cache else None
+    if path and os.path.exists(path):
+        with open(path, "rb") as f:
+            models, seeds = pickle.load(f)
+    else:
+        models, seeds = I.uneven_batch(count, seed)
+        if path:
+            os.makedirs(cache, exist_ok=True)
+            with open(path, "wb") as f:
+                pickle.dump((models, seeds), f)
+    temps = I.sa_temps(sweeps)
+    return models, seeds, temps
+
+
+def attempts_of(models, sweeps):
+    return float(sum(m.num_vars for m in models)) * 64.0 * sweeps
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = []
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[4]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        loaded = [r for r in rows if r[2] >= 50.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in loaded for i, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in loaded),
+                "reasons": reasons, "samples": len(loaded)}
+
+
+def host_bytes(models):
+    """Bytes the library copies per problem (its device layout): rows u32,
+    cols u32, vals f64, lin f64, packed integer entries u32 and per-site
+    constants i32 for integer-mode problems, clamp flags/values u8."""
+    h2d = 0
+    for m in models:
+        n, nnz = m.num_vars, m.nnz
+        h2d += 4 * (n + 1) + 4 * nnz + 8 * nnz + 8 * n + 2 * n + 32 + 64
+        if m.is_integral():
+            h2d += 4 * nnz + 4 * n
+    return h2d
+
+
+def run_ours(args):
+    ws, rank, local = dist_setup()
+    dist = Dist(ws, rank, "gloo")
+    from ising_engine_b200 import _ffi
+    from ising_engine_b200.engine import BatchEngine
+
+    models, seeds, temps = make_workload(args.count, args.seed + 7919 * rank, args.sweeps)
+    attempts = attempts_of(models, args.sweeps)
+    eng = BatchEngine(models, seeds, device=local, threads_per_block=args.threads_per_block,
+                      blocks_per_sm=args.blocks_per_sm)
+    eng.init_random()
+    for _ in range(args.warmup):
+        eng.run_schedule(temps)
+    dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    dev_ms = 0.0
+    launches = 0
+    for _ in range(args.steps):
+        dev_ms += eng.run_schedule(temps)
+        launches += eng.last_launches()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    dist.barrier()
+    dev_s = dist.max(dev_ms / 1e3)
+    total_attempts = dist.sum(attempts * args.steps)
+    value = total_attempts / dev_s
+    per_launch_s = dev_ms / 1e3 / max(launches, 1)
+
+    # roofline: measured int32 ALU peak and Xoshiro step rate on this GPU
+    import ctypes as C
+    ip = C.c_double()
+    xp = C.c_double()
+    _ffi.check(_ffi.lib().ie_probe_peaks(local, C.byref(ip), C.byref(xp)))
+    achieved_ops = attempts / per_launch_s * OPS_PER_ATTEMPT
+    # algorithmic bytes per launch: each sweep reads the CSR row entries
+    # (4 B integer / 12 B f64 per entry), the per-site constants, and reads and
+    # writes each spin word once per sweep (8 + 8 B), nothing cached.
+    alg_bytes = 0.0
+    for m in models:
+        per_entry = 4 if m.is_integral() else 12
+        alg_bytes += args.sweeps * (m.nnz * per_entry + m.num_vars * (8 + 16 + 4))
+    hbm_peak = None
+    try:
+        hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except Exception:
+        hbm_peak = 6650.0
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "batch_sa_kernel_traffic.json")
+    if os.path.exists(prof):
+        try:
+            t = json.load(open(prof))
+            traffic = t["dram_bytes_per_attempt"] * attempts
+        except Exception:
+            traffic = None
+
+    plain = None
+    if not args.no_plain and rank == 0:
+        order = np.argsort([m.num_vars for m in models])
+        pick = [int(order[i]) for i in np.linspace(0, len(order) - 1, 12).astype(int)]
+        sub = [models[i] for i in pick]
+        pe = BatchEngine(sub, seeds[pick], device=local)
+        pe.init_random()
+        pt = temps[:100]
+        pe.run_schedule_plain(pt[:5])
+        ms = pe.run_schedule_plain(pt)
+        plain = {"value": attempts_of(sub, len(pt)) / (ms / 1e3), "unit": UNIT,
+                 "sample": f"{len(sub)} instances spread over the size range, {len(pt)} sweeps each, "
+                           "one launch per instance in sequence",
+                 "launches": pe.last_launches()}
+        pe.close()
+
+    e2e = None
+    if not args.no_e2e:
+        ts = []
+        for _ in range(max(1, min(args.steps, 2))):
+            dist.barrier()
+            t1 = time.perf_counter()
+            b = BatchEngine(models, seeds, device=local)
+            b.init_random()
+            b.run_schedule(temps)
+            w = b.spins()
+            e = b.energies()
+            b.close()
+            ts.append(time.perf_counter() - t1)
+        e2e_s = dist.max(float(np.mean(ts)))
+        e2e = {"value": dist.sum(attempts) / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(host_bytes(models)),
+               "d2h_bytes_per_step": int(w.nbytes + e.nbytes)}
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and ws == 1:
+        cpu = cpu_baseline(models, seeds, temps)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "i32+f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "instances": len(models), "sweeps": args.sweeps,
+                       "replicas": 64, "sites": int(sum(m.num_vars for m in models)),
+                       "couplings": int(sum(m.nnz for m in models)),
+                       "l2": "inputs larger than L2 (problem data %.0f MB per GPU)" % (host_bytes(models) / 1e6),
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": {"bound": "alu", "achieved": achieved_ops / 1e9, "peak": ip.value / 1e9,
+                         "unit": "Gop/s", "frac": achieved_ops / ip.value, "traffic": traffic,
+                         "ops_per_attempt": OPS_PER_ATTEMPT,
+                         "peak_source": "measured in-run: int32 LOP3/IADD3 microkernel (ie_probe_peaks)",
+                         "xoshiro_sol_attempts_per_s": xp.value,
+                         "frac_of_xoshiro_sol": (attempts / per_launch_s) / xp.value,
+                         "hbm": {"achieved_gbs": alg_bytes / per_launch_s / 1e9, "peak_gbs": hbm_peak,
+                                 "frac": alg_bytes / per_launch_s / 1e9 / hbm_peak,
+                                 "alg_bytes_per_launch": alg_bytes}},
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "plain": plain,
+            "batched_over_plain": (value / ws / plain["value"]) if plain else None,
+            "wall_s_timed": wall,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    eng.close()
+    dist.close()
+
+
+def cpu_sample(models, seeds, temps):
+    order = np.arange(len(models))
+    stride = max(1, len(models) // 64)
+    return [int(i) for i in order[::stride]]
+
+
+def cpu_baseline(models, seeds, temps):
+    """The oracle (C++ restatement of the reference's Rayon path) on a bounded
+    sample of the workload (every 64th instance, full schedule), dynamically
+    scheduled over instances on every host core."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    pick = cpu_sample(models, seeds, temps)
+    sub = [models[i] for i in pick]
+    t0 = time.perf_counter()
+    O.run_sa_batch(sub, seeds[pick], temps, threads=cores, want_words=False)
+    dt = time.perf_counter() - t0
+    return {"value": attempts_of(sub, len(temps)) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(sub)} of {len(models)} instances (every {len(models) // len(pick)}th), full "
+                      f"{len(temps)}-sweep schedule, parallel over instances"}
+
+
+def run_reference(args):
+    ws, rank, local = dist_setup()
+    if rank != 0:
+        return
+    models, seeds, temps = make_workload(args.count, args.seed, args.sweeps)
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    pick = cpu_sample(models, seeds, temps)
+    # one step = a fixed sample sized to about a few seconds of host work
+    per_step = pick[: max(cores, min(len(pick), 2 * cores))]
+    sub = [models[i] for i in per_step]
+    ss = seeds[per_step]
+    for _ in range(args.warmup):
+        O.run_sa_batch(sub, ss, temps, threads=cores, want_words=False)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.run_sa_batch(sub, ss, temps, threads=cores, want_words=False)
+    dt = time.perf_counter() - t0
+    value = attempts_of(sub, len(temps)) * args.steps / dt
+    sample = (f"{len(sub)} of {len(models)} instances (every {len(models) // len(pick)}th), full "
+              f"{len(temps)}-sweep schedule per step, parallel over instances")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "i32+f64", "data": "synthetic (seeded)",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "instances": len(models), "sweeps": args.sweeps,
+                       "replicas": 64, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -159,6 +159,12 @@ ie_status ie_batch_last_run_ms(ie_batch* b, double* ms);
 /* Number of kernel launches the last run call issued. */
 ie_status ie_batch_last_launches(ie_batch* b, uint64_t* launches);
 
+/* ---- measurement helper (no reference counterpart) ----
+ * Measured roofline denominators on `device`: int32 LOP3/IADD3 throughput
+ * (ops/s) and Xoshiro256++ step+compare throughput (outputs/s), the per-attempt
+ * work the bit-exact sweep cannot avoid. */
+ie_status ie_probe_peaks(int32_t device, double* int_ops_per_s, double* xoshiro_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -995,4 +995,13 @@ ie_status ie_batch_last_launches(ie_batch* b, uint64_t* launches) {
     return IE_OK;
 }
 
+ie_status ie_probe_peaks(int32_t device, double* int_ops_per_s, double* xoshiro_per_s) {
+    if (!int_ops_per_s || !xoshiro_per_s) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    IE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    IE_CUDA(probe_peaks(sms, int_ops_per_s, xoshiro_per_s));
+    return IE_OK;
+}
+
 }  // extern "C"

@@ -572,6 +572,79 @@ __global__ void incumbent_kernel(DevArrays A, uint32_t inst, double offset, doub
 }
 
 // ---------------------------------------------------------------------------
+// Peak probes for the roofline denominators (measured, not part of the path).
+// alu_probe: independent chains of 3-input LOP3 / IADD3 on 32-bit registers,
+// 16 ops per chain per iteration (8 chains per thread).
+// xoshiro_probe: 4 independent Xoshiro256++ lanes per thread, each output
+// compared against a threshold (the per-attempt work the sweep cannot avoid).
+// ---------------------------------------------------------------------------
+__global__ void alu_probe_kernel(uint32_t seed, int iters, uint32_t* out) {
+    uint32_t a[8], b = seed ^ threadIdx.x, c = seed * 7u + blockIdx.x;
+#pragma unroll
+    for (int i = 0; i < 8; i++) a[i] = seed + i * 0x9E3779B9u + threadIdx.x;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                asm volatile("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(a[i]) : "r"(b), "r"(c));
+                asm volatile("add.u32 %0, %0, %1;" : "+r"(a[i]) : "r"(c));
+            }
+        }
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) x ^= a[i];
+    if (x == 0x12345678u) out[0] = x;
+}
+
+__global__ void xoshiro_probe_kernel(uint64_t seed, int iters, uint64_t thr, uint32_t* out) {
+    Xoshiro x[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) x[i].seed_lane(seed + blockIdx.x * 1024 + threadIdx.x, i);
+    uint32_t acc = 0;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc += x[i].next() <= thr;
+    }
+    if (acc == 0xFFFFFFFFu) out[0] = acc;
+}
+
+cudaError_t probe_peaks(int sm_count, double* int_ops_per_s, double* xoshiro_per_s) {
+    uint32_t* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(uint32_t));
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sm_count * 8, threads = 256;
+    float best_alu = 1e30f, best_xo = 1e30f;
+    const int it_alu = 4096, it_xo = 8192;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(a);
+        alu_probe_kernel<<<blocks, threads>>>(1u + rep, it_alu, d);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms;
+        cudaEventElapsedTime(&ms, a, b);
+        best_alu = ms < best_alu ? ms : best_alu;
+        cudaEventRecord(a);
+        xoshiro_probe_kernel<<<blocks, threads>>>(7ULL + rep, it_xo, 0x8000000000000000ULL, d);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        best_xo = ms < best_xo ? ms : best_xo;
+    }
+    e = cudaGetLastError();
+    *int_ops_per_s = (double)blocks * threads * it_alu * 8.0 * 16.0 / (best_alu * 1e-3);
+    *xoshiro_per_s = (double)blocks * threads * it_xo * 4.0 / (best_xo * 1e-3);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    return e;
+}
+
+// ---------------------------------------------------------------------------
 // Host-side launch wrappers (declared in ie_launch.h).
 // ---------------------------------------------------------------------------
 cudaError_t set_smem_limits(size_t batch_bytes, size_t pt_bytes) {
