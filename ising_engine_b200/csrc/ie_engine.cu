@@ -236,12 +236,74 @@ ie_status build_xtables(const double* temps, uint32_t nt, XTables& X) {
     return IE_OK;
 }
 
+// Appends the chunk-packed site-record stream of one instance (layout in
+// ie_kernels.cuh); the stream starts and ends on a chunk boundary.
+ie_status build_records(const HostInst& h, const std::vector<uint8_t>& clampf, size_t site0,
+                        std::vector<uint32_t>& out, uint64_t& off, uint64_t& len) {
+    off = out.size();
+    uint32_t c = 0;
+    std::vector<uint32_t> rec;
+    auto emit = [&](const std::vector<uint32_t>& r) {
+        if (c + r.size() > kChunk) {
+            out.push_back(kRecPad);
+            while (out.size() % kChunk) out.push_back(0);
+            c = 0;
+        }
+        out.insert(out.end(), r.begin(), r.end());
+        c = (uint32_t)((c + r.size()) % kChunk);
+    };
+    for (uint32_t v = 0; v < h.n; v++) {
+        const uint32_t beg = h.rows[v], end = h.rows[v + 1];
+        const bool clamp = clampf[site0 + v] != 0;
+        if (clamp) {
+            emit({kRecClamp, 0, 0, 0});
+            continue;
+        }
+        uint32_t e0 = beg;
+        do {
+            const uint32_t deg = std::min<uint32_t>(end - e0, kRecMaxDeg);
+            const uint32_t deg4 = (deg + 3u) & ~3u;
+            const uint32_t cont = (e0 + deg < end) ? kRecCont : 0u;
+            rec.clear();
+            if (h.mode == kModeInt) {
+                rec.push_back(deg | cont | ((uint32_t)(h.linp[v] + 128) << 16));
+                rec.push_back(0);
+                rec.push_back(0);
+                rec.push_back(0);
+                for (uint32_t e = 0; e < deg4; e++) rec.push_back(e < deg ? h.ents[e0 + e] : 0u);
+            } else {
+                uint32_t w2[2];
+                rec.push_back(deg | cont);
+                rec.push_back(0);
+                std::memcpy(w2, &h.lin[v], 8);
+                rec.push_back(w2[0]);
+                rec.push_back(w2[1]);
+                for (uint32_t e = 0; e < deg4; e++) rec.push_back(e < deg ? h.cols[e0 + e] : 0u);
+                for (uint32_t e = 0; e < deg4; e++) {
+                    const double w = e < deg ? h.vals[e0 + e] : 0.0;
+                    std::memcpy(w2, &w, 8);
+                    rec.push_back(w2[0]);
+                    rec.push_back(w2[1]);
+                }
+            }
+            emit(rec);
+            e0 += deg;
+        } while (e0 < end);
+    }
+    if (c != 0 || out.size() == off) {
+        if (c != 0) out.push_back(kRecPad);
+        while (out.size() % kChunk || out.size() == off) out.push_back(0);
+    }
+    len = out.size() - off;
+    return IE_OK;
+}
+
 int g_sm_count = -1;
 
 struct Engine {
     int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     uint32_t count = 0;
     uint32_t nt = 1;
     std::vector<InstDesc> desc;
@@ -253,7 +315,7 @@ struct Engine {
     int32_t maxH = 0;
 
     DevBuf<InstDesc> d_desc;
-    DevBuf<uint32_t> d_rows, d_ents, d_cols, d_keys, d_quads, d_queue, d_draw_idx, d_unclamped;
+    DevBuf<uint32_t> d_rows, d_ents, d_cols, d_keys, d_queue, d_draw_idx, d_unclamped, d_recs;
     DevBuf<int32_t> d_linp, d_Ei, d_deo, d_err;
     DevBuf<double> d_vals, d_lin, d_Ef, d_temps, d_dbeta, d_scratch;
     DevBuf<uint8_t> d_clampf;
@@ -261,7 +323,8 @@ struct Engine {
     DevBuf<uint64_t> d_spins, d_pos, d_att, d_acc, d_xtab, d_xoff, d_xdmax, d_xdund;
 
     uint64_t steps_done = 0;
-    uint32_t nquads = 0;
+    bool quads_built = false;
+    bool recs_dirty = true;
     double last_ms = 0.0;
     uint64_t last_launches = 0;
     uint32_t threads_per_block = 0, blocks_per_sm = 0;
@@ -272,7 +335,13 @@ struct Engine {
         if (device >= 0) cudaSetDevice(device);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev2) cudaEventDestroy(ev2);
         if (stream) cudaStreamDestroy(stream);
+        if (stream2) cudaStreamDestroy(stream2);
+        for (int i = 0; i < 6; i++) {
+            if (cstreams[i]) cudaStreamDestroy(cstreams[i]);
+            if (cevents[i]) cudaEventDestroy(cevents[i]);
+        }
     }
 
     DevArrays arrays() const {
@@ -286,6 +355,7 @@ struct Engine {
         A.lin = d_lin.p;
         A.clampf = d_clampf.p;
         A.clampv = d_clampv.p;
+        A.recs = d_recs.p;
         A.keys = d_keys.p;
         A.spins = d_spins.p;
         A.Ei = d_Ei.p;
@@ -305,8 +375,10 @@ struct Engine {
         if (dev < 0 || dev >= ndev) return fail(IE_ERR_INVALID, "invalid CUDA device ordinal");
         IE_CUDA(cudaSetDevice(dev));
         IE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        IE_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
         IE_CUDA(cudaEventCreate(&ev0));
         IE_CUDA(cudaEventCreate(&ev1));
+        IE_CUDA(cudaEventCreate(&ev2));
         if (g_sm_count < 0) IE_CUDA(cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev));
         return IE_OK;
     }
@@ -389,7 +461,7 @@ struct Engine {
         IE_TRY(d_att.upload(zstat, stream));
         IE_TRY(d_acc.upload(zstat, stream));
         IE_TRY(d_err.upload(std::vector<int32_t>(1, 0), stream));
-        IE_TRY(d_queue.alloc(1));
+        IE_TRY(d_queue.alloc(6));
         IE_TRY(d_scratch.alloc(std::max<size_t>((size_t)nt * kReplicas, 1)));
         IE_TRY(upload_draw_idx());
         IE_CUDA(cudaStreamSynchronize(stream));
@@ -421,6 +493,18 @@ struct Engine {
         IE_CUDA(cudaMemcpyAsync(d_clampv.p, clampv.data(), clampv.size(), cudaMemcpyHostToDevice, stream));
         IE_TRY(upload_draw_idx());
         IE_CUDA(cudaStreamSynchronize(stream));
+        recs_dirty = true;
+        return IE_OK;
+    }
+
+    ie_status build_record_streams() {
+        std::vector<uint32_t> recs;
+        for (uint32_t i = 0; i < count; i++) IE_TRY(build_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].rec_len));
+        recs.resize(recs.size() + kChunk, 0);
+        IE_TRY(d_recs.upload(recs, stream));
+        IE_CUDA(cudaMemcpyAsync(d_desc.p, desc.data(), desc.size() * sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
+        IE_CUDA(cudaStreamSynchronize(stream));
+        recs_dirty = false;
         return IE_OK;
     }
 
@@ -433,116 +517,193 @@ struct Engine {
         return IE_OK;
     }
 
-    size_t batch_smem(int block) const { return (size_t)(block / 8) * (2 * maxH + 1) * sizeof(uint64_t); }
-
-    // Orders instances longest-first into quads of similar size and degree
-    // (same mode) so the four groups of a warp stay in step.
-    void build_quads() {
-        std::vector<uint32_t> order(count);
-        std::iota(order.begin(), order.end(), 0u);
-        auto degree = [&](uint32_t i) {
-            return insts[i].n ? (uint32_t)((insts[i].cols.size() + insts[i].n / 2) / insts[i].n) : 0u;
-        };
-        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-            if (desc[a].mode != desc[b].mode) return desc[a].mode > desc[b].mode;
-            if (degree(a) != degree(b)) return degree(a) > degree(b);
-            return desc[a].n > desc[b].n;
-        });
-        std::vector<std::vector<uint32_t>> quads;
-        for (size_t i = 0; i < order.size();) {
-            std::vector<uint32_t> q;
-            const uint32_t m = desc[order[i]].mode, dg = degree(order[i]);
-            while (q.size() < 4 && i < order.size() && desc[order[i]].mode == m && degree(order[i]) == dg)
-                q.push_back(order[i++]);
-            quads.push_back(q);
-        }
-        auto work = [&](const std::vector<uint32_t>& q) {
-            double w = 0;
-            for (uint32_t i : q) {
-                const double c = (double)insts[i].n * ((double)insts[i].cols.size() / std::max(1u, insts[i].n) + 8.0) *
-                                 (desc[i].mode == kModeF64 ? 3.0 : 1.0);
-                w = std::max(w, c);
-            }
-            return w;
-        };
-        std::stable_sort(quads.begin(), quads.end(),
-                         [&](const std::vector<uint32_t>& a, const std::vector<uint32_t>& b) { return work(a) > work(b); });
-        std::vector<uint32_t> flat;
-        for (auto& q : quads)
-            for (int k = 0; k < 4; k++) flat.push_back(k < (int)q.size() ? q[k] : 0xffffffffu);
-        nquads = (uint32_t)quads.size();
-        d_quads.upload(flat, stream);
+    static double inst_work(const HostInst& h) {
+        const double deg = h.n ? (double)h.cols.size() / h.n : 0.0;
+        return (double)h.n * (deg + 12.0) * (h.mode == kModeF64 ? 2.5 : 1.0);
     }
 
-    // Runs temps[steps] on every single-cell instance in one persistent launch.
+    // Work classes: (mode, TPL) with TPL threads per Xoshiro lane; the largest
+    // instances get more threads so their sequential site chain is shorter.
+    static constexpr int kTpls[3] = {1, 2, 4};
+    // size thresholds of the thread classes per mode: n > n4 -> 4 threads per
+    // lane, n > n2 -> 2, else 1 (set by the autotuner)
+    uint32_t tune_n4[2] = {1536, 768}, tune_n2[2] = {512, 256};
+    uint32_t nitems[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    uint32_t spin_cap[2][3] = {{64, 64, 64}, {64, 64, 64}};
+    double class_work[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    DevBuf<uint32_t> d_items[2][3];
+    DevBuf<int32_t> d_itemh[2][3];
+    cudaStream_t cstreams[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t cevents[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+
+    ie_status ensure_class_streams() {
+        for (int i = 0; i < 6; i++) {
+            if (!cstreams[i]) IE_CUDA(cudaStreamCreateWithFlags(&cstreams[i], cudaStreamNonBlocking));
+            if (!cevents[i]) IE_CUDA(cudaEventCreateWithFlags(&cevents[i], cudaEventDisableTiming));
+        }
+        return IE_OK;
+    }
+
+    int tpl_class(uint32_t i) const {
+        const uint32_t n = desc[i].n, m = desc[i].mode;
+        if (n > tune_n4[m]) return 2;
+        if (n > tune_n2[m]) return 1;
+        return 0;
+    }
+
+    // Per class: instances ordered by degree then size into items of 4/TPL
+    // (the groups of a warp stay in step sweep by sweep), items ordered by
+    // work, longest first.
+    ie_status build_quads() {
+        for (uint32_t mode = 0; mode < 2; mode++)
+            for (int ci = 0; ci < 3; ci++) {
+                const int ng = 4 / kTpls[ci];
+                std::vector<uint32_t> order;
+                for (uint32_t i = 0; i < count; i++)
+                    if (desc[i].mode == mode && tpl_class(i) == ci) order.push_back(i);
+                auto degree = [&](uint32_t i) {
+                    return insts[i].n ? (uint32_t)((insts[i].cols.size() + insts[i].n / 2) / insts[i].n) : 0u;
+                };
+                std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+                    if (degree(a) != degree(b)) return degree(a) > degree(b);
+                    return desc[a].n > desc[b].n;
+                });
+                std::vector<std::vector<uint32_t>> items;
+                for (size_t i = 0; i < order.size();) {
+                    std::vector<uint32_t> q;
+                    const uint32_t dg = degree(order[i]);
+                    while ((int)q.size() < ng && i < order.size() && degree(order[i]) == dg) q.push_back(order[i++]);
+                    items.push_back(q);
+                }
+                auto work = [&](const std::vector<uint32_t>& q) {
+                    double w = 0;
+                    for (uint32_t i : q) w = std::max(w, inst_work(insts[i]));
+                    return w;
+                };
+                std::stable_sort(items.begin(), items.end(), [&](const std::vector<uint32_t>& a,
+                                                                 const std::vector<uint32_t>& b) { return work(a) > work(b); });
+                std::vector<uint32_t> flat;
+                std::vector<int32_t> qh;
+                class_work[mode][ci] = 0;
+                uint32_t cap = 64;
+                for (uint32_t i : order) cap = std::max(cap, (desc[i].n + 63u) & ~63u);
+                spin_cap[mode][ci] = cap;
+                for (auto& q : items) {
+                    int32_t hh = 0;
+                    for (int k = 0; k < 4; k++) {
+                        flat.push_back(k < (int)q.size() ? q[k] : 0xffffffffu);
+                        if (k < (int)q.size()) hh = std::max(hh, desc[q[k]].H);
+                    }
+                    qh.push_back(hh);
+                    class_work[mode][ci] += work(q) * (double)q.size() * kTpls[ci];
+                }
+                nitems[mode][ci] = (uint32_t)items.size();
+                if (flat.empty()) {
+                    flat.assign(4, 0xffffffffu);
+                    qh.assign(1, 0);
+                }
+                IE_TRY(d_items[mode][ci].upload(flat, stream));
+                IE_TRY(d_itemh[mode][ci].upload(qh, stream));
+            }
+        quads_built = true;
+        return IE_OK;
+    }
+
+    RunArgs sa_args(uint64_t steps) const {
+        RunArgs R{};
+        R.temps = d_temps.p;
+        R.temps_per_step = 1;
+        R.steps = (uint32_t)steps;
+        R.step_base = steps_done;
+        R.exchange_interval = 1;
+        return R;
+    }
+
+    // Runs temps[steps] on every single-cell instance: one persistent launch
+    // per work class, all in flight together on their own streams.
     ie_status run_batch(const double* temps, uint64_t steps) {
         if (nt != 1) return fail(IE_ERR_INVALID, "batched runs need single-cell instances");
         if (!initialized) return fail(IE_ERR_INVALID, "call init_random before running");
         if (steps == 0) return IE_OK;
         if (steps > 0xffffffffULL) return fail(IE_ERR_INVALID, "too many steps in one call");
-        if (!nquads) build_quads();
+        if (recs_dirty) IE_TRY(build_record_streams());
+        if (!quads_built) IE_TRY(build_quads());
+        IE_TRY(ensure_class_streams());
         std::vector<double> t(temps, temps + steps);
         for (double x : t)
             if (!(x > 0.0) || !std::isfinite(x)) return fail(IE_ERR_INVALID, "temperatures must be positive");
         IE_TRY(d_temps.upload(t, stream));
-        int block = threads_per_block ? (int)threads_per_block : 128;
-        const size_t smem = batch_smem(block);
-        IE_CUDA(set_smem_limits(std::max<size_t>(smem, 48 * 1024), pt_smem_cap()));
-        int occ = batch_occupancy(block, smem);
-        if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
-        if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
-        const int warps_per_block = block / 32;
-        const int want = (int)((nquads + warps_per_block - 1) / warps_per_block);
-        const int grid = std::max(1, std::min(want, occ * g_sm_count));
-        RunArgs R{};
-        R.temps = d_temps.p;
-        R.temps_per_step = 1;
-        R.steps = (uint32_t)steps;
-        R.step_base = steps_done;
-        R.exchange_interval = 1;
-        R.quads = d_quads.p;
-        R.nquads = nquads;
-        R.queue = d_queue.p;
-        IE_CUDA(cudaMemsetAsync(d_queue.p, 0, sizeof(uint32_t), stream));
+        double wsum = 0;
+        for (int m = 0; m < 2; m++)
+            for (int ci = 0; ci < 3; ci++) wsum += class_work[m][ci];
+        IE_CUDA(cudaMemsetAsync(d_queue.p, 0, 6 * sizeof(uint32_t), stream));
         IE_CUDA(cudaEventRecord(ev0, stream));
-        IE_CUDA(launch_batch_sa(arrays(), R, grid, block, 2 * maxH + 1, smem, stream));
+        uint64_t launches = 0;
+        for (uint32_t m = 0; m < 2; m++)
+            for (int ci = 0; ci < 3; ci++) {
+                const int k = 3 * (int)m + ci;
+                if (!nitems[m][ci]) continue;
+                IE_CUDA(cudaStreamWaitEvent(cstreams[k], ev0, 0));
+                const int occ = batch_occupancy(m, kTpls[ci], spin_cap[m][ci]);
+                if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
+                const double share = wsum > 0 ? class_work[m][ci] / wsum : 1.0;
+                int per_sm = std::max(1, (int)std::ceil(occ * share));
+                if (blocks_per_sm) per_sm = (int)blocks_per_sm;
+                const int grid = std::max(1, std::min<int>((int)nitems[m][ci], per_sm * g_sm_count));
+                RunArgs R = sa_args(steps);
+                R.quads = d_items[m][ci].p;
+                R.quad_h = d_itemh[m][ci].p;
+                R.nquads = nitems[m][ci];
+                R.queue = d_queue.p + k;
+                IE_CUDA(launch_batch(arrays(), R, m, kTpls[ci], spin_cap[m][ci], grid, cstreams[k]));
+                IE_CUDA(cudaEventRecord(cevents[k], cstreams[k]));
+                IE_CUDA(cudaStreamWaitEvent(stream, cevents[k], 0));
+                launches++;
+            }
         IE_CUDA(cudaEventRecord(ev1, stream));
         IE_CUDA(cudaEventSynchronize(ev1));
         float ms = 0;
         IE_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
         last_ms = ms;
-        last_launches = 1;
+        last_launches = launches;
         steps_done += steps;
         return IE_OK;
     }
 
-    // The plain method: one launch per instance, in sequence.
+    // The plain method: one launch per instance, in sequence, on one stream
+    // (eight threads per instance, the reference's lane count).
     ie_status run_plain(const double* temps, uint64_t steps, uint32_t first, uint32_t n_inst) {
         if (nt != 1) return fail(IE_ERR_INVALID, "plain runs need single-cell instances");
         if (!initialized) return fail(IE_ERR_INVALID, "call init_random before running");
         if ((uint64_t)first + n_inst > count) return fail(IE_ERR_INVALID, "instance range out of bounds");
         if (steps == 0 || n_inst == 0) return IE_OK;
+        if (recs_dirty) IE_TRY(build_record_streams());
         std::vector<double> t(temps, temps + steps);
         IE_TRY(d_temps.upload(t, stream));
         std::vector<uint32_t> quads((size_t)4 * n_inst, 0xffffffffu);
-        for (uint32_t i = 0; i < n_inst; i++) quads[4 * (size_t)i] = first + i;
+        std::vector<int32_t> qh(n_inst);
+        for (uint32_t i = 0; i < n_inst; i++) {
+            quads[4 * (size_t)i] = first + i;
+            qh[i] = desc[first + i].H;
+        }
         DevBuf<uint32_t> dq;
+        DevBuf<int32_t> dh;
         IE_TRY(dq.upload(quads, stream));
-        const size_t smem = batch_smem(32);
-        IE_CUDA(set_smem_limits(std::max<size_t>(smem, 48 * 1024), pt_smem_cap()));
-        RunArgs R{};
-        R.temps = d_temps.p;
-        R.temps_per_step = 1;
-        R.steps = (uint32_t)steps;
-        R.step_base = steps_done;
-        R.exchange_interval = 1;
-        R.nquads = 1;
-        R.queue = d_queue.p;
+        IE_TRY(dh.upload(qh, stream));
+        std::vector<uint32_t> zeros(n_inst, 0);
+        DevBuf<uint32_t> counters;
+        IE_TRY(counters.upload(zeros, stream));
         IE_CUDA(cudaEventRecord(ev0, stream));
         for (uint32_t i = 0; i < n_inst; i++) {
+            RunArgs R = sa_args(steps);
             R.quads = dq.p + 4 * (size_t)i;
-            IE_CUDA(cudaMemsetAsync(d_queue.p, 0, sizeof(uint32_t), stream));
-            IE_CUDA(launch_batch_sa(arrays(), R, 1, 32, 2 * maxH + 1, smem, stream));
+            R.quad_h = dh.p + i;
+            R.nquads = 1;
+            R.queue = counters.p + i;
+            const uint32_t cap = std::max(64u, (desc[first + i].n + 63u) & ~63u);
+            if (batch_occupancy(desc[first + i].mode, 1, cap) <= 0)
+                return fail(IE_ERR_UNSUPPORTED, "instance too large for the plain kernel's shared memory");
+            IE_CUDA(launch_batch(arrays(), R, desc[first + i].mode, 1, cap, 1, stream));
         }
         IE_CUDA(cudaEventRecord(ev1, stream));
         IE_CUDA(cudaEventSynchronize(ev1));
@@ -556,11 +717,6 @@ struct Engine {
     size_t pt_smem(uint32_t cells, int32_t H, uint32_t mode) const {
         const size_t tab = mode == kModeInt ? (size_t)cells * (2 * H + 1) : 0;
         return (tab + (size_t)cells * kReplicas + cells + 2) * sizeof(uint64_t);
-    }
-    size_t pt_smem_cap() const {
-        size_t m = 48 * 1024;
-        for (uint32_t i = 0; i < count; i++) m = std::max(m, pt_smem(nt, desc[i].H, desc[i].mode));
-        return std::min<size_t>(m, 227 * 1024);
     }
 
     // engine::step n_steps times on instance 0 (all nt cells) with a constant
@@ -602,7 +758,7 @@ struct Engine {
         if (block > 1024) return fail(IE_ERR_UNSUPPORTED, "at most 128 temperatures per instance");
         const size_t smem = pt_smem(nt, d.H, d.mode);
         if (smem > 227 * 1024) return fail(IE_ERR_UNSUPPORTED, "temperature ladder too large for shared memory");
-        IE_CUDA(set_smem_limits(48 * 1024, std::max<size_t>(smem, 48 * 1024)));
+        IE_CUDA(set_smem_limits(std::max<size_t>(smem, 48 * 1024)));
         RunArgs R{};
         R.temps = d_temps.p;
         R.temps_per_step = per_step ? 1 : 0;

@@ -145,9 +145,7 @@ __device__ __forceinline__ void sweep_f64(const DevArrays& A, const InstDesc& d,
 
 // calculate_replica_energies_local (engine.rs:333-368) for the thread's 8
 // replicas, f64 in reference order (site order, CSR order, v < j edges).
-__device__ void energies_f64(const DevArrays& A, const InstDesc& d, const uint64_t* words, int lane,
-                             double (&E)[8]) {
-    const uint8_t* sp = reinterpret_cast<const uint8_t*>(words) + lane;
+__device__ void energies_f64_sp(const DevArrays& A, const InstDesc& d, const uint8_t* sp, double (&E)[8]) {
     const uint32_t* rows = A.rows + d.row;
     const uint32_t* cols = A.cols + d.ent;
     const double* vals = A.vals + d.ent;
@@ -175,6 +173,11 @@ __device__ void energies_f64(const DevArrays& A, const InstDesc& d, const uint64
     }
 }
 
+__device__ __forceinline__ void energies_f64(const DevArrays& A, const InstDesc& d, const uint64_t* words, int lane,
+                                             double (&E)[8]) {
+    energies_f64_sp(A, d, reinterpret_cast<const uint8_t*>(words) + lane, E);
+}
+
 __device__ __forceinline__ unsigned group_mask(int tid) { return 0xFFu << (8 * ((tid >> 3) & 3)); }
 
 // Number of exchange phases executed in global steps (base, base + steps].
@@ -183,63 +186,377 @@ __device__ __forceinline__ uint32_t exchanges_in(uint64_t base, uint32_t steps, 
 }
 
 // ---------------------------------------------------------------------------
-// Batched single-cell kernel: persistent; each warp pulls a quad of up to 4
-// instances (same mode, similar size and degree) from a global queue ordered
-// longest-first, and its four 8-thread groups run one instance each through
-// the whole temperature schedule. Shared memory: one threshold table per group.
+// Batched single-cell kernel.
+//
+// Persistent one-warp CTAs pull work items from a global queue ordered
+// longest-first. An instance is run by a group of 8*TPL threads: TPL threads
+// per Xoshiro lane, each running the lane's generator and owning the
+// decisions of the calls k = h, h+TPL, ... (h = its index within the lane).
+// Integer mode splits each site's neighbour sum across the TPL threads
+// (SWAR partial sums, reduced with two shuffles per level); f64 mode splits the
+// replicas. A warp holds 4/TPL instances; they run the same schedule in step
+// and share one threshold table per sweep. Each instance streams its site
+// records through a 3-slot shared-memory ring with cp.async (two 512-byte
+// chunks in flight ahead of the sweep). Spin bytes stay in global memory,
+// resident in L1; every thread of a lane writes the same combined byte, so
+// each thread's later reads see the update in program order.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) batch_sa_kernel(DevArrays A, RunArgs R, int tab_stride) {
-    extern __shared__ uint64_t smem[];
+__device__ __forceinline__ void cp_async16(uint32_t* smem_dst, const uint32_t* gsrc) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// Copies chunk k of a stream into its ring slot (32 x 16 bytes spread over
+// the G threads of the group) and commits a group; beyond the stream end
+// only an empty group is committed.
+template <int G>
+__device__ __forceinline__ void ring_fetch(uint32_t* ring, const uint32_t* stream, uint32_t nchunks,
+                                           uint32_t k, int t) {
+    if (k < nchunks) {
+        uint32_t* dst = ring + (k % kSlots) * kChunk;
+        const uint32_t* src = stream + (size_t)k * kChunk;
+#pragma unroll
+        for (int i = 0; i < 32 / G; i++) cp_async16(dst + 4 * (t + G * i), src + 4 * (t + G * i));
+    }
+    cp_async_commit();
+}
+
+// f32 evaluation of fast_exp, every operation rounded separately (no fused
+// multiply-add), used only to pre-decide u < fast_exp(x) outside a relative
+// band of 2^-10 around the f64 value; the worst relative gap between this and
+// the f64 evaluation over [-20, 0] is below 6e-6.
+__device__ __forceinline__ float fast_exp_f32(float x) {
+    x = fminf(fmaxf(x, -20.0f), 0.0f);
+    const float r = __fmul_rn(x, 0.0625f);
+    const float r2 = __fmul_rn(r, r);
+    const float r3 = __fmul_rn(r2, r);
+    float p = __fadd_rn(1.0f, r);
+    p = __fadd_rn(p, __fmul_rn(0.5f, r2));
+    p = __fadd_rn(p, __fmul_rn(1.0f / 6.0f, r3));
+    p = __fadd_rn(p, __fmul_rn(__fmul_rn(1.0f / 24.0f, r2), r2));
+    p = __fadd_rn(p, __fmul_rn(__fmul_rn(1.0f / 120.0f, r2), r3));
+    p = __fadd_rn(p, __fmul_rn(__fmul_rn(1.0f / 720.0f, r3), r3));
+    const float p2 = __fmul_rn(p, p);
+    const float p4 = __fmul_rn(p2, p2);
+    const float p8 = __fmul_rn(p4, p4);
+    return __fmul_rn(p8, p8);
+}
+
+// Exact f64 decision, out of line: only reached inside the f32 band.
+__device__ __noinline__ bool metropolis_exact_f64(double x, uint64_t m) {
+    return __dmul_rn((double)m, 2.220446049250313e-16) < fast_exp_rn(x);
+}
+
+// The reference decision dE <= 0 || u < fast_exp(-dE * beta) (engine.rs:665-666),
+// u = (res >> 12) * 2^-52: decided in f32 when the f32 value is clear of the
+// band, otherwise in f64 exactly.
+__device__ __forceinline__ bool metropolis_accept_f64(double de, double beta, uint64_t res) {
+    const double x = __dmul_rn(-de, beta);
+    const uint64_t m = res >> 12;
+    const float f = fast_exp_f32((float)x);
+    const float u = __fmul_rn(__ull2float_rn(m), 2.220446049250313e-16f);
+    const bool sure_yes = u < __fmul_rn(f, 0.9990234375f);
+    const bool sure_no = u > __fmul_rn(f, 1.0009765625f);
+    bool acc = sure_yes;
+    if (!sure_yes && !sure_no && de > 0.0) acc = metropolis_exact_f64(x, m);
+    return de <= 0.0 || acc;
+}
+
+template <int TPL>
+__device__ __forceinline__ uint32_t lane_or(uint32_t v, unsigned gmask) {
+    if constexpr (TPL >= 2) v |= __shfl_xor_sync(gmask, v, 1);
+    if constexpr (TPL >= 4) v |= __shfl_xor_sync(gmask, v, 2);
+    return v;
+}
+template <int TPL>
+__device__ __forceinline__ uint32_t lane_add(uint32_t v, unsigned gmask) {
+    if constexpr (TPL >= 2) v += __shfl_xor_sync(gmask, v, 1);
+    if constexpr (TPL >= 4) v += __shfl_xor_sync(gmask, v, 2);
+    return v;
+}
+
+template <uint32_t MODE, int TPL>
+using ETypeT = typename std::conditional<MODE == kModeInt, int32_t, double>::type;
+
+template <uint32_t MODE, int TPL>
+__device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc& d, uint32_t* ring, uint8_t* sp,
+                                             const uint2* __restrict__ lut, int lane, int h, unsigned gmask,
+                                             const uint64_t* __restrict__ tab,
+                                             int H, double beta, uint64_t cell_seed,
+                                             ETypeT<MODE, TPL> (&E)[8 / TPL]) {
+    constexpr int G = 8 * TPL;
+    constexpr int KP = 8 / TPL;    // calls owned by this thread: k = j*TPL + h
+    constexpr int EP = 16 / TPL;   // integer mode: record entries summed by this thread
+    const int t = lane * TPL + h;
+    // Thread h of a lane runs the lane's generator h steps ahead, so the calls
+    // it owns (k = j*TPL + h) fall on its local steps j*TPL.
+    Xoshiro x;
+    x.seed_lane(cell_seed, lane);
+    for (int i = 0; i < h; i++) x.advance();
+    const uint32_t* stream = A.recs + d.rec;
+    const uint32_t nchunks = (uint32_t)(d.rec_len / kChunk);
+    ring_fetch<G>(ring, stream, nchunks, 0, t);
+    ring_fetch<G>(ring, stream, nchunks, 1, t);
+    ring_fetch<G>(ring, stream, nchunks, 2, t);
+    cp_async_wait2();
+    __syncwarp(gmask);
+    uint32_t k = 0, c = 0;
+    const uint32_t* chunk = ring;
+    bool open = false;
+    uint64_t res[KP];
+    uint32_t xb = 0, aL = 0, aH = 0;
+    int lp = 0;
+    double dl[KP], tp[KP];
+    for (uint32_t v = 0; v < d.n;) {
+        const uint32_t hdr = (c < kChunk) ? chunk[c] : kRecPad;
+        if (hdr == kRecPad) {
+            __syncwarp(gmask);
+            k++;
+            c = 0;
+            ring_fetch<G>(ring, stream, nchunks, k + 2, t);
+            cp_async_wait2();
+            __syncwarp(gmask);
+            chunk = ring + (k % kSlots) * kChunk;
+            continue;
+        }
+        const uint32_t* rec = chunk + c;
+        const uint32_t deg = hdr & 0x1Fu;
+        const uint32_t deg4 = (deg + 3u) & ~3u;
+        if (!open) {
+            // first record of site v: this site's uniforms and current spins
+#pragma unroll
+            for (int kk = 0; kk < 8; kk++) {
+                if (kk % TPL == 0) res[kk / TPL] = x.next();
+                else x.advance();
+            }
+            xb = sp[8u * v];
+            if constexpr (MODE == kModeInt) {
+                aL = aH = 0;
+                lp = (int)(hdr >> 16) - 128;
+            } else {
+                const double wl = *reinterpret_cast<const double*>(rec + 2);
+#pragma unroll
+                for (int j = 0; j < KP; j++) {
+                    const bool xv = (xb >> (j * TPL + h)) & 1u;
+                    tp[j] = xv ? -1.0 : 1.0;
+                    dl[j] = xv ? -wl : wl;
+                }
+            }
+        }
+        const bool clamped = hdr & kRecClamp;
+        if constexpr (MODE == kModeInt) {
+            c += 4 + deg4;
+            const uint32_t* ent = rec + 4 + EP * h;
+#pragma unroll
+            for (int qd = 0; qd < EP / 4; qd++) {
+                if ((uint32_t)(EP * h + 4 * qd) < deg) {
+                    const uint4 e4 = *reinterpret_cast<const uint4*>(ent + 4 * qd);
+                    const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
+                    uint32_t li[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) li[e] = sp[8u * (en[e] & 0xFFFFFFu)] | ((en[e] >> 23) & 0x100u);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const uint2 sv = lut[li[e]];
+                        const uint32_t w = (en[e] >> 24) & 0x7Fu;
+                        aL += w * sv.x;
+                        aH += w * sv.y;
+                    }
+                }
+            }
+        } else {
+            const uint32_t* cols = rec + 4;
+            const double* vals = reinterpret_cast<const double*>(rec + 4 + deg4);
+            c += 4 + 3 * deg4;
+#pragma unroll
+            for (int qd = 0; qd < 4; qd++) {
+                if ((uint32_t)(4 * qd) < deg) {
+                    const uint4 c4 = *reinterpret_cast<const uint4*>(cols + 4 * qd);
+                    const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+                    const double2 w01 = *reinterpret_cast<const double2*>(vals + 4 * qd);
+                    const double2 w23 = *reinterpret_cast<const double2*>(vals + 4 * qd + 2);
+                    const double ww[4] = {w01.x, w01.y, w23.x, w23.y};
+                    uint32_t bj[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) bj[e] = sp[8u * cc[e]];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        if ((uint32_t)(4 * qd + e) < deg) {
+#pragma unroll
+                            for (int j = 0; j < KP; j++) {
+                                // t = (x_j ^ x_v) - x_v = x_j ? (x_v ? -1 : 1) : 0; w * t is
+                                // exact, so fma(w, t, dE) equals the reference's dE + w * t.
+                                const double tt = ((bj[e] >> (j * TPL + h)) & 1u) ? tp[j] : 0.0;
+                                dl[j] = __fma_rn(ww[e], tt, dl[j]);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (hdr & kRecCont) {
+            open = true;
+            continue;
+        }
+        open = false;
+        if (!clamped) {
+            uint32_t flips = 0;
+            if constexpr (MODE == kModeInt) {
+                aL = lane_add<TPL>(aL, gmask);
+                aH = lane_add<TPL>(aH, gmask);
+                const uint32_t cA = (uint32_t)(H + lp) * 0x01010101u;
+                const uint32_t cB = (uint32_t)(H - lp) * 0x01010101u;
+                const uint32_t xL = spread4(xb) * 0xFFu;
+                const uint32_t xH = spread4(xb >> 4) * 0xFFu;
+                const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
+                const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
+#pragma unroll
+                for (int j = 0; j < KP; j++) {
+                    const int kk = j * TPL + h;
+                    const uint32_t idx = ((kk < 4 ? iL : iH) >> (8 * (kk & 3))) & 0xFFu;
+                    if (res[j] <= tab[idx]) {
+                        flips |= 1u << kk;
+                        E[j] += (int32_t)idx - H;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < KP; j++) {
+                    if (metropolis_accept_f64(dl[j], beta, res[j])) {
+                        flips |= 1u << (j * TPL + h);
+                        E[j] = __dadd_rn(E[j], dl[j]);
+                    }
+                }
+            }
+            flips = lane_or<TPL>(flips, gmask);
+            sp[8u * v] = (uint8_t)(xb ^ flips);
+        }
+        v++;
+    }
+    cp_async_wait0();
+    __syncwarp(gmask);
+}
+
+// f64 recompute of the energies of the calls this thread owns (engine.rs:333-368).
+template <int TPL>
+__device__ void energies_f64_calls(const DevArrays& A, const InstDesc& d, const uint8_t* sp, int h,
+                                   double (&E)[8 / TPL]) {
+    double e8[8];
+    energies_f64_sp(A, d, sp, e8);
+#pragma unroll
+    for (int j = 0; j < 8 / TPL; j++) {
+        double v = e8[0];
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++)
+            if (kk == j * TPL + h) v = e8[kk];
+        E[j] = v;
+    }
+}
+
+// Dynamic shared memory of a batched CTA: threshold table (2 KB) | spread
+// table (4 KB) | NG rings | NG spin arrays of spin_cap words each (the
+// instance's spins stay resident in shared memory for the whole schedule).
+__host__ __device__ constexpr size_t batch_smem_bytes(int ng, uint32_t spin_cap) {
+    return 2048 + 4096 + (size_t)ng * kSlots * kChunk * 4 + (size_t)ng * spin_cap * 8;
+}
+
+template <uint32_t MODE, int TPL>
+__global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint32_t spin_cap) {
+    constexpr int G = 8 * TPL;
+    constexpr int NG = 4 / TPL;  // instances per warp
+    constexpr int KP = 8 / TPL;
+    extern __shared__ __align__(16) uint64_t dsm[];
+    uint64_t* tab = dsm;
     const int tid = threadIdx.x;
-    const int lane = tid & 7;
-    const int gw = (tid >> 3) & 3;
-    const unsigned gmask = group_mask(tid);
-    uint64_t* tab = smem + (size_t)(tid >> 3) * tab_stride;
+    const int g = tid / G;
+    const int t = tid % G;
+    const int lane = t / TPL;
+    const int h = t % TPL;
+    uint2* lut = reinterpret_cast<uint2*>(dsm + 256);
+    uint32_t* ring = reinterpret_cast<uint32_t*>(dsm + 256 + 512) + (size_t)g * kSlots * kChunk;
+    uint64_t* sw = reinterpret_cast<uint64_t*>(reinterpret_cast<uint32_t*>(dsm + 256 + 512) +
+                                               (size_t)NG * kSlots * kChunk) +
+                   (size_t)g * spin_cap;
+    // spread table: entry b (and 256 + b for a negative coupling, which
+    // contributes |w| (1 - x_j)) holds bit k of b (resp. ~b) in byte k of
+    // (lo word: k < 4, hi word: k >= 4)
+    if constexpr (MODE == kModeInt) {
+        for (int i = tid; i < 512; i += 32) {
+            const uint32_t b = (i < 256 ? (uint32_t)i : (uint32_t)(i - 256) ^ 0xFFu);
+            lut[i] = make_uint2(spread4(b), spread4(b >> 4));
+        }
+        __syncwarp();
+    }
+    uint8_t* sp = reinterpret_cast<uint8_t*>(sw) + lane;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (G * g));
+    typedef ETypeT<MODE, TPL> EType;
     for (;;) {
         uint32_t q = 0;
-        if ((tid & 31) == 0) q = atomicAdd(R.queue, 1u);
+        if (tid == 0) q = atomicAdd(R.queue, 1u);
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= R.nquads) break;
-        const uint32_t inst = R.quads[4 * q + gw];
-        if (inst == 0xffffffffu) continue;
-        const InstDesc d = A.desc[inst];
-        uint64_t* words = A.spins + d.spin;
+        const uint32_t inst = R.quads[4 * q + g];
+        const bool active = inst != 0xffffffffu;
+        const int H = MODE == kModeInt ? R.quad_h[q] : 0;
+        InstDesc d{};
         uint32_t key[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
-        const uint64_t pos0 = A.pos[inst];
-        if (d.mode == kModeInt) {
-            int32_t E[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) E[k] = A.Ei[d.energy + lane + 8 * k];
-            const int ts = 2 * d.H + 1;
-            for (uint32_t s = 0; s < R.steps; s++) {
-                const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
-                __syncwarp(gmask);
-                for (int i = lane; i < ts; i += 8) tab[i] = metropolis_threshold(i - d.H, beta);
-                __syncwarp(gmask);
-                const uint64_t base = chacha8_draw(key, pos0 + s);
-                sweep_int(A, d, words, lane, tab, base, E);
+        uint64_t pos0 = 0;
+        EType E[KP];
+        if (active) {
+            d = A.desc[inst];
+            if (d.n > spin_cap) {  // host sizing error: report and skip the instance
+                if (t == 0) atomicExch(A.err, 2);
+                continue;
             }
 #pragma unroll
-            for (int k = 0; k < 8; k++) A.Ei[d.energy + lane + 8 * k] = E[k];
-        } else {
-            double E[8];
+            for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
+            pos0 = A.pos[inst];
 #pragma unroll
-            for (int k = 0; k < 8; k++) E[k] = A.Ef[d.energy + lane + 8 * k];
-            for (uint32_t s = 0; s < R.steps; s++) {
-                const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
-                const uint64_t base = chacha8_draw(key, pos0 + s);
-                sweep_f64(A, d, words, lane, beta, base, E);
-                if ((R.step_base + s + 1) % kResyncEvery == 0) energies_f64(A, d, words, lane, E);
+            for (int j = 0; j < KP; j++) {
+                const size_t o = d.energy + lane + 8 * (j * TPL + h);
+                if constexpr (MODE == kModeInt) E[j] = A.Ei[o];
+                else E[j] = A.Ef[o];
             }
-#pragma unroll
-            for (int k = 0; k < 8; k++) A.Ef[d.energy + lane + 8 * k] = E[k];
+            const uint64_t* gw = A.spins + d.spin;
+            for (uint32_t i = t; i < d.n; i += G) sw[i] = gw[i];
+            __syncwarp(gmask);
         }
-        __syncwarp(gmask);
-        if (lane == 0) {
-            A.pos[inst] = pos0 + R.steps;
-            A.deo[inst] ^= (int32_t)(exchanges_in(R.step_base, R.steps, R.exchange_interval) & 1u);
+        for (uint32_t s = 0; s < R.steps; s++) {
+            const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
+            if constexpr (MODE == kModeInt) {
+                __syncwarp();
+                for (int i = tid; i < 2 * H + 1; i += 32) tab[i] = metropolis_threshold(i - H, beta);
+                __syncwarp();
+            }
+            if (active) {
+                const uint64_t base = chacha8_draw(key, pos0 + s);
+                sweep_stream<MODE, TPL>(A, d, ring, sp, lut, lane, h, gmask, tab, H, beta, base, E);
+                if constexpr (MODE == kModeF64) {
+                    if ((R.step_base + s + 1) % kResyncEvery == 0) {
+                        __syncwarp(gmask);
+                        energies_f64_calls<TPL>(A, d, sp, h, E);
+                    }
+                }
+            }
+        }
+        if (active) {
+            __syncwarp(gmask);
+            uint64_t* gw = A.spins + d.spin;
+            for (uint32_t i = t; i < d.n; i += G) gw[i] = sw[i];
+#pragma unroll
+            for (int j = 0; j < KP; j++) {
+                const size_t o = d.energy + lane + 8 * (j * TPL + h);
+                if constexpr (MODE == kModeInt) A.Ei[o] = E[j];
+                else A.Ef[o] = E[j];
+            }
+            __syncwarp(gmask);
+            if (t == 0) {
+                A.pos[inst] = pos0 + R.steps;
+                A.deo[inst] ^= (int32_t)(exchanges_in(R.step_base, R.steps, R.exchange_interval) & 1u);
+            }
         }
     }
 }
@@ -647,23 +964,42 @@ cudaError_t probe_peaks(int sm_count, double* int_ops_per_s, double* xoshiro_per
 // ---------------------------------------------------------------------------
 // Host-side launch wrappers (declared in ie_launch.h).
 // ---------------------------------------------------------------------------
-cudaError_t set_smem_limits(size_t batch_bytes, size_t pt_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(batch_sa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_bytes);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(pt_kernel<kModeInt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pt_bytes);
+cudaError_t set_smem_limits(size_t pt_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(pt_kernel<kModeInt>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pt_bytes);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(pt_kernel<kModeF64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pt_bytes);
 }
 
-int batch_occupancy(int block, size_t smem) {
+template <uint32_t MODE, int TPL>
+static int occ_of(size_t smem) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_sa_kernel, block, smem) != cudaSuccess) return 0;
-    return n;
+    if (cudaFuncSetAttribute(batch_kernel<MODE, TPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<MODE, TPL>, 32, smem) == cudaSuccess ? n : 0;
 }
 
-cudaError_t launch_batch_sa(const DevArrays& A, const RunArgs& R, int grid, int block, int tab_stride,
-                            size_t smem, cudaStream_t st) {
-    batch_sa_kernel<<<grid, block, smem, st>>>(A, R, tab_stride);
+size_t batch_smem(int tpl, uint32_t spin_cap) { return batch_smem_bytes(4 / tpl, spin_cap); }
+
+int batch_occupancy(uint32_t mode, int tpl, uint32_t spin_cap) {
+    const size_t sm = batch_smem(tpl, spin_cap);
+    if (mode == kModeInt)
+        return tpl == 1 ? occ_of<kModeInt, 1>(sm) : tpl == 2 ? occ_of<kModeInt, 2>(sm) : occ_of<kModeInt, 4>(sm);
+    return tpl == 1 ? occ_of<kModeF64, 1>(sm) : tpl == 2 ? occ_of<kModeF64, 2>(sm) : occ_of<kModeF64, 4>(sm);
+}
+
+cudaError_t launch_batch(const DevArrays& A, const RunArgs& R, uint32_t mode, int tpl, uint32_t spin_cap, int grid,
+                         cudaStream_t st) {
+    const size_t sm = batch_smem(tpl, spin_cap);
+    if (mode == kModeInt) {
+        if (tpl == 1) batch_kernel<kModeInt, 1><<<grid, 32, sm, st>>>(A, R, spin_cap);
+        else if (tpl == 2) batch_kernel<kModeInt, 2><<<grid, 32, sm, st>>>(A, R, spin_cap);
+        else batch_kernel<kModeInt, 4><<<grid, 32, sm, st>>>(A, R, spin_cap);
+    } else {
+        if (tpl == 1) batch_kernel<kModeF64, 1><<<grid, 32, sm, st>>>(A, R, spin_cap);
+        else if (tpl == 2) batch_kernel<kModeF64, 2><<<grid, 32, sm, st>>>(A, R, spin_cap);
+        else batch_kernel<kModeF64, 4><<<grid, 32, sm, st>>>(A, R, spin_cap);
+    }
     return cudaGetLastError();
 }
 

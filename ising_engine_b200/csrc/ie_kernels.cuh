@@ -24,7 +24,26 @@ struct InstDesc {
     uint64_t spin;   // spins[]: cell c word v at spin + c*n + v (lane-major bytes)
     uint64_t energy; // Ei[] / Ef[]: cell c replica r at energy + c*64 + r
     uint64_t stat;   // swap stats base ([nt-1] per instance)
+    uint64_t rec;    // site-record stream (batched kernel): recs[rec .. rec + rec_len)
+    uint64_t rec_len;
 };
+
+// Site-record streams of the batched kernel. Each instance's stream is a
+// sequence of chunks of kChunk words (16-byte aligned); records are 16-byte
+// aligned, never straddle a chunk, and kRecPad marks "continue at the next
+// chunk". A site with more than 16 couplings spans several records, all but
+// the last flagged kRecCont; a clamped site is a bare header.
+//  integer record: [hdr, 0, 0, 0, e_0 .. e_{d-1}, 0-padding to 4 words],
+//                  hdr = d | cont << 14 | clamp << 15 | (linp + 128) << 16,
+//                  e = col | |w| << 24 | (w < 0) << 31
+//  f64 record:     [hdr, 0, lin (2 words), col_0 .. (padded to a multiple of 4),
+//                   w_0 .. (f64, padded to a multiple of 4)], hdr = d | cont << 14 | clamp << 15
+constexpr uint32_t kChunk = 128;
+constexpr uint32_t kSlots = 3;
+constexpr uint32_t kRecPad = 0xFFFFFFFFu;
+constexpr uint32_t kRecCont = 1u << 14;
+constexpr uint32_t kRecClamp = 1u << 15;
+constexpr uint32_t kRecMaxDeg = 16;
 
 struct DevArrays {
     const InstDesc* desc;
@@ -36,6 +55,7 @@ struct DevArrays {
     const double* lin;
     const uint8_t* clampf;   // 1 = clamped site
     const int8_t* clampv;    // clamp value (0/1)
+    const uint32_t* recs;    // site-record streams
     const uint32_t* keys;    // master ChaCha8 key [inst][8]
     uint64_t* spins;
     int32_t* Ei;
@@ -62,6 +82,7 @@ struct RunArgs {
     const double* dbeta;      // [nt-1] 1/T_t - 1/T_{t+1}
     // batched work queue
     const uint32_t* quads;    // [nquads][4] instance ids (0xffffffff = empty)
+    const int32_t* quad_h;    // [nquads] largest H of the quad (integer mode)
     uint32_t nquads;
     uint32_t* queue;          // atomic counter
 };

@@ -200,3 +200,24 @@ def test_golden_pt_trajectory_and_solve():
     state = solver.solve(m)
     assert state.tolist() == GOLDEN["golden_state"]
     assert abs(m.calculate_total_energy(state) - GOLDEN["golden_energy"]) < GOLDEN["energy_tolerance"]
+
+
+def test_batch_long_rows_and_thread_classes():
+    """Rows longer than one record (> 16 couplings) and instances of every
+    size class (1, 2 and 4 threads per generator lane) in one batch."""
+    rng = np.random.default_rng(33)
+    models = [I.maxcut_gnm(160, 2600, seed=4),                       # degree ~32, integer
+              I.random_regular_qubo(300, 20, rng, integer=False),    # degree 20, f64
+              I.random_regular_qubo(260, 18, rng, integer=True)]
+    models += [I.random_regular_qubo(int(n), 6, rng, integer=bool(i % 2))
+               for i, n in enumerate(rng.integers(40, 200, size=13) * 2)]
+    seeds = np.arange(len(models), dtype=np.uint64) * 7 + 3
+    temps = I.sa_temps(30, 0.2, 3.0)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
+    b = BatchEngine(models, seeds)
+    b.init_random()
+    b.run_schedule(temps[:11])
+    b.run_schedule(temps[11:])
+    assert (b.spins() == words_ref).all()
+    assert b.energies().tobytes() == ref_e.tobytes()
+    b.close()
