@@ -159,6 +159,35 @@ ie_status ie_batch_last_run_ms(ie_batch* b, double* ms);
 /* Number of kernel launches the last run call issued. */
 ie_status ie_batch_last_launches(ie_batch* b, uint64_t* launches);
 
+/* ---- one SA run with no device allocation (no reference counterpart) ----
+ * For callers that cannot allocate device memory: code that runs while a CUDA
+ * graph is being captured, hosts whose framework owns a fixed device pool and
+ * forbids other allocators, services that must not block or fail on an
+ * allocation mid-request. The problem and the outputs are in device memory the
+ * caller already owns; all scratch lives in one file-scope device array of
+ * 12 MiB that every GPU loading this library holds until process exit.
+ * Limits: num_vars <= 16384, nnz <= 262144 (both triangles), n_steps <= 65536;
+ * larger inputs return IE_ERR_INVALID. The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Calls share the array, so calls that overlap on the GPU (other threads or
+ * streams) race; serialize them. The run is the f64 mode of the batched sweep
+ * (same spins and energies as ie_batch_run_schedule for the same problem, seed
+ * and temperatures); it returns after the stream has finished the run. */
+typedef struct ie_problem_device {
+    uint32_t num_vars;
+    uint32_t nnz;
+    const uint32_t* row_offsets; /* device, [num_vars + 1] */
+    const uint32_t* col_indices; /* device, [nnz] */
+    const double* values;        /* device, [nnz] */
+    const double* linear;        /* device, [num_vars] */
+} ie_problem_device;
+
+/* temps: host [n_steps]; words: device [num_vars] (bit r = replica r);
+ * energies: device [64]; stream: a cudaStream_t or NULL. */
+ie_status ie_sa_run_static(const ie_problem_device* problem, uint64_t seed, const double* temps,
+                           uint64_t n_steps, uint64_t* words, double* energies, int32_t device,
+                           void* stream);
+
 /* ---- measurement helper (no reference counterpart) ----
  * Measured roofline denominators on `device`: int32 LOP3/IADD3 throughput
  * (ops/s) and Xoshiro256++ step+compare throughput (outputs/s), the per-attempt

@@ -40,6 +40,11 @@ class ie_config(C.Structure):
                 ("force_f64", C.c_int32), ("device", C.c_int32)]
 
 
+class ie_problem_device(C.Structure):
+    _fields_ = [("num_vars", C.c_uint32), ("nnz", C.c_uint32), ("row_offsets", C.c_void_p),
+                ("col_indices", C.c_void_p), ("values", C.c_void_p), ("linear", C.c_void_p)]
+
+
 class ie_batch_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("force_f64", C.c_int32),
                 ("threads_per_block", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
@@ -77,6 +82,7 @@ _SIGS = {
     "ie_batch_last_run_ms": ([_vp, _vp], C.c_int),
     "ie_batch_last_launches": ([_vp, _vp], C.c_int),
     "ie_probe_peaks": ([C.c_int32, _vp, _vp], C.c_int),
+    "ie_sa_run_static": ([_vp, C.c_uint64, _vp, C.c_uint64, _vp, _vp, C.c_int32, _vp], C.c_int),
 }
 
 

@@ -878,6 +878,10 @@ struct ie_batch {
     Engine eng;
 };
 
+namespace ie {
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace ie
+
 extern "C" {
 
 const char* ie_last_error(void) { return g_err.c_str(); }

@@ -20,5 +20,6 @@ cudaError_t launch_model_energy(const DevArrays& A, uint32_t inst, uint32_t nt, 
                                 cudaStream_t st);
 cudaError_t launch_incumbent(const DevArrays& A, uint32_t inst, double offset, double* inc_e, uint64_t* inc_state,
                              uint32_t n_words, cudaStream_t st);
+void set_last_error(const char* msg);
 cudaError_t probe_peaks(int sm_count, double* int_ops_per_s, double* xoshiro_per_s);
 }  // namespace ie
