@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--threads-per-block", type=int, default=0)
     p.add_argument("--blocks-per-sm", type=int, default=0)
     return p.parse_args()
@@ -195,6 +196,7 @@ def run_ours(args):
     eng = BatchEngine(models, seeds, device=local, threads_per_block=args.threads_per_block,
                       blocks_per_sm=args.blocks_per_sm)
     eng.init_random()
+    tuned = eng.autotune(temps, 16) if not args.no_autotune else None
     for _ in range(args.warmup):
         eng.run_schedule(temps)
     dist.barrier()
@@ -288,7 +290,9 @@ def run_ours(args):
                        "replicas": 64, "sites": int(sum(m.num_vars for m in models)),
                        "couplings": int(sum(m.nnz for m in models)),
                        "l2": "inputs larger than L2 (problem data %.0f MB per GPU)" % (host_bytes(models) / 1e6),
-                       "parallelism": f"replicas x{ws}"},
+                       "parallelism": f"replicas x{ws}",
+                       "thread_classes": ({"n4_int": tuned[0], "n2_int": tuned[1], "n4_f64": tuned[2],
+                                           "n2_f64": tuned[3]} if tuned else "default")},
             "roofline": {"bound": "alu", "achieved": achieved_ops / 1e9, "peak": ip.value / 1e9,
                          "unit": "Gop/s", "frac": achieved_ops / ip.value, "traffic": traffic,
                          "ops_per_attempt": OPS_PER_ATTEMPT,

@@ -148,6 +148,11 @@ ie_status ie_batch_run_schedule(ie_batch* b, const double* temps, uint64_t n_ste
 /* Same schedule, one launch per instance in sequence (the plain method). */
 ie_status ie_batch_run_schedule_plain(ie_batch* b, const double* temps, uint64_t n_steps,
                                       uint32_t first, uint32_t count);
+/* Autotuner: times trial_steps of the schedule temps[] for a grid of
+ * thread-class thresholds (instances above a size threshold get 2 or 4 threads
+ * per generator lane), restoring the device state after every trial, and keeps
+ * the fastest. chosen[4] (may be NULL) receives {n4_int, n2_int, n4_f64, n2_f64}. */
+ie_status ie_batch_autotune(ie_batch* b, const double* temps, uint64_t trial_steps, uint32_t* chosen);
 /* Spin words of instance i at words + offsets[i] (offsets = prefix sums of n). */
 ie_status ie_batch_read_spins(ie_batch* b, uint64_t* words);
 ie_status ie_batch_read_energies(ie_batch* b, double* energies /* [count][64] */);

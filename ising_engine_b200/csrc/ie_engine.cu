@@ -10,6 +10,7 @@
 #include <memory>
 #include <numeric>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/ising_b200.h"
@@ -338,10 +339,8 @@ struct Engine {
         if (ev2) cudaEventDestroy(ev2);
         if (stream) cudaStreamDestroy(stream);
         if (stream2) cudaStreamDestroy(stream2);
-        for (int i = 0; i < 6; i++) {
-            if (cstreams[i]) cudaStreamDestroy(cstreams[i]);
-            if (cevents[i]) cudaEventDestroy(cevents[i]);
-        }
+        for (cudaStream_t st : cstreams) cudaStreamDestroy(st);
+        for (cudaEvent_t ev : cevents) cudaEventDestroy(ev);
     }
 
     DevArrays arrays() const {
@@ -461,7 +460,7 @@ struct Engine {
         IE_TRY(d_att.upload(zstat, stream));
         IE_TRY(d_acc.upload(zstat, stream));
         IE_TRY(d_err.upload(std::vector<int32_t>(1, 0), stream));
-        IE_TRY(d_queue.alloc(6));
+        IE_TRY(d_queue.alloc(1));
         IE_TRY(d_scratch.alloc(std::max<size_t>((size_t)nt * kReplicas, 1)));
         IE_TRY(upload_draw_idx());
         IE_CUDA(cudaStreamSynchronize(stream));
@@ -522,89 +521,111 @@ struct Engine {
         return (double)h.n * (deg + 12.0) * (h.mode == kModeF64 ? 2.5 : 1.0);
     }
 
-    // Work classes: (mode, TPL) with TPL threads per Xoshiro lane; the largest
-    // instances get more threads so their sequential site chain is shorter.
-    static constexpr int kTpls[3] = {1, 2, 4};
-    // size thresholds of the thread classes per mode: n > n4 -> 4 threads per
-    // lane, n > n2 -> 2, else 1 (set by the autotuner)
+    // Work classes (mode, TPL, spin capacity): TPL threads per Xoshiro lane,
+    // so the largest instances, whose sequential site chain sets the
+    // makespan, get the most threads; the shared-memory capacity of a class
+    // is the smallest of kCaps that holds its instances.
+    static constexpr uint32_t kCaps[10] = {256, 512, 768, 1024, 1536, 2048, 3072, 4096, 8192, 16384};
+    // thread-class size thresholds per mode: n > n4 -> 4 threads per lane,
+    // n > n2 -> 2, else 1 (set by the autotuner)
     uint32_t tune_n4[2] = {1536, 768}, tune_n2[2] = {512, 256};
-    uint32_t nitems[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    uint32_t spin_cap[2][3] = {{64, 64, 64}, {64, 64, 64}};
-    double class_work[2][3] = {{0, 0, 0}, {0, 0, 0}};
-    DevBuf<uint32_t> d_items[2][3];
-    DevBuf<int32_t> d_itemh[2][3];
-    cudaStream_t cstreams[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t cevents[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    struct WorkClass {
+        uint32_t mode = 0;
+        int tpl = 1;
+        uint32_t cap = 64;
+        uint32_t nitems = 0;
+        double work = 0;  // longest item
+        DevBuf<uint32_t> items;
+        DevBuf<int32_t> itemh;
+    };
+    std::vector<std::unique_ptr<WorkClass>> classes;
+    std::vector<cudaStream_t> cstreams;
+    std::vector<cudaEvent_t> cevents;
 
-    ie_status ensure_class_streams() {
-        for (int i = 0; i < 6; i++) {
-            if (!cstreams[i]) IE_CUDA(cudaStreamCreateWithFlags(&cstreams[i], cudaStreamNonBlocking));
-            if (!cevents[i]) IE_CUDA(cudaEventCreateWithFlags(&cevents[i], cudaEventDisableTiming));
+    ie_status ensure_class_streams(size_t k) {
+        while (cstreams.size() < k) {
+            cudaStream_t st;
+            cudaEvent_t ev;
+            IE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            IE_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            cstreams.push_back(st);
+            cevents.push_back(ev);
         }
         return IE_OK;
     }
 
-    int tpl_class(uint32_t i) const {
+    int tpl_of(uint32_t i) const {
         const uint32_t n = desc[i].n, m = desc[i].mode;
-        if (n > tune_n4[m]) return 2;
-        if (n > tune_n2[m]) return 1;
-        return 0;
+        return n > tune_n4[m] ? 4 : (n > tune_n2[m] ? 2 : 1);
+    }
+    static uint32_t cap_of(uint32_t n) {
+        for (uint32_t c : kCaps)
+            if (n <= c) return c;
+        return (n + 63u) & ~63u;
     }
 
     // Per class: instances ordered by degree then size into items of 4/TPL
     // (the groups of a warp stay in step sweep by sweep), items ordered by
-    // work, longest first.
+    // work, longest first; classes ordered by their longest item.
     ie_status build_quads() {
-        for (uint32_t mode = 0; mode < 2; mode++)
-            for (int ci = 0; ci < 3; ci++) {
-                const int ng = 4 / kTpls[ci];
-                std::vector<uint32_t> order;
-                for (uint32_t i = 0; i < count; i++)
-                    if (desc[i].mode == mode && tpl_class(i) == ci) order.push_back(i);
-                auto degree = [&](uint32_t i) {
-                    return insts[i].n ? (uint32_t)((insts[i].cols.size() + insts[i].n / 2) / insts[i].n) : 0u;
-                };
-                std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-                    if (degree(a) != degree(b)) return degree(a) > degree(b);
-                    return desc[a].n > desc[b].n;
-                });
-                std::vector<std::vector<uint32_t>> items;
-                for (size_t i = 0; i < order.size();) {
-                    std::vector<uint32_t> q;
-                    const uint32_t dg = degree(order[i]);
-                    while ((int)q.size() < ng && i < order.size() && degree(order[i]) == dg) q.push_back(order[i++]);
-                    items.push_back(q);
-                }
-                auto work = [&](const std::vector<uint32_t>& q) {
-                    double w = 0;
-                    for (uint32_t i : q) w = std::max(w, inst_work(insts[i]));
-                    return w;
-                };
-                std::stable_sort(items.begin(), items.end(), [&](const std::vector<uint32_t>& a,
-                                                                 const std::vector<uint32_t>& b) { return work(a) > work(b); });
-                std::vector<uint32_t> flat;
-                std::vector<int32_t> qh;
-                class_work[mode][ci] = 0;
-                uint32_t cap = 64;
-                for (uint32_t i : order) cap = std::max(cap, (desc[i].n + 63u) & ~63u);
-                spin_cap[mode][ci] = cap;
-                for (auto& q : items) {
-                    int32_t hh = 0;
-                    for (int k = 0; k < 4; k++) {
-                        flat.push_back(k < (int)q.size() ? q[k] : 0xffffffffu);
-                        if (k < (int)q.size()) hh = std::max(hh, desc[q[k]].H);
-                    }
-                    qh.push_back(hh);
-                    class_work[mode][ci] += work(q) * (double)q.size() * kTpls[ci];
-                }
-                nitems[mode][ci] = (uint32_t)items.size();
-                if (flat.empty()) {
-                    flat.assign(4, 0xffffffffu);
-                    qh.assign(1, 0);
-                }
-                IE_TRY(d_items[mode][ci].upload(flat, stream));
-                IE_TRY(d_itemh[mode][ci].upload(qh, stream));
+        classes.clear();
+        std::vector<std::tuple<uint32_t, int, uint32_t>> keys;
+        for (uint32_t i = 0; i < count; i++) {
+            auto k = std::make_tuple(desc[i].mode, tpl_of(i), cap_of(desc[i].n));
+            if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
+        }
+        auto degree = [&](uint32_t i) {
+            return insts[i].n ? (uint32_t)((insts[i].cols.size() + insts[i].n / 2) / insts[i].n) : 0u;
+        };
+        for (auto& k : keys) {
+            std::unique_ptr<WorkClass> wc(new WorkClass());
+            wc->mode = std::get<0>(k);
+            wc->tpl = std::get<1>(k);
+            wc->cap = std::get<2>(k);
+            const int ng = 4 / wc->tpl;
+            std::vector<uint32_t> order;
+            for (uint32_t i = 0; i < count; i++)
+                if (desc[i].mode == wc->mode && tpl_of(i) == wc->tpl && cap_of(desc[i].n) == wc->cap)
+                    order.push_back(i);
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+                if (degree(a) != degree(b)) return degree(a) > degree(b);
+                return desc[a].n > desc[b].n;
+            });
+            std::vector<std::vector<uint32_t>> items;
+            for (size_t i = 0; i < order.size();) {
+                std::vector<uint32_t> q;
+                const uint32_t dg = degree(order[i]);
+                while ((int)q.size() < ng && i < order.size() && degree(order[i]) == dg) q.push_back(order[i++]);
+                items.push_back(q);
             }
+            auto work = [&](const std::vector<uint32_t>& q) {
+                double w = 0;
+                for (uint32_t i : q) w = std::max(w, inst_work(insts[i]) / wc->tpl);
+                return w;
+            };
+            std::stable_sort(items.begin(), items.end(), [&](const std::vector<uint32_t>& a,
+                                                             const std::vector<uint32_t>& b) { return work(a) > work(b); });
+            std::vector<uint32_t> flat;
+            std::vector<int32_t> qh;
+            for (auto& q : items) {
+                int32_t hh = 0;
+                for (int j = 0; j < 4; j++) {
+                    flat.push_back(j < (int)q.size() ? q[j] : 0xffffffffu);
+                    if (j < (int)q.size()) hh = std::max(hh, desc[q[j]].H);
+                }
+                qh.push_back(hh);
+                wc->work = std::max(wc->work, work(q));
+            }
+            wc->nitems = (uint32_t)items.size();
+            IE_TRY(wc->items.upload(flat, stream));
+            IE_TRY(wc->itemh.upload(qh, stream));
+            classes.push_back(std::move(wc));
+        }
+        std::stable_sort(classes.begin(), classes.end(),
+                         [](const std::unique_ptr<WorkClass>& a, const std::unique_ptr<WorkClass>& b) {
+                             return a->work > b->work;
+                         });
+        IE_TRY(d_queue.alloc(std::max<size_t>(classes.size(), 1)));
         quads_built = true;
         return IE_OK;
     }
@@ -628,38 +649,34 @@ struct Engine {
         if (steps > 0xffffffffULL) return fail(IE_ERR_INVALID, "too many steps in one call");
         if (recs_dirty) IE_TRY(build_record_streams());
         if (!quads_built) IE_TRY(build_quads());
-        IE_TRY(ensure_class_streams());
+        IE_TRY(ensure_class_streams(classes.size()));
         std::vector<double> t(temps, temps + steps);
         for (double x : t)
             if (!(x > 0.0) || !std::isfinite(x)) return fail(IE_ERR_INVALID, "temperatures must be positive");
         IE_TRY(d_temps.upload(t, stream));
-        double wsum = 0;
-        for (int m = 0; m < 2; m++)
-            for (int ci = 0; ci < 3; ci++) wsum += class_work[m][ci];
-        IE_CUDA(cudaMemsetAsync(d_queue.p, 0, 6 * sizeof(uint32_t), stream));
+        IE_CUDA(cudaMemsetAsync(d_queue.p, 0, classes.size() * sizeof(uint32_t), stream));
         IE_CUDA(cudaEventRecord(ev0, stream));
         uint64_t launches = 0;
-        for (uint32_t m = 0; m < 2; m++)
-            for (int ci = 0; ci < 3; ci++) {
-                const int k = 3 * (int)m + ci;
-                if (!nitems[m][ci]) continue;
-                IE_CUDA(cudaStreamWaitEvent(cstreams[k], ev0, 0));
-                const int occ = batch_occupancy(m, kTpls[ci], spin_cap[m][ci]);
-                if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
-                const double share = wsum > 0 ? class_work[m][ci] / wsum : 1.0;
-                int per_sm = std::max(1, (int)std::ceil(occ * share));
-                if (blocks_per_sm) per_sm = (int)blocks_per_sm;
-                const int grid = std::max(1, std::min<int>((int)nitems[m][ci], per_sm * g_sm_count));
-                RunArgs R = sa_args(steps);
-                R.quads = d_items[m][ci].p;
-                R.quad_h = d_itemh[m][ci].p;
-                R.nquads = nitems[m][ci];
-                R.queue = d_queue.p + k;
-                IE_CUDA(launch_batch(arrays(), R, m, kTpls[ci], spin_cap[m][ci], grid, cstreams[k]));
-                IE_CUDA(cudaEventRecord(cevents[k], cstreams[k]));
-                IE_CUDA(cudaStreamWaitEvent(stream, cevents[k], 0));
-                launches++;
-            }
+        // largest classes first: their CTAs are dispatched first and the
+        // smaller classes fill the remaining room
+        for (size_t k = 0; k < classes.size(); k++) {
+            WorkClass& wc = *classes[k];
+            if (!wc.nitems) continue;
+            IE_CUDA(cudaStreamWaitEvent(cstreams[k], ev0, 0));
+            int occ = batch_occupancy(wc.mode, wc.tpl, wc.cap);
+            if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
+            if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
+            const int grid = std::max(1, std::min<int>((int)wc.nitems, occ * g_sm_count));
+            RunArgs R = sa_args(steps);
+            R.quads = wc.items.p;
+            R.quad_h = wc.itemh.p;
+            R.nquads = wc.nitems;
+            R.queue = d_queue.p + k;
+            IE_CUDA(launch_batch(arrays(), R, wc.mode, wc.tpl, wc.cap, grid, cstreams[k]));
+            IE_CUDA(cudaEventRecord(cevents[k], cstreams[k]));
+            IE_CUDA(cudaStreamWaitEvent(stream, cevents[k], 0));
+            launches++;
+        }
         IE_CUDA(cudaEventRecord(ev1, stream));
         IE_CUDA(cudaEventSynchronize(ev1));
         float ms = 0;
@@ -667,6 +684,77 @@ struct Engine {
         last_ms = ms;
         last_launches = launches;
         steps_done += steps;
+        return IE_OK;
+    }
+
+    // Autotuner: times a short trial of the schedule for a grid of thread-class
+    // thresholds (the device state is saved before and restored after every
+    // trial) and keeps the fastest. Returns the chosen thresholds.
+    ie_status autotune(const double* temps, uint64_t trial_steps, uint32_t out[4]) {
+        if (!initialized) return fail(IE_ERR_INVALID, "call init_random before autotuning");
+        if (trial_steps == 0) return fail(IE_ERR_INVALID, "trial_steps must be >= 1");
+        if (recs_dirty) IE_TRY(build_record_streams());
+        DevBuf<uint64_t> s_spins, s_pos;
+        DevBuf<int32_t> s_ei, s_deo;
+        DevBuf<double> s_ef;
+        IE_TRY(s_spins.alloc(std::max<size_t>(total_words, 1)));
+        IE_TRY(s_pos.alloc(count));
+        IE_TRY(s_ei.alloc(std::max<size_t>(total_energy, 1)));
+        IE_TRY(s_deo.alloc(count));
+        IE_TRY(s_ef.alloc(std::max<size_t>(total_energy, 1)));
+        auto copy_all = [&](bool save) -> ie_status {
+            auto cp = [&](void* dst, const void* src, size_t bytes) -> ie_status {
+                IE_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream));
+                return IE_OK;
+            };
+            const size_t w = std::max<size_t>(total_words, 1) * 8, e = std::max<size_t>(total_energy, 1);
+            if (save) {
+                IE_TRY(cp(s_spins.p, d_spins.p, w));
+                IE_TRY(cp(s_pos.p, d_pos.p, count * 8));
+                IE_TRY(cp(s_ei.p, d_Ei.p, e * 4));
+                IE_TRY(cp(s_deo.p, d_deo.p, count * 4));
+                IE_TRY(cp(s_ef.p, d_Ef.p, e * 8));
+            } else {
+                IE_TRY(cp(d_spins.p, s_spins.p, w));
+                IE_TRY(cp(d_pos.p, s_pos.p, count * 8));
+                IE_TRY(cp(d_Ei.p, s_ei.p, e * 4));
+                IE_TRY(cp(d_deo.p, s_deo.p, count * 4));
+                IE_TRY(cp(d_Ef.p, s_ef.p, e * 8));
+            }
+            IE_CUDA(cudaStreamSynchronize(stream));
+            return IE_OK;
+        };
+        IE_TRY(copy_all(true));
+        const uint64_t saved_steps = steps_done;
+        const uint32_t n4s[3] = {768, 1536, 3072}, n2s[2] = {256, 512};
+        double best = 1e300;
+        uint32_t bi[4] = {tune_n4[0], tune_n2[0], tune_n4[1], tune_n2[1]};
+        for (uint32_t a : n4s)
+            for (uint32_t b : n2s)
+                for (uint32_t c : n4s)
+                    for (uint32_t dd : n2s) {
+                        tune_n4[0] = a;
+                        tune_n2[0] = b;
+                        tune_n4[1] = c;
+                        tune_n2[1] = dd;
+                        quads_built = false;
+                        IE_TRY(run_batch(temps, trial_steps));
+                        IE_TRY(copy_all(false));
+                        steps_done = saved_steps;
+                        if (last_ms < best) {
+                            best = last_ms;
+                            bi[0] = a;
+                            bi[1] = b;
+                            bi[2] = c;
+                            bi[3] = dd;
+                        }
+                    }
+        tune_n4[0] = bi[0];
+        tune_n2[0] = bi[1];
+        tune_n4[1] = bi[2];
+        tune_n2[1] = bi[3];
+        quads_built = false;
+        if (out) std::copy(bi, bi + 4, out);
         return IE_OK;
     }
 
@@ -1141,6 +1229,12 @@ ie_status ie_batch_recompute_energies(ie_batch* b, double* energies) {
     if (!b || !energies) return fail(IE_ERR_INVALID, "NULL argument");
     IE_CUDA(cudaSetDevice(b->eng.device));
     return b->eng.recompute_energies(energies);
+}
+
+ie_status ie_batch_autotune(ie_batch* b, const double* temps, uint64_t trial_steps, uint32_t* chosen) {
+    if (!b || !temps) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    return b->eng.autotune(temps, trial_steps, chosen);
 }
 
 ie_status ie_batch_last_run_ms(ie_batch* b, double* ms) {

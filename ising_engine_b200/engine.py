@@ -184,6 +184,15 @@ class BatchEngine:
         _ffi.check(self._L.ie_batch_run_schedule(self._h, _p(t), len(t)))
         return self.last_ms()
 
+    def autotune(self, temps, trial_steps: int = 16):
+        """Chooses the thread-class thresholds by timing short trials of the
+        schedule (state restored after each); returns (n4_int, n2_int,
+        n4_f64, n2_f64)."""
+        t = np.ascontiguousarray(temps, dtype=np.float64).reshape(-1)
+        out = np.zeros(4, dtype=np.uint32)
+        _ffi.check(self._L.ie_batch_autotune(self._h, _p(t), min(int(trial_steps), len(t)), _p(out)))
+        return tuple(int(x) for x in out)
+
     def run_schedule_plain(self, temps, first: int = 0, count: int | None = None) -> float:
         t = np.ascontiguousarray(temps, dtype=np.float64).reshape(-1)
         count = self.count - first if count is None else count

@@ -221,3 +221,20 @@ def test_batch_long_rows_and_thread_classes():
     assert (b.spins() == words_ref).all()
     assert b.energies().tobytes() == ref_e.tobytes()
     b.close()
+
+
+def test_autotune_restores_state():
+    """The autotuner's trial runs leave no trace: after tuning, the run equals
+    the oracle's from the same initial state."""
+    models, seeds = I.uneven_batch(20, seed=99, n_max=900)
+    temps = I.sa_temps(24)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
+    b = BatchEngine(models, seeds)
+    b.init_random()
+    chosen = b.autotune(temps, 4)
+    assert len(chosen) == 4
+    b.run_schedule(temps)
+    assert (b.spins() == words_ref).all()
+    assert b.energies().tobytes() == ref_e.tobytes()
+    assert (b.draws() == np.array([m.num_vars + 24 for m in models], np.uint64)).all()
+    b.close()
