@@ -104,6 +104,8 @@ struct HostInst {
     std::vector<uint32_t> cols;
     std::vector<double> vals;
     std::vector<double> lin;
+    std::vector<uint32_t> recpos, reclen;  // first record of each site: word offset and length in its stream
+    bool windowed_ok = false;              // eligible for the windowed kernel
 };
 
 ie_status ingest(const ie_problem* p, bool force_f64, HostInst& out) {
@@ -239,9 +241,13 @@ ie_status build_xtables(const double* temps, uint32_t nt, XTables& X) {
 
 // Appends the chunk-packed site-record stream of one instance (layout in
 // ie_kernels.cuh); the stream starts and ends on a chunk boundary.
-ie_status build_records(const HostInst& h, const std::vector<uint8_t>& clampf, size_t site0,
+ie_status build_records(HostInst& h, const std::vector<uint8_t>& clampf, size_t site0,
                         std::vector<uint32_t>& out, uint64_t& off, uint64_t& len) {
     off = out.size();
+    h.recpos.assign(h.n, 0);
+    h.reclen.assign(h.n, 0);
+    bool first_of_site = true;
+    uint32_t cur_site = 0;
     uint32_t c = 0;
     std::vector<uint32_t> rec;
     auto emit = [&](const std::vector<uint32_t>& r) {
@@ -250,12 +256,19 @@ ie_status build_records(const HostInst& h, const std::vector<uint8_t>& clampf, s
             while (out.size() % kChunk) out.push_back(0);
             c = 0;
         }
+        if (first_of_site) {
+            h.recpos[cur_site] = (uint32_t)(out.size() - off);
+            h.reclen[cur_site] = (uint32_t)r.size();
+            first_of_site = false;
+        }
         out.insert(out.end(), r.begin(), r.end());
         c = (uint32_t)((c + r.size()) % kChunk);
     };
     for (uint32_t v = 0; v < h.n; v++) {
         const uint32_t beg = h.rows[v], end = h.rows[v + 1];
         const bool clamp = clampf[site0 + v] != 0;
+        cur_site = v;
+        first_of_site = true;
         if (clamp) {
             emit({kRecClamp, 0, 0, 0});
             continue;
@@ -316,7 +329,7 @@ struct Engine {
     int32_t maxH = 0;
 
     DevBuf<InstDesc> d_desc;
-    DevBuf<uint32_t> d_rows, d_ents, d_cols, d_keys, d_queue, d_draw_idx, d_unclamped, d_recs;
+    DevBuf<uint32_t> d_rows, d_ents, d_cols, d_keys, d_queue, d_draw_idx, d_unclamped, d_recs, d_wtab;
     DevBuf<int32_t> d_linp, d_Ei, d_deo, d_err;
     DevBuf<double> d_vals, d_lin, d_Ef, d_temps, d_dbeta, d_scratch;
     DevBuf<uint8_t> d_clampf;
@@ -355,6 +368,7 @@ struct Engine {
         A.clampf = d_clampf.p;
         A.clampv = d_clampv.p;
         A.recs = d_recs.p;
+        A.wtab = d_wtab.p;
         A.keys = d_keys.p;
         A.spins = d_spins.p;
         A.Ei = d_Ei.p;
@@ -496,11 +510,55 @@ struct Engine {
         return IE_OK;
     }
 
+    // Window tables of the windowed kernel (layout in ie_kernels.cu): an
+    // instance qualifies when every site has at most 16 couplings (one record)
+    // and its windows of 8 sites have on average at least 2 sites per level.
+    void build_window_table(uint32_t i, std::vector<uint32_t>& wt) {
+        HostInst& h = insts[i];
+        h.windowed_ok = false;
+        desc[i].win = 0;
+        if (h.n < 8 || nt != 1) return;
+        for (uint32_t v = 0; v < h.n; v++)
+            if (h.rows[v + 1] - h.rows[v] > kRecMaxDeg) return;
+        const uint32_t nwin = (h.n + 7) / 8;
+        std::vector<uint32_t> tab((size_t)nwin * 16, 0);
+        double par = 0;
+        for (uint32_t w = 0; w < nwin; w++) {
+            uint32_t lvl[8] = {0, 0, 0, 0, 0, 0, 0, 0}, maxl = 0, levels = 0;
+            for (uint32_t k = 0; k < 8; k++) {
+                const uint32_t v = 8 * w + k;
+                if (v >= h.n) break;
+                uint32_t l = 0;
+                for (uint32_t e = h.rows[v]; e < h.rows[v + 1]; e++) {
+                    const uint32_t j = h.cols[e];
+                    if (j >= 8 * w && j < v) l = std::max(l, lvl[j - 8 * w] + 1);
+                }
+                lvl[k] = l;
+                maxl = std::max(maxl, l);
+                levels |= l << (4 * k);
+                tab[16 * (size_t)w + k] = (h.recpos[v] / 4) | ((h.reclen[v] / 4) << 24);
+            }
+            tab[16 * (size_t)w + 8] = levels;
+            tab[16 * (size_t)w + 9] = maxl;
+            par += 8.0 / (maxl + 1);
+        }
+        if (par / nwin < 2.0) return;
+        h.windowed_ok = true;
+        desc[i].win = wt.size();
+        wt.insert(wt.end(), tab.begin(), tab.end());
+    }
+
     ie_status build_record_streams() {
-        std::vector<uint32_t> recs;
-        for (uint32_t i = 0; i < count; i++) IE_TRY(build_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].rec_len));
+        std::vector<uint32_t> recs, wt;
+        for (uint32_t i = 0; i < count; i++) {
+            IE_TRY(build_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].rec_len));
+            build_window_table(i, wt);
+        }
         recs.resize(recs.size() + kChunk, 0);
+        if (wt.empty()) wt.assign(16, 0);
         IE_TRY(d_recs.upload(recs, stream));
+        IE_TRY(d_wtab.upload(wt, stream));
+        quads_built = false;
         IE_CUDA(cudaMemcpyAsync(d_desc.p, desc.data(), desc.size() * sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
         IE_CUDA(cudaStreamSynchronize(stream));
         recs_dirty = false;
@@ -554,10 +612,13 @@ struct Engine {
         return IE_OK;
     }
 
+    // TPL 8 marks the windowed kernel (one warp per instance).
     int tpl_of(uint32_t i) const {
         const uint32_t n = desc[i].n, m = desc[i].mode;
-        return n > tune_n4[m] ? 4 : (n > tune_n2[m] ? 2 : 1);
+        if (n > tune_n4[m]) return insts[i].windowed_ok && use_windows ? 8 : 4;
+        return n > tune_n2[m] ? 2 : 1;
     }
+    bool use_windows = true;
     static uint32_t cap_of(uint32_t n) {
         for (uint32_t c : kCaps)
             if (n <= c) return c;
@@ -582,7 +643,7 @@ struct Engine {
             wc->mode = std::get<0>(k);
             wc->tpl = std::get<1>(k);
             wc->cap = std::get<2>(k);
-            const int ng = 4 / wc->tpl;
+            const int ng = wc->tpl == 8 ? 1 : 4 / wc->tpl;
             std::vector<uint32_t> order;
             for (uint32_t i = 0; i < count; i++)
                 if (desc[i].mode == wc->mode && tpl_of(i) == wc->tpl && cap_of(desc[i].n) == wc->cap)
@@ -600,7 +661,7 @@ struct Engine {
             }
             auto work = [&](const std::vector<uint32_t>& q) {
                 double w = 0;
-                for (uint32_t i : q) w = std::max(w, inst_work(insts[i]) / wc->tpl);
+                for (uint32_t i : q) w = std::max(w, inst_work(insts[i]) / (wc->tpl == 8 ? 5 : wc->tpl));
                 return w;
             };
             std::stable_sort(items.begin(), items.end(), [&](const std::vector<uint32_t>& a,
@@ -663,7 +724,7 @@ struct Engine {
             WorkClass& wc = *classes[k];
             if (!wc.nitems) continue;
             IE_CUDA(cudaStreamWaitEvent(cstreams[k], ev0, 0));
-            int occ = batch_occupancy(wc.mode, wc.tpl, wc.cap);
+            int occ = wc.tpl == 8 ? window_occupancy(wc.mode, wc.cap) : batch_occupancy(wc.mode, wc.tpl, wc.cap);
             if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
             if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
             const int grid = std::max(1, std::min<int>((int)wc.nitems, occ * g_sm_count));
@@ -672,7 +733,8 @@ struct Engine {
             R.quad_h = wc.itemh.p;
             R.nquads = wc.nitems;
             R.queue = d_queue.p + k;
-            IE_CUDA(launch_batch(arrays(), R, wc.mode, wc.tpl, wc.cap, grid, cstreams[k]));
+            if (wc.tpl == 8) IE_CUDA(launch_window(arrays(), R, wc.mode, wc.cap, grid, cstreams[k]));
+            else IE_CUDA(launch_batch(arrays(), R, wc.mode, wc.tpl, wc.cap, grid, cstreams[k]));
             IE_CUDA(cudaEventRecord(cevents[k], cstreams[k]));
             IE_CUDA(cudaStreamWaitEvent(stream, cevents[k], 0));
             launches++;
@@ -1174,6 +1236,7 @@ ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint
     IE_TRY(b->eng.setup_device(cfg.device));
     b->eng.threads_per_block = cfg.threads_per_block;
     b->eng.blocks_per_sm = cfg.blocks_per_sm;
+    b->eng.use_windows = cfg.disable_windows == 0;
     if (cfg.threads_per_block && (cfg.threads_per_block % 32 || cfg.threads_per_block > 256))
         return fail(IE_ERR_INVALID, "threads_per_block must be a multiple of 32, at most 256");
     IE_TRY(b->eng.build(problems, count, 1, seeds, cfg.force_f64 != 0));

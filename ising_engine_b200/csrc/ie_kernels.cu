@@ -207,6 +207,7 @@ __device__ __forceinline__ void cp_async16(uint32_t* smem_dst, const uint32_t* g
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
 // Copies chunk k of a stream into its ring slot (32 x 16 bytes spread over
@@ -557,6 +558,313 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
                 A.pos[inst] = pos0 + R.steps;
                 A.deo[inst] ^= (int32_t)(exchanges_in(R.step_base, R.steps, R.exchange_interval) & 1u);
             }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Windowed kernel for large instances whose consecutive sites are rarely
+// coupled (random graphs). One warp runs one instance through windows of 8
+// consecutive sites:
+//  1. generator phase: thread (lane rl = t/4, offset rh = t%4) advances lane
+//     rl's Xoshiro chain over the window's 64 steps and stores the outputs of
+//     the calls it owns (rh, rh+4) for each site in shared memory;
+//  2. decision phase: 64 (site, lane) tasks, two per thread, run level by
+//     level inside the window (a site waits only for lower-indexed neighbours
+//     in the same window; the levels come from a host-built window table), so
+//     the outcome equals the reference's site order exactly;
+//  3. each accepted dE goes to shared memory and every replica's energy is
+//     accumulated in site order, the reference's f64 summation order.
+// The next window's site records stream into a shared double buffer with
+// cp.async while the current window is processed.
+// Window table entry (16 words): word i (< 8) = record position | length << 24
+// of site i (16-byte units within the instance's record stream), word 8 = level
+// of site i in nibble i, word 9 = largest level.
+// ---------------------------------------------------------------------------
+constexpr int kWin = 8;
+constexpr uint32_t kWinRecWords = 8 * 52;  // eight records of degree <= 16
+
+__host__ __device__ constexpr size_t window_smem_bytes(uint32_t spin_cap) {
+    // tab 2 KB | spread table 4 KB | outputs 4 KB | accepted dE 4 KB | records 2 x 1664 B | spins
+    return 2048 + 4096 + 4096 + 4096 + 2 * kWinRecWords * 4 + (size_t)spin_cap * 8;
+}
+
+// Copies the records of one window (positions from its table entry) into buf.
+__device__ __forceinline__ void window_fetch(const uint32_t* ent, const uint32_t* stream, uint32_t* buf, int tid) {
+    uint32_t pos[8], off[9];
+    off[0] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const uint32_t e = ent[i];
+        pos[i] = e & 0xFFFFFFu;
+        off[i + 1] = off[i] + (e >> 24);
+    }
+    for (uint32_t j = tid; j < off[8]; j += 32) {
+        uint32_t src = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if (j >= off[i] && j < off[i + 1]) src = pos[i] + (j - off[i]);
+        cp_async16(buf + 4 * j, stream + 4 * (size_t)src);
+    }
+}
+
+template <uint32_t MODE>
+__device__ __forceinline__ void window_sweep(const DevArrays& A, const InstDesc& d, uint64_t* rngb, void* deb_,
+                                             uint32_t* recb, uint8_t* spc, const uint2* __restrict__ lut,
+                                             const uint64_t* __restrict__ tab, int H, double beta,
+                                             uint64_t cell_seed, int tid,
+                                             typename std::conditional<MODE == kModeInt, int32_t, double>::type (&E)[2]) {
+    const int rl = tid >> 2, rh = tid & 3;  // generator lane and offset
+    const int cl = tid & 7, cs = tid >> 3;  // decision lane and first site
+    Xoshiro x;
+    x.seed_lane(cell_seed, rl);
+    for (int i = 0; i < rh; i++) x.advance();
+    const uint32_t nwin = (d.n + kWin - 1) / kWin;
+    const uint32_t* wt = A.wtab + d.win;
+    const uint32_t* stream = A.recs + d.rec;
+    window_fetch(wt, stream, recb, tid);
+    cp_async_commit();
+    uint32_t nxt[10];
+#pragma unroll
+    for (int i = 0; i < 10; i++) nxt[i] = wt[i];
+    for (uint32_t w = 0; w < nwin; w++) {
+        uint32_t cur[10];
+#pragma unroll
+        for (int i = 0; i < 10; i++) cur[i] = nxt[i];
+        // 1. generator phase
+#pragma unroll
+        for (int i = 0; i < kWin; i++) {
+#pragma unroll
+            for (int kk = 0; kk < 8; kk++) {
+                if (kk % 4 == 0) rngb[(i * 8 + rl) * 8 + rh + kk] = x.next();
+                else x.advance();
+            }
+        }
+        if (w + 1 < nwin) {
+            const uint32_t* en = wt + 16 * (size_t)(w + 1);
+            window_fetch(en, stream, recb + ((w + 1) & 1) * kWinRecWords, tid);
+#pragma unroll
+            for (int i = 0; i < 10; i++) nxt[i] = en[i];
+        }
+        cp_async_commit();
+        cp_async_wait1();
+        __syncwarp();
+        // 2. decision phase
+        const uint32_t* rb = recb + (w & 1) * kWinRecWords;
+        uint32_t off[8];
+        off[0] = 0;
+#pragma unroll
+        for (int i = 1; i < 8; i++) off[i] = off[i - 1] + (cur[i - 1] >> 24);
+        const uint32_t levels = cur[8], maxl = cur[9];
+        for (uint32_t L = 0; L <= maxl; L++) {
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+                const int i = cs + 4 * m;
+                const uint32_t v = w * kWin + i;
+                if (v < d.n && ((levels >> (4 * i)) & 15u) == L) {
+                    const uint32_t* rec = rb + 4 * off[i];
+                    const uint32_t hdr = rec[0];
+                    const uint32_t deg = hdr & 0x1Fu;
+                    const uint32_t deg4 = (deg + 3u) & ~3u;
+                    const uint32_t xb = spc[8u * v];
+                    uint64_t res[8];
+                    const uint64_t* rp = rngb + (i * 8 + cl) * 8;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) res[k] = rp[k];
+                    uint32_t flips = 0;
+                    if constexpr (MODE == kModeInt) {
+                        int32_t* deb = reinterpret_cast<int32_t*>(deb_) + (i * 8 + cl) * 8;
+                        if (!(hdr & kRecClamp)) {
+                            uint32_t aL = 0, aH = 0;
+#pragma unroll
+                            for (int qd = 0; qd < 4; qd++) {
+                                if ((uint32_t)(4 * qd) < deg) {
+                                    const uint4 e4 = *reinterpret_cast<const uint4*>(rec + 4 + 4 * qd);
+                                    const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
+                                    uint32_t li[4];
+#pragma unroll
+                                    for (int e = 0; e < 4; e++)
+                                        li[e] = spc[8u * (en[e] & 0xFFFFFFu)] | ((en[e] >> 23) & 0x100u);
+#pragma unroll
+                                    for (int e = 0; e < 4; e++) {
+                                        const uint2 sv = lut[li[e]];
+                                        const uint32_t ww = (en[e] >> 24) & 0x7Fu;
+                                        aL += ww * sv.x;
+                                        aH += ww * sv.y;
+                                    }
+                                }
+                            }
+                            const int lp = (int)(hdr >> 16) - 128;
+                            const uint32_t cA = (uint32_t)(H + lp) * 0x01010101u;
+                            const uint32_t cB = (uint32_t)(H - lp) * 0x01010101u;
+                            const uint32_t xL = spread4(xb) * 0xFFu;
+                            const uint32_t xH = spread4(xb >> 4) * 0xFFu;
+                            const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
+                            const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
+#pragma unroll
+                            for (int k = 0; k < 8; k++) {
+                                const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
+                                const bool acc = res[k] <= tab[idx];
+                                flips |= (uint32_t)acc << k;
+                                deb[k] = acc ? (int32_t)idx - H : 0;
+                            }
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < 8; k++) deb[k] = 0;
+                        }
+                    } else {
+                        double* deb = reinterpret_cast<double*>(deb_) + (i * 8 + cl) * 8;
+                        if (!(hdr & kRecClamp)) {
+                            const double wl = *reinterpret_cast<const double*>(rec + 2);
+                            const uint32_t* cols = rec + 4;
+                            const double* vals = reinterpret_cast<const double*>(rec + 4 + deg4);
+                            double dl[8], tp[8];
+#pragma unroll
+                            for (int k = 0; k < 8; k++) {
+                                const bool xv = (xb >> k) & 1u;
+                                tp[k] = xv ? -1.0 : 1.0;
+                                dl[k] = xv ? -wl : wl;
+                            }
+#pragma unroll
+                            for (int qd = 0; qd < 4; qd++) {
+                                if ((uint32_t)(4 * qd) < deg) {
+                                    const uint4 c4 = *reinterpret_cast<const uint4*>(cols + 4 * qd);
+                                    const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+                                    const double2 w01 = *reinterpret_cast<const double2*>(vals + 4 * qd);
+                                    const double2 w23 = *reinterpret_cast<const double2*>(vals + 4 * qd + 2);
+                                    const double wv[4] = {w01.x, w01.y, w23.x, w23.y};
+                                    uint32_t bj[4];
+#pragma unroll
+                                    for (int e = 0; e < 4; e++) bj[e] = spc[8u * cc[e]];
+#pragma unroll
+                                    for (int e = 0; e < 4; e++) {
+                                        if ((uint32_t)(4 * qd + e) < deg) {
+#pragma unroll
+                                            for (int k = 0; k < 8; k++)
+                                                dl[k] = __fma_rn(wv[e], ((bj[e] >> k) & 1u) ? tp[k] : 0.0, dl[k]);
+                                        }
+                                    }
+                                }
+                            }
+#pragma unroll
+                            for (int k = 0; k < 8; k++) {
+                                const bool acc = metropolis_accept_f64(dl[k], beta, res[k]);
+                                flips |= (uint32_t)acc << k;
+                                deb[k] = acc ? dl[k] : 0.0;
+                            }
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < 8; k++) deb[k] = 0.0;
+                        }
+                    }
+                    spc[8u * v] = (uint8_t)(xb ^ flips);
+                }
+            }
+            __syncwarp();
+        }
+        // 3. energies in site order (calls rh and rh + 4 of lane rl)
+#pragma unroll
+        for (int i = 0; i < kWin; i++) {
+            if (w * kWin + i < d.n) {
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int o = (i * 8 + rl) * 8 + rh + 4 * j;
+                    if constexpr (MODE == kModeInt) E[j] += reinterpret_cast<const int32_t*>(deb_)[o];
+                    else E[j] = __dadd_rn(E[j], reinterpret_cast<const double*>(deb_)[o]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    cp_async_wait0();
+    __syncwarp();
+}
+
+template <uint32_t MODE>
+__global__ void __launch_bounds__(32, 1) window_kernel(DevArrays A, RunArgs R, uint32_t spin_cap) {
+    extern __shared__ __align__(16) uint64_t dsm[];
+    uint64_t* tab = dsm;
+    uint2* lut = reinterpret_cast<uint2*>(dsm + 256);
+    uint64_t* rngb = dsm + 768;
+    void* deb = dsm + 768 + 512;
+    uint32_t* recb = reinterpret_cast<uint32_t*>(dsm + 768 + 1024);
+    uint64_t* sw = dsm + 768 + 1024 + kWinRecWords;
+    const int tid = threadIdx.x;
+    const int rl = tid >> 2, rh = tid & 3;
+    uint8_t* spc = reinterpret_cast<uint8_t*>(sw) + (tid & 7);
+    typedef typename std::conditional<MODE == kModeInt, int32_t, double>::type EType;
+    if constexpr (MODE == kModeInt) {
+        for (int i = tid; i < 512; i += 32) {
+            const uint32_t b = (i < 256 ? (uint32_t)i : (uint32_t)(i - 256) ^ 0xFFu);
+            lut[i] = make_uint2(spread4(b), spread4(b >> 4));
+        }
+        __syncwarp();
+    }
+    for (;;) {
+        uint32_t q = 0;
+        if (tid == 0) q = atomicAdd(R.queue, 1u);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= R.nquads) break;
+        const uint32_t inst = R.quads[4 * q];
+        if (inst == 0xffffffffu) continue;
+        const int H = MODE == kModeInt ? R.quad_h[q] : 0;
+        const InstDesc d = A.desc[inst];
+        if (d.n > spin_cap) {
+            if (tid == 0) atomicExch(A.err, 2);
+            continue;
+        }
+        uint32_t key[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
+        const uint64_t pos0 = A.pos[inst];
+        EType E[2];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const size_t o = d.energy + rl + 8 * (rh + 4 * j);
+            if constexpr (MODE == kModeInt) E[j] = A.Ei[o];
+            else E[j] = A.Ef[o];
+        }
+        const uint64_t* gw = A.spins + d.spin;
+        for (uint32_t i = tid; i < d.n; i += 32) sw[i] = gw[i];
+        __syncwarp();
+        for (uint32_t s = 0; s < R.steps; s++) {
+            const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
+            if constexpr (MODE == kModeInt) {
+                __syncwarp();
+                for (int i = tid; i < 2 * H + 1; i += 32) tab[i] = metropolis_threshold(i - H, beta);
+                __syncwarp();
+            }
+            const uint64_t base = chacha8_draw(key, pos0 + s);
+            window_sweep<MODE>(A, d, rngb, deb, recb, spc, lut, tab, H, beta, base, tid, E);
+            if constexpr (MODE == kModeF64) {
+                if ((R.step_base + s + 1) % kResyncEvery == 0) {
+                    double e8[8];
+                    energies_f64_sp(A, d, reinterpret_cast<const uint8_t*>(sw) + rl, e8);
+#pragma unroll
+                    for (int j = 0; j < 2; j++) {
+                        double vv = e8[0];
+#pragma unroll
+                        for (int k = 0; k < 8; k++)
+                            if (k == rh + 4 * j) vv = e8[k];
+                        E[j] = vv;
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        __syncwarp();
+        uint64_t* gwo = A.spins + d.spin;
+        for (uint32_t i = tid; i < d.n; i += 32) gwo[i] = sw[i];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const size_t o = d.energy + rl + 8 * (rh + 4 * j);
+            if constexpr (MODE == kModeInt) A.Ei[o] = E[j];
+            else A.Ef[o] = E[j];
+        }
+        __syncwarp();
+        if (tid == 0) {
+            A.pos[inst] = pos0 + R.steps;
+            A.deo[inst] ^= (int32_t)(exchanges_in(R.step_base, R.steps, R.exchange_interval) & 1u);
         }
     }
 }
@@ -1000,6 +1308,27 @@ cudaError_t launch_batch(const DevArrays& A, const RunArgs& R, uint32_t mode, in
         else if (tpl == 2) batch_kernel<kModeF64, 2><<<grid, 32, sm, st>>>(A, R, spin_cap);
         else batch_kernel<kModeF64, 4><<<grid, 32, sm, st>>>(A, R, spin_cap);
     }
+    return cudaGetLastError();
+}
+
+template <uint32_t MODE>
+static int occ_win(size_t smem) {
+    int n = 0;
+    if (cudaFuncSetAttribute(window_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, window_kernel<MODE>, 32, smem) == cudaSuccess ? n : 0;
+}
+
+int window_occupancy(uint32_t mode, uint32_t spin_cap) {
+    const size_t sm = window_smem_bytes(spin_cap);
+    return mode == kModeInt ? occ_win<kModeInt>(sm) : occ_win<kModeF64>(sm);
+}
+
+cudaError_t launch_window(const DevArrays& A, const RunArgs& R, uint32_t mode, uint32_t spin_cap, int grid,
+                          cudaStream_t st) {
+    const size_t sm = window_smem_bytes(spin_cap);
+    if (mode == kModeInt) window_kernel<kModeInt><<<grid, 32, sm, st>>>(A, R, spin_cap);
+    else window_kernel<kModeF64><<<grid, 32, sm, st>>>(A, R, spin_cap);
     return cudaGetLastError();
 }
 

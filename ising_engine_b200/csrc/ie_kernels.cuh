@@ -26,6 +26,7 @@ struct InstDesc {
     uint64_t stat;   // swap stats base ([nt-1] per instance)
     uint64_t rec;    // site-record stream (batched kernel): recs[rec .. rec + rec_len)
     uint64_t rec_len;
+    uint64_t win;    // window table (windowed kernel): wtab[win .. win + 16 * ceil(n / 8))
 };
 
 // Site-record streams of the batched kernel. Each instance's stream is a
@@ -56,6 +57,7 @@ struct DevArrays {
     const uint8_t* clampf;   // 1 = clamped site
     const int8_t* clampv;    // clamp value (0/1)
     const uint32_t* recs;    // site-record streams
+    const uint32_t* wtab;    // window tables of the windowed kernel
     const uint32_t* keys;    // master ChaCha8 key [inst][8]
     uint64_t* spins;
     int32_t* Ei;

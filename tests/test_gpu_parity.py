@@ -238,3 +238,38 @@ def test_autotune_restores_state():
     assert b.energies().tobytes() == ref_e.tobytes()
     assert (b.draws() == np.array([m.num_vars + 24 for m in models], np.uint64)).all()
     b.close()
+
+
+def test_windowed_kernel_large_instances():
+    """Large random-regular instances take the windowed kernel (generator
+    phase + level-ordered decisions per window of 8 sites); a large lattice
+    (consecutive sites coupled) stays on the per-lane kernel. Both bit-exact."""
+    rng = np.random.default_rng(77)
+    models = [I.random_regular_qubo(1700, 12, rng, integer=True),
+              I.random_regular_qubo(1600, 3, rng, integer=True),
+              I.random_regular_qubo(900, 16, rng, integer=False),
+              I.random_regular_qubo(2100, 5, rng, integer=False),
+              I.pm_j_lattice(48, 2, seed=5)]
+    seeds = np.arange(len(models), dtype=np.uint64) + 11
+    temps = I.sa_temps(30, 0.2, 4.0)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
+    b = BatchEngine(models, seeds)
+    b.init_random()
+    b.run_schedule(temps[:13])
+    b.run_schedule(temps[13:])
+    assert (b.spins() == words_ref).all()
+    assert b.energies().tobytes() == ref_e.tobytes()
+    b.close()
+
+
+def test_windowed_kernel_f64_resync():
+    rng = np.random.default_rng(78)
+    m = I.random_regular_qubo(800, 9, rng, integer=False)
+    temps = I.sa_temps(1002, 0.2, 3.0)
+    words_ref, _, ref_e = O.run_sa_batch([m], [5], temps, threads=1)
+    b = BatchEngine([m], [5])
+    b.init_random()
+    b.run_schedule(temps)
+    assert (b.spins() == words_ref).all()
+    assert b.energies().tobytes() == ref_e.tobytes()
+    b.close()
