@@ -210,18 +210,21 @@ def run_ours(args):
         launches += eng.last_launches()
     wall = time.perf_counter() - t0
     clk = clocks.stop()
+    classes = eng.class_report()
     dist.barrier()
     dev_s = dist.max(dev_ms / 1e3)
     total_attempts = dist.sum(attempts * args.steps)
     value = total_attempts / dev_s
-    per_launch_s = dev_ms / 1e3 / max(launches, 1)
+    # one step is a group of concurrent class launches (one per size/mode class);
+    # the roofline is taken over that group, per step
+    per_step_s = dev_ms / 1e3 / args.steps
 
     # roofline: measured int32 ALU peak and Xoshiro step rate on this GPU
     import ctypes as C
     ip = C.c_double()
     xp = C.c_double()
     _ffi.check(_ffi.lib().ie_probe_peaks(local, C.byref(ip), C.byref(xp)))
-    achieved_ops = attempts / per_launch_s * OPS_PER_ATTEMPT
+    achieved_ops = attempts / per_step_s * OPS_PER_ATTEMPT
     # algorithmic bytes per launch: each sweep reads the CSR row entries
     # (4 B integer / 12 B f64 per entry), the per-site constants, and reads and
     # writes each spin word once per sweep (8 + 8 B), nothing cached.
@@ -235,11 +238,11 @@ def run_ours(args):
     except Exception:
         hbm_peak = 6650.0
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "batch_sa_kernel_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "batched_step_traffic.json")
     if os.path.exists(prof):
         try:
             t = json.load(open(prof))
-            traffic = t["dram_bytes_per_attempt"] * attempts
+            traffic = t["dram_bytes_per_attempt"] * attempts  # per step
         except Exception:
             traffic = None
 
@@ -297,17 +300,20 @@ def run_ours(args):
                          "unit": "Gop/s", "frac": achieved_ops / ip.value, "traffic": traffic,
                          "ops_per_attempt": OPS_PER_ATTEMPT,
                          "peak_source": "measured in-run: int32 LOP3/IADD3 microkernel (ie_probe_peaks)",
+                         "per": "step: one group of concurrent class launches",
                          "xoshiro_sol_attempts_per_s": xp.value,
-                         "frac_of_xoshiro_sol": (attempts / per_launch_s) / xp.value,
-                         "hbm": {"achieved_gbs": alg_bytes / per_launch_s / 1e9, "peak_gbs": hbm_peak,
-                                 "frac": alg_bytes / per_launch_s / 1e9 / hbm_peak,
-                                 "alg_bytes_per_launch": alg_bytes}},
+                         "frac_of_xoshiro_sol": (attempts / per_step_s) / xp.value,
+                         "hbm": {"achieved_gbs": alg_bytes / per_step_s / 1e9, "peak_gbs": hbm_peak,
+                                 "frac": alg_bytes / per_step_s / 1e9 / hbm_peak,
+                                 "alg_bytes_per_step": alg_bytes}},
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
             "plain": plain,
             "batched_over_plain": (value / ws / plain["value"]) if plain else None,
             "wall_s_timed": wall,
+            "classes": [{"mode": c[0], "threads_per_lane": c[1], "cap": c[2], "items": c[3],
+                         "ms": round(c[4], 1)} for c in classes],
         }
         if cpu:
             line["cpu_baseline"] = cpu

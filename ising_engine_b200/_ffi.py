@@ -82,6 +82,7 @@ _SIGS = {
     "ie_batch_recompute_energies": ([_vp, _vp], C.c_int),
     "ie_batch_last_run_ms": ([_vp, _vp], C.c_int),
     "ie_batch_autotune": ([_vp, _vp, C.c_uint64, _vp], C.c_int),
+    "ie_batch_class_report": ([_vp, C.c_uint32, _vp, _vp, _vp], C.c_int),
     "ie_batch_last_launches": ([_vp, _vp], C.c_int),
     "ie_probe_peaks": ([C.c_int32, _vp, _vp], C.c_int),
     "ie_sa_run_static": ([_vp, C.c_uint64, _vp, C.c_uint64, _vp, _vp, C.c_int32, _vp], C.c_int),

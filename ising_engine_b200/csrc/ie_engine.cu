@@ -354,6 +354,7 @@ struct Engine {
         if (stream2) cudaStreamDestroy(stream2);
         for (cudaStream_t st : cstreams) cudaStreamDestroy(st);
         for (cudaEvent_t ev : cevents) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : cstart) cudaEventDestroy(ev);
     }
 
     DevArrays arrays() const {
@@ -592,22 +593,26 @@ struct Engine {
         int tpl = 1;
         uint32_t cap = 64;
         uint32_t nitems = 0;
-        double work = 0;  // longest item
+        double work = 0;       // longest item
+        double site_steps = 0; // sites summed over the class (per sweep)
         DevBuf<uint32_t> items;
         DevBuf<int32_t> itemh;
     };
     std::vector<std::unique_ptr<WorkClass>> classes;
     std::vector<cudaStream_t> cstreams;
-    std::vector<cudaEvent_t> cevents;
+    std::vector<cudaEvent_t> cevents, cstart;
+    std::vector<double> class_ms;  // device time of each class launch in the last run
 
     ie_status ensure_class_streams(size_t k) {
         while (cstreams.size() < k) {
             cudaStream_t st;
-            cudaEvent_t ev;
+            cudaEvent_t ev, ev0;
             IE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-            IE_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            IE_CUDA(cudaEventCreate(&ev));
+            IE_CUDA(cudaEventCreate(&ev0));
             cstreams.push_back(st);
             cevents.push_back(ev);
+            cstart.push_back(ev0);
         }
         return IE_OK;
     }
@@ -672,7 +677,10 @@ struct Engine {
                 int32_t hh = 0;
                 for (int j = 0; j < 4; j++) {
                     flat.push_back(j < (int)q.size() ? q[j] : 0xffffffffu);
-                    if (j < (int)q.size()) hh = std::max(hh, desc[q[j]].H);
+                    if (j < (int)q.size()) {
+                        hh = std::max(hh, desc[q[j]].H);
+                        wc->site_steps += (double)desc[q[j]].n;
+                    }
                 }
                 qh.push_back(hh);
                 wc->work = std::max(wc->work, work(q));
@@ -733,6 +741,7 @@ struct Engine {
             R.quad_h = wc.itemh.p;
             R.nquads = wc.nitems;
             R.queue = d_queue.p + k;
+            IE_CUDA(cudaEventRecord(cstart[k], cstreams[k]));
             if (wc.tpl == 8) IE_CUDA(launch_window(arrays(), R, wc.mode, wc.cap, grid, cstreams[k]));
             else IE_CUDA(launch_batch(arrays(), R, wc.mode, wc.tpl, wc.cap, grid, cstreams[k]));
             IE_CUDA(cudaEventRecord(cevents[k], cstreams[k]));
@@ -746,6 +755,13 @@ struct Engine {
         last_ms = ms;
         last_launches = launches;
         steps_done += steps;
+        class_ms.assign(classes.size(), 0.0);
+        for (size_t k = 0; k < classes.size(); k++) {
+            if (!classes[k]->nitems) continue;
+            float cm = 0;
+            IE_CUDA(cudaEventElapsedTime(&cm, cstart[k], cevents[k]));
+            class_ms[k] = cm;
+        }
         return IE_OK;
     }
 
@@ -816,6 +832,7 @@ struct Engine {
         tune_n4[1] = bi[2];
         tune_n2[1] = bi[3];
         quads_built = false;
+        IE_TRY(build_quads());
         if (out) std::copy(bi, bi + 4, out);
         return IE_OK;
     }
@@ -940,6 +957,13 @@ struct Engine {
         last_ms = ms;
         last_launches = launches;
         steps_done += steps;
+        class_ms.assign(classes.size(), 0.0);
+        for (size_t k = 0; k < classes.size(); k++) {
+            if (!classes[k]->nitems) continue;
+            float cm = 0;
+            IE_CUDA(cudaEventElapsedTime(&cm, cstart[k], cevents[k]));
+            class_ms[k] = cm;
+        }
         return IE_OK;
     }
 
@@ -1303,6 +1327,24 @@ ie_status ie_batch_autotune(ie_batch* b, const double* temps, uint64_t trial_ste
 ie_status ie_batch_last_run_ms(ie_batch* b, double* ms) {
     if (!b || !ms) return fail(IE_ERR_INVALID, "NULL argument");
     *ms = b->eng.last_ms;
+    return IE_OK;
+}
+
+ie_status ie_batch_class_report(ie_batch* b, uint32_t max_classes, uint32_t* n_classes, uint32_t* info,
+                                double* ms) {
+    if (!b || !n_classes) return fail(IE_ERR_INVALID, "NULL argument");
+    Engine& E = b->eng;
+    *n_classes = (uint32_t)E.classes.size();
+    for (uint32_t k = 0; k < std::min<uint32_t>(max_classes, *n_classes); k++) {
+        if (info) {
+            info[5 * k + 0] = E.classes[k]->mode;
+            info[5 * k + 1] = (uint32_t)E.classes[k]->tpl;
+            info[5 * k + 2] = E.classes[k]->cap;
+            info[5 * k + 3] = E.classes[k]->nitems;
+            info[5 * k + 4] = k < E.class_ms.size() ? 1u : 0u;
+        }
+        if (ms) ms[k] = k < E.class_ms.size() ? E.class_ms[k] : 0.0;
+    }
     return IE_OK;
 }
 

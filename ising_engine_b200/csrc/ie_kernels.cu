@@ -584,13 +584,10 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
 constexpr int kWin = 8;
 constexpr uint32_t kWinRecWords = 8 * 52;  // eight records of degree <= 16
 
-__host__ __device__ constexpr size_t window_smem_bytes(uint32_t spin_cap) {
-    // tab 2 KB | spread table 4 KB | outputs 4 KB | accepted dE 4 KB | records 2 x 1664 B | spins
-    return 2048 + 4096 + 4096 + 4096 + 2 * kWinRecWords * 4 + (size_t)spin_cap * 8;
-}
 
 // Copies the records of one window (positions from its table entry) into buf.
-__device__ __forceinline__ void window_fetch(const uint32_t* ent, const uint32_t* stream, uint32_t* buf, int tid) {
+__device__ __forceinline__ void window_fetch(const uint32_t* ent, const uint32_t* stream, uint32_t* buf, int tid,
+                                             int nthreads) {
     uint32_t pos[8], off[9];
     off[0] = 0;
 #pragma unroll
@@ -599,7 +596,7 @@ __device__ __forceinline__ void window_fetch(const uint32_t* ent, const uint32_t
         pos[i] = e & 0xFFFFFFu;
         off[i + 1] = off[i] + (e >> 24);
     }
-    for (uint32_t j = tid; j < off[8]; j += 32) {
+    for (uint32_t j = tid; j < off[8]; j += nthreads) {
         uint32_t src = 0;
 #pragma unroll
         for (int i = 0; i < 8; i++)
@@ -608,202 +605,178 @@ __device__ __forceinline__ void window_fetch(const uint32_t* ent, const uint32_t
     }
 }
 
-template <uint32_t MODE>
-__device__ __forceinline__ void window_sweep(const DevArrays& A, const InstDesc& d, uint64_t* rngb, void* deb_,
-                                             uint32_t* recb, uint8_t* spc, const uint2* __restrict__ lut,
-                                             const uint64_t* __restrict__ tab, int H, double beta,
-                                             uint64_t cell_seed, int tid,
-                                             typename std::conditional<MODE == kModeInt, int32_t, double>::type (&E)[2]) {
-    const int rl = tid >> 2, rh = tid & 3;  // generator lane and offset
-    const int cl = tid & 7, cs = tid >> 3;  // decision lane and first site
-    Xoshiro x;
-    x.seed_lane(cell_seed, rl);
-    for (int i = 0; i < rh; i++) x.advance();
-    const uint32_t nwin = (d.n + kWin - 1) / kWin;
-    const uint32_t* wt = A.wtab + d.win;
-    const uint32_t* stream = A.recs + d.rec;
-    window_fetch(wt, stream, recb, tid);
-    cp_async_commit();
-    uint32_t nxt[10];
-#pragma unroll
-    for (int i = 0; i < 10; i++) nxt[i] = wt[i];
-    for (uint32_t w = 0; w < nwin; w++) {
-        uint32_t cur[10];
-#pragma unroll
-        for (int i = 0; i < 10; i++) cur[i] = nxt[i];
-        // 1. generator phase
-#pragma unroll
-        for (int i = 0; i < kWin; i++) {
-#pragma unroll
-            for (int kk = 0; kk < 8; kk++) {
-                if (kk % 4 == 0) rngb[(i * 8 + rl) * 8 + rh + kk] = x.next();
-                else x.advance();
-            }
-        }
-        if (w + 1 < nwin) {
-            const uint32_t* en = wt + 16 * (size_t)(w + 1);
-            window_fetch(en, stream, recb + ((w + 1) & 1) * kWinRecWords, tid);
-#pragma unroll
-            for (int i = 0; i < 10; i++) nxt[i] = en[i];
-        }
-        cp_async_commit();
-        cp_async_wait1();
-        __syncwarp();
-        // 2. decision phase
-        const uint32_t* rb = recb + (w & 1) * kWinRecWords;
-        uint32_t off[8];
-        off[0] = 0;
-#pragma unroll
-        for (int i = 1; i < 8; i++) off[i] = off[i - 1] + (cur[i - 1] >> 24);
-        const uint32_t levels = cur[8], maxl = cur[9];
-        for (uint32_t L = 0; L <= maxl; L++) {
-#pragma unroll
-            for (int m = 0; m < 2; m++) {
-                const int i = cs + 4 * m;
-                const uint32_t v = w * kWin + i;
-                if (v < d.n && ((levels >> (4 * i)) & 15u) == L) {
-                    const uint32_t* rec = rb + 4 * off[i];
-                    const uint32_t hdr = rec[0];
-                    const uint32_t deg = hdr & 0x1Fu;
-                    const uint32_t deg4 = (deg + 3u) & ~3u;
-                    const uint32_t xb = spc[8u * v];
-                    uint64_t res[8];
-                    const uint64_t* rp = rngb + (i * 8 + cl) * 8;
-#pragma unroll
-                    for (int k = 0; k < 8; k++) res[k] = rp[k];
-                    uint32_t flips = 0;
-                    if constexpr (MODE == kModeInt) {
-                        int32_t* deb = reinterpret_cast<int32_t*>(deb_) + (i * 8 + cl) * 8;
-                        if (!(hdr & kRecClamp)) {
-                            uint32_t aL = 0, aH = 0;
-#pragma unroll
-                            for (int qd = 0; qd < 4; qd++) {
-                                if ((uint32_t)(4 * qd) < deg) {
-                                    const uint4 e4 = *reinterpret_cast<const uint4*>(rec + 4 + 4 * qd);
-                                    const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
-                                    uint32_t li[4];
-#pragma unroll
-                                    for (int e = 0; e < 4; e++)
-                                        li[e] = spc[8u * (en[e] & 0xFFFFFFu)] | ((en[e] >> 23) & 0x100u);
-#pragma unroll
-                                    for (int e = 0; e < 4; e++) {
-                                        const uint2 sv = lut[li[e]];
-                                        const uint32_t ww = (en[e] >> 24) & 0x7Fu;
-                                        aL += ww * sv.x;
-                                        aH += ww * sv.y;
-                                    }
-                                }
-                            }
-                            const int lp = (int)(hdr >> 16) - 128;
-                            const uint32_t cA = (uint32_t)(H + lp) * 0x01010101u;
-                            const uint32_t cB = (uint32_t)(H - lp) * 0x01010101u;
-                            const uint32_t xL = spread4(xb) * 0xFFu;
-                            const uint32_t xH = spread4(xb >> 4) * 0xFFu;
-                            const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
-                            const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
-#pragma unroll
-                            for (int k = 0; k < 8; k++) {
-                                const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
-                                const bool acc = res[k] <= tab[idx];
-                                flips |= (uint32_t)acc << k;
-                                deb[k] = acc ? (int32_t)idx - H : 0;
-                            }
-                        } else {
-#pragma unroll
-                            for (int k = 0; k < 8; k++) deb[k] = 0;
-                        }
-                    } else {
-                        double* deb = reinterpret_cast<double*>(deb_) + (i * 8 + cl) * 8;
-                        if (!(hdr & kRecClamp)) {
-                            const double wl = *reinterpret_cast<const double*>(rec + 2);
-                            const uint32_t* cols = rec + 4;
-                            const double* vals = reinterpret_cast<const double*>(rec + 4 + deg4);
-                            double dl[8], tp[8];
-#pragma unroll
-                            for (int k = 0; k < 8; k++) {
-                                const bool xv = (xb >> k) & 1u;
-                                tp[k] = xv ? -1.0 : 1.0;
-                                dl[k] = xv ? -wl : wl;
-                            }
-#pragma unroll
-                            for (int qd = 0; qd < 4; qd++) {
-                                if ((uint32_t)(4 * qd) < deg) {
-                                    const uint4 c4 = *reinterpret_cast<const uint4*>(cols + 4 * qd);
-                                    const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
-                                    const double2 w01 = *reinterpret_cast<const double2*>(vals + 4 * qd);
-                                    const double2 w23 = *reinterpret_cast<const double2*>(vals + 4 * qd + 2);
-                                    const double wv[4] = {w01.x, w01.y, w23.x, w23.y};
-                                    uint32_t bj[4];
-#pragma unroll
-                                    for (int e = 0; e < 4; e++) bj[e] = spc[8u * cc[e]];
-#pragma unroll
-                                    for (int e = 0; e < 4; e++) {
-                                        if ((uint32_t)(4 * qd + e) < deg) {
-#pragma unroll
-                                            for (int k = 0; k < 8; k++)
-                                                dl[k] = __fma_rn(wv[e], ((bj[e] >> k) & 1u) ? tp[k] : 0.0, dl[k]);
-                                        }
-                                    }
-                                }
-                            }
-#pragma unroll
-                            for (int k = 0; k < 8; k++) {
-                                const bool acc = metropolis_accept_f64(dl[k], beta, res[k]);
-                                flips |= (uint32_t)acc << k;
-                                deb[k] = acc ? dl[k] : 0.0;
-                            }
-                        } else {
-#pragma unroll
-                            for (int k = 0; k < 8; k++) deb[k] = 0.0;
-                        }
-                    }
-                    spc[8u * v] = (uint8_t)(xb ^ flips);
-                }
-            }
-            __syncwarp();
-        }
-        // 3. energies in site order (calls rh and rh + 4 of lane rl)
-#pragma unroll
-        for (int i = 0; i < kWin; i++) {
-            if (w * kWin + i < d.n) {
-#pragma unroll
-                for (int j = 0; j < 2; j++) {
-                    const int o = (i * 8 + rl) * 8 + rh + 4 * j;
-                    if constexpr (MODE == kModeInt) E[j] += reinterpret_cast<const int32_t*>(deb_)[o];
-                    else E[j] = __dadd_rn(E[j], reinterpret_cast<const double*>(deb_)[o]);
-                }
-            }
-        }
-        __syncwarp();
-    }
-    cp_async_wait0();
-    __syncwarp();
+// Warp-specialized form: warp 0 is the generator (producer) and NC warps are
+// deciders (consumers); the generator fills window w+1's outputs while the
+// deciders work on window w. Hand-over through two output buffers guarded by
+// named barriers (bar.arrive by the producing side, bar.sync by the waiting
+// side, with the exact thread count of the CTA), so no thread spins.
+constexpr int kRS = 10;  // u64 per (site, lane) row of the output / dE buffers (8 calls + padding against bank conflicts)
+constexpr int kBarFull0 = 1, kBarEmpty0 = 3, kBarCons = 5;
+
+__device__ __forceinline__ void bar_sync(int id, int count) { asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
+__device__ __forceinline__ void bar_arrive(int id, int count) { asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
+
+__host__ __device__ constexpr size_t ws_smem_bytes(uint32_t spin_cap) {
+    // tab 2 KB | spread table 4 KB | outputs 2 x 64 rows | dE 64 rows | records 2 x 1664 B | spins
+    return 2048 + 4096 + 2 * 64 * kRS * 8 + 64 * kRS * 8 + 2 * kWinRecWords * 4 + (size_t)spin_cap * 8;
 }
 
 template <uint32_t MODE>
-__global__ void __launch_bounds__(32, 1) window_kernel(DevArrays A, RunArgs R, uint32_t spin_cap) {
+struct WsCfg {
+    static constexpr int NC = MODE == kModeInt ? 2 : 4;   // decider warps
+    static constexpr int THREADS = 32 * (1 + NC);
+    static constexpr int SPLIT = MODE == kModeInt ? 1 : 2;  // decider threads per (site, lane) task
+    static constexpr int KPT = 8 / SPLIT;                  // calls decided per thread
+};
+
+// One (site, lane) decision task (or one half of it in f64 mode): dE of the
+// thread's calls, Metropolis decisions, the accepted dE into deb, and the new
+// spin byte. Returns the flip bits of the thread's calls.
+template <uint32_t MODE>
+__device__ __forceinline__ uint32_t ws_task(const uint32_t* rec, uint8_t* spc, uint32_t v, const uint64_t* rp,
+                                            void* debrow, const uint2* __restrict__ lut,
+                                            const uint64_t* __restrict__ tab, int H, double beta, int half) {
+    constexpr int KPT = WsCfg<MODE>::KPT;
+    const uint32_t hdr = rec[0];
+    const uint32_t deg = hdr & 0x1Fu;
+    const uint32_t deg4 = (deg + 3u) & ~3u;
+    const uint32_t xb = spc[8u * v];
+    uint32_t flips = 0;
+    if constexpr (MODE == kModeInt) {
+        int64_t* deb = reinterpret_cast<int64_t*>(debrow);
+        if (hdr & kRecClamp) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) deb[k] = 0;
+            return 0;
+        }
+        uint64_t res[8];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const ulonglong2 r2 = *reinterpret_cast<const ulonglong2*>(rp + 2 * q);
+            res[2 * q] = r2.x;
+            res[2 * q + 1] = r2.y;
+        }
+        uint32_t aL = 0, aH = 0;
+#pragma unroll
+        for (int qd = 0; qd < 4; qd++) {
+            if ((uint32_t)(4 * qd) < deg) {
+                const uint4 e4 = *reinterpret_cast<const uint4*>(rec + 4 + 4 * qd);
+                const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
+                uint32_t li[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) li[e] = spc[8u * (en[e] & 0xFFFFFFu)] | ((en[e] >> 23) & 0x100u);
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const uint2 sv = lut[li[e]];
+                    const uint32_t ww = (en[e] >> 24) & 0x7Fu;
+                    aL += ww * sv.x;
+                    aH += ww * sv.y;
+                }
+            }
+        }
+        const int lp = (int)(hdr >> 16) - 128;
+        const uint32_t cA = (uint32_t)(H + lp) * 0x01010101u;
+        const uint32_t cB = (uint32_t)(H - lp) * 0x01010101u;
+        const uint32_t xL = spread4(xb) * 0xFFu;
+        const uint32_t xH = spread4(xb >> 4) * 0xFFu;
+        const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
+        const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
+            const bool acc = res[k] <= tab[idx];
+            flips |= (uint32_t)acc << k;
+            deb[k] = acc ? (int64_t)((int32_t)idx - H) : 0;
+        }
+    } else {
+        double* deb = reinterpret_cast<double*>(debrow) + KPT * half;
+        if (hdr & kRecClamp) {
+#pragma unroll
+            for (int j = 0; j < KPT; j++) deb[j] = 0.0;
+            return 0;
+        }
+        uint64_t res[KPT];
+#pragma unroll
+        for (int q = 0; q < KPT / 2; q++) {
+            const ulonglong2 r2 = *reinterpret_cast<const ulonglong2*>(rp + KPT * half + 2 * q);
+            res[2 * q] = r2.x;
+            res[2 * q + 1] = r2.y;
+        }
+        const double wl = *reinterpret_cast<const double*>(rec + 2);
+        const uint32_t* cols = rec + 4;
+        const double* vals = reinterpret_cast<const double*>(rec + 4 + deg4);
+        const uint32_t xs = xb >> (KPT * half);
+        double dl[KPT], tp[KPT];
+#pragma unroll
+        for (int j = 0; j < KPT; j++) {
+            const bool xv = (xs >> j) & 1u;
+            tp[j] = xv ? -1.0 : 1.0;
+            dl[j] = xv ? -wl : wl;
+        }
+#pragma unroll
+        for (int qd = 0; qd < 4; qd++) {
+            if ((uint32_t)(4 * qd) < deg) {
+                const uint4 c4 = *reinterpret_cast<const uint4*>(cols + 4 * qd);
+                const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+                const double2 w01 = *reinterpret_cast<const double2*>(vals + 4 * qd);
+                const double2 w23 = *reinterpret_cast<const double2*>(vals + 4 * qd + 2);
+                const double wv[4] = {w01.x, w01.y, w23.x, w23.y};
+                uint32_t bj[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) bj[e] = spc[8u * cc[e]] >> (KPT * half);
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    if ((uint32_t)(4 * qd + e) < deg) {
+#pragma unroll
+                        for (int j = 0; j < KPT; j++) dl[j] = __fma_rn(wv[e], ((bj[e] >> j) & 1u) ? tp[j] : 0.0, dl[j]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < KPT; j++) {
+            const bool acc = metropolis_accept_f64(dl[j], beta, res[j]);
+            flips |= (uint32_t)acc << (KPT * half + j);
+            deb[j] = acc ? dl[j] : 0.0;
+        }
+    }
+    return flips;
+}
+
+template <uint32_t MODE>
+__global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArrays A, RunArgs R, uint32_t spin_cap) {
+    constexpr int NC = WsCfg<MODE>::NC;
+    constexpr int NT = WsCfg<MODE>::THREADS;
+    constexpr int SPLIT = WsCfg<MODE>::SPLIT;
     extern __shared__ __align__(16) uint64_t dsm[];
+    __shared__ uint32_t s_item;
     uint64_t* tab = dsm;
     uint2* lut = reinterpret_cast<uint2*>(dsm + 256);
-    uint64_t* rngb = dsm + 768;
-    void* deb = dsm + 768 + 512;
-    uint32_t* recb = reinterpret_cast<uint32_t*>(dsm + 768 + 1024);
-    uint64_t* sw = dsm + 768 + 1024 + kWinRecWords;
+    uint64_t* rngb = dsm + 768;                            // 2 x 64 rows of kRS
+    uint64_t* deb = rngb + 2 * 64 * kRS;                   // 64 rows of kRS
+    uint32_t* recb = reinterpret_cast<uint32_t*>(deb + 64 * kRS);
+    uint64_t* sw = reinterpret_cast<uint64_t*>(recb + 2 * kWinRecWords);
     const int tid = threadIdx.x;
-    const int rl = tid >> 2, rh = tid & 3;
-    uint8_t* spc = reinterpret_cast<uint8_t*>(sw) + (tid & 7);
+    const bool producer = tid < 32;
+    const int c = tid - 32;  // decider index
+    // decider task: site ti (0..7), lane tl, half th
+    const int ti = producer ? 0 : c / (8 * SPLIT);
+    const int tl = producer ? 0 : (c / SPLIT) & 7;
+    const int th = producer ? 0 : c % SPLIT;
+    uint8_t* spc = reinterpret_cast<uint8_t*>(sw) + tl;
     typedef typename std::conditional<MODE == kModeInt, int32_t, double>::type EType;
     if constexpr (MODE == kModeInt) {
-        for (int i = tid; i < 512; i += 32) {
+        for (int i = tid; i < 512; i += NT) {
             const uint32_t b = (i < 256 ? (uint32_t)i : (uint32_t)(i - 256) ^ 0xFFu);
             lut[i] = make_uint2(spread4(b), spread4(b >> 4));
         }
-        __syncwarp();
     }
+    __syncthreads();
     for (;;) {
-        uint32_t q = 0;
-        if (tid == 0) q = atomicAdd(R.queue, 1u);
-        q = __shfl_sync(0xffffffffu, q, 0);
+        if (tid == 0) s_item = atomicAdd(R.queue, 1u);
+        __syncthreads();
+        const uint32_t q = s_item;
+        __syncthreads();
         if (q >= R.nquads) break;
         const uint32_t inst = R.quads[4 * q];
         if (inst == 0xffffffffu) continue;
@@ -817,55 +790,136 @@ __global__ void __launch_bounds__(32, 1) window_kernel(DevArrays A, RunArgs R, u
 #pragma unroll
         for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
         const uint64_t pos0 = A.pos[inst];
-        EType E[2];
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const size_t o = d.energy + rl + 8 * (rh + 4 * j);
-            if constexpr (MODE == kModeInt) E[j] = A.Ei[o];
-            else E[j] = A.Ef[o];
+        // energies: decider c < 64 owns replica (lane c / 8, call c % 8)
+        const int el = c >> 3, ek = c & 7;
+        const bool eown = !producer && c < 64;
+        EType E = 0;
+        if (eown) {
+            const size_t o = d.energy + el + 8 * ek;
+            if constexpr (MODE == kModeInt) E = A.Ei[o];
+            else E = A.Ef[o];
         }
         const uint64_t* gw = A.spins + d.spin;
-        for (uint32_t i = tid; i < d.n; i += 32) sw[i] = gw[i];
-        __syncwarp();
+        for (uint32_t i = tid; i < d.n; i += NT) sw[i] = gw[i];
+        const uint32_t nwin = (d.n + kWin - 1) / kWin;
+        const uint32_t* wt = A.wtab + d.win;
+        const uint32_t* stream = A.recs + d.rec;
         for (uint32_t s = 0; s < R.steps; s++) {
+            __syncthreads();
             const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
             if constexpr (MODE == kModeInt) {
-                __syncwarp();
-                for (int i = tid; i < 2 * H + 1; i += 32) tab[i] = metropolis_threshold(i - H, beta);
-                __syncwarp();
+                for (int i = tid; i < 2 * H + 1; i += NT) tab[i] = metropolis_threshold(i - H, beta);
+                __syncthreads();
             }
             const uint64_t base = chacha8_draw(key, pos0 + s);
-            window_sweep<MODE>(A, d, rngb, deb, recb, spc, lut, tab, H, beta, base, tid, E);
-            if constexpr (MODE == kModeF64) {
-                if ((R.step_base + s + 1) % kResyncEvery == 0) {
-                    double e8[8];
-                    energies_f64_sp(A, d, reinterpret_cast<const uint8_t*>(sw) + rl, e8);
+            if (producer) {
+                const int rl = tid >> 2, rh = tid & 3;
+                Xoshiro x;
+                x.seed_lane(base, rl);
+                for (int i = 0; i < rh; i++) x.advance();
+                for (uint32_t w = 0; w < nwin; w++) {
+                    const int b = w & 1;
+                    if (w >= 2) bar_sync(kBarEmpty0 + b, NT);
+                    uint64_t* ob = rngb + b * 64 * kRS;
 #pragma unroll
-                    for (int j = 0; j < 2; j++) {
-                        double vv = e8[0];
+                    for (int i = 0; i < kWin; i++) {
 #pragma unroll
-                        for (int k = 0; k < 8; k++)
-                            if (k == rh + 4 * j) vv = e8[k];
-                        E[j] = vv;
+                        for (int kk = 0; kk < 8; kk++) {
+                            if (kk % 4 == 0) ob[(i * 8 + rl) * kRS + rh + kk] = x.next();
+                            else x.advance();
+                        }
                     }
-                    __syncwarp();
+                    bar_arrive(kBarFull0 + b, NT);
+                }
+                for (uint32_t w = nwin >= 2 ? nwin - 2 : 0; w < nwin; w++) bar_sync(kBarEmpty0 + (w & 1), NT);
+            } else {
+                window_fetch(wt, stream, recb, c, 32 * NC);
+                cp_async_commit();
+                uint32_t nxt[10];
+#pragma unroll
+                for (int i = 0; i < 10; i++) nxt[i] = wt[i];
+                for (uint32_t w = 0; w < nwin; w++) {
+                    const int b = w & 1;
+                    uint32_t cur[10];
+#pragma unroll
+                    for (int i = 0; i < 10; i++) cur[i] = nxt[i];
+                    if (w + 1 < nwin) {
+                        const uint32_t* en = wt + 16 * (size_t)(w + 1);
+                        window_fetch(en, stream, recb + ((w + 1) & 1) * kWinRecWords, c, 32 * NC);
+#pragma unroll
+                        for (int i = 0; i < 10; i++) nxt[i] = en[i];
+                    }
+                    cp_async_commit();
+                    cp_async_wait1();
+                    bar_sync(kBarFull0 + b, NT);  // outputs of window w are ready; records visible too
+                    const uint32_t* rb = recb + (w & 1) * kWinRecWords;
+                    uint32_t off = 0;
+#pragma unroll
+                    for (int i = 0; i < 8; i++)
+                        if (i < ti) off += cur[i] >> 24;
+                    const uint32_t v = w * kWin + ti;
+                    const uint32_t lev = (cur[8] >> (4 * ti)) & 15u;
+                    const uint64_t* rp = rngb + b * 64 * kRS + (ti * 8 + tl) * kRS;
+                    uint64_t* drow = deb + (ti * 8 + tl) * kRS;
+                    for (uint32_t L = 0; L <= cur[9]; L++) {
+                        if (v < d.n && lev == L) {
+                            // the SPLIT threads of a task read the byte before any of
+                            // them writes (the shuffles order them), then all write
+                            // the same combined value
+                            const uint32_t xb0 = spc[8u * v];
+                            uint32_t f = ws_task<MODE>(rb + 4 * off, spc, v, rp, drow, lut, tab, H, beta, th);
+                            if constexpr (SPLIT >= 2) {
+                                const unsigned pm = ((1u << SPLIT) - 1u) << (tid & 31 & ~(SPLIT - 1));
+                                f |= __shfl_xor_sync(pm, f, 1);
+                                if constexpr (SPLIT >= 4) f |= __shfl_xor_sync(pm, f, 2);
+                            }
+                            spc[8u * v] = (uint8_t)(xb0 ^ f);
+                        }
+                        bar_sync(kBarCons, 32 * NC);
+                    }
+                    bar_arrive(kBarEmpty0 + b, NT);
+                    if (eown) {
+#pragma unroll
+                        for (int i = 0; i < kWin; i++) {
+                            if (w * kWin + i < d.n) {
+                                const uint64_t* dr = deb + (i * 8 + el) * kRS;
+                                if constexpr (MODE == kModeInt) E += (int32_t) reinterpret_cast<const int64_t*>(dr)[ek];
+                                else E = __dadd_rn(E, reinterpret_cast<const double*>(dr)[ek]);
+                            }
+                        }
+                    }
+                    bar_sync(kBarCons, 32 * NC);
+                }
+                cp_async_wait0();
+                if constexpr (MODE == kModeF64) {
+                    if ((R.step_base + s + 1) % kResyncEvery == 0) {
+                        bar_sync(kBarCons, 32 * NC);
+                        if (eown) {
+                            double e8[8];
+                            energies_f64_sp(A, d, reinterpret_cast<const uint8_t*>(sw) + el, e8);
+                            double vv = e8[0];
+#pragma unroll
+                            for (int k = 0; k < 8; k++)
+                                if (k == ek) vv = e8[k];
+                            E = vv;
+                        }
+                    }
                 }
             }
         }
-        __syncwarp();
+        __syncthreads();
         uint64_t* gwo = A.spins + d.spin;
-        for (uint32_t i = tid; i < d.n; i += 32) gwo[i] = sw[i];
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const size_t o = d.energy + rl + 8 * (rh + 4 * j);
-            if constexpr (MODE == kModeInt) A.Ei[o] = E[j];
-            else A.Ef[o] = E[j];
+        for (uint32_t i = tid; i < d.n; i += NT) gwo[i] = sw[i];
+        if (eown) {
+            const size_t o = d.energy + el + 8 * ek;
+            if constexpr (MODE == kModeInt) A.Ei[o] = E;
+            else A.Ef[o] = E;
         }
-        __syncwarp();
         if (tid == 0) {
             A.pos[inst] = pos0 + R.steps;
             A.deo[inst] ^= (int32_t)(exchanges_in(R.step_base, R.steps, R.exchange_interval) & 1u);
         }
+        __syncthreads();
     }
 }
 
@@ -1316,19 +1370,22 @@ static int occ_win(size_t smem) {
     int n = 0;
     if (cudaFuncSetAttribute(window_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, window_kernel<MODE>, 32, smem) == cudaSuccess ? n : 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, window_kernel<MODE>, WsCfg<MODE>::THREADS, smem) ==
+                   cudaSuccess
+               ? n
+               : 0;
 }
 
 int window_occupancy(uint32_t mode, uint32_t spin_cap) {
-    const size_t sm = window_smem_bytes(spin_cap);
+    const size_t sm = ws_smem_bytes(spin_cap);
     return mode == kModeInt ? occ_win<kModeInt>(sm) : occ_win<kModeF64>(sm);
 }
 
 cudaError_t launch_window(const DevArrays& A, const RunArgs& R, uint32_t mode, uint32_t spin_cap, int grid,
                           cudaStream_t st) {
-    const size_t sm = window_smem_bytes(spin_cap);
-    if (mode == kModeInt) window_kernel<kModeInt><<<grid, 32, sm, st>>>(A, R, spin_cap);
-    else window_kernel<kModeF64><<<grid, 32, sm, st>>>(A, R, spin_cap);
+    const size_t sm = ws_smem_bytes(spin_cap);
+    if (mode == kModeInt) window_kernel<kModeInt><<<grid, WsCfg<kModeInt>::THREADS, sm, st>>>(A, R, spin_cap);
+    else window_kernel<kModeF64><<<grid, WsCfg<kModeF64>::THREADS, sm, st>>>(A, R, spin_cap);
     return cudaGetLastError();
 }
 

@@ -228,6 +228,17 @@ class BatchEngine:
         _ffi.check(self._L.ie_batch_last_run_ms(self._h, _p(ms)))
         return float(ms[0])
 
+    def class_report(self):
+        """Per work class of the last run: (mode, threads per lane, capacity,
+        items, device ms); threads per lane 8 marks the windowed kernel."""
+        n = np.zeros(1, dtype=np.uint32)
+        info = np.zeros(5 * 64, dtype=np.uint32)
+        ms = np.zeros(64, dtype=np.float64)
+        _ffi.check(self._L.ie_batch_class_report(self._h, 64, _p(n), _p(info), _p(ms)))
+        k = int(min(n[0], 64))
+        return [(("int", "f64")[info[5 * i]], int(info[5 * i + 1]), int(info[5 * i + 2]),
+                 int(info[5 * i + 3]), float(ms[i])) for i in range(k)]
+
     def last_launches(self) -> int:
         n = np.zeros(1, dtype=np.uint64)
         _ffi.check(self._L.ie_batch_last_launches(self._h, _p(n)))
