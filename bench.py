@@ -297,7 +297,7 @@ def run_ours(args):
                        "thread_classes": ({"n4_int": tuned[0], "n2_int": tuned[1], "n4_f64": tuned[2],
                                            "n2_f64": tuned[3]} if tuned else "default")},
             "roofline": {"bound": "alu", "achieved": achieved_ops / 1e9, "peak": ip.value / 1e9,
-                         "unit": "Gop/s", "frac": achieved_ops / ip.value, "traffic": traffic,
+                         "unit": "Gop/s", "frac": achieved_ops / ip.value, "traffic": traffic, "traffic_source": "profiles/batched_step_traffic.json (ncu, bytes per attempt x attempts per step)" if traffic else None,
                          "ops_per_attempt": OPS_PER_ATTEMPT,
                          "peak_source": "measured in-run: int32 LOP3/IADD3 microkernel (ie_probe_peaks)",
                          "per": "step: one group of concurrent class launches",
