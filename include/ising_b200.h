@@ -199,6 +199,53 @@ ie_status ie_sa_run_static(const ie_problem_device* problem, uint64_t seed, cons
                            uint64_t n_steps, uint64_t* words, double* energies, int32_t device,
                            void* stream);
 
+/* ---- serving: continuous batching of SA requests ----
+ * Replaces the request loop of the reference's HTTP server
+ * (src/bin/server_api.rs:180-213: validate, take a compute permit, solve on the
+ * Rayon pool, return) with a device-resident request pool. Requests are
+ * single-cell SA solves (64 replicas, one temperature per step). A request
+ * is admitted, first come first served, once a slot and room in every device
+ * pool (sites, couplings, records, schedule) are free; it stays resident
+ * (spins, energies, generator position) until its schedule is done, and
+ * every tick advances each resident request by up to max(1, site_budget / N)
+ * steps in one group of persistent launches, so requests of different sizes
+ * and arrival times share the GPU. A request's result does not depend on
+ * what else is resident: it equals ie_batch_run_schedule of the same problem,
+ * seed and temperatures alone.
+ * ie_serve_submit, ie_serve_poll and ie_serve_result may be called from any
+ * thread, also while ie_serve_tick runs; ie_serve_tick from one thread at a
+ * time. */
+typedef struct ie_serve ie_serve;
+typedef struct ie_serve_config {
+    int32_t device;
+    int32_t force_f64;
+    uint32_t max_requests;       /* resident request slots (0: 4096) */
+    uint32_t site_budget;        /* site-steps per request per tick (0: 65536) */
+    uint64_t max_sites;          /* summed num_vars of resident requests (0: 2^24) */
+    uint64_t max_couplings;      /* summed stored couplings, both triangles (0: 2^27) */
+    uint64_t max_schedule_steps; /* summed schedule lengths (0: 2^25) */
+} ie_serve_config;
+
+ie_status ie_serve_create(const ie_serve_config* config, ie_serve** out);
+ie_status ie_serve_destroy(ie_serve* s);
+/* Validates and prepares the request on the calling thread and queues it.
+ * temps: host [n_steps]; is_clamped / clamp_val: [num_vars] or NULL.
+ * IE_ERR_OOM when the request alone exceeds a pool's capacity,
+ * IE_ERR_UNSUPPORTED when it does not fit the kernels' shared memory. */
+ie_status ie_serve_submit(ie_serve* s, const ie_problem* problem, uint64_t seed, const double* temps,
+                          uint64_t n_steps, const uint8_t* is_clamped, const int8_t* clamp_val, uint64_t* id);
+/* Admits queued requests, runs one tick, retires finished requests. */
+ie_status ie_serve_tick(ie_serve* s, uint32_t* n_active, uint32_t* n_pending, uint32_t* n_finished);
+/* Ids of finished requests whose results have not been taken yet. */
+ie_status ie_serve_poll(ie_serve* s, uint64_t* ids, uint32_t max_ids, uint32_t* n_ids);
+/* Takes a finished request's result: words [num_vars] (bit r = replica r) and
+ * energies [64] (model energy without the offset); frees its record. */
+ie_status ie_serve_result(ie_serve* s, uint64_t id, uint64_t* words, double* energies);
+/* Device bytes a request would hold while resident (its admission footprint). */
+ie_status ie_serve_footprint(ie_serve* s, const ie_problem* problem, uint64_t n_steps, uint64_t* bytes);
+/* Device time of the last tick and kernel launches in it. */
+ie_status ie_serve_last_tick(ie_serve* s, double* ms, uint64_t* launches);
+
 /* ---- measurement helper (no reference counterpart) ----
  * Measured roofline denominators on `device`: int32 LOP3/IADD3 throughput
  * (ops/s) and Xoshiro256++ step+compare throughput (outputs/s), the per-attempt

@@ -106,6 +106,7 @@ struct HostInst {
     std::vector<double> lin;
     std::vector<uint32_t> recpos, reclen;  // first record of each site: word offset and length in its stream
     bool windowed_ok = false;              // eligible for the windowed kernel
+    uint64_t nnz = 0;
 };
 
 ie_status ingest(const ie_problem* p, bool force_f64, HostInst& out) {
@@ -119,6 +120,7 @@ ie_status ingest(const ie_problem* p, bool force_f64, HostInst& out) {
     if (nnz >= (1ULL << 32)) return fail(IE_ERR_INVALID, "too many couplings");
     if (nnz && (!p->col_indices || !p->values)) return fail(IE_ERR_INVALID, "col_indices/values must be non-NULL");
     out.n = (uint32_t)n;
+    out.nnz = nnz;
     out.offset = p->energy_offset;
     out.rows.resize(n + 1);
     out.lin.assign(p->linear, p->linear + n);
@@ -312,6 +314,46 @@ ie_status build_records(HostInst& h, const std::vector<uint8_t>& clampf, size_t 
     return IE_OK;
 }
 
+// Window table of the windowed kernel (layout in ie_kernels.cu), 16 words per
+// window of 8 sites: an instance qualifies when every site has at most 16
+// couplings (one record) and its windows have on average at least 2 sites per
+// dependency level. Sets h.windowed_ok; needs h.recpos / h.reclen.
+bool window_table(HostInst& h, std::vector<uint32_t>& tab) {
+    h.windowed_ok = false;
+    tab.clear();
+    if (h.n < 8) return false;
+    for (uint32_t v = 0; v < h.n; v++)
+        if (h.rows[v + 1] - h.rows[v] > kRecMaxDeg) return false;
+    const uint32_t nwin = (h.n + 7) / 8;
+    tab.assign((size_t)nwin * 16, 0);
+    double par = 0;
+    for (uint32_t w = 0; w < nwin; w++) {
+        uint32_t lvl[8] = {0, 0, 0, 0, 0, 0, 0, 0}, maxl = 0, levels = 0;
+        for (uint32_t k = 0; k < 8; k++) {
+            const uint32_t v = 8 * w + k;
+            if (v >= h.n) break;
+            uint32_t l = 0;
+            for (uint32_t e = h.rows[v]; e < h.rows[v + 1]; e++) {
+                const uint32_t j = h.cols[e];
+                if (j >= 8 * w && j < v) l = std::max(l, lvl[j - 8 * w] + 1);
+            }
+            lvl[k] = l;
+            maxl = std::max(maxl, l);
+            levels |= l << (4 * k);
+            tab[16 * (size_t)w + k] = (h.recpos[v] / 4) | ((h.reclen[v] / 4) << 24);
+        }
+        tab[16 * (size_t)w + 8] = levels;
+        tab[16 * (size_t)w + 9] = maxl;
+        par += 8.0 / (maxl + 1);
+    }
+    if (par / nwin < 2.0) {
+        tab.clear();
+        return false;
+    }
+    h.windowed_ok = true;
+    return true;
+}
+
 int g_sm_count = -1;
 
 struct Engine {
@@ -334,7 +376,7 @@ struct Engine {
     DevBuf<double> d_vals, d_lin, d_Ef, d_temps, d_dbeta, d_scratch;
     DevBuf<uint8_t> d_clampf;
     DevBuf<int8_t> d_clampv;
-    DevBuf<uint64_t> d_spins, d_pos, d_att, d_acc, d_xtab, d_xoff, d_xdmax, d_xdund;
+    DevBuf<uint64_t> d_spins, d_pos, d_att, d_acc, d_xtab, d_xoff, d_xdmax, d_xdund, d_done;
 
     uint64_t steps_done = 0;
     bool quads_built = false;
@@ -358,7 +400,7 @@ struct Engine {
     }
 
     DevArrays arrays() const {
-        DevArrays A;
+        DevArrays A{};
         A.desc = d_desc.p;
         A.rows = d_rows.p;
         A.ents = d_ents.p;
@@ -379,6 +421,7 @@ struct Engine {
         A.att = d_att.p;
         A.acc = d_acc.p;
         A.err = d_err.p;
+        A.done = d_done.p;
         return A;
     }
 
@@ -511,40 +554,10 @@ struct Engine {
         return IE_OK;
     }
 
-    // Window tables of the windowed kernel (layout in ie_kernels.cu): an
-    // instance qualifies when every site has at most 16 couplings (one record)
-    // and its windows of 8 sites have on average at least 2 sites per level.
     void build_window_table(uint32_t i, std::vector<uint32_t>& wt) {
-        HostInst& h = insts[i];
-        h.windowed_ok = false;
         desc[i].win = 0;
-        if (h.n < 8 || nt != 1) return;
-        for (uint32_t v = 0; v < h.n; v++)
-            if (h.rows[v + 1] - h.rows[v] > kRecMaxDeg) return;
-        const uint32_t nwin = (h.n + 7) / 8;
-        std::vector<uint32_t> tab((size_t)nwin * 16, 0);
-        double par = 0;
-        for (uint32_t w = 0; w < nwin; w++) {
-            uint32_t lvl[8] = {0, 0, 0, 0, 0, 0, 0, 0}, maxl = 0, levels = 0;
-            for (uint32_t k = 0; k < 8; k++) {
-                const uint32_t v = 8 * w + k;
-                if (v >= h.n) break;
-                uint32_t l = 0;
-                for (uint32_t e = h.rows[v]; e < h.rows[v + 1]; e++) {
-                    const uint32_t j = h.cols[e];
-                    if (j >= 8 * w && j < v) l = std::max(l, lvl[j - 8 * w] + 1);
-                }
-                lvl[k] = l;
-                maxl = std::max(maxl, l);
-                levels |= l << (4 * k);
-                tab[16 * (size_t)w + k] = (h.recpos[v] / 4) | ((h.reclen[v] / 4) << 24);
-            }
-            tab[16 * (size_t)w + 8] = levels;
-            tab[16 * (size_t)w + 9] = maxl;
-            par += 8.0 / (maxl + 1);
-        }
-        if (par / nwin < 2.0) return;
-        h.windowed_ok = true;
+        std::vector<uint32_t> tab;
+        if (nt != 1 || !window_table(insts[i], tab)) return;
         desc[i].win = wt.size();
         wt.insert(wt.end(), tab.begin(), tab.end());
     }
@@ -576,7 +589,7 @@ struct Engine {
     }
 
     static double inst_work(const HostInst& h) {
-        const double deg = h.n ? (double)h.cols.size() / h.n : 0.0;
+        const double deg = h.n ? (double)h.nnz / h.n : 0.0;
         return (double)h.n * (deg + 12.0) * (h.mode == kModeF64 ? 2.5 : 1.0);
     }
 
@@ -624,6 +637,7 @@ struct Engine {
         return n > tune_n2[m] ? 2 : 1;
     }
     bool use_windows = true;
+    std::vector<uint8_t> active;  // instances in the work classes (empty: all)
     static uint32_t cap_of(uint32_t n) {
         for (uint32_t c : kCaps)
             if (n <= c) return c;
@@ -636,12 +650,14 @@ struct Engine {
     ie_status build_quads() {
         classes.clear();
         std::vector<std::tuple<uint32_t, int, uint32_t>> keys;
+        auto live = [&](uint32_t i) { return active.empty() || active[i] != 0; };
         for (uint32_t i = 0; i < count; i++) {
+            if (!live(i)) continue;
             auto k = std::make_tuple(desc[i].mode, tpl_of(i), cap_of(desc[i].n));
             if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
         }
         auto degree = [&](uint32_t i) {
-            return insts[i].n ? (uint32_t)((insts[i].cols.size() + insts[i].n / 2) / insts[i].n) : 0u;
+            return insts[i].n ? (uint32_t)((insts[i].nnz + insts[i].n / 2) / insts[i].n) : 0u;
         };
         for (auto& k : keys) {
             std::unique_ptr<WorkClass> wc(new WorkClass());
@@ -651,7 +667,7 @@ struct Engine {
             const int ng = wc->tpl == 8 ? 1 : 4 / wc->tpl;
             std::vector<uint32_t> order;
             for (uint32_t i = 0; i < count; i++)
-                if (desc[i].mode == wc->mode && tpl_of(i) == wc->tpl && cap_of(desc[i].n) == wc->cap)
+                if (live(i) && desc[i].mode == wc->mode && tpl_of(i) == wc->tpl && cap_of(desc[i].n) == wc->cap)
                     order.push_back(i);
             std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
                 if (degree(a) != degree(b)) return degree(a) > degree(b);
@@ -723,20 +739,29 @@ struct Engine {
         for (double x : t)
             if (!(x > 0.0) || !std::isfinite(x)) return fail(IE_ERR_INVALID, "temperatures must be positive");
         IE_TRY(d_temps.upload(t, stream));
+        IE_TRY(launch_classes(sa_args(steps)));
+        steps_done += steps;
+        return IE_OK;
+    }
+
+    // One persistent launch per work class, all in flight together on their
+    // own streams, largest classes first (their CTAs are dispatched first and
+    // the smaller classes fill the remaining room); waits for all of them.
+    ie_status launch_classes(const RunArgs& base) {
+        IE_TRY(ensure_class_streams(classes.size()));
         IE_CUDA(cudaMemsetAsync(d_queue.p, 0, classes.size() * sizeof(uint32_t), stream));
         IE_CUDA(cudaEventRecord(ev0, stream));
         uint64_t launches = 0;
-        // largest classes first: their CTAs are dispatched first and the
-        // smaller classes fill the remaining room
         for (size_t k = 0; k < classes.size(); k++) {
             WorkClass& wc = *classes[k];
             if (!wc.nitems) continue;
             IE_CUDA(cudaStreamWaitEvent(cstreams[k], ev0, 0));
-            int occ = wc.tpl == 8 ? window_occupancy(wc.mode, wc.cap) : batch_occupancy(wc.mode, wc.tpl, wc.cap);
+            int occ = wc.tpl == 8 ? window_occupancy(wc.mode, wc.cap)
+                                  : batch_occupancy(wc.mode, wc.tpl, wc.cap, base.serve != 0);
             if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
             if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
             const int grid = std::max(1, std::min<int>((int)wc.nitems, occ * g_sm_count));
-            RunArgs R = sa_args(steps);
+            RunArgs R = base;
             R.quads = wc.items.p;
             R.quad_h = wc.itemh.p;
             R.nquads = wc.nitems;
@@ -754,7 +779,6 @@ struct Engine {
         IE_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
         last_ms = ms;
         last_launches = launches;
-        steps_done += steps;
         class_ms.assign(classes.size(), 0.0);
         for (size_t k = 0; k < classes.size(); k++) {
             if (!classes[k]->nitems) continue;
@@ -868,7 +892,7 @@ struct Engine {
             R.nquads = 1;
             R.queue = counters.p + i;
             const uint32_t cap = std::max(64u, (desc[first + i].n + 63u) & ~63u);
-            if (batch_occupancy(desc[first + i].mode, 1, cap) <= 0)
+            if (batch_occupancy(desc[first + i].mode, 1, cap, false) <= 0)
                 return fail(IE_ERR_UNSUPPORTED, "instance too large for the plain kernel's shared memory");
             IE_CUDA(launch_batch(arrays(), R, desc[first + i].mode, 1, cap, 1, stream));
         }

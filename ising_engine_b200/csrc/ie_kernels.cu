@@ -185,6 +185,36 @@ __device__ __forceinline__ uint32_t exchanges_in(uint64_t base, uint32_t steps, 
     return (uint32_t)((base + steps) / k - base / k);
 }
 
+// The steps one instance runs in a batched launch: the launch's own schedule,
+// or in a serving launch the instance's schedule from its next unexecuted
+// step, at most max(1, site_budget / n) steps. Step s of the launch is global
+// step base + s of the instance and runs at temperature temps[tstride * s].
+struct StepPlan {
+    uint64_t base;
+    uint32_t steps;
+    uint32_t tstride;
+    const double* temps;
+};
+
+__device__ __forceinline__ StepPlan step_plan(const DevArrays& A, const RunArgs& R, const InstDesc& d,
+                                              uint32_t inst) {
+    StepPlan P;
+    if (R.serve) {
+        P.base = A.done[inst];
+        const uint64_t left = d.sched_len > P.base ? d.sched_len - P.base : 0;
+        const uint64_t want = max(1u, R.site_budget / max(d.n, 1u));
+        P.steps = (uint32_t)min(left, want);
+        P.tstride = 1;
+        P.temps = R.temps + d.sched + P.base;
+    } else {
+        P.base = R.step_base;
+        P.steps = R.steps;
+        P.tstride = R.temps_per_step;
+        P.temps = R.temps;
+    }
+    return P;
+}
+
 // ---------------------------------------------------------------------------
 // Batched single-cell kernel.
 //
@@ -457,11 +487,13 @@ __device__ void energies_f64_calls(const DevArrays& A, const InstDesc& d, const 
     }
 }
 
-// Dynamic shared memory of a batched CTA: threshold table (2 KB) | spread
-// table (4 KB) | NG rings | NG spin arrays of spin_cap words each (the
-// instance's spins stay resident in shared memory for the whole schedule).
-__host__ __device__ constexpr size_t batch_smem_bytes(int ng, uint32_t spin_cap) {
-    return 2048 + 4096 + (size_t)ng * kSlots * kChunk * 4 + (size_t)ng * spin_cap * 8;
+// Dynamic shared memory of a batched CTA: threshold tables (2 KB each: one
+// shared by the warp, or in a serving launch one per instance, whose
+// temperatures differ) | spread table (4 KB) | NG rings | NG spin arrays of
+// spin_cap words each (the instance's spins stay resident in shared memory
+// for the whole schedule).
+__host__ __device__ constexpr size_t batch_smem_bytes(int ng, uint32_t spin_cap, bool serve) {
+    return 2048 * (size_t)(serve ? ng : 1) + 4096 + (size_t)ng * kSlots * kChunk * 4 + (size_t)ng * spin_cap * 8;
 }
 
 template <uint32_t MODE, int TPL>
@@ -470,15 +502,17 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
     constexpr int NG = 4 / TPL;  // instances per warp
     constexpr int KP = 8 / TPL;
     extern __shared__ __align__(16) uint64_t dsm[];
-    uint64_t* tab = dsm;
     const int tid = threadIdx.x;
     const int g = tid / G;
     const int t = tid % G;
     const int lane = t / TPL;
     const int h = t % TPL;
-    uint2* lut = reinterpret_cast<uint2*>(dsm + 256);
-    uint32_t* ring = reinterpret_cast<uint32_t*>(dsm + 256 + 512) + (size_t)g * kSlots * kChunk;
-    uint64_t* sw = reinterpret_cast<uint64_t*>(reinterpret_cast<uint32_t*>(dsm + 256 + 512) +
+    const bool own_tab = R.serve != 0;  // per-instance threshold tables
+    const int ntab = own_tab ? NG : 1;
+    uint64_t* tab = dsm + (own_tab ? 256 * g : 0);
+    uint2* lut = reinterpret_cast<uint2*>(dsm + 256 * ntab);
+    uint32_t* ring = reinterpret_cast<uint32_t*>(dsm + 256 * ntab + 512) + (size_t)g * kSlots * kChunk;
+    uint64_t* sw = reinterpret_cast<uint64_t*>(reinterpret_cast<uint32_t*>(dsm + 256 * ntab + 512) +
                                                (size_t)NG * kSlots * kChunk) +
                    (size_t)g * spin_cap;
     // spread table: entry b (and 256 + b for a negative coupling, which
@@ -506,12 +540,14 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
         uint32_t key[8];
         uint64_t pos0 = 0;
         EType E[KP];
+        StepPlan P{R.step_base, own_tab ? 0u : R.steps, R.temps_per_step, R.temps};
         if (active) {
             d = A.desc[inst];
             if (d.n > spin_cap) {  // host sizing error: report and skip the instance
                 if (t == 0) atomicExch(A.err, 2);
                 continue;
             }
+            P = step_plan(A, R, d, inst);
 #pragma unroll
             for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
             pos0 = A.pos[inst];
@@ -525,18 +561,27 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
             for (uint32_t i = t; i < d.n; i += G) sw[i] = gw[i];
             __syncwarp(gmask);
         }
-        for (uint32_t s = 0; s < R.steps; s++) {
-            const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
+        // Shared table: every group (active or not) runs the launch's steps in
+        // step and the warp fills the table. Own tables: each active group runs
+        // its own steps and fills its own table.
+        for (uint32_t s = 0; s < P.steps; s++) {
+            const double beta = __ddiv_rn(1.0, P.temps[P.tstride ? s : 0]);
             if constexpr (MODE == kModeInt) {
-                __syncwarp();
-                for (int i = tid; i < 2 * H + 1; i += 32) tab[i] = metropolis_threshold(i - H, beta);
-                __syncwarp();
+                if (own_tab) {
+                    __syncwarp(gmask);
+                    for (int i = t; i < 2 * H + 1; i += G) tab[i] = metropolis_threshold(i - H, beta);
+                    __syncwarp(gmask);
+                } else {
+                    __syncwarp();
+                    for (int i = tid; i < 2 * H + 1; i += 32) tab[i] = metropolis_threshold(i - H, beta);
+                    __syncwarp();
+                }
             }
             if (active) {
                 const uint64_t base = chacha8_draw(key, pos0 + s);
                 sweep_stream<MODE, TPL>(A, d, ring, sp, lut, lane, h, gmask, tab, H, beta, base, E);
                 if constexpr (MODE == kModeF64) {
-                    if ((R.step_base + s + 1) % kResyncEvery == 0) {
+                    if ((P.base + s + 1) % kResyncEvery == 0) {
                         __syncwarp(gmask);
                         energies_f64_calls<TPL>(A, d, sp, h, E);
                     }
@@ -555,8 +600,9 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
             }
             __syncwarp(gmask);
             if (t == 0) {
-                A.pos[inst] = pos0 + R.steps;
-                A.deo[inst] ^= (int32_t)(exchanges_in(R.step_base, R.steps, R.exchange_interval) & 1u);
+                A.pos[inst] = pos0 + P.steps;
+                A.deo[inst] ^= (int32_t)(exchanges_in(P.base, P.steps, R.exchange_interval) & 1u);
+                if (R.serve) A.done[inst] = P.base + P.steps;
             }
         }
     }
@@ -786,6 +832,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
             if (tid == 0) atomicExch(A.err, 2);
             continue;
         }
+        const StepPlan P = step_plan(A, R, d, inst);
         uint32_t key[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
@@ -804,9 +851,9 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
         const uint32_t nwin = (d.n + kWin - 1) / kWin;
         const uint32_t* wt = A.wtab + d.win;
         const uint32_t* stream = A.recs + d.rec;
-        for (uint32_t s = 0; s < R.steps; s++) {
+        for (uint32_t s = 0; s < P.steps; s++) {
             __syncthreads();
-            const double beta = __ddiv_rn(1.0, R.temps[R.temps_per_step ? s : 0]);
+            const double beta = __ddiv_rn(1.0, P.temps[P.tstride ? s : 0]);
             if constexpr (MODE == kModeInt) {
                 for (int i = tid; i < 2 * H + 1; i += NT) tab[i] = metropolis_threshold(i - H, beta);
                 __syncthreads();
@@ -892,7 +939,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
                 }
                 cp_async_wait0();
                 if constexpr (MODE == kModeF64) {
-                    if ((R.step_base + s + 1) % kResyncEvery == 0) {
+                    if ((P.base + s + 1) % kResyncEvery == 0) {
                         bar_sync(kBarCons, 32 * NC);
                         if (eown) {
                             double e8[8];
@@ -916,8 +963,9 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
             else A.Ef[o] = E;
         }
         if (tid == 0) {
-            A.pos[inst] = pos0 + R.steps;
-            A.deo[inst] ^= (int32_t)(exchanges_in(R.step_base, R.steps, R.exchange_interval) & 1u);
+            A.pos[inst] = pos0 + P.steps;
+            A.deo[inst] ^= (int32_t)(exchanges_in(P.base, P.steps, R.exchange_interval) & 1u);
+            if (R.serve) A.done[inst] = P.base + P.steps;
         }
         __syncthreads();
     }
@@ -1341,10 +1389,10 @@ static int occ_of(size_t smem) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<MODE, TPL>, 32, smem) == cudaSuccess ? n : 0;
 }
 
-size_t batch_smem(int tpl, uint32_t spin_cap) { return batch_smem_bytes(4 / tpl, spin_cap); }
+size_t batch_smem(int tpl, uint32_t spin_cap, bool serve) { return batch_smem_bytes(4 / tpl, spin_cap, serve); }
 
-int batch_occupancy(uint32_t mode, int tpl, uint32_t spin_cap) {
-    const size_t sm = batch_smem(tpl, spin_cap);
+int batch_occupancy(uint32_t mode, int tpl, uint32_t spin_cap, bool serve) {
+    const size_t sm = batch_smem(tpl, spin_cap, serve);
     if (mode == kModeInt)
         return tpl == 1 ? occ_of<kModeInt, 1>(sm) : tpl == 2 ? occ_of<kModeInt, 2>(sm) : occ_of<kModeInt, 4>(sm);
     return tpl == 1 ? occ_of<kModeF64, 1>(sm) : tpl == 2 ? occ_of<kModeF64, 2>(sm) : occ_of<kModeF64, 4>(sm);
@@ -1352,7 +1400,7 @@ int batch_occupancy(uint32_t mode, int tpl, uint32_t spin_cap) {
 
 cudaError_t launch_batch(const DevArrays& A, const RunArgs& R, uint32_t mode, int tpl, uint32_t spin_cap, int grid,
                          cudaStream_t st) {
-    const size_t sm = batch_smem(tpl, spin_cap);
+    const size_t sm = batch_smem(tpl, spin_cap, R.serve != 0);
     if (mode == kModeInt) {
         if (tpl == 1) batch_kernel<kModeInt, 1><<<grid, 32, sm, st>>>(A, R, spin_cap);
         else if (tpl == 2) batch_kernel<kModeInt, 2><<<grid, 32, sm, st>>>(A, R, spin_cap);

@@ -27,6 +27,8 @@ struct InstDesc {
     uint64_t rec;    // site-record stream (batched kernel): recs[rec .. rec + rec_len)
     uint64_t rec_len;
     uint64_t win;    // window table (windowed kernel): wtab[win .. win + 16 * ceil(n / 8))
+    uint64_t sched;  // serving: the instance's per-step temperatures at temps[sched .. sched + sched_len)
+    uint64_t sched_len;
 };
 
 // Site-record streams of the batched kernel. Each instance's stream is a
@@ -67,6 +69,7 @@ struct DevArrays {
     uint64_t* att;           // swap attempts [stat + pair]
     uint64_t* acc;           // swap accepts
     int32_t* err;            // device error word
+    uint64_t* done;          // serving: steps of its schedule each instance has executed
 };
 
 // Run parameters of one launch.
@@ -87,6 +90,11 @@ struct RunArgs {
     const int32_t* quad_h;    // [nquads] largest H of the quad (integer mode)
     uint32_t nquads;
     uint32_t* queue;          // atomic counter
+    // serving: every instance runs its own schedule (InstDesc::sched) from
+    // its next unexecuted step (DevArrays::done) for up to
+    // max(1, site_budget / n) steps in this launch
+    uint32_t serve;
+    uint32_t site_budget;
 };
 
 }  // namespace ie

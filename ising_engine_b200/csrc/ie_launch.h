@@ -6,8 +6,8 @@
 
 namespace ie {
 cudaError_t set_smem_limits(size_t pt_bytes);
-size_t batch_smem(int tpl, uint32_t spin_cap);
-int batch_occupancy(uint32_t mode, int tpl, uint32_t spin_cap);
+size_t batch_smem(int tpl, uint32_t spin_cap, bool serve);
+int batch_occupancy(uint32_t mode, int tpl, uint32_t spin_cap, bool serve);
 cudaError_t launch_batch(const DevArrays& A, const RunArgs& R, uint32_t mode, int tpl, uint32_t spin_cap, int grid,
                          cudaStream_t st);
 int window_occupancy(uint32_t mode, uint32_t spin_cap);

@@ -266,7 +266,7 @@ extern "C" ie_status ie_sa_run_static(const ie_problem_device* problem, uint64_t
     R.nquads = 1;
     R.queue = d_queue;
     const uint32_t cap = (n + 63u) & ~63u;
-    if (batch_occupancy(kModeF64, 4, cap) <= 0) return static_fail(IE_ERR_UNSUPPORTED, "kernel does not fit");
+    if (batch_occupancy(kModeF64, 4, cap, false) <= 0) return static_fail(IE_ERR_UNSUPPORTED, "kernel does not fit");
     if (launch_batch(A, R, kModeF64, 4, cap, 1, st) != cudaSuccess)
         return static_fail(IE_ERR_CUDA, "sweep launch failed");
     static_export_kernel<<<(n + 255) / 256, 256, 0, st>>>(d_spins, n, words);
