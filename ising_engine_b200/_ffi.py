@@ -51,6 +51,12 @@ class ie_batch_config(C.Structure):
                 ("disable_windows", C.c_int32)]
 
 
+class ie_serve_config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("force_f64", C.c_int32), ("max_requests", C.c_uint32),
+                ("site_budget", C.c_uint32), ("max_sites", C.c_uint64), ("max_couplings", C.c_uint64),
+                ("max_schedule_steps", C.c_uint64)]
+
+
 _vp = C.c_void_p
 _SIGS = {
     "ie_last_error": ([], C.c_char_p),
@@ -86,6 +92,14 @@ _SIGS = {
     "ie_batch_last_launches": ([_vp, _vp], C.c_int),
     "ie_probe_peaks": ([C.c_int32, _vp, _vp], C.c_int),
     "ie_sa_run_static": ([_vp, C.c_uint64, _vp, C.c_uint64, _vp, _vp, C.c_int32, _vp], C.c_int),
+    "ie_serve_create": ([_vp, _vp], C.c_int),
+    "ie_serve_destroy": ([_vp], C.c_int),
+    "ie_serve_submit": ([_vp, _vp, C.c_uint64, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
+    "ie_serve_tick": ([_vp, _vp, _vp, _vp], C.c_int),
+    "ie_serve_poll": ([_vp, _vp, C.c_uint32, _vp], C.c_int),
+    "ie_serve_result": ([_vp, C.c_uint64, _vp, _vp], C.c_int),
+    "ie_serve_footprint": ([_vp, _vp, C.c_uint64, _vp], C.c_int),
+    "ie_serve_last_tick": ([_vp, _vp, _vp], C.c_int),
 }
 
 

@@ -6,8 +6,11 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <deque>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <tuple>
@@ -67,10 +70,12 @@ double powi_rt(double a, int b) {
     return recip ? 1.0 / r : r;
 }
 
+// Device array; alloc() keeps the allocation when it is large enough (the
+// contents are not preserved either way).
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
-    size_t n = 0;
+    size_t n = 0, cap = 0;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
@@ -78,11 +83,13 @@ struct DevBuf {
         if (p) cudaFree(p);
     }
     ie_status alloc(size_t count) {
+        n = count;
+        if (count == 0 || (p && count <= cap)) return IE_OK;
         if (p) cudaFree(p);
         p = nullptr;
-        n = count;
-        if (count == 0) return IE_OK;
+        cap = 0;
         IE_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        cap = count;
         return IE_OK;
     }
     ie_status upload(const std::vector<T>& h, cudaStream_t st) {
@@ -1045,6 +1052,373 @@ struct Engine {
     }
 };
 
+// First-fit range allocator over [0, cap) in elements of one device pool;
+// freed ranges coalesce with their neighbours.
+struct RangeAlloc {
+    uint64_t cap = 0, used = 0;
+    std::map<uint64_t, uint64_t> fr;  // free ranges: offset -> length
+    void reset(uint64_t c) {
+        cap = c;
+        used = 0;
+        fr.clear();
+        if (c) fr[0] = c;
+    }
+    bool alloc(uint64_t n, uint64_t align, uint64_t& off) {
+        off = 0;
+        if (n == 0) return true;
+        for (auto it = fr.begin(); it != fr.end(); ++it) {
+            const uint64_t b = it->first, e = it->first + it->second;
+            const uint64_t a = (b + align - 1) / align * align;
+            if (a + n > e) continue;
+            fr.erase(it);
+            if (a > b) fr[b] = a - b;
+            if (a + n < e) fr[a + n] = e - (a + n);
+            off = a;
+            used += n;
+            return true;
+        }
+        return false;
+    }
+    void release(uint64_t off, uint64_t n) {
+        if (n == 0) return;
+        used -= n;
+        auto it = fr.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != fr.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            fr.erase(nx);
+        }
+        if (it != fr.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                fr.erase(it);
+            }
+        }
+    }
+};
+
+// One serving request: the host-side layout prepared at submission, its
+// placement in the device pools while resident, and its result.
+struct ServeReq {
+    uint64_t id = 0;
+    HostInst h;
+    std::vector<uint8_t> clampf;
+    std::vector<int8_t> clampv;
+    std::vector<uint32_t> recs, wtab, draw_idx;
+    uint32_t unclamped = 0;
+    std::vector<double> temps;
+    uint32_t key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t slot = 0, o_row = 0, o_site = 0, o_ent = 0, o_rec = 0, o_win = 0, o_sched = 0;
+    uint64_t done = 0;  // steps executed (host mirror of DevArrays::done)
+    std::vector<uint64_t> words;
+    std::vector<double> energies;
+};
+
+// Serving engine: an Engine whose device arrays are pools sized at creation;
+// each resident request owns ranges of them (slot: descriptor, key, generator
+// position, energies; rows; sites: linear terms, clamps, draw indices and spin
+// words; couplings; site records; window table; schedule).
+struct ServeEngine {
+    Engine eng;
+    ie_serve_config cfg{};
+    RangeAlloc a_slot, a_row, a_site, a_ent, a_rec, a_win, a_sched;
+    std::mutex mu;  // guards pending, finished, next_id
+    std::deque<std::unique_ptr<ServeReq>> pending;
+    std::vector<std::unique_ptr<ServeReq>> slots;
+    std::map<uint64_t, std::unique_ptr<ServeReq>> finished;
+    uint64_t next_id = 1;
+    uint32_t n_active = 0;
+
+    uint64_t rec_cap() const { return 8 * cfg.max_sites + 4 * cfg.max_couplings + kChunk; }
+    uint64_t win_cap() const { return 2 * cfg.max_sites + 16 * (uint64_t)cfg.max_requests; }
+
+    ie_status create(const ie_serve_config* c) {
+        if (c) cfg = *c;
+        if (!cfg.max_requests) cfg.max_requests = 4096;
+        if (!cfg.site_budget) cfg.site_budget = 65536;
+        if (!cfg.max_sites) cfg.max_sites = 1ull << 24;
+        if (!cfg.max_couplings) cfg.max_couplings = 1ull << 27;
+        if (!cfg.max_schedule_steps) cfg.max_schedule_steps = 1ull << 25;
+        if (cfg.max_sites >= (1ull << 32) || cfg.max_couplings >= (1ull << 32))
+            return fail(IE_ERR_INVALID, "max_sites and max_couplings must be below 2^32");
+        IE_TRY(eng.setup_device(cfg.device));
+        const uint32_t S = cfg.max_requests;
+        eng.nt = 1;
+        eng.count = S;
+        eng.desc.assign(S, InstDesc{});
+        eng.insts.assign(S, HostInst{});
+        eng.active.assign(S, 0);
+        IE_TRY(eng.d_desc.alloc(S));
+        IE_TRY(eng.d_keys.alloc(8 * (size_t)S));
+        IE_TRY(eng.d_pos.alloc(S));
+        IE_TRY(eng.d_deo.alloc(S));
+        IE_TRY(eng.d_done.alloc(S));
+        IE_TRY(eng.d_unclamped.alloc(S));
+        IE_TRY(eng.d_Ei.alloc((size_t)kReplicas * S));
+        IE_TRY(eng.d_Ef.alloc((size_t)kReplicas * S));
+        IE_TRY(eng.d_rows.alloc(cfg.max_sites + S));
+        IE_TRY(eng.d_lin.alloc(cfg.max_sites));
+        IE_TRY(eng.d_linp.alloc(cfg.max_sites));
+        IE_TRY(eng.d_clampf.alloc(cfg.max_sites));
+        IE_TRY(eng.d_clampv.alloc(cfg.max_sites));
+        IE_TRY(eng.d_draw_idx.alloc(cfg.max_sites));
+        IE_TRY(eng.d_spins.alloc(cfg.max_sites));
+        IE_TRY(eng.d_ents.alloc(std::max<uint64_t>(cfg.max_couplings, 1)));
+        IE_TRY(eng.d_cols.alloc(std::max<uint64_t>(cfg.max_couplings, 1)));
+        IE_TRY(eng.d_vals.alloc(std::max<uint64_t>(cfg.max_couplings, 1)));
+        IE_TRY(eng.d_recs.alloc(rec_cap() + kChunk));
+        IE_TRY(eng.d_wtab.alloc(win_cap()));
+        IE_TRY(eng.d_temps.alloc(cfg.max_schedule_steps));
+        IE_TRY(eng.d_att.alloc(1));
+        IE_TRY(eng.d_acc.alloc(1));
+        IE_TRY(eng.d_err.upload(std::vector<int32_t>(1, 0), eng.stream));
+        IE_TRY(eng.d_queue.alloc(64));
+        IE_CUDA(cudaMemsetAsync(eng.d_recs.p, 0, eng.d_recs.n * sizeof(uint32_t), eng.stream));
+        IE_CUDA(cudaStreamSynchronize(eng.stream));
+        a_slot.reset(S);
+        a_row.reset(cfg.max_sites + S);
+        a_site.reset(cfg.max_sites);
+        a_ent.reset(cfg.max_couplings);
+        a_rec.reset(rec_cap());
+        a_win.reset(win_cap());
+        a_sched.reset(cfg.max_schedule_steps);
+        slots.resize(S);
+        eng.initialized = true;
+        eng.recs_dirty = false;
+        return IE_OK;
+    }
+
+    // Host-side preparation of one request (any thread; touches no shared state).
+    ie_status prepare(const ie_problem* p, uint64_t seed, const double* temps, uint64_t n_steps,
+                      const uint8_t* is_clamped, const int8_t* clamp_val, ServeReq& r) const {
+        if (!p || !temps) return fail(IE_ERR_INVALID, "NULL argument");
+        if (p->num_vars == 0) return fail(IE_ERR_INVALID, "num_vars must be > 0");
+        if (n_steps == 0) return fail(IE_ERR_INVALID, "n_steps must be >= 1");
+        IE_TRY(ingest(p, cfg.force_f64 != 0, r.h));
+        const uint32_t n = r.h.n;
+        r.temps.assign(temps, temps + n_steps);
+        for (double x : r.temps)
+            if (!(x > 0.0) || !std::isfinite(x)) return fail(IE_ERR_INVALID, "temperatures must be positive");
+        r.clampf.assign(n, 0);
+        r.clampv.assign(n, 0);
+        if (is_clamped)
+            for (uint32_t i = 0; i < n; i++) {
+                r.clampf[i] = is_clamped[i] ? 1 : 0;
+                r.clampv[i] = (is_clamped[i] && clamp_val && clamp_val[i] == 1) ? 1 : 0;
+            }
+        r.draw_idx.assign(n, 0);
+        uint32_t c = 0;
+        for (uint32_t v = 0; v < n; v++) {
+            r.draw_idx[v] = c;
+            if (!r.clampf[v]) c++;
+        }
+        r.unclamped = c;
+        uint64_t off = 0, len = 0;
+        IE_TRY(build_records(r.h, r.clampf, 0, r.recs, off, len));
+        window_table(r.h, r.wtab);
+        chacha_key_from_u64(seed, r.key);
+        // capacity checks: the request alone must fit every pool and the
+        // shared memory of the kernels that can run it
+        if (n + 1 > a_row.cap || n > a_site.cap || r.h.nnz > a_ent.cap || r.recs.size() > a_rec.cap ||
+            r.wtab.size() > a_win.cap || n_steps > a_sched.cap)
+            return fail(IE_ERR_OOM, "request exceeds the serving engine's capacity");
+        const uint32_t cap = Engine::cap_of(n);
+        if (batch_smem(4, cap, true) > 227 * 1024)
+            return fail(IE_ERR_UNSUPPORTED, "num_vars too large for the serving kernels' shared memory");
+        return IE_OK;
+    }
+
+    static uint64_t bytes_of(const ServeReq& r) {
+        const uint64_t n = r.h.n;
+        return (n + 1) * 4 + n * (8 + 4 + 1 + 1 + 4 + 8) + r.h.nnz * (4 + 4 + 8) + r.recs.size() * 4 +
+               r.wtab.size() * 4 + r.temps.size() * 8 + sizeof(InstDesc) + 32 + 8 + 4 + 8 + 4 +
+               kReplicas * (4 + 8);
+    }
+
+    // Reserves every pool range of r; all or nothing.
+    bool place(ServeReq& r) {
+        const uint64_t n = r.h.n;
+        uint64_t o[7];
+        RangeAlloc* al[7] = {&a_slot, &a_row, &a_site, &a_ent, &a_rec, &a_win, &a_sched};
+        const uint64_t len[7] = {1, n + 1, n, r.h.nnz, r.recs.size(), r.wtab.size(), r.temps.size()};
+        const uint64_t align[7] = {1, 4, 4, 4, kChunk, 4, 2};
+        int k = 0;
+        for (; k < 7; k++)
+            if (!al[k]->alloc(len[k], align[k], o[k])) break;
+        if (k < 7) {
+            for (int j = 0; j < k; j++) al[j]->release(o[j], len[j]);
+            return false;
+        }
+        r.slot = o[0];
+        r.o_row = o[1];
+        r.o_site = o[2];
+        r.o_ent = o[3];
+        r.o_rec = o[4];
+        r.o_win = o[5];
+        r.o_sched = o[6];
+        return true;
+    }
+
+    void unplace(const ServeReq& r) {
+        const uint64_t n = r.h.n;
+        a_slot.release(r.slot, 1);
+        a_row.release(r.o_row, n + 1);
+        a_site.release(r.o_site, n);
+        a_ent.release(r.o_ent, r.h.nnz);
+        a_rec.release(r.o_rec, r.recs.size());
+        a_win.release(r.o_win, r.wtab.size());
+        a_sched.release(r.o_sched, r.temps.size());
+    }
+
+    template <typename T>
+    ie_status put(T* base, uint64_t off, const T* src, size_t count) {
+        if (count) IE_CUDA(cudaMemcpyAsync(base + off, src, count * sizeof(T), cudaMemcpyHostToDevice, eng.stream));
+        return IE_OK;
+    }
+
+    // Uploads an admitted request and draws its initial state (ultimate.rs:248-290).
+    ie_status upload(ServeReq& r) {
+        const HostInst& h = r.h;
+        const uint32_t s = (uint32_t)r.slot;
+        InstDesc& d = eng.desc[s];
+        d = InstDesc{};
+        d.n = h.n;
+        d.H = h.H;
+        d.mode = h.mode;
+        d.nt = 1;
+        d.row = r.o_row;
+        d.ent = r.o_ent;
+        d.site = r.o_site;
+        d.spin = r.o_site;
+        d.energy = (uint64_t)s * kReplicas;
+        d.stat = 0;
+        d.rec = r.o_rec;
+        d.rec_len = r.recs.size();
+        d.win = r.o_win;
+        d.sched = r.o_sched;
+        d.sched_len = r.temps.size();
+        HostInst& e = eng.insts[s];
+        e = HostInst();
+        e.n = h.n;
+        e.H = h.H;
+        e.mode = h.mode;
+        e.nnz = h.nnz;
+        e.windowed_ok = h.windowed_ok;
+        IE_TRY(put(eng.d_rows.p, r.o_row, h.rows.data(), h.rows.size()));
+        IE_TRY(put(eng.d_lin.p, r.o_site, h.lin.data(), h.n));
+        if (h.mode == kModeInt) {
+            IE_TRY(put(eng.d_linp.p, r.o_site, h.linp.data(), h.n));
+            IE_TRY(put(eng.d_ents.p, r.o_ent, h.ents.data(), h.nnz));
+        }
+        IE_TRY(put(eng.d_cols.p, r.o_ent, h.cols.data(), h.nnz));
+        IE_TRY(put(eng.d_vals.p, r.o_ent, h.vals.data(), h.nnz));
+        IE_TRY(put(eng.d_clampf.p, r.o_site, r.clampf.data(), h.n));
+        IE_TRY(put(eng.d_clampv.p, r.o_site, r.clampv.data(), h.n));
+        IE_TRY(put(eng.d_draw_idx.p, r.o_site, r.draw_idx.data(), h.n));
+        IE_TRY(put(eng.d_recs.p, r.o_rec, r.recs.data(), r.recs.size()));
+        IE_TRY(put(eng.d_wtab.p, r.o_win, r.wtab.data(), r.wtab.size()));
+        IE_TRY(put(eng.d_temps.p, r.o_sched, r.temps.data(), r.temps.size()));
+        IE_TRY(put(eng.d_keys.p, 8 * (uint64_t)s, r.key, 8));
+        IE_TRY(put(eng.d_unclamped.p, s, &r.unclamped, 1));
+        IE_TRY(put(eng.d_desc.p, s, &d, 1));
+        IE_CUDA(cudaMemsetAsync(eng.d_pos.p + s, 0, sizeof(uint64_t), eng.stream));
+        IE_CUDA(cudaMemsetAsync(eng.d_deo.p + s, 0, sizeof(int32_t), eng.stream));
+        IE_CUDA(cudaMemsetAsync(eng.d_done.p + s, 0, sizeof(uint64_t), eng.stream));
+        const DevArrays A = eng.arrays();
+        IE_CUDA(launch_init(A, s, 1, eng.d_draw_idx.p, eng.d_unclamped.p, eng.stream));
+        IE_CUDA(launch_energy(A, s, 1, eng.stream));
+        eng.active[s] = 1;
+        r.done = 0;
+        return IE_OK;
+    }
+
+    // Copies a finished request's result to the host and frees its ranges.
+    ie_status retire(std::unique_ptr<ServeReq>& rp) {
+        ServeReq& r = *rp;
+        const uint32_t s = (uint32_t)r.slot;
+        const InstDesc& d = eng.desc[s];
+        std::vector<uint64_t> w(r.h.n);
+        std::vector<int32_t> ei(kReplicas);
+        r.energies.assign(kReplicas, 0.0);
+        IE_CUDA(cudaMemcpyAsync(w.data(), eng.d_spins.p + d.spin, w.size() * 8, cudaMemcpyDeviceToHost, eng.stream));
+        if (d.mode == kModeInt)
+            IE_CUDA(cudaMemcpyAsync(ei.data(), eng.d_Ei.p + d.energy, kReplicas * 4, cudaMemcpyDeviceToHost, eng.stream));
+        else
+            IE_CUDA(cudaMemcpyAsync(r.energies.data(), eng.d_Ef.p + d.energy, kReplicas * 8, cudaMemcpyDeviceToHost,
+                                    eng.stream));
+        IE_CUDA(cudaStreamSynchronize(eng.stream));
+        if (d.mode == kModeInt)
+            for (int k = 0; k < kReplicas; k++) r.energies[k] = (double)ei[k];
+        r.words.resize(w.size());
+        for (size_t i = 0; i < w.size(); i++) r.words[i] = transpose8x8(w[i]);
+        eng.active[s] = 0;
+        unplace(r);
+        // the host layout is no longer needed
+        r.h = HostInst();
+        r.recs.clear();
+        r.wtab.clear();
+        r.temps.clear();
+        r.clampf.clear();
+        r.clampv.clear();
+        r.draw_idx.clear();
+        std::lock_guard<std::mutex> lk(mu);
+        finished[r.id] = std::move(rp);
+        return IE_OK;
+    }
+
+    ie_status tick(uint32_t* na, uint32_t* np, uint32_t* nf) {
+        // admission, first come first served: stop at the first request that
+        // does not fit, so a large request is not overtaken indefinitely
+        std::vector<ServeReq*> admitted;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            while (!pending.empty()) {
+                ServeReq& r = *pending.front();
+                if (!place(r)) break;
+                const uint64_t s = r.slot;
+                slots[s] = std::move(pending.front());
+                pending.pop_front();
+                admitted.push_back(slots[s].get());
+            }
+        }
+        for (ServeReq* r : admitted) {
+            IE_TRY(upload(*r));
+            n_active++;
+        }
+        eng.last_ms = 0.0;
+        eng.last_launches = 0;
+        if (n_active) {
+            IE_TRY(eng.build_quads());
+            RunArgs R{};
+            R.temps = eng.d_temps.p;
+            R.temps_per_step = 1;
+            R.exchange_interval = 1;
+            R.serve = 1;
+            R.site_budget = cfg.site_budget;
+            IE_TRY(eng.launch_classes(R));
+            IE_TRY(eng.check_err());
+            for (uint32_t s = 0; s < cfg.max_requests; s++) {
+                if (!slots[s] || !eng.active[s]) continue;
+                ServeReq& r = *slots[s];
+                const uint64_t left = r.temps.size() - r.done;
+                const uint64_t want = std::max<uint64_t>(1, cfg.site_budget / std::max<uint32_t>(r.h.n, 1));
+                r.done += std::min(left, want);
+                if (r.done == r.temps.size()) {
+                    IE_TRY(retire(slots[s]));
+                    slots[s].reset();
+                    n_active--;
+                }
+            }
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        if (na) *na = n_active;
+        if (np) *np = (uint32_t)pending.size();
+        if (nf) *nf = (uint32_t)finished.size();
+        return IE_OK;
+    }
+};
+
 bool cfg_valid(const ie_config* c, std::string& why) {
     if (!c) {
         why = "config is NULL";
@@ -1074,6 +1448,10 @@ struct ie_handle {
 
 struct ie_batch {
     Engine eng;
+};
+
+struct ie_serve {
+    ServeEngine s;
 };
 
 namespace ie {
@@ -1375,6 +1753,80 @@ ie_status ie_batch_class_report(ie_batch* b, uint32_t max_classes, uint32_t* n_c
 ie_status ie_batch_last_launches(ie_batch* b, uint64_t* launches) {
     if (!b || !launches) return fail(IE_ERR_INVALID, "NULL argument");
     *launches = b->eng.last_launches;
+    return IE_OK;
+}
+
+// ---- serving ----
+
+ie_status ie_serve_create(const ie_serve_config* config, ie_serve** out) {
+    if (!out) return fail(IE_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    std::unique_ptr<ie_serve> s(new ie_serve());
+    IE_TRY(s->s.create(config));
+    *out = s.release();
+    return IE_OK;
+}
+
+ie_status ie_serve_destroy(ie_serve* s) {
+    delete s;
+    return IE_OK;
+}
+
+ie_status ie_serve_submit(ie_serve* s, const ie_problem* problem, uint64_t seed, const double* temps,
+                          uint64_t n_steps, const uint8_t* is_clamped, const int8_t* clamp_val, uint64_t* id) {
+    if (!s || !id) return fail(IE_ERR_INVALID, "NULL argument");
+    std::unique_ptr<ServeReq> r(new ServeReq());
+    IE_TRY(s->s.prepare(problem, seed, temps, n_steps, is_clamped, clamp_val, *r));
+    std::lock_guard<std::mutex> lk(s->s.mu);
+    r->id = s->s.next_id++;
+    *id = r->id;
+    s->s.pending.push_back(std::move(r));
+    return IE_OK;
+}
+
+ie_status ie_serve_tick(ie_serve* s, uint32_t* n_active, uint32_t* n_pending, uint32_t* n_finished) {
+    if (!s) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(s->s.eng.device));
+    return s->s.tick(n_active, n_pending, n_finished);
+}
+
+ie_status ie_serve_poll(ie_serve* s, uint64_t* ids, uint32_t max_ids, uint32_t* n_ids) {
+    if (!s || !n_ids || (max_ids && !ids)) return fail(IE_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->s.mu);
+    uint32_t k = 0;
+    for (auto it = s->s.finished.begin(); it != s->s.finished.end() && k < max_ids; ++it) ids[k++] = it->first;
+    *n_ids = k;
+    return IE_OK;
+}
+
+ie_status ie_serve_result(ie_serve* s, uint64_t id, uint64_t* words, double* energies) {
+    if (!s || !words || !energies) return fail(IE_ERR_INVALID, "NULL argument");
+    std::unique_ptr<ServeReq> r;
+    {
+        std::lock_guard<std::mutex> lk(s->s.mu);
+        auto it = s->s.finished.find(id);
+        if (it == s->s.finished.end()) return fail(IE_ERR_INVALID, "no finished request with this id");
+        r = std::move(it->second);
+        s->s.finished.erase(it);
+    }
+    std::copy(r->words.begin(), r->words.end(), words);
+    std::copy(r->energies.begin(), r->energies.end(), energies);
+    return IE_OK;
+}
+
+ie_status ie_serve_footprint(ie_serve* s, const ie_problem* problem, uint64_t n_steps, uint64_t* bytes) {
+    if (!s || !bytes || !problem) return fail(IE_ERR_INVALID, "NULL argument");
+    ServeReq r;
+    std::vector<double> t(std::max<uint64_t>(n_steps, 1), 1.0);
+    IE_TRY(s->s.prepare(problem, 0, t.data(), n_steps, nullptr, nullptr, r));
+    *bytes = ServeEngine::bytes_of(r);
+    return IE_OK;
+}
+
+ie_status ie_serve_last_tick(ie_serve* s, double* ms, uint64_t* launches) {
+    if (!s || !ms || !launches) return fail(IE_ERR_INVALID, "NULL argument");
+    *ms = s->s.eng.last_ms;
+    *launches = s->s.eng.last_launches;
     return IE_OK;
 }
 

@@ -172,6 +172,33 @@ def uneven_batch(count: int, seed: int, n_min: int = 64, n_max: int = 4096, d_mi
     return models, seeds
 
 
+def serve_requests(count: int, seed: int, n_min: int = 100, n_max: int = 20000, d_min: int = 4,
+                   d_max: int = 32, sweeps_min: int = 1000, sweeps_max: int = 20000):
+    """The serving stream's requests: N log-uniform in [n_min, n_max], degree
+    uniform in {d_min..d_max} (redrawn until N*d is even), integer couplings
+    in [-8, 8] or float32 N(0, 1) with probability 1/2 each, SA length uniform
+    in [sweeps_min, sweeps_max]. Returns [(model, seed, sweeps)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        while True:
+            n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+            d = int(rng.integers(d_min, d_max + 1))
+            if (n * d) % 2 == 0 and d < n:
+                break
+        integer = bool(rng.integers(2))
+        sweeps = int(rng.integers(sweeps_min, sweeps_max + 1))
+        m = random_regular_qubo(n, d, rng, integer=integer)
+        out.append((m, int((seed * 7919 + 104729 * i) & 0xFFFFFFFFFFFFFFFF), sweeps))
+    return out
+
+
+def poisson_arrivals(count: int, rate: float, seed: int) -> np.ndarray:
+    """Arrival times (s) of a Poisson stream of `rate` requests per second."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=count))
+
+
 def sa_temps(sweeps: int, beta0: float = 0.1, beta1: float = 5.0) -> np.ndarray:
     """Per-step temperatures 1/beta_k with beta linear from beta0 to beta1."""
     k = np.arange(sweeps, dtype=np.float64)
