@@ -57,6 +57,11 @@ def parse():
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--threads-per-block", type=int, default=0)
     p.add_argument("--blocks-per-sm", type=int, default=0)
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-count", type=int, default=64)
+    p.add_argument("--serve-rate", type=float, default=20.0)
+    p.add_argument("--serve-sweeps", type=int, nargs=2, default=[100, 2000])
+    p.add_argument("--serve-budget", type=int, default=65536)
     return p.parse_args()
 
 
@@ -196,7 +201,7 @@ def run_ours(args):
     eng = BatchEngine(models, seeds, device=local, threads_per_block=args.threads_per_block,
                       blocks_per_sm=args.blocks_per_sm)
     eng.init_random()
-    tuned = eng.autotune(temps, 16) if not args.no_autotune else None
+    tuned = eng.autotune(temps, 64) if not args.no_autotune else None
     for _ in range(args.warmup):
         eng.run_schedule(temps)
     dist.barrier()
@@ -280,6 +285,10 @@ def run_ours(args):
                "h2d_bytes_per_step": int(host_bytes(models)),
                "d2h_bytes_per_step": int(w.nbytes + e.nbytes)}
 
+    serve = None
+    if not args.no_serve and rank == 0:
+        serve = run_serve(args, local)
+
     cpu = None
     if not args.no_cpu and rank == 0 and ws == 1:
         cpu = cpu_baseline(models, seeds, temps)
@@ -315,11 +324,41 @@ def run_ours(args):
             "classes": [{"mode": c[0], "threads_per_lane": c[1], "cap": c[2], "items": c[3],
                          "ms": round(c[4], 1)} for c in classes],
         }
+        if serve:
+            line["serve"] = serve
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))
     eng.close()
     dist.close()
+
+
+def run_serve(args, device):
+    """Serving stream: Poisson arrivals at a fixed rate of SA requests with N
+    log-uniform in [100, 20000], degree 4..32, integer [-8, 8] or float32
+    N(0, 1) couplings (half each), SA lengths uniform in the given range; the
+    pool admits by device-memory footprint and ticks until all are done.
+    Latency = result taken - arrival, on the host clock."""
+    from ising_engine_b200 import instances as I
+    from ising_engine_b200.serve import ServeEngine, serve_stream
+    lo, hi = args.serve_sweeps
+    reqs = I.serve_requests(args.serve_count, args.seed + 5, sweeps_min=lo, sweeps_max=hi)
+    reqs = [(m, s, I.sa_temps(sw)) for (m, s, sw) in reqs]
+    attempts = sum(m.num_vars * 64.0 * len(t) for m, _, t in reqs)
+    arrivals = I.poisson_arrivals(len(reqs), args.serve_rate, args.seed + 6)
+    with ServeEngine(device=device, site_budget=args.serve_budget) as srv:
+        m0, s0, t0 = reqs[0]
+        srv.submit(m0, s0, t0[:2])
+        srv.run_all()  # warm-up: kernels loaded, pools touched
+        tr = serve_stream(srv, reqs, arrivals, keep_results=False)
+    s = tr.summary()
+    return {"p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"], "mean_ms": s["mean_ms"],
+            "rate_req_per_s": args.serve_rate, "requests": s["requests"],
+            "attempts_per_s": attempts / s["makespan_s"], "makespan_s": s["makespan_s"],
+            "ticks": s["ticks"], "mean_tick_ms": s["mean_tick_ms"], "gpu_launches": tr.launches,
+            "site_budget": args.serve_budget,
+            "stream": f"N log-uniform [100, 20000], degree 4..32, int [-8,8] / f32 N(0,1) half each, "
+                      f"SA {lo}..{hi} sweeps (beta 0.1 -> 5.0), Poisson arrivals"}
 
 
 def cpu_sample(models, seeds, temps):

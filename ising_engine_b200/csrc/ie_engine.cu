@@ -251,7 +251,7 @@ ie_status build_xtables(const double* temps, uint32_t nt, XTables& X) {
 // Appends the chunk-packed site-record stream of one instance (layout in
 // ie_kernels.cuh); the stream starts and ends on a chunk boundary.
 ie_status build_records(HostInst& h, const std::vector<uint8_t>& clampf, size_t site0,
-                        std::vector<uint32_t>& out, uint64_t& off, uint64_t& len) {
+                        std::vector<uint32_t>& out, uint64_t& off, uint64_t& len, uint32_t max_deg = kRecMaxDeg) {
     off = out.size();
     h.recpos.assign(h.n, 0);
     h.reclen.assign(h.n, 0);
@@ -284,7 +284,7 @@ ie_status build_records(HostInst& h, const std::vector<uint8_t>& clampf, size_t 
         }
         uint32_t e0 = beg;
         do {
-            const uint32_t deg = std::min<uint32_t>(end - e0, kRecMaxDeg);
+            const uint32_t deg = std::min<uint32_t>(end - e0, max_deg);
             const uint32_t deg4 = (deg + 3u) & ~3u;
             const uint32_t cont = (e0 + deg < end) ? kRecCont : 0u;
             rec.clear();
@@ -322,15 +322,16 @@ ie_status build_records(HostInst& h, const std::vector<uint8_t>& clampf, size_t 
 }
 
 // Window table of the windowed kernel (layout in ie_kernels.cu), 16 words per
-// window of 8 sites: an instance qualifies when every site has at most 16
-// couplings (one record) and its windows have on average at least 2 sites per
-// dependency level. Sets h.windowed_ok; needs h.recpos / h.reclen.
+// window of 8 sites: an instance qualifies when every site has at most 32
+// couplings and its windows have on average at least 2 sites per dependency
+// level. Sets h.windowed_ok; needs h.recpos / h.reclen of a stream with one
+// record per site (window_records).
 bool window_table(HostInst& h, std::vector<uint32_t>& tab) {
     h.windowed_ok = false;
     tab.clear();
     if (h.n < 8) return false;
     for (uint32_t v = 0; v < h.n; v++)
-        if (h.rows[v + 1] - h.rows[v] > kRecMaxDeg) return false;
+        if (h.rows[v + 1] - h.rows[v] > kWinMaxDeg) return false;
     const uint32_t nwin = (h.n + 7) / 8;
     tab.assign((size_t)nwin * 16, 0);
     double par = 0;
@@ -359,6 +360,20 @@ bool window_table(HostInst& h, std::vector<uint32_t>& tab) {
     }
     h.windowed_ok = true;
     return true;
+}
+
+// Appends the windowed kernel's record stream when the batched stream (at
+// off, records of at most 16 couplings) does not already have one record per
+// site, i.e. when some site has 17..32 couplings; returns the stream's offset
+// in wrec and leaves h.recpos / h.reclen describing it.
+ie_status window_records(HostInst& h, const std::vector<uint8_t>& clampf, size_t site0,
+                         std::vector<uint32_t>& out, uint64_t off, uint64_t& wrec) {
+    wrec = off;
+    uint32_t maxdeg = 0;
+    for (uint32_t v = 0; v < h.n; v++) maxdeg = std::max(maxdeg, h.rows[v + 1] - h.rows[v]);
+    if (maxdeg <= kRecMaxDeg || maxdeg > kWinMaxDeg) return IE_OK;
+    uint64_t len = 0;
+    return build_records(h, clampf, site0, out, wrec, len, kWinMaxDeg);
 }
 
 int g_sm_count = -1;
@@ -573,6 +588,7 @@ struct Engine {
         std::vector<uint32_t> recs, wt;
         for (uint32_t i = 0; i < count; i++) {
             IE_TRY(build_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].rec_len));
+            if (nt == 1) IE_TRY(window_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].wrec));
             build_window_table(i, wt);
         }
         recs.resize(recs.size() + kChunk, 0);
@@ -835,29 +851,43 @@ struct Engine {
         };
         IE_TRY(copy_all(true));
         const uint64_t saved_steps = steps_done;
-        const uint32_t n4s[3] = {768, 1536, 3072}, n2s[2] = {256, 512};
-        double best = 1e300;
+        // Coordinate search: the (n4, n2) pair of one mode over its grid with
+        // the other mode's pair held, integer then f64, two passes; each trial
+        // is timed on the same state (restored after it).
+        const uint32_t n4s[4] = {512, 768, 1536, 3072}, n2s[2] = {256, 512};
         uint32_t bi[4] = {tune_n4[0], tune_n2[0], tune_n4[1], tune_n2[1]};
-        for (uint32_t a : n4s)
-            for (uint32_t b : n2s)
-                for (uint32_t c : n4s)
-                    for (uint32_t dd : n2s) {
-                        tune_n4[0] = a;
-                        tune_n2[0] = b;
-                        tune_n4[1] = c;
-                        tune_n2[1] = dd;
-                        quads_built = false;
-                        IE_TRY(run_batch(temps, trial_steps));
-                        IE_TRY(copy_all(false));
-                        steps_done = saved_steps;
-                        if (last_ms < best) {
-                            best = last_ms;
-                            bi[0] = a;
-                            bi[1] = b;
-                            bi[2] = c;
-                            bi[3] = dd;
+        auto trial = [&](double& ms) -> ie_status {
+            tune_n4[0] = bi[0];
+            tune_n2[0] = bi[1];
+            tune_n4[1] = bi[2];
+            tune_n2[1] = bi[3];
+            quads_built = false;
+            IE_TRY(run_batch(temps, trial_steps));
+            IE_TRY(copy_all(false));
+            steps_done = saved_steps;
+            ms = last_ms;
+            return IE_OK;
+        };
+        for (int pass = 0; pass < 2; pass++)
+            for (int m = 0; m < 2; m++) {
+                double best = 1e300;
+                uint32_t b4 = bi[2 * m], b2 = bi[2 * m + 1];
+                for (uint32_t a4 : n4s)
+                    for (uint32_t a2 : n2s) {
+                        if (a2 >= a4) continue;
+                        bi[2 * m] = a4;
+                        bi[2 * m + 1] = a2;
+                        double ms = 0;
+                        IE_TRY(trial(ms));
+                        if (ms < best) {
+                            best = ms;
+                            b4 = a4;
+                            b2 = a2;
                         }
                     }
+                bi[2 * m] = b4;
+                bi[2 * m + 1] = b2;
+            }
         tune_n4[0] = bi[0];
         tune_n2[0] = bi[1];
         tune_n4[1] = bi[2];
@@ -1107,6 +1137,7 @@ struct ServeReq {
     std::vector<int8_t> clampv;
     std::vector<uint32_t> recs, wtab, draw_idx;
     uint32_t unclamped = 0;
+    uint64_t wrec = 0;  // offset of the windowed record stream within recs
     std::vector<double> temps;
     uint32_t key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     uint64_t slot = 0, o_row = 0, o_site = 0, o_ent = 0, o_rec = 0, o_win = 0, o_sched = 0;
@@ -1216,6 +1247,7 @@ struct ServeEngine {
         r.unclamped = c;
         uint64_t off = 0, len = 0;
         IE_TRY(build_records(r.h, r.clampf, 0, r.recs, off, len));
+        IE_TRY(window_records(r.h, r.clampf, 0, r.recs, 0, r.wrec));
         window_table(r.h, r.wtab);
         chacha_key_from_u64(seed, r.key);
         // capacity checks: the request alone must fit every pool and the
@@ -1294,6 +1326,7 @@ struct ServeEngine {
         d.energy = (uint64_t)s * kReplicas;
         d.stat = 0;
         d.rec = r.o_rec;
+        d.wrec = r.o_rec + r.wrec;
         d.rec_len = r.recs.size();
         d.win = r.o_win;
         d.sched = r.o_sched;

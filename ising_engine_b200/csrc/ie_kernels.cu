@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
 // of site i in nibble i, word 9 = largest level.
 // ---------------------------------------------------------------------------
 constexpr int kWin = 8;
-constexpr uint32_t kWinRecWords = 8 * 52;  // eight records of degree <= 16
+constexpr uint32_t kWinRecWords = 8 * (4 + 3 * kWinMaxDeg);  // eight f64 records of degree <= 32
 
 
 // Copies the records of one window (positions from its table entry) into buf.
@@ -663,7 +663,7 @@ __device__ __forceinline__ void bar_sync(int id, int count) { asm volatile("bar.
 __device__ __forceinline__ void bar_arrive(int id, int count) { asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
 
 __host__ __device__ constexpr size_t ws_smem_bytes(uint32_t spin_cap) {
-    // tab 2 KB | spread table 4 KB | outputs 2 x 64 rows | dE 64 rows | records 2 x 1664 B | spins
+    // tab 2 KB | spread table 4 KB | outputs 2 x 64 rows | dE 64 rows | records 2 x 3200 B | spins
     return 2048 + 4096 + 2 * 64 * kRS * 8 + 64 * kRS * 8 + 2 * kWinRecWords * 4 + (size_t)spin_cap * 8;
 }
 
@@ -684,7 +684,7 @@ __device__ __forceinline__ uint32_t ws_task(const uint32_t* rec, uint8_t* spc, u
                                             const uint64_t* __restrict__ tab, int H, double beta, int half) {
     constexpr int KPT = WsCfg<MODE>::KPT;
     const uint32_t hdr = rec[0];
-    const uint32_t deg = hdr & 0x1Fu;
+    const uint32_t deg = hdr & 0x3Fu;
     const uint32_t deg4 = (deg + 3u) & ~3u;
     const uint32_t xb = spc[8u * v];
     uint32_t flips = 0;
@@ -704,7 +704,7 @@ __device__ __forceinline__ uint32_t ws_task(const uint32_t* rec, uint8_t* spc, u
         }
         uint32_t aL = 0, aH = 0;
 #pragma unroll
-        for (int qd = 0; qd < 4; qd++) {
+        for (int qd = 0; qd < (int)kWinMaxDeg / 4; qd++) {
             if ((uint32_t)(4 * qd) < deg) {
                 const uint4 e4 = *reinterpret_cast<const uint4*>(rec + 4 + 4 * qd);
                 const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
@@ -760,7 +760,7 @@ __device__ __forceinline__ uint32_t ws_task(const uint32_t* rec, uint8_t* spc, u
             dl[j] = xv ? -wl : wl;
         }
 #pragma unroll
-        for (int qd = 0; qd < 4; qd++) {
+        for (int qd = 0; qd < (int)kWinMaxDeg / 4; qd++) {
             if ((uint32_t)(4 * qd) < deg) {
                 const uint4 c4 = *reinterpret_cast<const uint4*>(cols + 4 * qd);
                 const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
@@ -850,7 +850,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
         for (uint32_t i = tid; i < d.n; i += NT) sw[i] = gw[i];
         const uint32_t nwin = (d.n + kWin - 1) / kWin;
         const uint32_t* wt = A.wtab + d.win;
-        const uint32_t* stream = A.recs + d.rec;
+        const uint32_t* stream = A.recs + d.wrec;
         for (uint32_t s = 0; s < P.steps; s++) {
             __syncthreads();
             const double beta = __ddiv_rn(1.0, P.temps[P.tstride ? s : 0]);

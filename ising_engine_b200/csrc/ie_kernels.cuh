@@ -27,6 +27,7 @@ struct InstDesc {
     uint64_t rec;    // site-record stream (batched kernel): recs[rec .. rec + rec_len)
     uint64_t rec_len;
     uint64_t win;    // window table (windowed kernel): wtab[win .. win + 16 * ceil(n / 8))
+    uint64_t wrec;   // windowed kernel's record stream (one record per site): recs[wrec ..)
     uint64_t sched;  // serving: the instance's per-step temperatures at temps[sched .. sched + sched_len)
     uint64_t sched_len;
 };
@@ -47,6 +48,7 @@ constexpr uint32_t kRecPad = 0xFFFFFFFFu;
 constexpr uint32_t kRecCont = 1u << 14;
 constexpr uint32_t kRecClamp = 1u << 15;
 constexpr uint32_t kRecMaxDeg = 16;
+constexpr uint32_t kWinMaxDeg = 32;  // windowed kernel: one record of up to 32 couplings per site
 
 struct DevArrays {
     const InstDesc* desc;

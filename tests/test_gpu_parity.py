@@ -262,6 +262,35 @@ def test_windowed_kernel_large_instances():
     b.close()
 
 
+def small_weight_regular(n, d, rng):
+    """Random d-regular QUBO with couplings in {-2, -1, 1, 2}: local fields stay
+    within the integer mode's bound at degrees up to 32."""
+    e = I.random_regular_edges(n, d, rng)
+    q = rng.choice(np.array([-2.0, -1.0, 1.0, 2.0]), size=len(e))
+    lin = rng.integers(-4, 5, size=n).astype(np.float64)
+    return QuboModel.from_edges(n, lin, np.concatenate([e.astype(np.float64), q[:, None]], axis=1))
+
+
+def test_windowed_kernel_degree_17_to_32():
+    """Sites with 17..32 couplings: the windowed kernel reads its own stream of
+    one record per site (the batched kernels split such sites into
+    continuation records). Integer and f64 modes, and a clamped instance."""
+    rng = np.random.default_rng(79)
+    models = [small_weight_regular(2000, 24, rng), small_weight_regular(1800, 32, rng),
+              I.random_regular_qubo(1600, 32, rng, integer=False),
+              I.random_regular_qubo(1000, 20, rng, integer=False)]
+    assert models[0].is_integral()
+    seeds = np.arange(len(models), dtype=np.uint64) + 21
+    temps = I.sa_temps(25, 0.2, 4.0)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
+    b = BatchEngine(models, seeds)
+    b.init_random()
+    b.run_schedule(temps)
+    assert (b.spins() == words_ref).all()
+    assert b.energies().tobytes() == ref_e.tobytes()
+    b.close()
+
+
 def test_windowed_kernel_f64_resync():
     rng = np.random.default_rng(78)
     m = I.random_regular_qubo(800, 9, rng, integer=False)
