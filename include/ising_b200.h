@@ -66,6 +66,9 @@ typedef struct ie_config {
     uint32_t exchange_interval;
     int32_t force_f64;   /* nonzero: use the f64 mode even for integral input */
     int32_t device;      /* CUDA device ordinal */
+    int32_t pt_path;     /* 0: chosen by size; 1: one CTA runs all cells of the instance;
+                            2: every cell is its own work item of the batched kernels, the
+                            exchange runs between their launches (same results) */
 } ie_config;
 
 typedef struct ie_handle ie_handle;

@@ -112,7 +112,8 @@ struct HostInst {
     std::vector<double> vals;
     std::vector<double> lin;
     std::vector<uint32_t> recpos, reclen;  // first record of each site: word offset and length in its stream
-    bool windowed_ok = false;              // eligible for the windowed kernel
+    bool windowed_ok = false;              // the windowed kernel is preferred (parallel windows)
+    bool has_wtab = false;                 // has a window table (the windowed kernel can run it)
     uint64_t nnz = 0;
 };
 
@@ -322,12 +323,14 @@ ie_status build_records(HostInst& h, const std::vector<uint8_t>& clampf, size_t 
 }
 
 // Window table of the windowed kernel (layout in ie_kernels.cu), 16 words per
-// window of 8 sites: an instance qualifies when every site has at most 32
-// couplings and its windows have on average at least 2 sites per dependency
-// level. Sets h.windowed_ok; needs h.recpos / h.reclen of a stream with one
-// record per site (window_records).
+// window of 8 sites, built when every site has at most 32 couplings (sets
+// h.has_wtab). The windowed kernel is preferred (h.windowed_ok) when the
+// windows have on average at least 2 sites per dependency level; it is the
+// only form for instances whose spins do not fit shared memory. Needs
+// h.recpos / h.reclen of a stream with one record per site (window_records).
 bool window_table(HostInst& h, std::vector<uint32_t>& tab) {
     h.windowed_ok = false;
+    h.has_wtab = false;
     tab.clear();
     if (h.n < 8) return false;
     for (uint32_t v = 0; v < h.n; v++)
@@ -354,11 +357,8 @@ bool window_table(HostInst& h, std::vector<uint32_t>& tab) {
         tab[16 * (size_t)w + 9] = maxl;
         par += 8.0 / (maxl + 1);
     }
-    if (par / nwin < 2.0) {
-        tab.clear();
-        return false;
-    }
-    h.windowed_ok = true;
+    h.has_wtab = true;
+    h.windowed_ok = par / nwin >= 2.0;
     return true;
 }
 
@@ -482,6 +482,8 @@ struct Engine {
             d.H = h.H;
             d.mode = h.mode;
             d.nt = nt;
+            d.owner = i;
+            d.cell = 0;
             d.row = site + i;  // rows are n+1 per instance
             d.ent = ent;
             d.site = site;
@@ -579,7 +581,7 @@ struct Engine {
     void build_window_table(uint32_t i, std::vector<uint32_t>& wt) {
         desc[i].win = 0;
         std::vector<uint32_t> tab;
-        if (nt != 1 || !window_table(insts[i], tab)) return;
+        if (!window_table(insts[i], tab)) return;
         desc[i].win = wt.size();
         wt.insert(wt.end(), tab.begin(), tab.end());
     }
@@ -588,7 +590,7 @@ struct Engine {
         std::vector<uint32_t> recs, wt;
         for (uint32_t i = 0; i < count; i++) {
             IE_TRY(build_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].rec_len));
-            if (nt == 1) IE_TRY(window_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].wrec));
+            IE_TRY(window_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].wrec));
             build_window_table(i, wt);
         }
         recs.resize(recs.size() + kChunk, 0);
@@ -653,14 +655,29 @@ struct Engine {
         return IE_OK;
     }
 
-    // TPL 8 marks the windowed kernel (one warp per instance).
-    int tpl_of(uint32_t i) const {
-        const uint32_t n = desc[i].n, m = desc[i].mode;
-        if (n > tune_n4[m]) return insts[i].windowed_ok && use_windows ? 8 : 4;
+    // TPL 8 marks the windowed kernel (one CTA per instance); -1: no form can
+    // run the instance (spins beyond shared memory and no window table).
+    static constexpr uint32_t kSmemSpinCap = 24576;
+    int tpl_of(const InstDesc& d, const HostInst& h) const {
+        const uint32_t n = d.n, m = d.mode;
+        if (cap_of(n) > kSmemSpinCap) return h.has_wtab ? 8 : -1;
+        if (n > tune_n4[m]) return h.windowed_ok && use_windows ? 8 : 4;
         return n > tune_n2[m] ? 2 : 1;
     }
+    // shared-memory spin capacity of the instance's class; 0: spins in global memory
+    static uint32_t class_cap(const InstDesc& d) { return cap_of(d.n) > kSmemSpinCap ? 0u : cap_of(d.n); }
     bool use_windows = true;
     std::vector<uint8_t> active;  // instances in the work classes (empty: all)
+
+    // PT cells as work items: 0 chooses by size, 1 runs one CTA per instance
+    // (pt_kernel), 2 runs every cell as its own work item of the batched /
+    // windowed kernels with the exchange in exchange_kernel
+    int pt_path = 0;
+    std::vector<InstDesc> cdesc;
+    std::vector<HostInst> cinsts;
+    DevBuf<InstDesc> d_cdesc;
+    DevBuf<uint64_t> d_xmask;
+    bool cells_built = false;
     static uint32_t cap_of(uint32_t n) {
         for (uint32_t c : kCaps)
             if (n <= c) return c;
@@ -670,17 +687,26 @@ struct Engine {
     // Per class: instances ordered by degree then size into items of 4/TPL
     // (the groups of a warp stay in step sweep by sweep), items ordered by
     // work, longest first; classes ordered by their longest item.
-    ie_status build_quads() {
+    // Work classes over an instance view (D, HI): the engine's instances, or
+    // the cells of its PT instances.
+    ie_status build_quads(const std::vector<InstDesc>* Dp = nullptr, const std::vector<HostInst>* Hp = nullptr) {
+        const std::vector<InstDesc>& D = Dp ? *Dp : desc;
+        const std::vector<HostInst>& HI = Hp ? *Hp : insts;
+        const uint32_t N = (uint32_t)D.size();
         classes.clear();
+        cells_built = false;
         std::vector<std::tuple<uint32_t, int, uint32_t>> keys;
-        auto live = [&](uint32_t i) { return active.empty() || active[i] != 0; };
-        for (uint32_t i = 0; i < count; i++) {
+        auto live = [&](uint32_t i) { return Dp || active.empty() || active[i] != 0; };
+        for (uint32_t i = 0; i < N; i++) {
             if (!live(i)) continue;
-            auto k = std::make_tuple(desc[i].mode, tpl_of(i), cap_of(desc[i].n));
+            if (tpl_of(D[i], HI[i]) < 0)
+                return fail(IE_ERR_UNSUPPORTED, "instance too large for shared memory and not eligible for the "
+                                                "global-memory windowed kernel (a site has more than 32 couplings)");
+            auto k = std::make_tuple(D[i].mode, tpl_of(D[i], HI[i]), class_cap(D[i]));
             if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
         }
         auto degree = [&](uint32_t i) {
-            return insts[i].n ? (uint32_t)((insts[i].nnz + insts[i].n / 2) / insts[i].n) : 0u;
+            return HI[i].n ? (uint32_t)((HI[i].nnz + HI[i].n / 2) / HI[i].n) : 0u;
         };
         for (auto& k : keys) {
             std::unique_ptr<WorkClass> wc(new WorkClass());
@@ -689,12 +715,12 @@ struct Engine {
             wc->cap = std::get<2>(k);
             const int ng = wc->tpl == 8 ? 1 : 4 / wc->tpl;
             std::vector<uint32_t> order;
-            for (uint32_t i = 0; i < count; i++)
-                if (live(i) && desc[i].mode == wc->mode && tpl_of(i) == wc->tpl && cap_of(desc[i].n) == wc->cap)
+            for (uint32_t i = 0; i < N; i++)
+                if (live(i) && D[i].mode == wc->mode && tpl_of(D[i], HI[i]) == wc->tpl && class_cap(D[i]) == wc->cap)
                     order.push_back(i);
             std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
                 if (degree(a) != degree(b)) return degree(a) > degree(b);
-                return desc[a].n > desc[b].n;
+                return D[a].n > D[b].n;
             });
             std::vector<std::vector<uint32_t>> items;
             for (size_t i = 0; i < order.size();) {
@@ -705,7 +731,7 @@ struct Engine {
             }
             auto work = [&](const std::vector<uint32_t>& q) {
                 double w = 0;
-                for (uint32_t i : q) w = std::max(w, inst_work(insts[i]) / (wc->tpl == 8 ? 5 : wc->tpl));
+                for (uint32_t i : q) w = std::max(w, inst_work(HI[i]) / (wc->tpl == 8 ? 5 : wc->tpl));
                 return w;
             };
             std::stable_sort(items.begin(), items.end(), [&](const std::vector<uint32_t>& a,
@@ -717,8 +743,8 @@ struct Engine {
                 for (int j = 0; j < 4; j++) {
                     flat.push_back(j < (int)q.size() ? q[j] : 0xffffffffu);
                     if (j < (int)q.size()) {
-                        hh = std::max(hh, desc[q[j]].H);
-                        wc->site_steps += (double)desc[q[j]].n;
+                        hh = std::max(hh, D[q[j]].H);
+                        wc->site_steps += (double)D[q[j]].n;
                     }
                 }
                 qh.push_back(hh);
@@ -735,6 +761,97 @@ struct Engine {
                          });
         IE_TRY(d_queue.alloc(std::max<size_t>(classes.size(), 1)));
         quads_built = true;
+        return IE_OK;
+    }
+
+    bool use_cells() const {
+        if (pt_path == 1) return false;
+        if (pt_path == 2) return true;
+        return desc[0].n >= 256;
+    }
+
+    // Cell view: cell c of instance i as its own entry (spins and energies of
+    // the cell, records and window table of the instance, owner i).
+    ie_status build_cells() {
+        if (recs_dirty) IE_TRY(build_record_streams());
+        cdesc.clear();
+        cinsts.clear();
+        for (uint32_t i = 0; i < count; i++)
+            for (uint32_t c = 0; c < desc[i].nt; c++) {
+                InstDesc e = desc[i];
+                e.nt = 1;
+                e.spin = desc[i].spin + (uint64_t)c * desc[i].n;
+                e.energy = desc[i].energy + (uint64_t)c * kReplicas;
+                e.owner = i;
+                e.cell = c;
+                cdesc.push_back(e);
+                HostInst l;
+                l.n = insts[i].n;
+                l.H = insts[i].H;
+                l.mode = insts[i].mode;
+                l.nnz = insts[i].nnz;
+                l.windowed_ok = insts[i].windowed_ok;
+                l.has_wtab = insts[i].has_wtab;
+                cinsts.push_back(l);
+            }
+        IE_TRY(d_cdesc.upload(cdesc, stream));
+        IE_TRY(d_xmask.alloc(std::max<size_t>(d_att.n, 1)));
+        IE_TRY(build_quads(&cdesc, &cinsts));
+        quads_built = false;
+        cells_built = true;
+        return IE_OK;
+    }
+
+    // PT steps with the cells as work items: launches of the cells' sweeps
+    // end at every exchange step (and f64 resync step); after each, the
+    // exchange kernel decides the DEO pairs and advances the stream, the swap
+    // kernel exchanges configurations, and on resync steps the energies are
+    // recomputed (ultimate.rs:316-324: after the step's exchange).
+    ie_status run_pt_cells(uint64_t steps, bool per_step, const RunArgs& X) {
+        if (recs_dirty || !cells_built) IE_TRY(build_cells());
+        const uint32_t mode = desc[0].mode;
+        DevArrays A = arrays();
+        A.xmask = d_xmask.p;
+        DevArrays AC = A;
+        AC.desc = d_cdesc.p;
+        RunArgs R = X;
+        R.cells = 1;
+        R.ladder = nt;
+        R.temps_per_step = per_step ? 1 : 0;
+        const uint64_t kx = R.exchange_interval;
+        IE_CUDA(cudaEventRecord(ev2, stream));
+        uint64_t done = 0, launches = 0;
+        while (done < steps) {
+            const uint64_t g0 = steps_done + done;
+            uint64_t k = kx - g0 % kx;
+            if (mode == kModeF64) k = std::min<uint64_t>(k, kResyncEvery - g0 % kResyncEvery);
+            k = std::min<uint64_t>(k, steps - done);
+            R.steps = (uint32_t)k;
+            R.step_base = g0;
+            R.temps = d_temps.p + (per_step ? done * nt : 0);
+            IE_TRY(launch_classes(R, AC));
+            launches += last_launches;
+            const bool ex = (g0 + k) % kx == 0;
+            IE_CUDA(launch_exchange(A, R, count, mode, (uint32_t)k, ex, stream));
+            launches++;
+            if (ex && nt > 1)
+                for (uint32_t i = 0; i < count; i++) {
+                    IE_CUDA(launch_swap(A, i, desc[i].n, g_sm_count, stream));
+                    launches++;
+                }
+            if (mode == kModeF64 && (g0 + k) % kResyncEvery == 0) {
+                IE_CUDA(launch_energy(A, 0, count, stream));
+                launches++;
+            }
+            done += k;
+        }
+        IE_CUDA(cudaEventRecord(ev1, stream));
+        IE_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0;
+        IE_CUDA(cudaEventElapsedTime(&ms, ev2, ev1));
+        last_ms = ms;
+        last_launches = launches;
+        steps_done += steps;
         return IE_OK;
     }
 
@@ -770,7 +887,8 @@ struct Engine {
     // One persistent launch per work class, all in flight together on their
     // own streams, largest classes first (their CTAs are dispatched first and
     // the smaller classes fill the remaining room); waits for all of them.
-    ie_status launch_classes(const RunArgs& base) {
+    ie_status launch_classes(const RunArgs& base) { return launch_classes(base, arrays()); }
+    ie_status launch_classes(const RunArgs& base, const DevArrays& A) {
         IE_TRY(ensure_class_streams(classes.size()));
         IE_CUDA(cudaMemsetAsync(d_queue.p, 0, classes.size() * sizeof(uint32_t), stream));
         IE_CUDA(cudaEventRecord(ev0, stream));
@@ -780,7 +898,7 @@ struct Engine {
             if (!wc.nitems) continue;
             IE_CUDA(cudaStreamWaitEvent(cstreams[k], ev0, 0));
             int occ = wc.tpl == 8 ? window_occupancy(wc.mode, wc.cap)
-                                  : batch_occupancy(wc.mode, wc.tpl, wc.cap, base.serve != 0);
+                                  : batch_occupancy(wc.mode, wc.tpl, wc.cap, base.serve != 0 || base.cells != 0);
             if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
             if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
             const int grid = std::max(1, std::min<int>((int)wc.nitems, occ * g_sm_count));
@@ -790,8 +908,8 @@ struct Engine {
             R.nquads = wc.nitems;
             R.queue = d_queue.p + k;
             IE_CUDA(cudaEventRecord(cstart[k], cstreams[k]));
-            if (wc.tpl == 8) IE_CUDA(launch_window(arrays(), R, wc.mode, wc.cap, grid, cstreams[k]));
-            else IE_CUDA(launch_batch(arrays(), R, wc.mode, wc.tpl, wc.cap, grid, cstreams[k]));
+            if (wc.tpl == 8) IE_CUDA(launch_window(A, R, wc.mode, wc.cap, grid, cstreams[k]));
+            else IE_CUDA(launch_batch(A, R, wc.mode, wc.tpl, wc.cap, grid, cstreams[k]));
             IE_CUDA(cudaEventRecord(cevents[k], cstreams[k]));
             IE_CUDA(cudaStreamWaitEvent(stream, cevents[k], 0));
             launches++;
@@ -982,6 +1100,16 @@ struct Engine {
             IE_TRY(d_dbeta.upload(db, stream));
         }
         IE_TRY(d_temps.upload(t, stream));
+        if (use_cells()) {
+            RunArgs X{};
+            X.exchange_interval = exchange_interval ? exchange_interval : 1;
+            X.xtab = d_xtab.p;
+            X.xoff = d_xoff.p;
+            X.xdmax = d_xdmax.p;
+            X.xdund = d_xdund.p;
+            X.dbeta = d_dbeta.p;
+            return run_pt_cells(steps, per_step, X);
+        }
         const int block = (int)(((nt * 8) + 31) / 32 * 32);
         if (block > 1024) return fail(IE_ERR_UNSUPPORTED, "at most 128 temperatures per instance");
         const size_t smem = pt_smem(nt, d.H, d.mode);
@@ -1255,9 +1383,8 @@ struct ServeEngine {
         if (n + 1 > a_row.cap || n > a_site.cap || r.h.nnz > a_ent.cap || r.recs.size() > a_rec.cap ||
             r.wtab.size() > a_win.cap || n_steps > a_sched.cap)
             return fail(IE_ERR_OOM, "request exceeds the serving engine's capacity");
-        const uint32_t cap = Engine::cap_of(n);
-        if (batch_smem(4, cap, true) > 227 * 1024)
-            return fail(IE_ERR_UNSUPPORTED, "num_vars too large for the serving kernels' shared memory");
+        if (Engine::cap_of(n) > Engine::kSmemSpinCap && !r.h.has_wtab)
+            return fail(IE_ERR_UNSUPPORTED, "num_vars too large for shared memory and a site has more than 32 couplings");
         return IE_OK;
     }
 
@@ -1327,6 +1454,7 @@ struct ServeEngine {
         d.stat = 0;
         d.rec = r.o_rec;
         d.wrec = r.o_rec + r.wrec;
+        d.owner = s;
         d.rec_len = r.recs.size();
         d.win = r.o_win;
         d.sched = r.o_sched;
@@ -1338,6 +1466,7 @@ struct ServeEngine {
         e.mode = h.mode;
         e.nnz = h.nnz;
         e.windowed_ok = h.windowed_ok;
+        e.has_wtab = h.has_wtab;
         IE_TRY(put(eng.d_rows.p, r.o_row, h.rows.data(), h.rows.size()));
         IE_TRY(put(eng.d_lin.p, r.o_site, h.lin.data(), h.n));
         if (h.mode == kModeInt) {
@@ -1538,7 +1667,9 @@ ie_status ie_create(const ie_problem* problem, const ie_config* config, ie_handl
     if (h->cfg.num_temps == 0) h->cfg.num_temps = 10;
     if (h->cfg.exchange_interval == 0) h->cfg.exchange_interval = 1;
     if (h->cfg.num_temps > 128) return fail(IE_ERR_UNSUPPORTED, "at most 128 temperatures");
+    if (h->cfg.pt_path < 0 || h->cfg.pt_path > 2) return fail(IE_ERR_INVALID, "pt_path must be 0, 1 or 2");
     IE_TRY(h->eng.setup_device(config->device));
+    h->eng.pt_path = h->cfg.pt_path;
     IE_TRY(h->eng.build(problem, 1, h->cfg.num_temps, &config->seed, config->force_f64 != 0));
     h->offset = problem->energy_offset;
     IE_TRY(h->d_inc_e.upload(std::vector<double>(1, std::numeric_limits<double>::infinity()), h->eng.stream));

@@ -22,6 +22,7 @@
 // (engine.rs:218-271, 663-670) with every operation explicitly rounded.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "ie_device.cuh"
@@ -200,7 +201,7 @@ __device__ __forceinline__ StepPlan step_plan(const DevArrays& A, const RunArgs&
                                               uint32_t inst) {
     StepPlan P;
     if (R.serve) {
-        P.base = A.done[inst];
+        P.base = A.done[d.owner];
         const uint64_t left = d.sched_len > P.base ? d.sched_len - P.base : 0;
         const uint64_t want = max(1u, R.site_budget / max(d.n, 1u));
         P.steps = (uint32_t)min(left, want);
@@ -209,8 +210,8 @@ __device__ __forceinline__ StepPlan step_plan(const DevArrays& A, const RunArgs&
     } else {
         P.base = R.step_base;
         P.steps = R.steps;
-        P.tstride = R.temps_per_step;
-        P.temps = R.temps;
+        P.tstride = R.temps_per_step ? (R.cells ? R.ladder : 1u) : 0u;
+        P.temps = R.temps + (R.cells ? d.cell : 0u);
     }
     return P;
 }
@@ -492,8 +493,8 @@ __device__ void energies_f64_calls(const DevArrays& A, const InstDesc& d, const 
 // temperatures differ) | spread table (4 KB) | NG rings | NG spin arrays of
 // spin_cap words each (the instance's spins stay resident in shared memory
 // for the whole schedule).
-__host__ __device__ constexpr size_t batch_smem_bytes(int ng, uint32_t spin_cap, bool serve) {
-    return 2048 * (size_t)(serve ? ng : 1) + 4096 + (size_t)ng * kSlots * kChunk * 4 + (size_t)ng * spin_cap * 8;
+__host__ __device__ constexpr size_t batch_smem_bytes(int ng, uint32_t spin_cap, bool own_tables) {
+    return 2048 * (size_t)(own_tables ? ng : 1) + 4096 + (size_t)ng * kSlots * kChunk * 4 + (size_t)ng * spin_cap * 8;
 }
 
 template <uint32_t MODE, int TPL>
@@ -507,7 +508,9 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
     const int t = tid % G;
     const int lane = t / TPL;
     const int h = t % TPL;
-    const bool own_tab = R.serve != 0;  // per-instance threshold tables
+    // per-instance threshold tables when the instances of a warp run at
+    // different temperatures (serving, PT cells)
+    const bool own_tab = R.serve != 0 || R.cells != 0;
     const int ntab = own_tab ? NG : 1;
     uint64_t* tab = dsm + (own_tab ? 256 * g : 0);
     uint2* lut = reinterpret_cast<uint2*>(dsm + 256 * ntab);
@@ -549,8 +552,8 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
             }
             P = step_plan(A, R, d, inst);
 #pragma unroll
-            for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
-            pos0 = A.pos[inst];
+            for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)d.owner + i];
+            pos0 = A.pos[d.owner];
 #pragma unroll
             for (int j = 0; j < KP; j++) {
                 const size_t o = d.energy + lane + 8 * (j * TPL + h);
@@ -578,10 +581,10 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
                 }
             }
             if (active) {
-                const uint64_t base = chacha8_draw(key, pos0 + s);
+                const uint64_t base = chacha8_draw(key, pos0 + s) + d.cell;
                 sweep_stream<MODE, TPL>(A, d, ring, sp, lut, lane, h, gmask, tab, H, beta, base, E);
                 if constexpr (MODE == kModeF64) {
-                    if ((P.base + s + 1) % kResyncEvery == 0) {
+                    if (!R.cells && (P.base + s + 1) % kResyncEvery == 0) {
                         __syncwarp(gmask);
                         energies_f64_calls<TPL>(A, d, sp, h, E);
                     }
@@ -599,10 +602,10 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
                 else A.Ef[o] = E[j];
             }
             __syncwarp(gmask);
-            if (t == 0) {
-                A.pos[inst] = pos0 + P.steps;
-                A.deo[inst] ^= (int32_t)(exchanges_in(P.base, P.steps, R.exchange_interval) & 1u);
-                if (R.serve) A.done[inst] = P.base + P.steps;
+            if (t == 0 && !R.cells) {
+                A.pos[d.owner] = pos0 + P.steps;
+                A.deo[d.owner] ^= (int32_t)(exchanges_in(P.base, P.steps, R.exchange_interval) & 1u);
+                if (R.serve) A.done[d.owner] = P.base + P.steps;
             }
         }
     }
@@ -789,7 +792,9 @@ __device__ __forceinline__ uint32_t ws_task(const uint32_t* rec, uint8_t* spc, u
     return flips;
 }
 
-template <uint32_t MODE>
+// GSP: the instance's spin words stay in global memory (instances too large
+// for shared memory); otherwise they are copied into shared memory per item.
+template <uint32_t MODE, bool GSP>
 __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArrays A, RunArgs R, uint32_t spin_cap) {
     constexpr int NC = WsCfg<MODE>::NC;
     constexpr int NT = WsCfg<MODE>::THREADS;
@@ -801,7 +806,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
     uint64_t* rngb = dsm + 768;                            // 2 x 64 rows of kRS
     uint64_t* deb = rngb + 2 * 64 * kRS;                   // 64 rows of kRS
     uint32_t* recb = reinterpret_cast<uint32_t*>(deb + 64 * kRS);
-    uint64_t* sw = reinterpret_cast<uint64_t*>(recb + 2 * kWinRecWords);
+    uint64_t* const ssw = reinterpret_cast<uint64_t*>(recb + 2 * kWinRecWords);
     const int tid = threadIdx.x;
     const bool producer = tid < 32;
     const int c = tid - 32;  // decider index
@@ -809,7 +814,6 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
     const int ti = producer ? 0 : c / (8 * SPLIT);
     const int tl = producer ? 0 : (c / SPLIT) & 7;
     const int th = producer ? 0 : c % SPLIT;
-    uint8_t* spc = reinterpret_cast<uint8_t*>(sw) + tl;
     typedef typename std::conditional<MODE == kModeInt, int32_t, double>::type EType;
     if constexpr (MODE == kModeInt) {
         for (int i = tid; i < 512; i += NT) {
@@ -828,15 +832,17 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
         if (inst == 0xffffffffu) continue;
         const int H = MODE == kModeInt ? R.quad_h[q] : 0;
         const InstDesc d = A.desc[inst];
-        if (d.n > spin_cap) {
+        if (!GSP && d.n > spin_cap) {
             if (tid == 0) atomicExch(A.err, 2);
             continue;
         }
+        uint64_t* const sw = GSP ? A.spins + d.spin : ssw;
+        uint8_t* const spc = reinterpret_cast<uint8_t*>(sw) + tl;
         const StepPlan P = step_plan(A, R, d, inst);
         uint32_t key[8];
 #pragma unroll
-        for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
-        const uint64_t pos0 = A.pos[inst];
+        for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)d.owner + i];
+        const uint64_t pos0 = A.pos[d.owner];
         // energies: decider c < 64 owns replica (lane c / 8, call c % 8)
         const int el = c >> 3, ek = c & 7;
         const bool eown = !producer && c < 64;
@@ -846,8 +852,10 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
             if constexpr (MODE == kModeInt) E = A.Ei[o];
             else E = A.Ef[o];
         }
-        const uint64_t* gw = A.spins + d.spin;
-        for (uint32_t i = tid; i < d.n; i += NT) sw[i] = gw[i];
+        if (!GSP) {
+            const uint64_t* gw = A.spins + d.spin;
+            for (uint32_t i = tid; i < d.n; i += NT) sw[i] = gw[i];
+        }
         const uint32_t nwin = (d.n + kWin - 1) / kWin;
         const uint32_t* wt = A.wtab + d.win;
         const uint32_t* stream = A.recs + d.wrec;
@@ -858,7 +866,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
                 for (int i = tid; i < 2 * H + 1; i += NT) tab[i] = metropolis_threshold(i - H, beta);
                 __syncthreads();
             }
-            const uint64_t base = chacha8_draw(key, pos0 + s);
+            const uint64_t base = chacha8_draw(key, pos0 + s) + d.cell;
             if (producer) {
                 const int rl = tid >> 2, rh = tid & 3;
                 Xoshiro x;
@@ -939,7 +947,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
                 }
                 cp_async_wait0();
                 if constexpr (MODE == kModeF64) {
-                    if ((P.base + s + 1) % kResyncEvery == 0) {
+                    if (!R.cells && (P.base + s + 1) % kResyncEvery == 0) {
                         bar_sync(kBarCons, 32 * NC);
                         if (eown) {
                             double e8[8];
@@ -955,17 +963,19 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
             }
         }
         __syncthreads();
-        uint64_t* gwo = A.spins + d.spin;
-        for (uint32_t i = tid; i < d.n; i += NT) gwo[i] = sw[i];
+        if (!GSP) {
+            uint64_t* gwo = A.spins + d.spin;
+            for (uint32_t i = tid; i < d.n; i += NT) gwo[i] = sw[i];
+        }
         if (eown) {
             const size_t o = d.energy + el + 8 * ek;
             if constexpr (MODE == kModeInt) A.Ei[o] = E;
             else A.Ef[o] = E;
         }
-        if (tid == 0) {
-            A.pos[inst] = pos0 + P.steps;
-            A.deo[inst] ^= (int32_t)(exchanges_in(P.base, P.steps, R.exchange_interval) & 1u);
-            if (R.serve) A.done[inst] = P.base + P.steps;
+        if (tid == 0 && !R.cells) {
+            A.pos[d.owner] = pos0 + P.steps;
+            A.deo[d.owner] ^= (int32_t)(exchanges_in(P.base, P.steps, R.exchange_interval) & 1u);
+            if (R.serve) A.done[d.owner] = P.base + P.steps;
         }
         __syncthreads();
     }
@@ -1138,6 +1148,124 @@ __global__ void __launch_bounds__(1024) pt_kernel(DevArrays A, RunArgs R, uint32
 
 template __global__ void pt_kernel<kModeInt>(DevArrays, RunArgs, uint32_t, int);
 template __global__ void pt_kernel<kModeF64>(DevArrays, RunArgs, uint32_t, int);
+
+// ---------------------------------------------------------------------------
+// Exchange step of PT cells run as separate work items (engine.rs:713-789),
+// one warp per instance. The sweep launch before it ran `steps` steps whose
+// base seeds were draws pos .. pos + steps - 1. On an exchange step the DEO
+// pairs of the current parity are decided from the cells' tracked energies
+// with draws from pos + steps on (ballots give each replica's draw position),
+// energies are swapped in place and each pair's swap mask (0 for pairs not
+// exchanged) goes to A.xmask for swap_kernel; the phase toggles. Otherwise
+// only the stream position advances.
+// ---------------------------------------------------------------------------
+template <uint32_t MODE>
+__global__ void __launch_bounds__(32) exchange_kernel(DevArrays A, RunArgs R, uint32_t steps, uint32_t exchange) {
+    const uint32_t inst = blockIdx.x;
+    const InstDesc d = A.desc[inst];
+    const int nt = (int)d.nt;
+    const int tid = threadIdx.x;
+    uint32_t key[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
+    uint64_t p = A.pos[inst] + steps;
+    int deo = A.deo[inst];
+    auto energy = [&](int t, int r) -> double {
+        if constexpr (MODE == kModeInt) return (double)A.Ei[d.energy + (size_t)t * kReplicas + r];
+        else return A.Ef[d.energy + (size_t)t * kReplicas + r];
+    };
+    auto swap_energy = [&](int t, int r) {
+        const size_t a = d.energy + (size_t)t * kReplicas + r, b = a + kReplicas;
+        if constexpr (MODE == kModeInt) {
+            const int32_t x = A.Ei[a];
+            A.Ei[a] = A.Ei[b];
+            A.Ei[b] = x;
+        } else {
+            const double x = A.Ef[a];
+            A.Ef[a] = A.Ef[b];
+            A.Ef[b] = x;
+        }
+    };
+    if (exchange) {
+        if (nt > 1) {
+            for (int t = tid; t + 1 < nt; t += 32)
+                if ((t & 1) != deo) A.xmask[d.stat + t] = 0;
+            const unsigned lt = (1u << tid) - 1u;
+            for (int t = deo; t + 1 < nt; t += 2) {
+                const double db = R.dbeta[t];
+                const double dea = __dsub_rn(energy(t, tid), energy(t + 1, tid));
+                const double deb = __dsub_rn(energy(t, tid + 32), energy(t + 1, tid + 32));
+                const double exa = __dmul_rn(db, dea);
+                const double exb = __dmul_rn(db, deb);
+                const bool na = exa < 0.0, nb = exb < 0.0;
+                const unsigned ma = __ballot_sync(0xffffffffu, na);
+                const unsigned mb = __ballot_sync(0xffffffffu, nb);
+                bool aa = !na, ab = !nb;
+                if (na) {
+                    const uint64_t m = chacha8_draw(key, p + __popc(ma & lt)) >> 11;
+                    if constexpr (MODE == kModeInt) {
+                        const uint64_t ad = (uint64_t)fabs(dea);
+                        const uint64_t th = ad <= R.xdmax[t] ? R.xtab[R.xoff[t] + ad - 1]
+                                                             : (ad <= R.xdund[t] ? 1ULL : 0ULL);
+                        aa = m < th;
+                    } else {
+                        aa = __dmul_rn((double)m, 1.1102230246251565e-16) < exp(exa);
+                    }
+                }
+                if (nb) {
+                    const uint64_t m = chacha8_draw(key, p + __popc(ma) + __popc(mb & lt)) >> 11;
+                    if constexpr (MODE == kModeInt) {
+                        const uint64_t ad = (uint64_t)fabs(deb);
+                        const uint64_t th = ad <= R.xdmax[t] ? R.xtab[R.xoff[t] + ad - 1]
+                                                             : (ad <= R.xdund[t] ? 1ULL : 0ULL);
+                        ab = m < th;
+                    } else {
+                        ab = __dmul_rn((double)m, 1.1102230246251565e-16) < exp(exb);
+                    }
+                }
+                p += (uint64_t)(__popc(ma) + __popc(mb));
+                const unsigned Aa = __ballot_sync(0xffffffffu, aa);
+                const unsigned Ab = __ballot_sync(0xffffffffu, ab);
+                if (aa) swap_energy(t, tid);
+                if (ab) swap_energy(t, tid + 32);
+                if (tid == 0) {
+                    A.xmask[d.stat + t] = (uint64_t)Aa | ((uint64_t)Ab << 32);
+                    A.att[d.stat + t] += kReplicas;
+                    A.acc[d.stat + t] += (uint64_t)(__popc(Aa) + __popc(Ab));
+                }
+            }
+        }
+        deo ^= 1;
+    }
+    if (tid == 0) {
+        A.pos[inst] = p;
+        A.deo[inst] = deo;
+    }
+}
+
+template __global__ void exchange_kernel<kModeInt>(DevArrays, RunArgs, uint32_t, uint32_t);
+template __global__ void exchange_kernel<kModeF64>(DevArrays, RunArgs, uint32_t, uint32_t);
+
+// Masked swap of whole configurations for the pairs exchange_kernel decided
+// (engine.rs:751-769): words of cells t and t+1 exchange the bits of the
+// swapped replicas.
+__global__ void swap_kernel(DevArrays A, uint32_t inst) {
+    const InstDesc d = A.desc[inst];
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (uint32_t t = 0; t + 1 < d.nt; t++) {
+        const uint64_t M = A.xmask[d.stat + t];
+        if (M == 0) continue;
+        const uint64_t LM = transpose8x8(M);
+        uint64_t* w1 = A.spins + d.spin + (size_t)t * d.n;
+        uint64_t* w2 = w1 + d.n;
+        for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < d.n; v += stride) {
+            const uint64_t a = w1[v], b = w2[v];
+            const uint64_t dd = (a ^ b) & LM;
+            w1[v] = a ^ dd;
+            w2[v] = b ^ dd;
+        }
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Random init (ultimate.rs:248-280): one gen::<u64>() word per unclamped
@@ -1400,7 +1528,7 @@ int batch_occupancy(uint32_t mode, int tpl, uint32_t spin_cap, bool serve) {
 
 cudaError_t launch_batch(const DevArrays& A, const RunArgs& R, uint32_t mode, int tpl, uint32_t spin_cap, int grid,
                          cudaStream_t st) {
-    const size_t sm = batch_smem(tpl, spin_cap, R.serve != 0);
+    const size_t sm = batch_smem(tpl, spin_cap, R.serve != 0 || R.cells != 0);
     if (mode == kModeInt) {
         if (tpl == 1) batch_kernel<kModeInt, 1><<<grid, 32, sm, st>>>(A, R, spin_cap);
         else if (tpl == 2) batch_kernel<kModeInt, 2><<<grid, 32, sm, st>>>(A, R, spin_cap);
@@ -1413,27 +1541,48 @@ cudaError_t launch_batch(const DevArrays& A, const RunArgs& R, uint32_t mode, in
     return cudaGetLastError();
 }
 
-template <uint32_t MODE>
+template <uint32_t MODE, bool GSP>
 static int occ_win(size_t smem) {
     int n = 0;
-    if (cudaFuncSetAttribute(window_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(window_kernel<MODE, GSP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
         return 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, window_kernel<MODE>, WsCfg<MODE>::THREADS, smem) ==
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, window_kernel<MODE, GSP>, WsCfg<MODE>::THREADS, smem) ==
                    cudaSuccess
                ? n
                : 0;
 }
 
+// spin_cap 0: spins stay in global memory
 int window_occupancy(uint32_t mode, uint32_t spin_cap) {
     const size_t sm = ws_smem_bytes(spin_cap);
-    return mode == kModeInt ? occ_win<kModeInt>(sm) : occ_win<kModeF64>(sm);
+    if (spin_cap == 0) return mode == kModeInt ? occ_win<kModeInt, true>(sm) : occ_win<kModeF64, true>(sm);
+    return mode == kModeInt ? occ_win<kModeInt, false>(sm) : occ_win<kModeF64, false>(sm);
 }
 
 cudaError_t launch_window(const DevArrays& A, const RunArgs& R, uint32_t mode, uint32_t spin_cap, int grid,
                           cudaStream_t st) {
     const size_t sm = ws_smem_bytes(spin_cap);
-    if (mode == kModeInt) window_kernel<kModeInt><<<grid, WsCfg<kModeInt>::THREADS, sm, st>>>(A, R, spin_cap);
-    else window_kernel<kModeF64><<<grid, WsCfg<kModeF64>::THREADS, sm, st>>>(A, R, spin_cap);
+    if (spin_cap == 0) {
+        if (mode == kModeInt) window_kernel<kModeInt, true><<<grid, WsCfg<kModeInt>::THREADS, sm, st>>>(A, R, 0);
+        else window_kernel<kModeF64, true><<<grid, WsCfg<kModeF64>::THREADS, sm, st>>>(A, R, 0);
+    } else {
+        if (mode == kModeInt) window_kernel<kModeInt, false><<<grid, WsCfg<kModeInt>::THREADS, sm, st>>>(A, R, spin_cap);
+        else window_kernel<kModeF64, false><<<grid, WsCfg<kModeF64>::THREADS, sm, st>>>(A, R, spin_cap);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exchange(const DevArrays& A, const RunArgs& R, uint32_t ninst, uint32_t mode, uint32_t steps,
+                            bool exchange, cudaStream_t st) {
+    if (mode == kModeInt) exchange_kernel<kModeInt><<<ninst, 32, 0, st>>>(A, R, steps, exchange ? 1u : 0u);
+    else exchange_kernel<kModeF64><<<ninst, 32, 0, st>>>(A, R, steps, exchange ? 1u : 0u);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_swap(const DevArrays& A, uint32_t inst, uint32_t n_words, int sm_count, cudaStream_t st) {
+    const int grid = (int)std::min<uint32_t>((n_words + 255) / 256, (uint32_t)(4 * sm_count));
+    swap_kernel<<<std::max(grid, 1), 256, 0, st>>>(A, inst);
     return cudaGetLastError();
 }
 

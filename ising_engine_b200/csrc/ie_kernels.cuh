@@ -30,6 +30,8 @@ struct InstDesc {
     uint64_t wrec;   // windowed kernel's record stream (one record per site): recs[wrec ..)
     uint64_t sched;  // serving: the instance's per-step temperatures at temps[sched .. sched + sched_len)
     uint64_t sched_len;
+    uint32_t owner;  // instance whose master key, stream position and DEO phase this entry uses
+    uint32_t cell;   // PT cell run as its own work item: Xoshiro seed offset and ladder column
 };
 
 // Site-record streams of the batched kernel. Each instance's stream is a
@@ -72,6 +74,7 @@ struct DevArrays {
     uint64_t* acc;           // swap accepts
     int32_t* err;            // device error word
     uint64_t* done;          // serving: steps of its schedule each instance has executed
+    uint64_t* xmask;         // PT cells: swap mask of each pair in the last exchange [stat + pair]
 };
 
 // Run parameters of one launch.
@@ -97,6 +100,12 @@ struct RunArgs {
     // max(1, site_budget / n) steps in this launch
     uint32_t serve;
     uint32_t site_budget;
+    // PT cells: every work item is one cell (InstDesc::owner, ::cell) of a
+    // ladder of `ladder` temperatures; the launch runs steps that end at an
+    // exchange or resync step at the latest, and leaves the stream position,
+    // DEO phase and f64 resync to the exchange step (exchange_kernel)
+    uint32_t cells;
+    uint32_t ladder;
 };
 
 }  // namespace ie

@@ -56,14 +56,18 @@ def test_lattice_2d_single_cell_1000_sweeps():
     b.close()
 
 
+PT_PATHS = [1, 2]  # one CTA per instance; every cell its own work item
+
+
+@pytest.mark.parametrize("path", PT_PATHS)
 @pytest.mark.parametrize("interval", [1, 3])
-def test_pt_maxcut_exchange(interval):
+def test_pt_maxcut_exchange(interval, path):
     m = I.maxcut_gnm(96, 700, seed=3)
     temps = I.geometric_beta_ladder(8, 0.1, 3.0)
     steps = 61
     ref = O.run_schedule(m, np.tile(temps, (steps, 1)), 77, exchange_interval=interval,
                          collect_stats=True)
-    with Engine(m, num_temps=8, seed=77, exchange_interval=interval) as eng:
+    with Engine(m, num_temps=8, seed=77, exchange_interval=interval, pt_path=path) as eng:
         eng.init_random()
         eng.step(temps, 20)
         eng.step(temps, steps - 20)  # split calls continue the same trajectory
@@ -72,7 +76,8 @@ def test_pt_maxcut_exchange(interval):
         assert deo == (steps // interval) % 2
 
 
-def test_maxcut_800_pt32_interval10():
+@pytest.mark.parametrize("path", PT_PATHS)
+def test_maxcut_800_pt32_interval10(path):
     """The G(n=800, m=19176) Max-Cut ladder: 32 temperatures, beta geometric
     0.1..3.0, exchange every 10 sweeps (a shortened run)."""
     m = I.maxcut_gnm(800, 19176, seed=42)
@@ -80,13 +85,14 @@ def test_maxcut_800_pt32_interval10():
     steps = 100
     ref = O.run_schedule(m, np.tile(temps, (steps, 1)), 1337, exchange_interval=10,
                          collect_stats=True, threads=8)
-    with Engine(m, num_temps=32, seed=1337, exchange_interval=10) as eng:
+    with Engine(m, num_temps=32, seed=1337, exchange_interval=10, pt_path=path) as eng:
         eng.init_random()
         eng.step(temps, steps)
         assert_same_run(eng, ref)
 
 
-def test_clamped_sites_int_and_f64():
+@pytest.mark.parametrize("path", PT_PATHS)
+def test_clamped_sites_int_and_f64(path):
     rng = np.random.default_rng(9)
     for integer in (True, False):
         m = I.random_regular_qubo(60, 4, rng, integer=integer)
@@ -97,19 +103,20 @@ def test_clamped_sites_int_and_f64():
         temps = [2.0, 1.0, 0.5, 0.25]
         ref = O.run_schedule(m, np.tile(temps, (40, 1)), 5, clamped=clamped, clamp_val=cval,
                              collect_stats=True)
-        with Engine(m, num_temps=4, seed=5) as eng:
+        with Engine(m, num_temps=4, seed=5, pt_path=path) as eng:
             eng.set_clamps(clamped, cval)
             eng.init_random()
             eng.step(temps, 40)
             assert_same_run(eng, ref)
 
 
+@pytest.mark.parametrize("path", PT_PATHS)
 @pytest.mark.parametrize("hot,cold,seed,favourable", [(0, 1, 1, True), (1, 0, 2, False)])
-def test_swap_statistics_known_answers(hot, cold, seed, favourable):
+def test_swap_statistics_known_answers(hot, cold, seed, favourable, path):
     """test_population_annealing.rs:354-420 on the device."""
     m = QuboModel(1, np.array([10.0]), CsrMatrix(np.zeros(0), np.zeros(0, np.uint64),
                                                  np.zeros(2, np.uint64)))
-    with Engine(m, num_temps=2, seed=seed) as eng:
+    with Engine(m, num_temps=2, seed=seed, pt_path=path) as eng:
         eng.set_clamps(np.ones(1, np.uint8), np.array([hot], np.int8))
         eng.set_spins(np.array([[~np.uint64(0) if hot else 0], [~np.uint64(0) if cold else 0]],
                                dtype=np.uint64))
@@ -120,6 +127,54 @@ def test_swap_statistics_known_answers(hot, cold, seed, favourable):
         assert rate == 1.0 and draws == 1
     else:
         assert rate < 0.01 and draws == 65
+
+
+@pytest.mark.parametrize("path", PT_PATHS)
+def test_pt_float_couplings_resync_across_1000(path):
+    """f64 PT with the step-1000 resync falling on an exchange step (interval
+    5) and per-step ladders through run_schedule."""
+    rng = np.random.default_rng(12)
+    m = I.random_regular_qubo(300, 6, rng, integer=False)
+    temps = I.geometric_beta_ladder(4, 0.3, 2.0)
+    steps = 1003
+    ref = O.run_schedule(m, np.tile(temps, (steps, 1)), 4, exchange_interval=5, collect_stats=True)
+    with Engine(m, num_temps=4, seed=4, exchange_interval=5, pt_path=path) as eng:
+        eng.init_random()
+        eng.step(temps, 998)
+        eng.step(temps, 5)
+        assert_same_run(eng, ref)
+    sched = np.stack([temps * (1.0 + 0.01 * k) for k in range(12)])
+    ref = O.run_schedule(m, sched, 6, exchange_interval=2, collect_stats=True)
+    with Engine(m, num_temps=4, seed=6, exchange_interval=2, pt_path=path) as eng:
+        eng.init_random()
+        eng.run_schedule(sched)
+        assert_same_run(eng, ref)
+
+
+def test_lattice_3d_cells_in_global_memory():
+    """A 3D lattice too large for shared memory (L=32, N=32768): the cells run
+    on the windowed kernel with spins in global memory (consecutive sites are
+    coupled, so every window level holds one site)."""
+    m = I.pm_j_lattice(32, 3, seed=8)
+    temps = I.geometric_beta_ladder(4, 0.2, 2.0)
+    ref = O.run_schedule(m, np.tile(temps, (7, 1)), 21, exchange_interval=5, collect_stats=True, threads=4)
+    with Engine(m, num_temps=4, seed=21, exchange_interval=5, pt_path=2) as eng:
+        eng.init_random()
+        eng.step(temps, 7)
+        assert_same_run(eng, ref)
+
+
+def test_lattice_3d_L64_64_temperatures_full_size():
+    """The 3D +-J lattice at full size (L=64, N=262144, 64 temperatures, beta
+    geometric 0.2..2.0, exchange every 5 sweeps) for 6 steps: spins,
+    energies, swap statistics and stream position equal the oracle's."""
+    m = I.pm_j_lattice(64, 3, seed=64)
+    temps = I.geometric_beta_ladder(64, 0.2, 2.0)
+    ref = O.run_schedule(m, np.tile(temps, (6, 1)), 99, exchange_interval=5, collect_stats=True, threads=16)
+    with Engine(m, num_temps=64, seed=99, exchange_interval=5) as eng:
+        eng.init_random()
+        eng.step(temps, 6)
+        assert_same_run(eng, ref)
 
 
 def test_uneven_batch_bit_exact_and_plain_equal():
