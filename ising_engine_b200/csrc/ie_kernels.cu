@@ -632,6 +632,7 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
 // ---------------------------------------------------------------------------
 constexpr int kWin = 8;
 constexpr uint32_t kWinRecWords = 8 * (4 + 3 * kWinMaxDeg);  // eight f64 records of degree <= 32
+constexpr uint32_t kWinBufs = 3;  // record buffers: window w in use, w+1 landed, w+2 in flight
 
 
 // Copies the records of one window (positions from its table entry) into buf.
@@ -666,8 +667,8 @@ __device__ __forceinline__ void bar_sync(int id, int count) { asm volatile("bar.
 __device__ __forceinline__ void bar_arrive(int id, int count) { asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
 
 __host__ __device__ constexpr size_t ws_smem_bytes(uint32_t spin_cap) {
-    // tab 2 KB | spread table 4 KB | outputs 2 x 64 rows | dE 64 rows | records 2 x 3200 B | spins
-    return 2048 + 4096 + 2 * 64 * kRS * 8 + 64 * kRS * 8 + 2 * kWinRecWords * 4 + (size_t)spin_cap * 8;
+    // tab 2 KB | spread table 4 KB | outputs 2 x 64 rows | dE 64 rows | records 3 x 3200 B | spins
+    return 2048 + 4096 + 2 * 64 * kRS * 8 + 64 * kRS * 8 + kWinBufs * kWinRecWords * 4 + (size_t)spin_cap * 8;
 }
 
 template <uint32_t MODE>
@@ -806,7 +807,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
     uint64_t* rngb = dsm + 768;                            // 2 x 64 rows of kRS
     uint64_t* deb = rngb + 2 * 64 * kRS;                   // 64 rows of kRS
     uint32_t* recb = reinterpret_cast<uint32_t*>(deb + 64 * kRS);
-    uint64_t* const ssw = reinterpret_cast<uint64_t*>(recb + 2 * kWinRecWords);
+    uint64_t* const ssw = reinterpret_cast<uint64_t*>(recb + kWinBufs * kWinRecWords);
     const int tid = threadIdx.x;
     const bool producer = tid < 32;
     const int c = tid - 32;  // decider index
@@ -888,26 +889,23 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
                 }
                 for (uint32_t w = nwin >= 2 ? nwin - 2 : 0; w < nwin; w++) bar_sync(kBarEmpty0 + (w & 1), NT);
             } else {
+                // records of window w + 2 are fetched while window w runs
                 window_fetch(wt, stream, recb, c, 32 * NC);
                 cp_async_commit();
-                uint32_t nxt[10];
-#pragma unroll
-                for (int i = 0; i < 10; i++) nxt[i] = wt[i];
+                if (nwin > 1) window_fetch(wt + 16, stream, recb + kWinRecWords, c, 32 * NC);
+                cp_async_commit();
                 for (uint32_t w = 0; w < nwin; w++) {
                     const int b = w & 1;
                     uint32_t cur[10];
 #pragma unroll
-                    for (int i = 0; i < 10; i++) cur[i] = nxt[i];
-                    if (w + 1 < nwin) {
-                        const uint32_t* en = wt + 16 * (size_t)(w + 1);
-                        window_fetch(en, stream, recb + ((w + 1) & 1) * kWinRecWords, c, 32 * NC);
-#pragma unroll
-                        for (int i = 0; i < 10; i++) nxt[i] = en[i];
-                    }
+                    for (int i = 0; i < 10; i++) cur[i] = wt[16 * (size_t)w + i];
+                    if (w + 2 < nwin)
+                        window_fetch(wt + 16 * (size_t)(w + 2), stream, recb + ((w + 2) % kWinBufs) * kWinRecWords, c,
+                                     32 * NC);
                     cp_async_commit();
                     cp_async_wait1();
-                    bar_sync(kBarFull0 + b, NT);  // outputs of window w are ready; records visible too
-                    const uint32_t* rb = recb + (w & 1) * kWinRecWords;
+                    bar_sync(kBarFull0 + b, NT);  // outputs of window w are ready; records of w, w+1 visible
+                    const uint32_t* rb = recb + (w % kWinBufs) * kWinRecWords;
                     uint32_t off = 0;
 #pragma unroll
                     for (int i = 0; i < 8; i++)
