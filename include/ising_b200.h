@@ -249,6 +249,37 @@ ie_status ie_serve_footprint(ie_serve* s, const ie_problem* problem, uint64_t n_
 /* Device time of the last tick and kernel launches in it. */
 ie_status ie_serve_last_tick(ie_serve* s, double* ms, uint64_t* launches);
 
+/* ---- engine_v2 (S2) bit-sliced state and operators ----
+ * The integral-couplings state backend SparseBitSlice
+ * (src/engine_v2/backends/sparse_bitslice.rs:19-346) on the device, driven at
+ * the granularity of one operator application: MetropolisSweep::apply
+ * (src/engine_v2/operators/metropolis_sweep.rs:95-146) and
+ * ReplicaExchange::apply (src/engine_v2/operators/replica_exchange.rs:61-110).
+ * The per-site delta_e_into / apply_flips of the SpinState trait
+ * (src/engine_v2/state.rs:70-148) are too fine for a device call and are not
+ * exported. `ir` is a ProblemIR (src/engine_v2/ir.rs:14-69): both triangles,
+ * rows sorted, duplicates merged, no zero weights, integral values.
+ * The operator's ChaCha8Rng is ChaCha8Rng::seed_from_u64(seed) after
+ * `draw_offset` 64-bit draws; a Metropolis call consumes sweeps * n * r
+ * draws, an exchange call one per attempted pair (*proposed). */
+typedef struct ie_v2 ie_v2;
+/* init: [num_vars] 0/1, copied into every replica (SparseBitSlice::new). */
+ie_status ie_v2_create(const ie_problem* ir, uint32_t num_replicas, const uint8_t* init, int32_t device,
+                       ie_v2** out);
+ie_status ie_v2_destroy(ie_v2* h);
+/* temps: per-replica temperatures, replica k uses temps[k % n_temps]. */
+ie_status ie_v2_metropolis(ie_v2* h, const double* temps, uint32_t n_temps, uint64_t sweeps, uint64_t seed,
+                           uint64_t draw_offset, uint64_t* proposed, uint64_t* accepted);
+ie_status ie_v2_exchange(ie_v2* h, const double* temps, uint32_t n_temps, uint64_t rounds, uint64_t seed,
+                         uint64_t draw_offset, uint64_t* proposed, uint64_t* accepted);
+/* planes: [num_vars * ceil(r / 64)] (bit b of word q of a site = replica 64q + b);
+ * energies: [r] from the ledger (either may be NULL). */
+ie_status ie_v2_read(ie_v2* h, uint64_t* planes, double* energies);
+/* SpinState::audit: largest |ledger - recomputed| energy; 0 on an exact state. */
+ie_status ie_v2_audit(ie_v2* h, double* drift);
+/* ProblemIR::greedy_coloring (src/engine_v2/ir.rs:114-139), host only. */
+ie_status ie_v2_coloring(const ie_problem* ir, uint32_t* colors);
+
 /* ---- measurement helper (no reference counterpart) ----
  * Measured roofline denominators on `device`: int32 LOP3/IADD3 throughput
  * (ops/s) and Xoshiro256++ step+compare throughput (outputs/s), the per-attempt

@@ -100,6 +100,13 @@ _SIGS = {
     "ie_serve_result": ([_vp, C.c_uint64, _vp, _vp], C.c_int),
     "ie_serve_footprint": ([_vp, _vp, C.c_uint64, _vp], C.c_int),
     "ie_serve_last_tick": ([_vp, _vp, _vp], C.c_int),
+    "ie_v2_create": ([_vp, C.c_uint32, _vp, C.c_int32, _vp], C.c_int),
+    "ie_v2_destroy": ([_vp], C.c_int),
+    "ie_v2_metropolis": ([_vp, _vp, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, _vp, _vp], C.c_int),
+    "ie_v2_exchange": ([_vp, _vp, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, _vp, _vp], C.c_int),
+    "ie_v2_read": ([_vp, _vp, _vp], C.c_int),
+    "ie_v2_audit": ([_vp, _vp], C.c_int),
+    "ie_v2_coloring": ([_vp, _vp], C.c_int),
 }
 
 

@@ -18,11 +18,12 @@
 
 #include "../../include/ising_b200.h"
 #include "ie_device.cuh"
+#include "ie_host.h"
 #include "ie_launch.h"
 
 using namespace ie;
 
-namespace {
+namespace ie {
 
 thread_local std::string g_err;
 
@@ -30,20 +31,6 @@ ie_status fail(ie_status s, const std::string& msg) {
     g_err = msg;
     return s;
 }
-
-#define IE_CUDA(call)                                                                      \
-    do {                                                                                   \
-        cudaError_t e_ = (call);                                                           \
-        if (e_ != cudaSuccess)                                                             \
-            return fail(e_ == cudaErrorMemoryAllocation ? IE_ERR_OOM : IE_ERR_CUDA,        \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
-    } while (0)
-
-#define IE_TRY(expr)                   \
-    do {                               \
-        ie_status s_ = (expr);         \
-        if (s_ != IE_OK) return s_;    \
-    } while (0)
 
 // rand_core 0.6.4 SeedableRng::seed_from_u64: PCG32 outputs fill the 32-byte
 // ChaCha8 key (little-endian), as ChaCha8Rng::seed_from_u64 (ultimate.rs:152).
@@ -57,6 +44,55 @@ void chacha_key_from_u64(uint64_t state, uint32_t key[8]) {
     }
 }
 
+// Exchange thresholds for the integer mode (engine.rs:725-727): for the pair
+// (t, t+1) with db = 1/T_t - 1/T_{t+1}, a swap with exponent db*de < 0 is
+// accepted iff gen::<f64>() < exp(db*de), i.e. iff (draw >> 11) <
+// ceil(exp(db*de) * 2^53), which depends only on |de|. Built with the host
+// libm exp, the same function the reference calls.
+ie_status build_xtables(const double* temps, uint32_t nt, XTables& X) {
+    X = XTables();
+    const uint32_t np = nt > 1 ? nt - 1 : 0;
+    X.off.resize(std::max<uint32_t>(np, 1));
+    X.dmax.resize(std::max<uint32_t>(np, 1));
+    X.dund.resize(std::max<uint32_t>(np, 1));
+    X.dbeta.resize(std::max<uint32_t>(np, 1));
+    for (uint32_t t = 0; t < np; t++) {
+        const double b1 = 1.0 / temps[t], b2 = 1.0 / temps[t + 1];
+        const double db = b1 - b2;
+        X.dbeta[t] = db;
+        X.off[t] = X.tab.size();
+        const double adb = std::fabs(db);
+        if (!(adb > 0.0) || !std::isfinite(adb)) {
+            X.dmax[t] = 0;
+            X.dund[t] = 0;
+            continue;
+        }
+        uint64_t a = 1;
+        for (;; a++) {
+            const double ex = -(adb * (double)a);
+            const double T = std::ceil(std::ldexp(std::exp(ex), 53));
+            if (T <= 1.0) break;
+            X.tab.push_back((uint64_t)T);
+            if (X.tab.size() > (1u << 24))
+                return fail(IE_ERR_UNSUPPORTED, "temperature ladder too fine for the integer exchange tables");
+        }
+        X.dmax[t] = a - 1;
+        // largest |de| with exp(-adb*|de|) > 0 (monotone), by bisection
+        uint64_t lo = a - 1, hi = (uint64_t)std::min(1e18, std::ceil(800.0 / adb) + 2.0);
+        while (hi - lo > 1) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (std::exp(-(adb * (double)mid)) > 0.0) lo = mid;
+            else hi = mid;
+        }
+        X.dund[t] = lo;
+    }
+    return IE_OK;
+}
+
+}  // namespace ie
+
+namespace {
+
 // f64::powi for a runtime exponent lowers to compiler-rt's __powidf2.
 double powi_rt(double a, int b) {
     const bool recip = b < 0;
@@ -69,35 +105,6 @@ double powi_rt(double a, int b) {
     }
     return recip ? 1.0 / r : r;
 }
-
-// Device array; alloc() keeps the allocation when it is large enough (the
-// contents are not preserved either way).
-template <typename T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0, cap = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    ie_status alloc(size_t count) {
-        n = count;
-        if (count == 0 || (p && count <= cap)) return IE_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        IE_CUDA(cudaMalloc(&p, count * sizeof(T)));
-        cap = count;
-        return IE_OK;
-    }
-    ie_status upload(const std::vector<T>& h, cudaStream_t st) {
-        IE_TRY(alloc(h.size()));
-        if (!h.empty()) IE_CUDA(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-        return IE_OK;
-    }
-};
 
 // One ingested problem (both triangles, reference row order).
 struct HostInst {
@@ -195,56 +202,6 @@ ie_status ingest(const ie_problem* p, bool force_f64, HostInst& out) {
     } else {
         out.mode = kModeF64;
         out.H = 0;
-    }
-    return IE_OK;
-}
-
-// Exchange thresholds for the integer mode (engine.rs:725-727): for the pair
-// (t, t+1) with db = 1/T_t - 1/T_{t+1}, a swap with exponent db*de < 0 is
-// accepted iff gen::<f64>() < exp(db*de), i.e. iff (draw >> 11) <
-// ceil(exp(db*de) * 2^53), which depends only on |de|. Built with the host
-// libm exp, the same function the reference calls.
-struct XTables {
-    std::vector<uint64_t> tab, off, dmax, dund;
-    std::vector<double> dbeta;
-};
-
-ie_status build_xtables(const double* temps, uint32_t nt, XTables& X) {
-    X = XTables();
-    const uint32_t np = nt > 1 ? nt - 1 : 0;
-    X.off.resize(std::max<uint32_t>(np, 1));
-    X.dmax.resize(std::max<uint32_t>(np, 1));
-    X.dund.resize(std::max<uint32_t>(np, 1));
-    X.dbeta.resize(std::max<uint32_t>(np, 1));
-    for (uint32_t t = 0; t < np; t++) {
-        const double b1 = 1.0 / temps[t], b2 = 1.0 / temps[t + 1];
-        const double db = b1 - b2;
-        X.dbeta[t] = db;
-        X.off[t] = X.tab.size();
-        const double adb = std::fabs(db);
-        if (!(adb > 0.0) || !std::isfinite(adb)) {
-            X.dmax[t] = 0;
-            X.dund[t] = 0;
-            continue;
-        }
-        uint64_t a = 1;
-        for (;; a++) {
-            const double ex = -(adb * (double)a);
-            const double T = std::ceil(std::ldexp(std::exp(ex), 53));
-            if (T <= 1.0) break;
-            X.tab.push_back((uint64_t)T);
-            if (X.tab.size() > (1u << 24))
-                return fail(IE_ERR_UNSUPPORTED, "temperature ladder too fine for the integer exchange tables");
-        }
-        X.dmax[t] = a - 1;
-        // largest |de| with exp(-adb*|de|) > 0 (monotone), by bisection
-        uint64_t lo = a - 1, hi = (uint64_t)std::min(1e18, std::ceil(800.0 / adb) + 2.0);
-        while (hi - lo > 1) {
-            const uint64_t mid = lo + (hi - lo) / 2;
-            if (std::exp(-(adb * (double)mid)) > 0.0) lo = mid;
-            else hi = mid;
-        }
-        X.dund[t] = lo;
     }
     return IE_OK;
 }

@@ -932,6 +932,173 @@ static void unpack_words(Field& f, const uint64_t* words) {
 // C API (ctypes). Problems are passed as (n, linear, row_offsets, cols, vals,
 // offset) with int64 CSR indices, mirroring QuboModel/CsrMatrix.
 // ===========================================================================
+namespace {
+
+// ---------------------------------------------------------------------------
+// engine_v2 (S2): the integral bit-sliced state with its i64 field ledger
+// (src/engine_v2/backends/sparse_bitslice.rs:19-346), the default
+// swap_replicas of the SpinState trait (src/engine_v2/state.rs:126-140),
+// ProblemIR::greedy_coloring (src/engine_v2/ir.rs:114-139), MetropolisSweep
+// (src/engine_v2/operators/metropolis_sweep.rs:40-146) and ReplicaExchange
+// (src/engine_v2/operators/replica_exchange.rs:61-110).
+// ---------------------------------------------------------------------------
+struct V2State {
+    int64_t n = 0, r = 0, w = 0;
+    std::vector<int64_t> row, col, ilin, iw;
+    int64_t offset = 0;
+    std::vector<uint64_t> spins;      // spins[site * w + word], bit b = replica 64 word + b
+    std::vector<int64_t> fields;      // fields[site * r + rep]
+    std::vector<int64_t> energies;    // [r]
+
+    uint64_t bit(int64_t site, int64_t rep) const { return (spins[site * w + rep / 64] >> (rep % 64)) & 1; }
+
+    // sparse_bitslice.rs:88-112
+    void rebuild() {
+        for (int64_t s = 0; s < n; s++)
+            for (int64_t k = 0; k < r; k++) fields[s * r + k] = ilin[s];
+        for (int64_t s = 0; s < n; s++)
+            for (int64_t e = row[s]; e < row[s + 1]; e++)
+                for (int64_t k = 0; k < r; k++)
+                    if (bit(s, k)) fields[col[e] * r + k] += iw[e];
+        for (int64_t k = 0; k < r; k++) energies[k] = energy_of(k);
+    }
+    // sparse_bitslice.rs:116-137
+    int64_t energy_of(int64_t rep) const {
+        int64_t l = 0, q = 0;
+        for (int64_t s = 0; s < n; s++) {
+            if (!bit(s, rep)) continue;
+            l += ilin[s];
+            for (int64_t e = row[s]; e < row[s + 1]; e++)
+                if (bit(col[e], rep)) q += iw[e];
+        }
+        return offset + l + q / 2;
+    }
+    // sparse_bitslice.rs:247-255
+    void delta_e_into(int64_t site, std::vector<double>& out) const {
+        for (int64_t k = 0; k < r; k++) {
+            const int64_t h = fields[site * r + k];
+            out[k] = (double)(bit(site, k) == 0 ? h : -h);
+        }
+    }
+    // sparse_bitslice.rs:145-174 (the dense form at :184-235 is bit-identical)
+    void apply_flips(int64_t site, const std::vector<uint64_t>& mask) {
+        for (int64_t q = 0; q < w; q++) {
+            const uint64_t mb = mask[q];
+            if (!mb) continue;
+            const uint64_t sw = spins[site * w + q];
+            uint64_t b = mb;
+            while (b) {
+                const int bp = __builtin_ctzll(b);
+                const int64_t rep = q * 64 + bp;
+                const uint64_t x = (sw >> bp) & 1;
+                const int64_t h = fields[site * r + rep];
+                energies[rep] += x == 0 ? h : -h;
+                const int64_t sign = x == 0 ? 1 : -1;
+                for (int64_t e = row[site]; e < row[site + 1]; e++) fields[col[e] * r + rep] += sign * iw[e];
+                b &= b - 1;
+            }
+            spins[site * w + q] ^= mb;
+        }
+    }
+    // state.rs:126-140
+    void swap_replicas(int64_t a, int64_t b) {
+        if (a == b) return;
+        std::vector<uint64_t> mask(w);
+        for (int64_t s = 0; s < n; s++) {
+            if (bit(s, a) != bit(s, b)) {
+                std::fill(mask.begin(), mask.end(), 0);
+                mask[a / 64] |= 1ull << (a % 64);
+                mask[b / 64] |= 1ull << (b % 64);
+                apply_flips(s, mask);
+            }
+        }
+    }
+};
+
+// ir.rs:114-139
+static std::vector<uint32_t> v2_greedy_coloring(const V2State& s) {
+    std::vector<uint32_t> colors(s.n, 0xFFFFFFFFu), used;
+    for (int64_t i = 0; i < s.n; i++) {
+        used.clear();
+        for (int64_t e = s.row[i]; e < s.row[i + 1]; e++)
+            if (colors[s.col[e]] != 0xFFFFFFFFu) used.push_back(colors[s.col[e]]);
+        std::sort(used.begin(), used.end());
+        uint32_t c = 0;
+        for (uint32_t u : used) {
+            if (u == c) c++;
+            else if (u > c) break;
+        }
+        colors[i] = c;
+    }
+    return colors;
+}
+
+// metropolis_sweep.rs:40-58 (order) and :95-146 (apply)
+static void v2_metropolis(V2State& s, const double* temps, int nt, int64_t sweeps, ChaCha8Rng& rng,
+                          int64_t& proposed, int64_t& accepted) {
+    const std::vector<uint32_t> colors = v2_greedy_coloring(s);
+    uint32_t ncol = 0;
+    for (uint32_t c : colors) ncol = std::max(ncol, c + 1);
+    std::vector<int64_t> order;
+    for (uint32_t c = 0; c < ncol; c++)
+        for (int64_t i = 0; i < s.n; i++)
+            if (colors[i] == c) order.push_back(i);
+    std::vector<double> de(s.r);
+    std::vector<uint64_t> mask(s.w);
+    for (int64_t sw = 0; sw < sweeps; sw++)
+        for (int64_t site : order) {
+            s.delta_e_into(site, de);
+            std::fill(mask.begin(), mask.end(), 0);
+            bool any = false;
+            for (int64_t rep = 0; rep < s.r; rep++) {
+                const double d = de[rep];
+                const double t = temps[rep % nt];
+                bool acc;
+                if (d <= 0.0) {
+                    (void)rng.gen_f64();
+                    acc = true;
+                } else {
+                    const double p = t > 0.0 ? std::exp(-d / t) : 0.0;
+                    const double u = rng.gen_f64();
+                    acc = u < p;
+                }
+                proposed++;
+                if (acc) {
+                    mask[rep / 64] |= 1ull << (rep % 64);
+                    accepted++;
+                    any = true;
+                }
+            }
+            if (any) s.apply_flips(site, mask);
+        }
+}
+
+// replica_exchange.rs:61-110
+static void v2_exchange(V2State& s, const double* temps, int nt, int64_t rounds, ChaCha8Rng& rng,
+                        int64_t& proposed, int64_t& accepted) {
+    if (s.r < 2 || nt == 0) return;
+    auto beta = [&](int64_t rep) {
+        const double t = temps[rep % nt];
+        return t > 0.0 ? 1.0 / t : std::numeric_limits<double>::infinity();
+    };
+    std::vector<double> e(s.r);
+    for (int64_t round = 0; round < rounds; round++) {
+        for (int64_t k = 0; k < s.r; k++) e[k] = (double)s.energies[k];
+        for (int64_t k = round & 1; k + 1 < s.r; k += 2) {
+            const double delta = (beta(k) - beta(k + 1)) * (e[k] - e[k + 1]);
+            proposed++;
+            const double u = rng.gen_f64();
+            if (delta >= 0.0 || u < std::exp(delta)) {
+                s.swap_replicas(k, k + 1);
+                std::swap(e[k], e[k + 1]);
+                accepted++;
+            }
+        }
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 int or_abi_version() { return 3; }
@@ -1118,6 +1285,60 @@ int or_run_sa_batch(int64_t count, const int64_t* ns, const double* const* lins,
         if (energies_out)
             for (int r = 0; r < NR; r++) energies_out[(size_t)i * NR + r] = f.energies[0][r];
     });
+    return 0;
+}
+
+// A program of S2 operator applications on one state with one master stream
+// (ChaCha8Rng::seed_from_u64(seed) after skip_draws draws): op i is
+// MetropolisSweep (kinds[i] == 0) for counts[i] sweeps or ReplicaExchange
+// (kinds[i] == 1) for counts[i] rounds, all at temps[nt]. Outputs the planes
+// [n * ceil(r/64)], the ledger energies [r], (proposed, accepted) per op, the
+// largest ledger drift against a rebuild and the stream position.
+int or_v2_program(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,
+                  double offset, int64_t r, const uint8_t* init, uint64_t seed, uint64_t skip_draws, int64_t nops,
+                  const int32_t* kinds, const int64_t* counts, const double* temps, int32_t nt,
+                  uint64_t* planes_out, double* energies_out, int64_t* stats_out, double* drift_out,
+                  uint64_t* draws_out) {
+    V2State s;
+    s.n = n;
+    s.r = r;
+    s.w = (r + 63) / 64;
+    s.row.assign(row, row + n + 1);
+    s.col.assign(col, col + row[n]);
+    s.offset = (int64_t)offset;
+    s.ilin.resize(n);
+    for (int64_t i = 0; i < n; i++) s.ilin[i] = (int64_t)lin[i];
+    s.iw.resize(row[n]);
+    for (int64_t e = 0; e < row[n]; e++) s.iw[e] = (int64_t)val[e];
+    s.spins.assign(n * s.w, 0);
+    for (int64_t i = 0; i < n; i++)
+        if (init[i] & 1)
+            for (int64_t q = 0; q < s.w; q++) {
+                const int64_t valid = std::min<int64_t>(r - 64 * q, 64);
+                s.spins[i * s.w + q] = valid == 64 ? ~0ull : ((1ull << valid) - 1);
+            }
+    s.fields.assign(n * r, 0);
+    s.energies.assign(r, 0);
+    s.rebuild();
+    ChaCha8Rng rng(seed);
+    for (uint64_t k = 0; k < skip_draws; k++) rng.next_u64();
+    for (int64_t i = 0; i < nops; i++) {
+        int64_t p = 0, a = 0;
+        if (kinds[i] == 0) v2_metropolis(s, temps, nt, counts[i], rng, p, a);
+        else v2_exchange(s, temps, nt, counts[i], rng, p, a);
+        stats_out[2 * i] = p;
+        stats_out[2 * i + 1] = a;
+    }
+    std::copy(s.spins.begin(), s.spins.end(), planes_out);
+    for (int64_t k = 0; k < r; k++) energies_out[k] = (double)s.energies[k];
+    // audit (sparse_bitslice.rs:317-346)
+    V2State fresh = s;
+    fresh.rebuild();
+    int64_t drift = 0;
+    for (size_t i = 0; i < s.fields.size(); i++) drift = std::max<int64_t>(drift, std::llabs(s.fields[i] - fresh.fields[i]));
+    for (int64_t k = 0; k < r; k++) drift = std::max<int64_t>(drift, std::llabs(s.energies[k] - fresh.energies[k]));
+    *drift_out = (double)drift;
+    *draws_out = rng.draws;
     return 0;
 }
 

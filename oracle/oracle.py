@@ -71,6 +71,9 @@ def lib():
         L.or_run_sa_batch.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int,
                                       C.c_void_p, C.c_void_p, C.c_void_p]
+        L.or_v2_program.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, C.c_int64, _u8p,
+                                    C.c_uint64, C.c_uint64, C.c_int64, C.c_void_p, _i64p, _f64p, C.c_int32,
+                                    _u64p, _f64p, _i64p, _f64p, _u64p]
         _lib = L
     return _lib
 
@@ -233,3 +236,27 @@ def run_sa_batch(models, seeds, temps, threads=1, want_words=True):
                           temps.ctypes.data_as(C.c_void_p), len(temps), threads, _ptr(words),
                           off.ctypes.data_as(C.c_void_p), en.ctypes.data_as(C.c_void_p))
     return words, off, en
+
+
+def v2_program(model, r, init, seed, ops, temps, skip_draws=0):
+    """S2 operators on one bit-sliced state with one master stream: ops is a
+    list of ("metropolis", sweeps) / ("exchange", rounds), all at per-replica
+    temperatures temps (replica k uses temps[k % len]). Returns (planes
+    [n, ceil(r/64)], energies [r], [(proposed, accepted)] per op, ledger drift,
+    stream position)."""
+    n, lin, row, col, val = _csr(model)
+    w = (r + 63) // 64
+    kinds = np.array([0 if k == "metropolis" else 1 for k, _ in ops], dtype=np.int32)
+    counts = np.array([c for _, c in ops], dtype=np.int64)
+    temps = np.ascontiguousarray(temps, dtype=np.float64)
+    planes = np.zeros(n * w, dtype=np.uint64)
+    en = np.zeros(r, dtype=np.float64)
+    stats = np.zeros(2 * max(len(ops), 1), dtype=np.int64)
+    drift = np.zeros(1, dtype=np.float64)
+    draws = np.zeros(1, dtype=np.uint64)
+    lib().or_v2_program(n, lin, row, col, val, float(model.energy_offset), r,
+                        np.ascontiguousarray(init, dtype=np.uint8), seed, skip_draws, len(ops),
+                        kinds.ctypes.data_as(C.c_void_p), counts, temps, len(temps), planes, en, stats,
+                        drift, draws)
+    return (planes.reshape(n, w), en, [(int(stats[2 * i]), int(stats[2 * i + 1])) for i in range(len(ops))],
+            float(drift[0]), int(draws[0]))
