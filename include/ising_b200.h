@@ -123,6 +123,11 @@ ie_status ie_read_incumbent(ie_handle* h, double* energy, int8_t* state);
 /* Best replica of the final field in (t, r) order with strict < on the model
  * energy (ultimate.rs:345-368), merged with the incumbent (ultimate.rs:371-373). */
 ie_status ie_read_best(ie_handle* h, double* energy, int8_t* state);
+/* steepest_descent_1opt (src/solver/local_search.rs:19-57) on the device with
+ * the handle's problem: polishes state [num_vars] (0/1) in place to a 1-opt
+ * local minimum over the unclamped variables (is_clamped [num_vars] or NULL);
+ * improvement = total energy decrease, as the reference returns it. */
+ie_status ie_one_opt(ie_handle* h, int8_t* state, const uint8_t* is_clamped, double* improvement);
 
 /* geometric ladder temps[i] = T_max * f^i, f = (T_min/T_max)^(1/(nt-1)),
  * computed with pow and powi exactly as ultimate.rs:238-246. */

@@ -75,6 +75,7 @@ _SIGS = {
     "ie_read_rng_state": ([_vp, _vp, _vp], C.c_int),
     "ie_read_incumbent": ([_vp, _vp, _vp], C.c_int),
     "ie_read_best": ([_vp, _vp, _vp], C.c_int),
+    "ie_one_opt": ([_vp, _vp, _vp, _vp], C.c_int),
     "ie_geometric_temps": ([C.c_double, C.c_double, C.c_uint32, _vp], C.c_int),
     "ie_suggested_temp_range": ([_vp, _vp, _vp], C.c_int),
     "ie_batch_create": ([_vp, C.c_uint32, _vp, _vp, _vp], C.c_int),

@@ -1738,25 +1738,21 @@ ie_status ie_read_best(ie_handle* h, double* energy, int8_t* state) {
     Engine& E = h->eng;
     const uint32_t nt = E.nt;
     const uint64_t n = E.desc[0].n;
-    DevBuf<double> es;
+    // model energies of every (cell, replica), argmin and the replica's
+    // configuration on the device (ultimate.rs:345-368)
+    DevBuf<double> es, be;
+    DevBuf<int8_t> st;
+    DevBuf<int32_t> fd;
     IE_TRY(es.alloc((size_t)nt * kReplicas));
+    IE_TRY(be.alloc(1));
+    IE_TRY(st.alloc(std::max<uint64_t>(n, 1)));
+    IE_TRY(fd.alloc(1));
     IE_CUDA(launch_model_energy(E.arrays(), 0, nt, h->offset, es.p, E.stream));
-    std::vector<double> he((size_t)nt * kReplicas);
-    IE_CUDA(cudaMemcpyAsync(he.data(), es.p, he.size() * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    IE_CUDA(launch_best_extract(E.arrays(), 0, es.p, nt * kReplicas, st.p, be.p, fd.p, E.stream));
+    double best = 0;
+    IE_CUDA(cudaMemcpyAsync(&best, be.p, sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    if (n) IE_CUDA(cudaMemcpyAsync(state, st.p, n, cudaMemcpyDeviceToHost, E.stream));
     IE_CUDA(cudaStreamSynchronize(E.stream));
-    double best = std::numeric_limits<double>::infinity();
-    size_t arg = 0;
-    bool found = false;
-    for (size_t i = 0; i < he.size(); i++)
-        if (he[i] < best) {
-            best = he[i];
-            arg = i;
-            found = true;
-        }
-    std::vector<uint64_t> words((size_t)nt * n);
-    IE_TRY(E.read_words(0, 1, words.data()));
-    for (uint64_t v = 0; v < n; v++)
-        state[v] = found ? (int8_t)((words[(arg / kReplicas) * n + v] >> (arg % kReplicas)) & 1) : 0;
     *energy = best;
     if (h->have_incumbent) {
         double ie_ = 0;
@@ -1767,6 +1763,42 @@ ie_status ie_read_best(ie_handle* h, double* energy, int8_t* state) {
             std::copy(inc.begin(), inc.end(), state);
         }
     }
+    return IE_OK;
+}
+
+ie_status ie_one_opt(ie_handle* h, int8_t* state, const uint8_t* is_clamped, double* improvement) {
+    if (!h || !state) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    Engine& E = h->eng;
+    const uint64_t n = E.desc[0].n;
+    if (n == 0) {
+        if (improvement) *improvement = 0.0;
+        return IE_OK;
+    }
+    for (uint64_t v = 0; v < n; v++)
+        if (state[v] != 0 && state[v] != 1) return fail(IE_ERR_INVALID, "state must be 0/1");
+    DevBuf<int8_t> st;
+    DevBuf<uint8_t> cl;
+    DevBuf<double> g, imp;
+    DevBuf<uint64_t> fl;
+    IE_TRY(st.alloc(n));
+    IE_TRY(g.alloc(n));
+    IE_TRY(imp.alloc(1));
+    IE_TRY(fl.alloc(1));
+    IE_CUDA(cudaMemcpyAsync(st.p, state, n, cudaMemcpyHostToDevice, E.stream));
+    if (is_clamped) {
+        IE_TRY(cl.alloc(n));
+        IE_CUDA(cudaMemcpyAsync(cl.p, is_clamped, n, cudaMemcpyHostToDevice, E.stream));
+    }
+    // every flip lowers the energy by more than 1e-12, so the descent ends;
+    // the bound only guards against non-finite input
+    IE_CUDA(launch_one_opt(E.arrays(), 0, st.p, is_clamped ? cl.p : nullptr, g.p, imp.p, fl.p, 64 * n + 1024,
+                           E.stream));
+    double total = 0;
+    IE_CUDA(cudaMemcpyAsync(state, st.p, n, cudaMemcpyDeviceToHost, E.stream));
+    IE_CUDA(cudaMemcpyAsync(&total, imp.p, sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+    IE_CUDA(cudaStreamSynchronize(E.stream));
+    if (improvement) *improvement = total;
     return IE_OK;
 }
 

@@ -1354,6 +1354,129 @@ __global__ void model_energy_kernel(DevArrays A, uint32_t inst, double offset, d
     out[t] = e;
 }
 
+// Best replica (ultimate.rs:345-368): argmin of the model energies es[count]
+// in (cell, replica) order with strict < (lowest index on ties), and that
+// replica's configuration as 0/1 bytes. Single CTA.
+__global__ void __launch_bounds__(1024) best_extract_kernel(DevArrays A, uint32_t inst, const double* es,
+                                                           uint32_t count, int8_t* state, double* best_out,
+                                                           int32_t* found_out) {
+    __shared__ double sv[32];
+    __shared__ uint32_t si[32];
+    const InstDesc d = A.desc[inst];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+    double bv = inf;
+    uint32_t bi = 0xFFFFFFFFu;
+    for (uint32_t i = tid; i < count; i += blockDim.x)
+        if (es[i] < bv) {
+            bv = es[i];
+            bi = i;
+        }
+    for (int o = 16; o; o >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, bv, o);
+        const uint32_t oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov < bv || (ov == bv && oi < bi)) {
+            bv = ov;
+            bi = oi;
+        }
+    }
+    if (lane == 0) {
+        sv[wid] = bv;
+        si[wid] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++)
+            if (sv[k] < sv[0] || (sv[k] == sv[0] && si[k] < si[0])) {
+                sv[0] = sv[k];
+                si[0] = si[k];
+            }
+        *best_out = sv[0];
+        *found_out = sv[0] < inf ? 1 : 0;
+    }
+    __syncthreads();
+    const bool found = sv[0] < inf;
+    const uint32_t arg = si[0];
+    const uint32_t c = found ? arg >> 6 : 0, r = found ? arg & 63 : 0;
+    const uint8_t* sp = reinterpret_cast<const uint8_t*>(A.spins + d.spin + (size_t)c * d.n) + (r & 7);
+    for (uint32_t v = tid; v < d.n; v += blockDim.x) state[v] = found ? (int8_t)((sp[8u * v] >> (r >> 3)) & 1u) : 0;
+}
+
+// steepest_descent_1opt (local_search.rs:19-57) on one configuration: gains
+// g_i = (1 - 2 x_i)(lin_i + sum_j w_ij x_j) in CSR order, then repeatedly the
+// steepest improving flip among free variables (g < -1e-12, lowest index on
+// ties) with the neighbours' gains updated in CSR order, all in the
+// reference's f64 operation order. Single CTA: a block-wide argmin per flip.
+__global__ void __launch_bounds__(1024) one_opt_kernel(DevArrays A, uint32_t inst, int8_t* state,
+                                                       const uint8_t* clamped, double* gains, double* improvement,
+                                                       uint64_t* flips_out, uint64_t max_flips) {
+    __shared__ double sv[32];
+    __shared__ uint32_t si[32];
+    const InstDesc d = A.desc[inst];
+    const uint32_t* rows = A.rows + d.row;
+    const uint32_t* cols = A.cols + d.ent;
+    const double* vals = A.vals + d.ent;
+    const double* lin = A.lin + d.site;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    for (uint32_t v = tid; v < d.n; v += blockDim.x) {
+        double field = lin[v];
+        for (uint32_t e = rows[v]; e < rows[v + 1]; e++) field = __dadd_rn(field, __dmul_rn(vals[e], (double)state[cols[e]]));
+        gains[v] = __dmul_rn(1.0 - 2.0 * (double)state[v], field);
+    }
+    __syncthreads();
+    double total = 0.0;
+    uint64_t flips = 0;
+    for (; flips < max_flips; flips++) {
+        double bv = -1e-12;
+        uint32_t bi = 0xFFFFFFFFu;
+        for (uint32_t v = tid; v < d.n; v += blockDim.x)
+            if (!(clamped && clamped[v]) && gains[v] < bv) {
+                bv = gains[v];
+                bi = v;
+            }
+        for (int o = 16; o; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, bv, o);
+            const uint32_t oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov < bv || (ov == bv && oi < bi)) {
+                bv = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            sv[wid] = bv;
+            si[wid] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int k = 1; k < nw; k++)
+                if (sv[k] < sv[0] || (sv[k] == sv[0] && si[k] < si[0])) {
+                    sv[0] = sv[k];
+                    si[0] = si[k];
+                }
+            const uint32_t i = si[0];
+            if (i != 0xFFFFFFFFu) {
+                const double g = sv[0];
+                total = __dsub_rn(total, g);
+                const double dir = 1.0 - 2.0 * (double)state[i];
+                state[i] = (int8_t)(1 - state[i]);
+                gains[i] = -g;
+                for (uint32_t e = rows[i]; e < rows[i + 1]; e++) {
+                    const uint32_t j = cols[e];
+                    gains[j] = __dadd_rn(gains[j], __dmul_rn(__dmul_rn(1.0 - 2.0 * (double)state[j], vals[e]), dir));
+                }
+            }
+        }
+        __syncthreads();
+        const bool done = si[0] == 0xFFFFFFFFu;
+        __syncthreads();
+        if (done) break;
+    }
+    if (tid == 0) {
+        *improvement = total;
+        *flips_out = flips;
+    }
+}
+
 // update_incumbent (ultimate.rs:397-430): argmin of the tracked energies in
 // (cell, replica) order with strict <, re-scored with the model energy; the
 // incumbent changes only on a strict improvement. Single CTA of 64 threads.
@@ -1617,6 +1740,18 @@ cudaError_t launch_model_energy(const DevArrays& A, uint32_t inst, uint32_t nt, 
 cudaError_t launch_incumbent(const DevArrays& A, uint32_t inst, double offset, double* inc_e, uint64_t* inc_state,
                              uint32_t n_words, cudaStream_t st) {
     incumbent_kernel<<<1, 64, 0, st>>>(A, inst, offset, inc_e, inc_state, n_words);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_best_extract(const DevArrays& A, uint32_t inst, const double* es, uint32_t count, int8_t* state,
+                                double* best, int32_t* found, cudaStream_t st) {
+    best_extract_kernel<<<1, 1024, 0, st>>>(A, inst, es, count, state, best, found);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_one_opt(const DevArrays& A, uint32_t inst, int8_t* state, const uint8_t* clamped, double* gains,
+                           double* improvement, uint64_t* flips, uint64_t max_flips, cudaStream_t st) {
+    one_opt_kernel<<<1, 1024, 0, st>>>(A, inst, state, clamped, gains, improvement, flips, max_flips);
     return cudaGetLastError();
 }
 

@@ -26,6 +26,10 @@ cudaError_t launch_model_energy(const DevArrays& A, uint32_t inst, uint32_t nt, 
                                 cudaStream_t st);
 cudaError_t launch_incumbent(const DevArrays& A, uint32_t inst, double offset, double* inc_e, uint64_t* inc_state,
                              uint32_t n_words, cudaStream_t st);
+cudaError_t launch_best_extract(const DevArrays& A, uint32_t inst, const double* es, uint32_t count, int8_t* state,
+                                double* best, int32_t* found, cudaStream_t st);
+cudaError_t launch_one_opt(const DevArrays& A, uint32_t inst, int8_t* state, const uint8_t* clamped, double* gains,
+                           double* improvement, uint64_t* flips, uint64_t max_flips, cudaStream_t st);
 void set_last_error(const char* msg);
 cudaError_t probe_peaks(int sm_count, double* int_ops_per_s, double* xoshiro_per_s);
 }  // namespace ie

@@ -141,6 +141,16 @@ class Engine:
         _ffi.check(self._L.ie_read_best(self._h, _p(e), _p(s)))
         return float(e[0]), s
 
+    def one_opt(self, state, is_clamped=None) -> float:
+        """local_search.rs:19-57 on the device: polishes ``state`` (int8 0/1)
+        in place; returns the total improvement."""
+        if not (isinstance(state, np.ndarray) and state.dtype == np.int8 and state.flags.c_contiguous):
+            raise TypeError("state must be a contiguous int8 array")
+        c = None if is_clamped is None else np.ascontiguousarray(is_clamped, dtype=np.uint8)
+        imp = np.zeros(1, dtype=np.float64)
+        _ffi.check(self._L.ie_one_opt(self._h, _p(state), None if c is None else _p(c), _p(imp)))
+        return float(imp[0])
+
 
 class BatchEngine:
     """Many single-cell problems (64 replicas each) resident on the device."""

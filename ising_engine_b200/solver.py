@@ -21,7 +21,8 @@ NUM_REPLICAS = 64
 
 def steepest_descent_1opt(model: QuboModel, state, is_clamped=None) -> float:
     """local_search.rs:19-57 (steepest improving flip, lowest index on ties),
-    in the same f64 evaluation order. Polishes ``state`` in place."""
+    in the same f64 evaluation order, on the host. Polishes ``state`` in
+    place. ``UltimateSolver.solve`` runs the device form (``Engine.one_opt``)."""
     n = model.num_vars
     state = np.asarray(state)
     clamped = np.zeros(n, dtype=bool) if is_clamped is None else np.asarray(is_clamped, dtype=bool)
@@ -101,5 +102,5 @@ class UltimateSolver:
             eng.init_random()
             eng.run_pt()
             _, best = eng.best()
-        steepest_descent_1opt(model, best, is_clamped.astype(bool))
+            eng.one_opt(best, is_clamped)
         return best

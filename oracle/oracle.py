@@ -160,13 +160,15 @@ def full_presolve(model, clamped=()):
     return [(int(oi[i]), int(ov[i])) for i in range(k)]
 
 
-def one_opt(model, state, is_clamped=None):
+def one_opt(model, state, is_clamped=None, with_improvement=False):
+    """local_search.rs:19-57 on a copy of state; returns the polished state
+    (and the total improvement when asked)."""
     n, lin, row, col, val = _csr(model)
     st = np.ascontiguousarray(state, dtype=np.int8).copy()
     cl = np.zeros(n, dtype=np.uint8) if is_clamped is None else \
         np.ascontiguousarray(is_clamped, dtype=np.uint8)
-    lib().or_one_opt(n, lin, row, col, val, st, cl)
-    return st
+    imp = lib().or_one_opt(n, lin, row, col, val, st, cl)
+    return (st, imp) if with_improvement else st
 
 
 class RunResult:

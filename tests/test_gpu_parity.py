@@ -177,6 +177,28 @@ def test_lattice_3d_L64_64_temperatures_full_size():
         assert_same_run(eng, ref)
 
 
+@pytest.mark.parametrize("integer", [True, False])
+def test_one_opt_and_best_extraction_on_device(integer):
+    """local_search.rs:19-57 on the device: the polished state and the total
+    improvement equal the oracle's, with and without clamps; the best
+    replica extraction returns a configuration whose model energy is the
+    reported one."""
+    rng = np.random.default_rng(31 if integer else 32)
+    m = I.random_regular_qubo(700, 7, rng, integer=integer)
+    with Engine(m, num_temps=3, seed=9) as eng:
+        for trial in range(3):
+            state = (rng.random(m.num_vars) < 0.5).astype(np.int8)
+            clamped = (rng.random(m.num_vars) < 0.1).astype(np.uint8) if trial else None
+            ref, ref_imp = O.one_opt(m, state, clamped, with_improvement=True)
+            imp = eng.one_opt(state, clamped)
+            assert (state == ref).all()
+            assert imp == ref_imp
+        eng.init_random()
+        eng.step(I.geometric_beta_ladder(3, 0.5, 2.0), 30)
+        e, s = eng.best()
+        assert e == m.calculate_total_energy(s)
+
+
 def test_uneven_batch_bit_exact_and_plain_equal():
     models, seeds = I.uneven_batch(24, seed=7, n_max=600)
     temps = I.sa_temps(60)
