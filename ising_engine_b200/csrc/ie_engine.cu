@@ -929,7 +929,7 @@ struct Engine {
         // Coordinate search: the (n4, n2) pair of one mode over its grid with
         // the other mode's pair held, integer then f64, two passes; each trial
         // is timed on the same state (restored after it).
-        const uint32_t n4s[4] = {512, 768, 1536, 3072}, n2s[2] = {256, 512};
+        const uint32_t n4s[5] = {256, 512, 768, 1536, 3072}, n2s[3] = {128, 256, 512};
         uint32_t bi[4] = {tune_n4[0], tune_n2[0], tune_n4[1], tune_n2[1]};
         auto trial = [&](double& ms) -> ie_status {
             tune_n4[0] = bi[0];
