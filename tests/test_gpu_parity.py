@@ -164,6 +164,25 @@ def test_lattice_3d_cells_in_global_memory():
         assert_same_run(eng, ref)
 
 
+def test_windowed_global_spins_random_graphs():
+    """Single-cell instances beyond shared memory (N = 30000) on the windowed
+    kernel with spins in global memory: random graphs (several sites per
+    window level, neighbours inside the window and the previous one),
+    integer and f64, through the batched entry point."""
+    rng = np.random.default_rng(41)
+    models = [small_weight_regular(30000, 12, rng), I.random_regular_qubo(26000, 7, rng, integer=False)]
+    seeds = np.array([3, 4], dtype=np.uint64)
+    temps = I.sa_temps(12, 0.3, 3.0)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=2)
+    b = BatchEngine(models, seeds)
+    b.init_random()
+    b.run_schedule(temps[:5])
+    b.run_schedule(temps[5:])
+    assert (b.spins() == words_ref).all()
+    assert b.energies().tobytes() == ref_e.tobytes()
+    b.close()
+
+
 def test_lattice_3d_L64_64_temperatures_full_size():
     """The 3D +-J lattice at full size (L=64, N=262144, 64 temperatures, beta
     geometric 0.2..2.0, exchange every 5 sweeps) for 6 steps: spins,
