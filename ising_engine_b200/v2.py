@@ -72,8 +72,20 @@ class ProblemIR:
         return f(self.offset) and f(self.linear) and f(self.weights)
 
     def energy(self, x) -> float:
-        """ir.rs:85-103."""
-        return self.model().calculate_total_energy(np.asarray(x))
+        """ir.rs:85-103: offset, then per set site its linear term and half of
+        the sum of its set neighbours' weights."""
+        x = np.asarray(x)
+        e = self.offset
+        for i in range(self.n):
+            if x[i] == 0:
+                continue
+            e += float(self.linear[i])
+            pair = 0.0
+            for k in range(int(self.row_ptr[i]), int(self.row_ptr[i + 1])):
+                if x[int(self.col_idx[k])] != 0:
+                    pair += float(self.weights[k])
+            e += 0.5 * pair
+        return e
 
     def greedy_coloring(self) -> np.ndarray:
         """ir.rs:114-139, computed by the library."""
