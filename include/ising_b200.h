@@ -143,6 +143,9 @@ typedef struct ie_batch_config {
     uint32_t threads_per_block; /* reserved, 0 */
     uint32_t blocks_per_sm;     /* cap on resident CTAs per SM per class, 0 = as many as fit */
     int32_t disable_windows;    /* nonzero: never use the windowed kernel for large instances */
+    int32_t use_graph;          /* nonzero: ie_batch_run_schedule replays one CUDA graph holding
+                                   the launches of every work class (captured on first use and
+                                   again when the classes or the schedule length change) */
 } ie_batch_config;
 
 /* count problems, each run as one cell of 64 replicas with its own seed. */

@@ -48,7 +48,7 @@ class ie_problem_device(C.Structure):
 class ie_batch_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("force_f64", C.c_int32),
                 ("threads_per_block", C.c_uint32), ("blocks_per_sm", C.c_uint32),
-                ("disable_windows", C.c_int32)]
+                ("disable_windows", C.c_int32), ("use_graph", C.c_int32)]
 
 
 class ie_serve_config(C.Structure):

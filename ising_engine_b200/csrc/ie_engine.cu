@@ -289,30 +289,30 @@ bool window_table(HostInst& h, std::vector<uint32_t>& tab) {
     h.windowed_ok = false;
     h.has_wtab = false;
     tab.clear();
-    if (h.n < 8) return false;
+    if (h.n < (uint32_t)kWin) return false;
     for (uint32_t v = 0; v < h.n; v++)
         if (h.rows[v + 1] - h.rows[v] > kWinMaxDeg) return false;
-    const uint32_t nwin = (h.n + 7) / 8;
-    tab.assign((size_t)nwin * 16, 0);
+    const uint32_t nwin = (h.n + kWin - 1) / kWin;
+    tab.assign((size_t)nwin * kWT, 0);
     double par = 0;
     for (uint32_t w = 0; w < nwin; w++) {
-        uint32_t lvl[8] = {0, 0, 0, 0, 0, 0, 0, 0}, maxl = 0, levels = 0;
-        for (uint32_t k = 0; k < 8; k++) {
-            const uint32_t v = 8 * w + k;
+        uint32_t lvl[kWin] = {}, maxl = 0;
+        uint32_t* e = &tab[(size_t)kWT * w];
+        for (uint32_t k = 0; k < (uint32_t)kWin; k++) {
+            const uint32_t v = kWin * w + k;
             if (v >= h.n) break;
             uint32_t l = 0;
-            for (uint32_t e = h.rows[v]; e < h.rows[v + 1]; e++) {
-                const uint32_t j = h.cols[e];
-                if (j >= 8 * w && j < v) l = std::max(l, lvl[j - 8 * w] + 1);
+            for (uint32_t q = h.rows[v]; q < h.rows[v + 1]; q++) {
+                const uint32_t j = h.cols[q];
+                if (j >= kWin * w && j < v) l = std::max(l, lvl[j - kWin * w] + 1);
             }
             lvl[k] = l;
             maxl = std::max(maxl, l);
-            levels |= l << (4 * k);
-            tab[16 * (size_t)w + k] = (h.recpos[v] / 4) | ((h.reclen[v] / 4) << 24);
+            e[kWin + k / 8] |= l << (4 * (k % 8));
+            e[k] = (h.recpos[v] / 4) | ((h.reclen[v] / 4) << 24);
         }
-        tab[16 * (size_t)w + 8] = levels;
-        tab[16 * (size_t)w + 9] = maxl;
-        par += 8.0 / (maxl + 1);
+        e[kWin + 2] = maxl;
+        par += (double)kWin / (maxl + 1);
     }
     h.has_wtab = true;
     h.windowed_ok = par / nwin >= 2.0;
@@ -368,6 +368,9 @@ struct Engine {
 
     ~Engine() {
         if (device >= 0) cudaSetDevice(device);
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        if (evfork) cudaEventDestroy(evfork);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (ev2) cudaEventDestroy(ev2);
@@ -376,6 +379,7 @@ struct Engine {
         for (cudaStream_t st : cstreams) cudaStreamDestroy(st);
         for (cudaEvent_t ev : cevents) cudaEventDestroy(ev);
         for (cudaEvent_t ev : cstart) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : cjoin) cudaEventDestroy(ev);
     }
 
     DevArrays arrays() const {
@@ -551,7 +555,7 @@ struct Engine {
             build_window_table(i, wt);
         }
         recs.resize(recs.size() + kChunk, 0);
-        if (wt.empty()) wt.assign(16, 0);
+        if (wt.empty()) wt.assign(kWT, 0);
         IE_TRY(d_recs.upload(recs, stream));
         IE_TRY(d_wtab.upload(wt, stream));
         quads_built = false;
@@ -595,19 +599,21 @@ struct Engine {
     };
     std::vector<std::unique_ptr<WorkClass>> classes;
     std::vector<cudaStream_t> cstreams;
-    std::vector<cudaEvent_t> cevents, cstart;
+    std::vector<cudaEvent_t> cevents, cstart, cjoin;
     std::vector<double> class_ms;  // device time of each class launch in the last run
 
     ie_status ensure_class_streams(size_t k) {
         while (cstreams.size() < k) {
             cudaStream_t st;
-            cudaEvent_t ev, ev0;
+            cudaEvent_t ev, ev0, ej;
             IE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
             IE_CUDA(cudaEventCreate(&ev));
             IE_CUDA(cudaEventCreate(&ev0));
+            IE_CUDA(cudaEventCreateWithFlags(&ej, cudaEventDisableTiming));
             cstreams.push_back(st);
             cevents.push_back(ev);
             cstart.push_back(ev0);
+            cjoin.push_back(ej);
         }
         return IE_OK;
     }
@@ -625,6 +631,17 @@ struct Engine {
     static uint32_t class_cap(const InstDesc& d) { return cap_of(d.n) > kSmemSpinCap ? 0u : cap_of(d.n); }
     bool use_windows = true;
     std::vector<uint8_t> active;  // instances in the work classes (empty: all)
+
+    // CUDA graph of one batched run (use_graph): valid for the classes it was
+    // captured with and for runs of g_steps steps; the step base is read from
+    // d_stepbase so replays continue the trajectory.
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t evfork = nullptr;
+    bool graph_valid = false;
+    uint64_t g_steps = 0;
+    DevBuf<uint64_t> d_stepbase;
 
     // PT cells as work items: 0 chooses by size, 1 runs one CTA per instance
     // (pt_kernel), 2 runs every cell as its own work item of the batched /
@@ -652,6 +669,7 @@ struct Engine {
         const uint32_t N = (uint32_t)D.size();
         classes.clear();
         cells_built = false;
+        graph_valid = false;
         std::vector<std::tuple<uint32_t, int, uint32_t>> keys;
         auto live = [&](uint32_t i) { return Dp || active.empty() || active[i] != 0; };
         for (uint32_t i = 0; i < N; i++) {
@@ -836,40 +854,102 @@ struct Engine {
         for (double x : t)
             if (!(x > 0.0) || !std::isfinite(x)) return fail(IE_ERR_INVALID, "temperatures must be positive");
         IE_TRY(d_temps.upload(t, stream));
-        IE_TRY(launch_classes(sa_args(steps)));
+        RunArgs R = sa_args(steps);
+        if (use_graph) {
+            IE_TRY(d_stepbase.alloc(1));
+            IE_CUDA(cudaMemcpyAsync(d_stepbase.p, &steps_done, sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
+            R.step_base_dev = d_stepbase.p;
+            IE_TRY(launch_classes(R, arrays(), true));
+        } else {
+            IE_TRY(launch_classes(R));
+        }
         steps_done += steps;
         return IE_OK;
     }
 
     // One persistent launch per work class, all in flight together on their
     // own streams, largest classes first (their CTAs are dispatched first and
-    // the smaller classes fill the remaining room); waits for all of them.
-    ie_status launch_classes(const RunArgs& base) { return launch_classes(base, arrays()); }
-    ie_status launch_classes(const RunArgs& base, const DevArrays& A) {
-        IE_TRY(ensure_class_streams(classes.size()));
-        IE_CUDA(cudaMemsetAsync(d_queue.p, 0, classes.size() * sizeof(uint32_t), stream));
-        IE_CUDA(cudaEventRecord(ev0, stream));
-        uint64_t launches = 0;
+    // the smaller classes fill the remaining room), forked from and joined
+    // back into the engine's stream. Only stream operations, so the sequence
+    // can be captured into a CUDA graph; grids are computed beforehand.
+    ie_status class_grids(const RunArgs& base, std::vector<int>& grids) {
+        grids.assign(classes.size(), 0);
         for (size_t k = 0; k < classes.size(); k++) {
             WorkClass& wc = *classes[k];
             if (!wc.nitems) continue;
-            IE_CUDA(cudaStreamWaitEvent(cstreams[k], ev0, 0));
             int occ = wc.tpl == 8 ? window_occupancy(wc.mode, wc.cap)
                                   : batch_occupancy(wc.mode, wc.tpl, wc.cap, base.serve != 0 || base.cells != 0);
             if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
             if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
-            const int grid = std::max(1, std::min<int>((int)wc.nitems, occ * g_sm_count));
+            grids[k] = std::max(1, std::min<int>((int)wc.nitems, occ * g_sm_count));
+        }
+        return IE_OK;
+    }
+
+    // capturing: the timing events become event-record nodes of the graph
+    // (cudaEventRecordExternal); the joins use their own events.
+    ie_status enqueue_classes(const RunArgs& base, const DevArrays& A, const std::vector<int>& grids,
+                              uint64_t& launches, bool capturing = false) {
+        const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+        launches = 0;
+        IE_CUDA(cudaMemsetAsync(d_queue.p, 0, classes.size() * sizeof(uint32_t), stream));
+        IE_CUDA(cudaEventRecord(evfork, stream));
+        for (size_t k = 0; k < classes.size(); k++) {
+            WorkClass& wc = *classes[k];
+            if (!wc.nitems) continue;
+            IE_CUDA(cudaStreamWaitEvent(cstreams[k], evfork, 0));
             RunArgs R = base;
             R.quads = wc.items.p;
             R.quad_h = wc.itemh.p;
             R.nquads = wc.nitems;
             R.queue = d_queue.p + k;
-            IE_CUDA(cudaEventRecord(cstart[k], cstreams[k]));
-            if (wc.tpl == 8) IE_CUDA(launch_window(A, R, wc.mode, wc.cap, grid, cstreams[k]));
-            else IE_CUDA(launch_batch(A, R, wc.mode, wc.tpl, wc.cap, grid, cstreams[k]));
-            IE_CUDA(cudaEventRecord(cevents[k], cstreams[k]));
-            IE_CUDA(cudaStreamWaitEvent(stream, cevents[k], 0));
+            IE_CUDA(cudaEventRecordWithFlags(cstart[k], cstreams[k], rec));
+            if (wc.tpl == 8) IE_CUDA(launch_window(A, R, wc.mode, wc.cap, grids[k], cstreams[k]));
+            else IE_CUDA(launch_batch(A, R, wc.mode, wc.tpl, wc.cap, grids[k], cstreams[k]));
+            IE_CUDA(cudaEventRecordWithFlags(cevents[k], cstreams[k], rec));
+            IE_CUDA(cudaEventRecord(cjoin[k], cstreams[k]));
+            IE_CUDA(cudaStreamWaitEvent(stream, cjoin[k], 0));
             launches++;
+        }
+        return IE_OK;
+    }
+
+    // Runs the class launches (directly, or by replaying the captured graph)
+    // and waits for them; records the device time of the run and of each class.
+    ie_status launch_classes(const RunArgs& base) { return launch_classes(base, arrays()); }
+    ie_status launch_classes(const RunArgs& base, const DevArrays& A, bool graphed = false) {
+        IE_TRY(ensure_class_streams(classes.size()));
+        if (!evfork) IE_CUDA(cudaEventCreateWithFlags(&evfork, cudaEventDisableTiming));
+        std::vector<int> grids;
+        IE_TRY(class_grids(base, grids));
+        uint64_t launches = 0;
+        if (graphed) {
+            if (!graph_valid || g_steps != base.steps) {
+                if (gexec) IE_CUDA(cudaGraphExecDestroy(gexec));
+                if (graph) IE_CUDA(cudaGraphDestroy(graph));
+                gexec = nullptr;
+                graph = nullptr;
+                IE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                uint64_t n = 0;
+                const ie_status st = enqueue_classes(base, A, grids, n, true);
+                cudaGraph_t g = nullptr;
+                const cudaError_t ce = cudaStreamEndCapture(stream, &g);
+                if (st != IE_OK) {
+                    if (g) cudaGraphDestroy(g);
+                    return st;
+                }
+                IE_CUDA(ce);
+                graph = g;
+                IE_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+                graph_valid = true;
+                g_steps = base.steps;
+            }
+            IE_CUDA(cudaEventRecord(ev0, stream));
+            IE_CUDA(cudaGraphLaunch(gexec, stream));
+            for (size_t k = 0; k < classes.size(); k++) launches += classes[k]->nitems ? 1 : 0;
+        } else {
+            IE_CUDA(cudaEventRecord(ev0, stream));
+            IE_TRY(enqueue_classes(base, A, grids, launches));
         }
         IE_CUDA(cudaEventRecord(ev1, stream));
         IE_CUDA(cudaEventSynchronize(ev1));
@@ -1247,7 +1327,7 @@ struct ServeEngine {
     uint32_t n_active = 0;
 
     uint64_t rec_cap() const { return 8 * cfg.max_sites + 4 * cfg.max_couplings + kChunk; }
-    uint64_t win_cap() const { return 2 * cfg.max_sites + 16 * (uint64_t)cfg.max_requests; }
+    uint64_t win_cap() const { return (uint64_t)kWT * ((cfg.max_sites + kWin - 1) / kWin + cfg.max_requests); }
 
     ie_status create(const ie_serve_config* c) {
         if (c) cfg = *c;
@@ -1816,6 +1896,7 @@ ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint
     b->eng.threads_per_block = cfg.threads_per_block;
     b->eng.blocks_per_sm = cfg.blocks_per_sm;
     b->eng.use_windows = cfg.disable_windows == 0;
+    b->eng.use_graph = cfg.use_graph != 0;
     if (cfg.threads_per_block && (cfg.threads_per_block % 32 || cfg.threads_per_block > 256))
         return fail(IE_ERR_INVALID, "threads_per_block must be a multiple of 32, at most 256");
     IE_TRY(b->eng.build(problems, count, 1, seeds, cfg.force_f64 != 0));

@@ -208,7 +208,7 @@ __device__ __forceinline__ StepPlan step_plan(const DevArrays& A, const RunArgs&
         P.tstride = 1;
         P.temps = R.temps + d.sched + P.base;
     } else {
-        P.base = R.step_base;
+        P.base = R.step_base_dev ? *R.step_base_dev : R.step_base;
         P.steps = R.steps;
         P.tstride = R.temps_per_step ? (R.cells ? R.ladder : 1u) : 0u;
         P.temps = R.temps + (R.cells ? d.cell : 0u);
@@ -626,30 +626,27 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
 //     accumulated in site order, the reference's f64 summation order.
 // The next window's site records stream into a shared double buffer with
 // cp.async while the current window is processed.
-// Window table entry (16 words): word i (< 8) = record position | length << 24
-// of site i (16-byte units within the instance's record stream), word 8 = level
-// of site i in nibble i, word 9 = largest level.
+// Window table layout: kWin / kWT in ie_kernels.cuh.
 // ---------------------------------------------------------------------------
-constexpr int kWin = 8;
-constexpr uint32_t kWinRecWords = 8 * (4 + 3 * kWinMaxDeg);  // eight f64 records of degree <= 32
+constexpr uint32_t kWinRecWords = kWin * (4 + 3 * kWinMaxDeg);  // kWin f64 records of degree <= 32
 constexpr uint32_t kWinBufs = 3;  // record buffers: window w in use, w+1 landed, w+2 in flight
 
 
 // Copies the records of one window (positions from its table entry) into buf.
 __device__ __forceinline__ void window_fetch(const uint32_t* ent, const uint32_t* stream, uint32_t* buf, int tid,
                                              int nthreads) {
-    uint32_t pos[8], off[9];
+    uint32_t pos[kWin], off[kWin + 1];
     off[0] = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < kWin; i++) {
         const uint32_t e = ent[i];
         pos[i] = e & 0xFFFFFFu;
         off[i + 1] = off[i] + (e >> 24);
     }
-    for (uint32_t j = tid; j < off[8]; j += nthreads) {
+    for (uint32_t j = tid; j < off[kWin]; j += nthreads) {
         uint32_t src = 0;
 #pragma unroll
-        for (int i = 0; i < 8; i++)
+        for (int i = 0; i < kWin; i++)
             if (j >= off[i] && j < off[i + 1]) src = pos[i] + (j - off[i]);
         cp_async16(buf + 4 * j, stream + 4 * (size_t)src);
     }
@@ -667,15 +664,16 @@ __device__ __forceinline__ void bar_sync(int id, int count) { asm volatile("bar.
 __device__ __forceinline__ void bar_arrive(int id, int count) { asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
 
 __host__ __device__ constexpr size_t ws_smem_bytes(uint32_t spin_cap) {
-    // tab 2 KB | spread table 4 KB | outputs 2 x 64 rows | dE 64 rows | records 3 x 3200 B | spins
-    return 2048 + 4096 + 2 * 64 * kRS * 8 + 64 * kRS * 8 + kWinBufs * kWinRecWords * 4 + (size_t)spin_cap * 8;
+    // tab 2 KB | spread table 4 KB | outputs 2 x 8 kWin rows | dE 8 kWin rows | records | spins
+    return 2048 + 4096 + 2 * (8 * kWin) * kRS * 8 + (8 * kWin) * kRS * 8 + kWinBufs * kWinRecWords * 4 +
+           (size_t)spin_cap * 8;
 }
 
 template <uint32_t MODE>
 struct WsCfg {
-    static constexpr int NC = MODE == kModeInt ? 2 : 4;   // decider warps
-    static constexpr int THREADS = 32 * (1 + NC);
     static constexpr int SPLIT = MODE == kModeInt ? 1 : 2;  // decider threads per (site, lane) task
+    static constexpr int NC = kWin * 8 * SPLIT / 32;        // decider warps: one thread per task share
+    static constexpr int THREADS = 32 * (1 + NC);
     static constexpr int KPT = 8 / SPLIT;                  // calls decided per thread
 };
 
@@ -804,14 +802,14 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
     __shared__ uint32_t s_item;
     uint64_t* tab = dsm;
     uint2* lut = reinterpret_cast<uint2*>(dsm + 256);
-    uint64_t* rngb = dsm + 768;                            // 2 x 64 rows of kRS
-    uint64_t* deb = rngb + 2 * 64 * kRS;                   // 64 rows of kRS
-    uint32_t* recb = reinterpret_cast<uint32_t*>(deb + 64 * kRS);
+    uint64_t* rngb = dsm + 768;                            // 2 x 8 kWin rows of kRS
+    uint64_t* deb = rngb + 2 * (8 * kWin) * kRS;           // 8 kWin rows of kRS
+    uint32_t* recb = reinterpret_cast<uint32_t*>(deb + (8 * kWin) * kRS);
     uint64_t* const ssw = reinterpret_cast<uint64_t*>(recb + kWinBufs * kWinRecWords);
     const int tid = threadIdx.x;
     const bool producer = tid < 32;
     const int c = tid - 32;  // decider index
-    // decider task: site ti (0..7), lane tl, half th
+    // decider task: site ti (0 .. kWin - 1), lane tl, half th
     const int ti = producer ? 0 : c / (8 * SPLIT);
     const int tl = producer ? 0 : (c / SPLIT) & 7;
     const int th = producer ? 0 : c % SPLIT;
@@ -876,7 +874,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
                 for (uint32_t w = 0; w < nwin; w++) {
                     const int b = w & 1;
                     if (w >= 2) bar_sync(kBarEmpty0 + b, NT);
-                    uint64_t* ob = rngb + b * 64 * kRS;
+                    uint64_t* ob = rngb + b * (8 * kWin) * kRS;
 #pragma unroll
                     for (int i = 0; i < kWin; i++) {
 #pragma unroll
@@ -892,15 +890,15 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
                 // records of window w + 2 are fetched while window w runs
                 window_fetch(wt, stream, recb, c, 32 * NC);
                 cp_async_commit();
-                if (nwin > 1) window_fetch(wt + 16, stream, recb + kWinRecWords, c, 32 * NC);
+                if (nwin > 1) window_fetch(wt + kWT, stream, recb + kWinRecWords, c, 32 * NC);
                 cp_async_commit();
                 for (uint32_t w = 0; w < nwin; w++) {
                     const int b = w & 1;
-                    uint32_t cur[10];
+                    uint32_t cur[kWin + 3];
 #pragma unroll
-                    for (int i = 0; i < 10; i++) cur[i] = wt[16 * (size_t)w + i];
+                    for (int i = 0; i < kWin + 3; i++) cur[i] = wt[kWT * (size_t)w + i];
                     if (w + 2 < nwin)
-                        window_fetch(wt + 16 * (size_t)(w + 2), stream, recb + ((w + 2) % kWinBufs) * kWinRecWords, c,
+                        window_fetch(wt + kWT * (size_t)(w + 2), stream, recb + ((w + 2) % kWinBufs) * kWinRecWords, c,
                                      32 * NC);
                     cp_async_commit();
                     cp_async_wait1();
@@ -908,13 +906,13 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
                     const uint32_t* rb = recb + (w % kWinBufs) * kWinRecWords;
                     uint32_t off = 0;
 #pragma unroll
-                    for (int i = 0; i < 8; i++)
+                    for (int i = 0; i < kWin; i++)
                         if (i < ti) off += cur[i] >> 24;
                     const uint32_t v = w * kWin + ti;
-                    const uint32_t lev = (cur[8] >> (4 * ti)) & 15u;
-                    const uint64_t* rp = rngb + b * 64 * kRS + (ti * 8 + tl) * kRS;
+                    const uint32_t lev = ((ti < 8 ? cur[kWin] : cur[kWin + 1]) >> (4 * (ti % 8))) & 15u;
+                    const uint64_t* rp = rngb + b * (8 * kWin) * kRS + (ti * 8 + tl) * kRS;
                     uint64_t* drow = deb + (ti * 8 + tl) * kRS;
-                    for (uint32_t L = 0; L <= cur[9]; L++) {
+                    for (uint32_t L = 0; L <= cur[kWin + 2]; L++) {
                         if (v < d.n && lev == L) {
                             // the SPLIT threads of a task read the byte before any of
                             // them writes (the shuffles order them), then all write
@@ -1629,11 +1627,17 @@ cudaError_t set_smem_limits(size_t pt_bytes) {
     return cudaFuncSetAttribute(pt_kernel<kModeF64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pt_bytes);
 }
 
+// The dynamic shared-memory limit of the batched and windowed kernels is set
+// to the per-CTA maximum, so occupancy queries for one class never lower the
+// limit below another class's launch of the same kernel.
+constexpr int kMaxDynSmem = 226 * 1024;  // 227 KB per CTA less room for static shared memory
+
 template <uint32_t MODE, int TPL>
 static int occ_of(size_t smem) {
     int n = 0;
-    if (cudaFuncSetAttribute(batch_kernel<MODE, TPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    if (smem > (size_t)kMaxDynSmem ||
+        cudaFuncSetAttribute(batch_kernel<MODE, TPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem) !=
+            cudaSuccess)
         return 0;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<MODE, TPL>, 32, smem) == cudaSuccess ? n : 0;
 }
@@ -1665,8 +1669,9 @@ cudaError_t launch_batch(const DevArrays& A, const RunArgs& R, uint32_t mode, in
 template <uint32_t MODE, bool GSP>
 static int occ_win(size_t smem) {
     int n = 0;
-    if (cudaFuncSetAttribute(window_kernel<MODE, GSP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    if (smem > (size_t)kMaxDynSmem ||
+        cudaFuncSetAttribute(window_kernel<MODE, GSP>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem) !=
+            cudaSuccess)
         return 0;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, window_kernel<MODE, GSP>, WsCfg<MODE>::THREADS, smem) ==
                    cudaSuccess

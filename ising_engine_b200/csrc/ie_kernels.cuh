@@ -51,6 +51,13 @@ constexpr uint32_t kRecCont = 1u << 14;
 constexpr uint32_t kRecClamp = 1u << 15;
 constexpr uint32_t kRecMaxDeg = 16;
 constexpr uint32_t kWinMaxDeg = 32;  // windowed kernel: one record of up to 32 couplings per site
+// Windowed kernel: windows of kWin consecutive sites; window table entry of
+// kWT words: word i < kWin = record position | length << 24 of site i (16-byte
+// units in the instance's windowed record stream), words kWin, kWin + 1 = level
+// of site i in nibble i % 8 of word kWin + i / 8, word kWin + 2 = largest level.
+// kWin may be 8 or 16 (levels fit the nibbles; kWT >= kWin + 3).
+constexpr int kWin = 8;
+constexpr int kWT = 16;
 
 struct DevArrays {
     const InstDesc* desc;
@@ -106,6 +113,9 @@ struct RunArgs {
     // DEO phase and f64 resync to the exchange step (exchange_kernel)
     uint32_t cells;
     uint32_t ladder;
+    // when set, the launch's step_base is read from device memory (so a
+    // captured CUDA graph of the launch stays valid across runs)
+    const uint64_t* step_base_dev;
 };
 
 }  // namespace ie

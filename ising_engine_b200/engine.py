@@ -156,7 +156,8 @@ class BatchEngine:
     """Many single-cell problems (64 replicas each) resident on the device."""
 
     def __init__(self, models, seeds, device: int = 0, force_f64: bool = False,
-                 threads_per_block: int = 0, blocks_per_sm: int = 0, windows: bool = True):
+                 threads_per_block: int = 0, blocks_per_sm: int = 0, windows: bool = True,
+                 graph: bool = False):
         self._L = _ffi.lib()
         self.models = list(models)
         self.count = len(self.models)
@@ -166,7 +167,7 @@ class BatchEngine:
         if self.seeds.shape != (self.count,):
             raise ValueError("one seed per problem")
         cfg = _ffi.ie_batch_config(device, int(force_f64), threads_per_block, blocks_per_sm,
-                                   0 if windows else 1)
+                                   0 if windows else 1, 1 if graph else 0)
         h = C.c_void_p()
         _ffi.check(self._L.ie_batch_create(probs, self.count, _p(self.seeds), C.byref(cfg),
                                            C.byref(h)))

@@ -387,6 +387,28 @@ def test_windowed_kernel_degree_17_to_32():
     b.close()
 
 
+def test_batched_runs_replayed_from_cuda_graph():
+    """use_graph: the class launches are captured once and replayed; the step
+    base comes from device memory, so replays continue the trajectory (the
+    f64 resync at step 1000 falls inside the second replay), and a run of a
+    different length is captured again."""
+    rng = np.random.default_rng(52)
+    models = [I.random_regular_qubo(1800, 9, rng, integer=False), I.random_regular_qubo(900, 6, rng, integer=True),
+              I.random_regular_qubo(300, 4, rng, integer=False), I.random_regular_qubo(120, 5, rng, integer=True)]
+    seeds = np.arange(len(models), dtype=np.uint64) + 61
+    temps = I.sa_temps(1250, 0.2, 3.0)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
+    b = BatchEngine(models, seeds, graph=True)
+    b.init_random()
+    b.run_schedule(temps[:600])
+    b.run_schedule(temps[600:1200])
+    b.run_schedule(temps[1200:])
+    assert (b.spins() == words_ref).all()
+    assert b.energies().tobytes() == ref_e.tobytes()
+    assert len(b.class_report()) >= 2 and all(c[4] > 0 for c in b.class_report())
+    b.close()
+
+
 def test_windowed_kernel_f64_resync():
     rng = np.random.default_rng(78)
     m = I.random_regular_qubo(800, 9, rng, integer=False)
