@@ -65,35 +65,50 @@ __device__ __forceinline__ uint64_t splitmix_at(uint64_t seed, uint64_t i) {
 
 __device__ __forceinline__ uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
 
+// Xoshiro256++ on 32-bit halves (lo, hi) of s0..s3. One step of the state
+// (engine.rs:113-121) is s1' = s1^s2^s0, s0' = s0^s3^s1, s2' = s2^s0^(s1<<17),
+// s3' = rotl(s3^s1, 45): one 3-input XOR per half for s0, s1, s2 and a funnel
+// shift pair for s3, so the step's dependency depth is two instructions.
 struct Xoshiro {
-    uint64_t s0, s1, s2, s3;
+    uint32_t a0, a1, b0, b1, c0, c1, d0, d1;  // s0, s1, s2, s3 as (lo, hi)
+    __device__ __forceinline__ static uint32_t xor3(uint32_t x, uint32_t y, uint32_t z) {
+        uint32_t r;
+        asm("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(r) : "r"(x), "r"(y), "r"(z));
+        return r;
+    }
+    __device__ __forceinline__ void set(int i, uint64_t v) {
+        const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+        if (i == 0) { a0 = lo; a1 = hi; }
+        else if (i == 1) { b0 = lo; b1 = hi; }
+        else if (i == 2) { c0 = lo; c1 = hi; }
+        else { d0 = lo; d1 = hi; }
+    }
     __device__ __forceinline__ void seed_lane(uint64_t cell_seed, int lane) {
-        s0 = splitmix_at(cell_seed, 4 * lane + 0);
-        s1 = splitmix_at(cell_seed, 4 * lane + 1);
-        s2 = splitmix_at(cell_seed, 4 * lane + 2);
-        s3 = splitmix_at(cell_seed, 4 * lane + 3);
+#pragma unroll
+        for (int i = 0; i < 4; i++) set(i, splitmix_at(cell_seed, 4 * lane + i));
+    }
+    __device__ __forceinline__ void advance() {
+        const uint32_t t0 = b0 << 17, t1 = __funnelshift_l(b0, b1, 17);
+        const uint32_t x0 = d0 ^ b0, x1 = d1 ^ b1;
+        const uint32_t nb0 = xor3(b0, c0, a0), nb1 = xor3(b1, c1, a1);
+        const uint32_t na0 = xor3(a0, d0, b0), na1 = xor3(a1, d1, b1);
+        const uint32_t nc0 = xor3(c0, a0, t0), nc1 = xor3(c1, a1, t1);
+        d1 = __funnelshift_l(x1, x0, 13);  // rotl by 45 = halves swapped, then rotl by 13
+        d0 = __funnelshift_l(x0, x1, 13);
+        a0 = na0;
+        a1 = na1;
+        b0 = nb0;
+        b1 = nb1;
+        c0 = nc0;
+        c1 = nc1;
     }
     // Raw 64-bit output of engine.rs:110-112; the reference's uniform is
     // (result >> 12) * 2^-52 exactly.
     __device__ __forceinline__ uint64_t next() {
+        const uint64_t s0 = ((uint64_t)a1 << 32) | a0, s3 = ((uint64_t)d1 << 32) | d0;
         const uint64_t result = rotl64(s0 + s3, 23) + s0;
-        const uint64_t t = s1 << 17;
-        s2 ^= s0;
-        s3 ^= s1;
-        s1 ^= s2;
-        s0 ^= s3;
-        s2 ^= t;
-        s3 = rotl64(s3, 45);
+        advance();
         return result;
-    }
-    __device__ __forceinline__ void advance() {
-        const uint64_t t = s1 << 17;
-        s2 ^= s0;
-        s3 ^= s1;
-        s1 ^= s2;
-        s0 ^= s3;
-        s2 ^= t;
-        s3 = rotl64(s3, 45);
     }
 };
 
