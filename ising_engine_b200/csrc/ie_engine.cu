@@ -618,13 +618,19 @@ struct Engine {
         return IE_OK;
     }
 
-    // TPL 8 marks the windowed kernel (one CTA per instance); -1: no form can
-    // run the instance (spins beyond shared memory and no window table).
+    // Kernel form of an instance: 1, 2, 4 threads per lane (batch_kernel), 8:
+    // the windowed kernel, 16: the chain kernel (one CTA per instance). Large
+    // instances whose windows are parallel take the windowed kernel, other
+    // instances above the small-instance threshold the chain kernel; spins
+    // beyond shared memory stay in global memory in either.
     static constexpr uint32_t kSmemSpinCap = 24576;
+    static constexpr int kChain = 16;
     int tpl_of(const InstDesc& d, const HostInst& h) const {
         const uint32_t n = d.n, m = d.mode;
-        if (cap_of(n) > kSmemSpinCap) return h.has_wtab ? 8 : -1;
-        if (n > tune_n4[m]) return h.windowed_ok && use_windows ? 8 : 4;
+        if (cap_of(n) > kSmemSpinCap) return h.windowed_ok && use_windows ? 8 : kChain;
+        if (!use_windows) return n > tune_n4[m] ? 4 : (n > tune_n2[m] ? 2 : 1);
+        if (n > tune_n4[m]) return h.windowed_ok ? 8 : kChain;
+        if (!h.windowed_ok && n > tune_n2[m]) return kChain;
         return n > tune_n2[m] ? 2 : 1;
     }
     // shared-memory spin capacity of the instance's class; 0: spins in global memory
@@ -674,9 +680,6 @@ struct Engine {
         auto live = [&](uint32_t i) { return Dp || active.empty() || active[i] != 0; };
         for (uint32_t i = 0; i < N; i++) {
             if (!live(i)) continue;
-            if (tpl_of(D[i], HI[i]) < 0)
-                return fail(IE_ERR_UNSUPPORTED, "instance too large for shared memory and not eligible for the "
-                                                "global-memory windowed kernel (a site has more than 32 couplings)");
             auto k = std::make_tuple(D[i].mode, tpl_of(D[i], HI[i]), class_cap(D[i]));
             if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
         }
@@ -688,7 +691,7 @@ struct Engine {
             wc->mode = std::get<0>(k);
             wc->tpl = std::get<1>(k);
             wc->cap = std::get<2>(k);
-            const int ng = wc->tpl == 8 ? 1 : 4 / wc->tpl;
+            const int ng = wc->tpl >= 8 ? 1 : 4 / wc->tpl;
             std::vector<uint32_t> order;
             for (uint32_t i = 0; i < N; i++)
                 if (live(i) && D[i].mode == wc->mode && tpl_of(D[i], HI[i]) == wc->tpl && class_cap(D[i]) == wc->cap)
@@ -706,7 +709,7 @@ struct Engine {
             }
             auto work = [&](const std::vector<uint32_t>& q) {
                 double w = 0;
-                for (uint32_t i : q) w = std::max(w, inst_work(HI[i]) / (wc->tpl == 8 ? 5 : wc->tpl));
+                for (uint32_t i : q) w = std::max(w, inst_work(HI[i]) / (wc->tpl == 8 ? 5 : wc->tpl == kChain ? 6 : wc->tpl));
                 return w;
             };
             std::stable_sort(items.begin(), items.end(), [&](const std::vector<uint32_t>& a,
@@ -877,8 +880,9 @@ struct Engine {
         for (size_t k = 0; k < classes.size(); k++) {
             WorkClass& wc = *classes[k];
             if (!wc.nitems) continue;
-            int occ = wc.tpl == 8 ? window_occupancy(wc.mode, wc.cap)
-                                  : batch_occupancy(wc.mode, wc.tpl, wc.cap, base.serve != 0 || base.cells != 0);
+            int occ = wc.tpl == 8       ? window_occupancy(wc.mode, wc.cap)
+                      : wc.tpl == kChain ? chain_occupancy(wc.mode, wc.cap)
+                                         : batch_occupancy(wc.mode, wc.tpl, wc.cap, base.serve != 0 || base.cells != 0);
             if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
             if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
             grids[k] = std::max(1, std::min<int>((int)wc.nitems, occ * g_sm_count));
@@ -905,6 +909,7 @@ struct Engine {
             R.queue = d_queue.p + k;
             IE_CUDA(cudaEventRecordWithFlags(cstart[k], cstreams[k], rec));
             if (wc.tpl == 8) IE_CUDA(launch_window(A, R, wc.mode, wc.cap, grids[k], cstreams[k]));
+            else if (wc.tpl == kChain) IE_CUDA(launch_chain(A, R, wc.mode, wc.cap, grids[k], cstreams[k]));
             else IE_CUDA(launch_batch(A, R, wc.mode, wc.tpl, wc.cap, grids[k], cstreams[k]));
             IE_CUDA(cudaEventRecordWithFlags(cevents[k], cstreams[k], rec));
             IE_CUDA(cudaEventRecord(cjoin[k], cstreams[k]));
@@ -1420,8 +1425,6 @@ struct ServeEngine {
         if (n + 1 > a_row.cap || n > a_site.cap || r.h.nnz > a_ent.cap || r.recs.size() > a_rec.cap ||
             r.wtab.size() > a_win.cap || n_steps > a_sched.cap)
             return fail(IE_ERR_OOM, "request exceeds the serving engine's capacity");
-        if (Engine::cap_of(n) > Engine::kSmemSpinCap && !r.h.has_wtab)
-            return fail(IE_ERR_UNSUPPORTED, "num_vars too large for shared memory and a site has more than 32 couplings");
         return IE_OK;
     }
 

@@ -310,15 +310,54 @@ __device__ __forceinline__ uint32_t lane_add(uint32_t v, unsigned gmask) {
     return v;
 }
 
+// Hand-over between a generator warp and decider warps: two output buffers of
+// one window of kWin sites each (row (site, lane) holds the lane's 8 calls),
+// guarded by named barriers: bar.arrive by the producing side, bar.sync by the
+// waiting side, with the exact thread count of the two sides.
+constexpr int kRS = 10;  // u64 per (site, lane) row of the output / dE buffers (8 calls + padding against bank conflicts)
+constexpr int kBarFull0 = 1, kBarEmpty0 = 3, kBarCons = 5;
+
+__device__ __forceinline__ void bar_sync(int id, int count) { asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
+__device__ __forceinline__ void bar_arrive(int id, int count) { asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
+
+// Generator of the windowed and chain kernels: thread (lane rl = t / 4, offset
+// rh = t % 4) runs lane rl's Xoshiro chain (engine.rs:87-123) over the sweep
+// and stores the calls it owns (rh, rh + 4) of every site into the window's
+// buffer; nthreads is the barrier count of the whole hand-over.
+__device__ __forceinline__ void produce_windows(uint64_t base, uint32_t n, uint64_t* rngb, int t, int nthreads) {
+    const int rl = t >> 2, rh = t & 3;
+    Xoshiro x;
+    x.seed_lane(base, rl);
+    for (int i = 0; i < rh; i++) x.advance();
+    const uint32_t nwin = (n + kWin - 1) / kWin;
+    for (uint32_t w = 0; w < nwin; w++) {
+        const int b = w & 1;
+        if (w >= 2) bar_sync(kBarEmpty0 + b, nthreads);
+        uint64_t* ob = rngb + b * (8 * kWin) * kRS;
+#pragma unroll
+        for (int i = 0; i < kWin; i++) {
+#pragma unroll
+            for (int kk = 0; kk < 8; kk++) {
+                if (kk % 4 == 0) ob[(i * 8 + rl) * kRS + rh + kk] = x.next();
+                else x.advance();
+            }
+        }
+        bar_arrive(kBarFull0 + b, nthreads);
+    }
+    for (uint32_t w = nwin >= 2 ? nwin - 2 : 0; w < nwin; w++) bar_sync(kBarEmpty0 + (w & 1), nthreads);
+}
+
 template <uint32_t MODE, int TPL>
 using ETypeT = typename std::conditional<MODE == kModeInt, int32_t, double>::type;
 
-template <uint32_t MODE, int TPL>
+// PROD: the uniforms come from a generator warp through rngb (produce_windows;
+// barrier count 64), window by window, instead of the thread's own generator.
+template <uint32_t MODE, int TPL, bool PROD = false>
 __device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc& d, uint32_t* ring, uint8_t* sp,
                                              const uint2* __restrict__ lut, int lane, int h, unsigned gmask,
                                              const uint64_t* __restrict__ tab,
                                              int H, double beta, uint64_t cell_seed,
-                                             ETypeT<MODE, TPL> (&E)[8 / TPL]) {
+                                             ETypeT<MODE, TPL> (&E)[8 / TPL], const uint64_t* rngb = nullptr) {
     constexpr int G = 8 * TPL;
     constexpr int KP = 8 / TPL;    // calls owned by this thread: k = j*TPL + h
     constexpr int EP = 16 / TPL;   // integer mode: record entries summed by this thread
@@ -326,8 +365,10 @@ __device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc&
     // Thread h of a lane runs the lane's generator h steps ahead, so the calls
     // it owns (k = j*TPL + h) fall on its local steps j*TPL.
     Xoshiro x;
-    x.seed_lane(cell_seed, lane);
-    for (int i = 0; i < h; i++) x.advance();
+    if (!PROD) {
+        x.seed_lane(cell_seed, lane);
+        for (int i = 0; i < h; i++) x.advance();
+    }
     const uint32_t* stream = A.recs + d.rec;
     const uint32_t nchunks = (uint32_t)(d.rec_len / kChunk);
     ring_fetch<G>(ring, stream, nchunks, 0, t);
@@ -359,10 +400,18 @@ __device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc&
         const uint32_t deg4 = (deg + 3u) & ~3u;
         if (!open) {
             // first record of site v: this site's uniforms and current spins
+            if constexpr (PROD) {
+                const uint32_t vw = v % kWin, b = (v / kWin) & 1u;
+                if (vw == 0) bar_sync(kBarFull0 + b, 64);
+                const uint64_t* rr = rngb + b * (8 * kWin) * kRS + (vw * 8 + lane) * kRS + h;
 #pragma unroll
-            for (int kk = 0; kk < 8; kk++) {
-                if (kk % TPL == 0) res[kk / TPL] = x.next();
-                else x.advance();
+                for (int j = 0; j < KP; j++) res[j] = rr[j * TPL];
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < 8; kk++) {
+                    if (kk % TPL == 0) res[kk / TPL] = x.next();
+                    else x.advance();
+                }
             }
             xb = sp[8u * v];
             if constexpr (MODE == kModeInt) {
@@ -465,6 +514,9 @@ __device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc&
             }
             flips = lane_or<TPL>(flips, gmask);
             sp[8u * v] = (uint8_t)(xb ^ flips);
+        }
+        if constexpr (PROD) {
+            if (v % kWin == kWin - 1 || v + 1 == d.n) bar_arrive(kBarEmpty0 + ((v / kWin) & 1u), 64);
         }
         v++;
     }
@@ -612,6 +664,117 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
 }
 
 // ---------------------------------------------------------------------------
+// Chain kernel: the per-lane sweep of batch_kernel<MODE, 4> (one instance per
+// CTA, 4 threads per Xoshiro lane) with the uniforms made ahead by a generator
+// warp (produce_windows), so the site chain carries no generator steps. For
+// instances whose consecutive sites are coupled (lattices), where the
+// windowed kernel has one site per level. GSP: spins stay in global memory.
+// Dynamic shared memory: threshold table | spread table | record ring |
+// generator buffers | spins (spin_cap words; none when GSP).
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr size_t chain_smem_bytes(uint32_t spin_cap) {
+    return 2048 + 4096 + (size_t)kSlots * kChunk * 4 + 2 * (8 * kWin) * kRS * 8 + (size_t)spin_cap * 8;
+}
+
+template <uint32_t MODE, bool GSP>
+__global__ void __launch_bounds__(64, 1) chain_kernel(DevArrays A, RunArgs R, uint32_t spin_cap) {
+    extern __shared__ __align__(16) uint64_t dsm[];
+    __shared__ uint32_t s_item;
+    uint64_t* tab = dsm;
+    uint2* lut = reinterpret_cast<uint2*>(dsm + 256);
+    uint32_t* ring = reinterpret_cast<uint32_t*>(dsm + 768);
+    uint64_t* rngb = reinterpret_cast<uint64_t*>(ring + kSlots * kChunk);
+    uint64_t* const ssw = rngb + 2 * (8 * kWin) * kRS;
+    const int tid = threadIdx.x;
+    const bool producer = tid < 32;
+    const int t = tid & 31;
+    const int lane = t >> 2, h = t & 3;
+    typedef ETypeT<MODE, 4> EType;
+    if constexpr (MODE == kModeInt) {
+        for (int i = tid; i < 512; i += 64) {
+            const uint32_t b = (i < 256 ? (uint32_t)i : (uint32_t)(i - 256) ^ 0xFFu);
+            lut[i] = make_uint2(spread4(b), spread4(b >> 4));
+        }
+    }
+    __syncthreads();
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(R.queue, 1u);
+        __syncthreads();
+        const uint32_t q = s_item;
+        __syncthreads();
+        if (q >= R.nquads) break;
+        const uint32_t inst = R.quads[4 * q];
+        if (inst == 0xffffffffu) continue;
+        const int H = MODE == kModeInt ? R.quad_h[q] : 0;
+        const InstDesc d = A.desc[inst];
+        if (!GSP && d.n > spin_cap) {
+            if (tid == 0) atomicExch(A.err, 2);
+            continue;
+        }
+        uint64_t* const sw = GSP ? A.spins + d.spin : ssw;
+        uint8_t* const sp = reinterpret_cast<uint8_t*>(sw) + lane;
+        const StepPlan P = step_plan(A, R, d, inst);
+        uint32_t key[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)d.owner + i];
+        const uint64_t pos0 = A.pos[d.owner];
+        EType E[2] = {0, 0};
+        if (!producer) {
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const size_t o = d.energy + lane + 8 * (j * 4 + h);
+                if constexpr (MODE == kModeInt) E[j] = A.Ei[o];
+                else E[j] = A.Ef[o];
+            }
+        }
+        if (!GSP) {
+            const uint64_t* gw = A.spins + d.spin;
+            for (uint32_t i = tid; i < d.n; i += 64) sw[i] = gw[i];
+        }
+        __syncthreads();
+        for (uint32_t s = 0; s < P.steps; s++) {
+            const double beta = __ddiv_rn(1.0, P.temps[P.tstride ? s : 0]);
+            const uint64_t base = chacha8_draw(key, pos0 + s) + d.cell;
+            if (producer) {
+                produce_windows(base, d.n, rngb, t, 64);
+            } else {
+                if constexpr (MODE == kModeInt) {
+                    __syncwarp();
+                    for (int i = t; i < 2 * H + 1; i += 32) tab[i] = metropolis_threshold(i - H, beta);
+                    __syncwarp();
+                }
+                sweep_stream<MODE, 4, true>(A, d, ring, sp, lut, lane, h, 0xffffffffu, tab, H, beta, base, E, rngb);
+                if constexpr (MODE == kModeF64) {
+                    if (!R.cells && (P.base + s + 1) % kResyncEvery == 0) {
+                        __syncwarp();
+                        energies_f64_calls<4>(A, d, sp, h, E);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (!GSP) {
+            uint64_t* gwo = A.spins + d.spin;
+            for (uint32_t i = tid; i < d.n; i += 64) gwo[i] = sw[i];
+        }
+        if (!producer) {
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const size_t o = d.energy + lane + 8 * (j * 4 + h);
+                if constexpr (MODE == kModeInt) A.Ei[o] = E[j];
+                else A.Ef[o] = E[j];
+            }
+        }
+        if (tid == 0 && !R.cells) {
+            A.pos[d.owner] = pos0 + P.steps;
+            A.deo[d.owner] ^= (int32_t)(exchanges_in(P.base, P.steps, R.exchange_interval) & 1u);
+            if (R.serve) A.done[d.owner] = P.base + P.steps;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Windowed kernel for large instances whose consecutive sites are rarely
 // coupled (random graphs). One warp runs one instance through windows of 8
 // consecutive sites:
@@ -657,11 +820,6 @@ __device__ __forceinline__ void window_fetch(const uint32_t* ent, const uint32_t
 // deciders work on window w. Hand-over through two output buffers guarded by
 // named barriers (bar.arrive by the producing side, bar.sync by the waiting
 // side, with the exact thread count of the CTA), so no thread spins.
-constexpr int kRS = 10;  // u64 per (site, lane) row of the output / dE buffers (8 calls + padding against bank conflicts)
-constexpr int kBarFull0 = 1, kBarEmpty0 = 3, kBarCons = 5;
-
-__device__ __forceinline__ void bar_sync(int id, int count) { asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
-__device__ __forceinline__ void bar_arrive(int id, int count) { asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory"); }
 
 __host__ __device__ constexpr size_t ws_smem_bytes(uint32_t spin_cap) {
     // tab 2 KB | spread table 4 KB | outputs 2 x 8 kWin rows | dE 8 kWin rows | records | spins
@@ -867,25 +1025,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
             }
             const uint64_t base = chacha8_draw(key, pos0 + s) + d.cell;
             if (producer) {
-                const int rl = tid >> 2, rh = tid & 3;
-                Xoshiro x;
-                x.seed_lane(base, rl);
-                for (int i = 0; i < rh; i++) x.advance();
-                for (uint32_t w = 0; w < nwin; w++) {
-                    const int b = w & 1;
-                    if (w >= 2) bar_sync(kBarEmpty0 + b, NT);
-                    uint64_t* ob = rngb + b * (8 * kWin) * kRS;
-#pragma unroll
-                    for (int i = 0; i < kWin; i++) {
-#pragma unroll
-                        for (int kk = 0; kk < 8; kk++) {
-                            if (kk % 4 == 0) ob[(i * 8 + rl) * kRS + rh + kk] = x.next();
-                            else x.advance();
-                        }
-                    }
-                    bar_arrive(kBarFull0 + b, NT);
-                }
-                for (uint32_t w = nwin >= 2 ? nwin - 2 : 0; w < nwin; w++) bar_sync(kBarEmpty0 + (w & 1), NT);
+                produce_windows(base, d.n, rngb, tid, NT);
             } else {
                 // records of window w + 2 are fetched while window w runs
                 window_fetch(wt, stream, recb, c, 32 * NC);
@@ -1695,6 +1835,36 @@ cudaError_t launch_window(const DevArrays& A, const RunArgs& R, uint32_t mode, u
     } else {
         if (mode == kModeInt) window_kernel<kModeInt, false><<<grid, WsCfg<kModeInt>::THREADS, sm, st>>>(A, R, spin_cap);
         else window_kernel<kModeF64, false><<<grid, WsCfg<kModeF64>::THREADS, sm, st>>>(A, R, spin_cap);
+    }
+    return cudaGetLastError();
+}
+
+template <uint32_t MODE, bool GSP>
+static int occ_chain(size_t smem) {
+    int n = 0;
+    if (smem > (size_t)kMaxDynSmem ||
+        cudaFuncSetAttribute(chain_kernel<MODE, GSP>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem) !=
+            cudaSuccess)
+        return 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, chain_kernel<MODE, GSP>, 64, smem) == cudaSuccess ? n : 0;
+}
+
+// spin_cap 0: spins stay in global memory
+int chain_occupancy(uint32_t mode, uint32_t spin_cap) {
+    const size_t sm = chain_smem_bytes(spin_cap);
+    if (spin_cap == 0) return mode == kModeInt ? occ_chain<kModeInt, true>(sm) : occ_chain<kModeF64, true>(sm);
+    return mode == kModeInt ? occ_chain<kModeInt, false>(sm) : occ_chain<kModeF64, false>(sm);
+}
+
+cudaError_t launch_chain(const DevArrays& A, const RunArgs& R, uint32_t mode, uint32_t spin_cap, int grid,
+                         cudaStream_t st) {
+    const size_t sm = chain_smem_bytes(spin_cap);
+    if (spin_cap == 0) {
+        if (mode == kModeInt) chain_kernel<kModeInt, true><<<grid, 64, sm, st>>>(A, R, 0);
+        else chain_kernel<kModeF64, true><<<grid, 64, sm, st>>>(A, R, 0);
+    } else {
+        if (mode == kModeInt) chain_kernel<kModeInt, false><<<grid, 64, sm, st>>>(A, R, spin_cap);
+        else chain_kernel<kModeF64, false><<<grid, 64, sm, st>>>(A, R, spin_cap);
     }
     return cudaGetLastError();
 }

@@ -13,6 +13,9 @@ cudaError_t launch_batch(const DevArrays& A, const RunArgs& R, uint32_t mode, in
 int window_occupancy(uint32_t mode, uint32_t spin_cap);
 cudaError_t launch_window(const DevArrays& A, const RunArgs& R, uint32_t mode, uint32_t spin_cap, int grid,
                           cudaStream_t st);
+int chain_occupancy(uint32_t mode, uint32_t spin_cap);
+cudaError_t launch_chain(const DevArrays& A, const RunArgs& R, uint32_t mode, uint32_t spin_cap, int grid,
+                         cudaStream_t st);
 cudaError_t launch_exchange(const DevArrays& A, const RunArgs& R, uint32_t ninst, uint32_t mode, uint32_t steps,
                             bool exchange, cudaStream_t st);
 cudaError_t launch_swap(const DevArrays& A, uint32_t inst, uint32_t n_words, int sm_count, cudaStream_t st);

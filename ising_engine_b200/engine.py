@@ -241,7 +241,8 @@ class BatchEngine:
 
     def class_report(self):
         """Per work class of the last run: (mode, threads per lane, capacity,
-        items, device ms); threads per lane 8 marks the windowed kernel."""
+        items, device ms); threads per lane 8 marks the windowed kernel, 16 the
+        chain kernel."""
         n = np.zeros(1, dtype=np.uint32)
         info = np.zeros(5 * 64, dtype=np.uint32)
         ms = np.zeros(64, dtype=np.float64)
