@@ -201,7 +201,7 @@ def run_ours(args):
     eng = BatchEngine(models, seeds, device=local, threads_per_block=args.threads_per_block,
                       blocks_per_sm=args.blocks_per_sm, graph=True)
     eng.init_random()
-    tuned = eng.autotune(temps, 96) if not args.no_autotune else None
+    tuned = eng.autotune(temps, 160) if not args.no_autotune else None
     for _ in range(args.warmup):
         eng.run_schedule(temps)
     dist.barrier()

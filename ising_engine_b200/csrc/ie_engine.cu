@@ -584,9 +584,9 @@ struct Engine {
     // makespan, get the most threads; the shared-memory capacity of a class
     // is the smallest of kCaps that holds its instances.
     static constexpr uint32_t kCaps[10] = {256, 512, 768, 1024, 1536, 2048, 3072, 4096, 8192, 16384};
-    // thread-class size thresholds per mode: n > n4 -> 4 threads per lane,
-    // n > n2 -> 2, else 1 (set by the autotuner)
-    uint32_t tune_n4[2] = {1536, 768}, tune_n2[2] = {512, 256};
+    // size thresholds per mode (see tpl_of); defaults are the autotuner's
+    // usual choice on uneven random-graph batches
+    uint32_t tune_n4[2] = {256, 768}, tune_n2[2] = {128, 256};
     struct WorkClass {
         uint32_t mode = 0;
         int tpl = 1;
@@ -619,10 +619,12 @@ struct Engine {
     }
 
     // Kernel form of an instance: 1, 2, 4 threads per lane (batch_kernel), 8:
-    // the windowed kernel, 16: the chain kernel (one CTA per instance). Large
-    // instances whose windows are parallel take the windowed kernel, other
-    // instances above the small-instance threshold the chain kernel; spins
-    // beyond shared memory stay in global memory in either.
+    // the windowed kernel, 16: the chain kernel (one CTA per instance). Above
+    // n4, instances whose windows are parallel take the windowed kernel; other
+    // instances above n2 (sequential site chains: lattices) the chain kernel;
+    // the rest run 2 to a warp above n2 and 4 to a warp below. Spins beyond
+    // shared memory stay in global memory. Without windows (use_windows
+    // false) the one-warp forms 4 / 2 / 1 only.
     static constexpr uint32_t kSmemSpinCap = 24576;
     static constexpr int kChain = 16;
     int tpl_of(const InstDesc& d, const HostInst& h) const {
@@ -630,7 +632,7 @@ struct Engine {
         if (cap_of(n) > kSmemSpinCap) return h.windowed_ok && use_windows ? 8 : kChain;
         if (!use_windows) return n > tune_n4[m] ? 4 : (n > tune_n2[m] ? 2 : 1);
         if (n > tune_n4[m]) return h.windowed_ok ? 8 : kChain;
-        if (!h.windowed_ok && n > tune_n2[m]) return kChain;
+        if (n > tune_n2[m] && !h.windowed_ok) return kChain;
         return n > tune_n2[m] ? 2 : 1;
     }
     // shared-memory spin capacity of the instance's class; 0: spins in global memory
@@ -1016,6 +1018,7 @@ struct Engine {
         // is timed on the same state (restored after it).
         const uint32_t n4s[5] = {256, 512, 768, 1536, 3072}, n2s[3] = {128, 256, 512};
         uint32_t bi[4] = {tune_n4[0], tune_n2[0], tune_n4[1], tune_n2[1]};
+        const uint32_t start[4] = {bi[0], bi[1], bi[2], bi[3]};
         auto trial = [&](double& ms) -> ie_status {
             tune_n4[0] = bi[0];
             tune_n2[0] = bi[1];
@@ -1048,6 +1051,23 @@ struct Engine {
                 bi[2 * m] = b4;
                 bi[2 * m + 1] = b2;
             }
+        // Single short trials are noisy: the search's choice replaces the
+        // starting thresholds only if it is faster on the best of three
+        // repeated trials each.
+        if (!std::equal(bi, bi + 4, start)) {
+            const uint32_t found[4] = {bi[0], bi[1], bi[2], bi[3]};
+            double t_found = 1e300, t_start = 1e300;
+            for (int rep = 0; rep < 3; rep++) {
+                double ms = 0;
+                std::copy(found, found + 4, bi);
+                IE_TRY(trial(ms));
+                t_found = std::min(t_found, ms);
+                std::copy(start, start + 4, bi);
+                IE_TRY(trial(ms));
+                t_start = std::min(t_start, ms);
+            }
+            std::copy(t_found < t_start ? found : start, (t_found < t_start ? found : start) + 4, bi);
+        }
         tune_n4[0] = bi[0];
         tune_n2[0] = bi[1];
         tune_n4[1] = bi[2];
