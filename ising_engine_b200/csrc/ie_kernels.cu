@@ -776,19 +776,20 @@ __global__ void __launch_bounds__(64, 1) chain_kernel(DevArrays A, RunArgs R, ui
 
 // ---------------------------------------------------------------------------
 // Windowed kernel for large instances whose consecutive sites are rarely
-// coupled (random graphs). One warp runs one instance through windows of 8
-// consecutive sites:
-//  1. generator phase: thread (lane rl = t/4, offset rh = t%4) advances lane
-//     rl's Xoshiro chain over the window's 64 steps and stores the outputs of
-//     the calls it owns (rh, rh+4) for each site in shared memory;
-//  2. decision phase: 64 (site, lane) tasks, two per thread, run level by
-//     level inside the window (a site waits only for lower-indexed neighbours
-//     in the same window; the levels come from a host-built window table), so
-//     the outcome equals the reference's site order exactly;
+// coupled (random graphs). One CTA runs one instance through windows of kWin
+// consecutive sites, warp-specialised:
+//  1. warp 0 is the generator (produce_windows): thread (lane rl, offset rh)
+//     runs lane rl's Xoshiro chain and stores the calls it owns (rh, rh + 4)
+//     of every site of window w + 1 while the deciders work on window w;
+//  2. NC decider warps take the window's 8 kWin (site, lane) tasks (SPLIT
+//     threads each) level by level (a site waits only for lower-indexed
+//     neighbours in the same window; the levels come from a host-built window
+//     table), so the outcome equals the reference's site order exactly;
 //  3. each accepted dE goes to shared memory and every replica's energy is
 //     accumulated in site order, the reference's f64 summation order.
-// The next window's site records stream into a shared double buffer with
-// cp.async while the current window is processed.
+// The records of window w + 2 stream into one of three shared buffers with
+// cp.async while window w is processed. Spins stay in shared memory, or in
+// global memory (GSP) for instances beyond it.
 // Window table layout: kWin / kWT in ie_kernels.cuh.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kWinRecWords = kWin * (4 + 3 * kWinMaxDeg);  // kWin f64 records of degree <= 32
@@ -814,12 +815,6 @@ __device__ __forceinline__ void window_fetch(const uint32_t* ent, const uint32_t
         cp_async16(buf + 4 * j, stream + 4 * (size_t)src);
     }
 }
-
-// Warp-specialized form: warp 0 is the generator (producer) and NC warps are
-// deciders (consumers); the generator fills window w+1's outputs while the
-// deciders work on window w. Hand-over through two output buffers guarded by
-// named barriers (bar.arrive by the producing side, bar.sync by the waiting
-// side, with the exact thread count of the CTA), so no thread spins.
 
 __host__ __device__ constexpr size_t ws_smem_bytes(uint32_t spin_cap) {
     // tab 2 KB | spread table 4 KB | outputs 2 x 8 kWin rows | dE 8 kWin rows | records | spins

@@ -26,7 +26,7 @@ struct InstDesc {
     uint64_t stat;   // swap stats base ([nt-1] per instance)
     uint64_t rec;    // site-record stream (batched kernel): recs[rec .. rec + rec_len)
     uint64_t rec_len;
-    uint64_t win;    // window table (windowed kernel): wtab[win .. win + 16 * ceil(n / 8))
+    uint64_t win;    // window table (windowed kernel): wtab[win .. win + kWT * ceil(n / kWin))
     uint64_t wrec;   // windowed kernel's record stream (one record per site): recs[wrec ..)
     uint64_t sched;  // serving: the instance's per-step temperatures at temps[sched .. sched + sched_len)
     uint64_t sched_len;
