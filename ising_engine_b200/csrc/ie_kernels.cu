@@ -225,11 +225,12 @@ __device__ __forceinline__ StepPlan step_plan(const DevArrays& A, const RunArgs&
 // decisions of the calls k = h, h+TPL, ... (h = its index within the lane).
 // Integer mode splits each site's neighbour sum across the TPL threads
 // (SWAR partial sums, reduced with two shuffles per level); f64 mode splits the
-// replicas. A warp holds 4/TPL instances; they run the same schedule in step
-// and share one threshold table per sweep. Each instance streams its site
-// records through a 3-slot shared-memory ring with cp.async (two 512-byte
-// chunks in flight ahead of the sweep). Spin bytes stay in global memory,
-// resident in L1; every thread of a lane writes the same combined byte, so
+// replicas. A warp holds 4/TPL instances; in a batched run they run the same
+// schedule in step and share one threshold table per sweep, in a serving or
+// PT-cells run each has its own schedule and table. Each instance streams its
+// site records through a 3-slot shared-memory ring with cp.async (two 512-byte
+// chunks in flight ahead of the sweep); its spin words stay in shared memory
+// for the whole run. Every thread of a lane writes the same combined byte, so
 // each thread's later reads see the update in program order.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void cp_async16(uint32_t* smem_dst, const uint32_t* gsrc) {
