@@ -15,7 +15,7 @@ HEADERS = ["ie_device.cuh", "ie_kernels.cuh", "ie_launch.h", "ie_host.h",
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC", "-shared", "-lpthread",
 ]
 
 

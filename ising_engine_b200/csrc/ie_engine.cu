@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -13,6 +14,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -92,6 +94,29 @@ ie_status build_xtables(const double* temps, uint32_t nt, XTables& X) {
 }  // namespace ie
 
 namespace {
+
+// Runs fn(i) for every i in [0, count) on up to 32 host threads, in chunks of
+// 16 indices handed out in order.
+template <typename F>
+void parallel_for(uint32_t count, F&& fn) {
+    const unsigned nth = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    if (count < 64 || nth == 1) {
+        for (uint32_t i = 0; i < count; i++) fn(i);
+        return;
+    }
+    std::atomic<uint32_t> next{0};
+    auto work = [&]() {
+        for (;;) {
+            const uint32_t i0 = next.fetch_add(16);
+            if (i0 >= count) break;
+            for (uint32_t i = i0; i < std::min(i0 + 16, count); i++) fn(i);
+        }
+    };
+    std::vector<std::thread> ts;
+    for (unsigned k = 1; k < nth; k++) ts.emplace_back(work);
+    work();
+    for (auto& t : ts) t.join();
+}
 
 // f64::powi for a runtime exponent lowers to compiler-rt's __powidf2.
 double powi_rt(double a, int b) {
@@ -431,9 +456,18 @@ struct Engine {
         insts.resize(count);
         desc.resize(count);
         keys.resize((size_t)count * 8);
-        for (uint32_t i = 0; i < count; i++) {
-            IE_TRY(ingest(&problems[i], force_f64, insts[i]));
-            chacha_key_from_u64(seeds[i], &keys[(size_t)8 * i]);
+        {
+            // per-instance ingestion on host threads; an error is raised again
+            // on this thread with its message
+            std::vector<ie_status> st(count, IE_OK);
+            std::vector<std::string> msg(count);
+            parallel_for(count, [&](uint32_t i) {
+                st[i] = ingest(&problems[i], force_f64, insts[i]);
+                if (st[i] != IE_OK) msg[i] = g_err;
+                chacha_key_from_u64(seeds[i], &keys[(size_t)8 * i]);
+            });
+            for (uint32_t i = 0; i < count; i++)
+                if (st[i] != IE_OK) return fail(st[i], msg[i]);
         }
         size_t site = 0, ent = 0, spin = 0, energy = 0, stat = 0;
         for (uint32_t i = 0; i < count; i++) {
@@ -465,7 +499,7 @@ struct Engine {
         std::vector<uint32_t> rows(site + count), ents(ent), cols(ent);
         std::vector<int32_t> linp(site, 0);
         std::vector<double> vals(ent), lin(site);
-        for (uint32_t i = 0; i < count; i++) {
+        parallel_for(count, [&](uint32_t i) {
             const HostInst& h = insts[i];
             const InstDesc& d = desc[i];
             std::copy(h.rows.begin(), h.rows.end(), rows.begin() + d.row);
@@ -476,7 +510,7 @@ struct Engine {
                 std::copy(h.ents.begin(), h.ents.end(), ents.begin() + d.ent);
                 std::copy(h.linp.begin(), h.linp.end(), linp.begin() + d.site);
             }
-        }
+        });
         clampf.assign(site, 0);
         clampv.assign(site, 0);
         IE_TRY(d_desc.upload(desc, stream));
@@ -547,15 +581,36 @@ struct Engine {
         wt.insert(wt.end(), tab.begin(), tab.end());
     }
 
+    // Record streams and window tables, built per instance on host threads
+    // (each stream a whole number of chunks) and concatenated.
     ie_status build_record_streams() {
-        std::vector<uint32_t> recs, wt;
+        std::vector<std::vector<uint32_t>> lrec(count), lwt(count);
+        std::vector<ie_status> st(count, IE_OK);
+        std::vector<std::string> msg(count);
+        parallel_for(count, [&](uint32_t i) {
+            st[i] = build_records(insts[i], clampf, desc[i].site, lrec[i], desc[i].rec, desc[i].rec_len);
+            if (st[i] == IE_OK) st[i] = window_records(insts[i], clampf, desc[i].site, lrec[i], desc[i].rec, desc[i].wrec);
+            if (st[i] != IE_OK) {
+                msg[i] = g_err;
+                return;
+            }
+            build_window_table(i, lwt[i]);
+        });
+        for (uint32_t i = 0; i < count; i++)
+            if (st[i] != IE_OK) return fail(st[i], msg[i]);
+        std::vector<uint64_t> roff(count + 1, 0), woff(count + 1, 0);
         for (uint32_t i = 0; i < count; i++) {
-            IE_TRY(build_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].rec_len));
-            IE_TRY(window_records(insts[i], clampf, desc[i].site, recs, desc[i].rec, desc[i].wrec));
-            build_window_table(i, wt);
+            roff[i + 1] = roff[i] + lrec[i].size();
+            woff[i + 1] = woff[i] + lwt[i].size();
         }
-        recs.resize(recs.size() + kChunk, 0);
-        if (wt.empty()) wt.assign(kWT, 0);
+        std::vector<uint32_t> recs(roff[count] + kChunk, 0), wt(std::max<uint64_t>(woff[count], kWT), 0);
+        parallel_for(count, [&](uint32_t i) {
+            std::copy(lrec[i].begin(), lrec[i].end(), recs.begin() + roff[i]);
+            std::copy(lwt[i].begin(), lwt[i].end(), wt.begin() + woff[i]);
+            desc[i].rec += roff[i];
+            desc[i].wrec += roff[i];
+            desc[i].win += woff[i];
+        });
         IE_TRY(d_recs.upload(recs, stream));
         IE_TRY(d_wtab.upload(wt, stream));
         quads_built = false;
