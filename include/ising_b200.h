@@ -61,7 +61,7 @@ typedef struct ie_config {
     uint64_t total_exchanges;
     uint64_t seed;
     uint32_t num_temps;  /* default 10 (ultimate.rs:75) */
-    uint32_t num_pops;   /* must be 1 (PA-PT is not on this path) */
+    uint32_t num_pops;   /* 1: PT; > 1: population annealing (ie_run_pa), cells t + num_temps * p */
     uint32_t num_slices; /* must be 1 (the Trotter branch is not on this path) */
     uint32_t exchange_interval;
     int32_t force_f64;   /* nonzero: use the f64 mode even for integral input */
@@ -73,6 +73,31 @@ typedef struct ie_config {
 
 typedef struct ie_handle ie_handle;
 typedef struct ie_batch ie_batch;
+
+/* The population-annealing knobs of UltimateSolver (ultimate.rs:29-52). */
+typedef struct ie_pa_config {
+    double ess_threshold;              /* resample when ESS < ess_threshold * R; 0.5 by default
+                                          (above 1: every stage after the first) */
+    uint32_t ladder_tuning_iters;      /* 8 by default; 0 keeps the geometric ladder */
+    uint32_t ladder_tuning_steps;      /* 10 by default */
+    uint32_t post_resample_relaxation; /* 5 by default */
+    int32_t ladder_mode;               /* 0: LadderMode::AcceptanceUniform (the default; the only mode here) */
+    int32_t use_icm;                   /* must be 0 (the default) */
+} ie_pa_config;
+
+/* PaDiagnostics (population_annealing.rs:34-45) plus the frozen ladder
+ * shape. The arrays are caller-owned and may be NULL; `capacity` entries are
+ * written at most, the counts are always complete. */
+typedef struct ie_pa_report {
+    double free_energy;
+    uint64_t resample_events;
+    uint64_t n_ess;          /* total_exchanges - 1 stages record an ESS */
+    double* ess_history;     /* [capacity] */
+    double* family_rho;      /* [capacity], one per resampling event */
+    uint64_t* family_count;  /* [capacity] */
+    uint64_t capacity;
+    double* alphas;          /* [num_temps] or NULL */
+} ie_pa_report;
 
 const char* ie_last_error(void);
 int ie_abi_version(void);
@@ -269,7 +294,8 @@ ie_status ie_serve_last_tick(ie_serve* s, double* ms, uint64_t* launches);
  * rows sorted, duplicates merged, no zero weights, integral values.
  * The operator's ChaCha8Rng is ChaCha8Rng::seed_from_u64(seed) after
  * `draw_offset` 64-bit draws; a Metropolis call consumes sweeps * n * r
- * draws, an exchange call one per attempted pair (*proposed). */
+ * draws (a Gibbs call as many), an exchange call one per attempted pair
+ * (*proposed). */
 typedef struct ie_v2 ie_v2;
 /* init: [num_vars] 0/1, copied into every replica (SparseBitSlice::new). */
 ie_status ie_v2_create(const ie_problem* ir, uint32_t num_replicas, const uint8_t* init, int32_t device,
@@ -280,6 +306,11 @@ ie_status ie_v2_metropolis(ie_v2* h, const double* temps, uint32_t n_temps, uint
                            uint64_t draw_offset, uint64_t* proposed, uint64_t* accepted);
 ie_status ie_v2_exchange(ie_v2* h, const double* temps, uint32_t n_temps, uint64_t rounds, uint64_t seed,
                          uint64_t draw_offset, uint64_t* proposed, uint64_t* accepted);
+/* GibbsColorSweep::apply (src/engine_v2/operators/gibbs_color_sweep.rs:119-165):
+ * heat-bath resampling in chromatic order, sweeps * n * r draws; a temperature
+ * <= 0 (or NaN) is the greedy limit, as in the reference. */
+ie_status ie_v2_gibbs(ie_v2* h, const double* temps, uint32_t n_temps, uint64_t sweeps, uint64_t seed,
+                      uint64_t draw_offset, uint64_t* proposed, uint64_t* accepted);
 /* planes: [num_vars * ceil(r / 64)] (bit b of word q of a site = replica 64q + b);
  * energies: [r] from the ledger (either may be NULL). */
 ie_status ie_v2_read(ie_v2* h, uint64_t* planes, double* energies);
@@ -287,6 +318,28 @@ ie_status ie_v2_read(ie_v2* h, uint64_t* planes, double* energies);
 ie_status ie_v2_audit(ie_v2* h, double* drift);
 /* ProblemIR::greedy_coloring (src/engine_v2/ir.rs:114-139), host only. */
 ie_status ie_v2_coloring(const ie_problem* ir, uint32_t* colors);
+
+/* ---- population annealing with PT equilibration (num_pops > 1) ----
+ * UltimateSolver::solve_population_annealing_diag (ultimate.rs:576-852) on a
+ * handle created with num_pops > 1, entered as solve_with_pa_diagnostics does
+ * (ultimate.rs:858-890: clamps from ie_set_clamps, no presolve): ladder
+ * tuning on a throwaway field, then total_exchanges annealing stages of
+ * sweeps_per_exchange engine::step calls over all populations, Boltzmann
+ * reweighting at the cold level, systematic resampling with shuffled
+ * offspring when the ESS falls below the threshold, post-resampling
+ * relaxation, an exact energy re-sync and the incumbent after every stage.
+ * The handle's master stream must be fresh (ChaCha8Rng::seed_from_u64(seed)).
+ * Afterwards ie_read_best / ie_one_opt finish the solve (ultimate.rs:806-845). */
+ie_status ie_run_pa(ie_handle* h, const ie_pa_config* config, ie_pa_report* report);
+
+/* population_annealing.rs primitives (host only). */
+ie_status ie_pa_normalized_weights(const double* log_w, uint64_t r, double* w_out);
+ie_status ie_pa_effective_sample_size(const double* w, uint64_t r, double* ess);
+ie_status ie_pa_free_energy_increment(const double* log_w, uint64_t r, double* out);
+/* families are summed in ascending id order */
+ie_status ie_pa_family_entropy(const uint64_t* family_ids, uint64_t r, double* rho, uint64_t* families);
+ie_status ie_pa_systematic_resample(const double* w, uint64_t r, double u, uint64_t* counts);
+ie_status ie_pa_adapt_spacings(const double* spacings, const double* acceptance, uint64_t k, double* out);
 
 /* ---- measurement helper (no reference counterpart) ----
  * Measured roofline denominators on `device`: int32 LOP3/IADD3 throughput

@@ -45,6 +45,18 @@ class ie_problem_device(C.Structure):
                 ("col_indices", C.c_void_p), ("values", C.c_void_p), ("linear", C.c_void_p)]
 
 
+class ie_pa_config(C.Structure):
+    _fields_ = [("ess_threshold", C.c_double), ("ladder_tuning_iters", C.c_uint32),
+                ("ladder_tuning_steps", C.c_uint32), ("post_resample_relaxation", C.c_uint32),
+                ("ladder_mode", C.c_int32), ("use_icm", C.c_int32)]
+
+
+class ie_pa_report(C.Structure):
+    _fields_ = [("free_energy", C.c_double), ("resample_events", C.c_uint64), ("n_ess", C.c_uint64),
+                ("ess_history", C.c_void_p), ("family_rho", C.c_void_p), ("family_count", C.c_void_p),
+                ("capacity", C.c_uint64), ("alphas", C.c_void_p)]
+
+
 class ie_batch_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("force_f64", C.c_int32),
                 ("threads_per_block", C.c_uint32), ("blocks_per_sm", C.c_uint32),
@@ -69,6 +81,13 @@ _SIGS = {
     "ie_step": ([_vp, _vp, C.c_uint32, C.c_uint64], C.c_int),
     "ie_run_schedule": ([_vp, _vp, C.c_uint32, C.c_uint64], C.c_int),
     "ie_run_pt": ([_vp], C.c_int),
+    "ie_run_pa": ([_vp, _vp, _vp], C.c_int),
+    "ie_pa_normalized_weights": ([_vp, C.c_uint64, _vp], C.c_int),
+    "ie_pa_effective_sample_size": ([_vp, C.c_uint64, _vp], C.c_int),
+    "ie_pa_free_energy_increment": ([_vp, C.c_uint64, _vp], C.c_int),
+    "ie_pa_family_entropy": ([_vp, C.c_uint64, _vp, _vp], C.c_int),
+    "ie_pa_systematic_resample": ([_vp, C.c_uint64, C.c_double, _vp], C.c_int),
+    "ie_pa_adapt_spacings": ([_vp, _vp, C.c_uint64, _vp], C.c_int),
     "ie_read_spins": ([_vp, _vp], C.c_int),
     "ie_read_energies": ([_vp, _vp], C.c_int),
     "ie_read_swap_stats": ([_vp, _vp, _vp], C.c_int),
@@ -105,6 +124,7 @@ _SIGS = {
     "ie_v2_destroy": ([_vp], C.c_int),
     "ie_v2_metropolis": ([_vp, _vp, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, _vp, _vp], C.c_int),
     "ie_v2_exchange": ([_vp, _vp, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, _vp, _vp], C.c_int),
+    "ie_v2_gibbs": ([_vp, _vp, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, _vp, _vp], C.c_int),
     "ie_v2_read": ([_vp, _vp, _vp], C.c_int),
     "ie_v2_audit": ([_vp, _vp], C.c_int),
     "ie_v2_coloring": ([_vp, _vp], C.c_int),

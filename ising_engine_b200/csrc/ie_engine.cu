@@ -390,6 +390,11 @@ struct Engine {
     uint32_t threads_per_block = 0, blocks_per_sm = 0;
     std::vector<double> xtemps;  // ladder the exchange tables were built for
     bool initialized = false;
+    // populations: the instance's nt cells are nt / pop_len populations of
+    // pop_len cells (0: one ladder of nt cells); the population driver
+    // re-syncs energies itself, so the PT loop's periodic re-sync is off
+    uint32_t pop_len = 0;
+    bool periodic_resync = true;
 
     ~Engine() {
         if (device >= 0) cudaSetDevice(device);
@@ -800,6 +805,7 @@ struct Engine {
     }
 
     bool use_cells() const {
+        if (pop_len) return true;
         if (pt_path == 1) return false;
         if (pt_path == 2) return true;
         return desc[0].n >= 256;
@@ -859,7 +865,7 @@ struct Engine {
         while (done < steps) {
             const uint64_t g0 = steps_done + done;
             uint64_t k = kx - g0 % kx;
-            if (mode == kModeF64) k = std::min<uint64_t>(k, kResyncEvery - g0 % kResyncEvery);
+            if (mode == kModeF64 && periodic_resync) k = std::min<uint64_t>(k, kResyncEvery - g0 % kResyncEvery);
             k = std::min<uint64_t>(k, steps - done);
             R.steps = (uint32_t)k;
             R.step_base = g0;
@@ -874,7 +880,7 @@ struct Engine {
                     IE_CUDA(launch_swap(A, i, desc[i].n, g_sm_count, stream));
                     launches++;
                 }
-            if (mode == kModeF64 && (g0 + k) % kResyncEvery == 0) {
+            if (mode == kModeF64 && periodic_resync && (g0 + k) % kResyncEvery == 0) {
                 IE_CUDA(launch_energy(A, 0, count, stream));
                 launches++;
             }
@@ -1192,23 +1198,24 @@ struct Engine {
         for (double x : t)
             if (!(x > 0.0) || !std::isfinite(x)) return fail(IE_ERR_INVALID, "temperatures must be positive");
         const InstDesc& d = desc[0];
+        const uint32_t L = pop_len ? pop_len : nt;  // one population's ladder
         if (per_step && nt > 1 && d.mode == kModeInt) {
             // exchange tables are per ladder: one launch per step
             for (uint64_t s = 0; s < steps; s++) IE_TRY(run_pt(temps + s * nt, 1, false, exchange_interval));
             return IE_OK;
         }
-        if (nt > 1 && d.mode == kModeInt && (xtemps.size() != nt || !std::equal(xtemps.begin(), xtemps.end(), t.begin()))) {
+        if (nt > 1 && d.mode == kModeInt && (xtemps.size() != L || !std::equal(xtemps.begin(), xtemps.end(), t.begin()))) {
             XTables X;
-            IE_TRY(build_xtables(t.data(), nt, X));
+            IE_TRY(build_xtables(t.data(), L, X));
             IE_TRY(d_xtab.upload(X.tab.empty() ? std::vector<uint64_t>(1, 0) : X.tab, stream));
             IE_TRY(d_xoff.upload(X.off, stream));
             IE_TRY(d_xdmax.upload(X.dmax, stream));
             IE_TRY(d_xdund.upload(X.dund, stream));
             IE_TRY(d_dbeta.upload(X.dbeta, stream));
-            xtemps.assign(t.begin(), t.begin() + nt);
+            xtemps.assign(t.begin(), t.begin() + L);
         } else if (nt > 1 && d.mode == kModeF64) {
-            std::vector<double> db(nt - 1);
-            for (uint32_t k = 0; k + 1 < nt; k++) db[k] = 1.0 / t[k] - 1.0 / t[k + 1];
+            std::vector<double> db(std::max<uint32_t>(L, 2) - 1);
+            for (uint32_t k = 0; k + 1 < L; k++) db[k] = 1.0 / t[k] - 1.0 / t[k + 1];
             if (per_step) {
                 // f64 exchange reads dbeta of the current ladder: one launch per step
                 for (uint64_t s = 0; s < steps; s++) IE_TRY(run_pt(temps + s * nt, 1, false, exchange_interval));
@@ -1225,6 +1232,7 @@ struct Engine {
             X.xdmax = d_xdmax.p;
             X.xdund = d_xdund.p;
             X.dbeta = d_dbeta.p;
+            X.pop_len = pop_len;
             return run_pt_cells(steps, per_step, X);
         }
         const int block = (int)(((nt * 8) + 31) / 32 * 32);
@@ -1701,8 +1709,8 @@ bool cfg_valid(const ie_config* c, std::string& why) {
         why = "config is NULL";
         return false;
     }
-    if (c->num_pops != 0 && c->num_pops != 1) {
-        why = "num_pops must be 1 (population annealing is not on this path)";
+    if (c->num_pops > 64) {
+        why = "at most 64 populations";
         return false;
     }
     if (c->num_slices != 0 && c->num_slices != 1) {
@@ -1785,7 +1793,14 @@ ie_status ie_create(const ie_problem* problem, const ie_config* config, ie_handl
     if (h->cfg.pt_path < 0 || h->cfg.pt_path > 2) return fail(IE_ERR_INVALID, "pt_path must be 0, 1 or 2");
     IE_TRY(h->eng.setup_device(config->device));
     h->eng.pt_path = h->cfg.pt_path;
-    IE_TRY(h->eng.build(problem, 1, h->cfg.num_temps, &config->seed, config->force_f64 != 0));
+    const uint32_t pops = std::max<uint32_t>(h->cfg.num_pops, 1);
+    if (pops > 1) {
+        // QuantumField::new(n, 1, num_temps, num_pops): cell t + num_temps * p,
+        // each a work item of the batched kernels
+        h->eng.pop_len = h->cfg.num_temps;
+        h->eng.periodic_resync = false;
+    }
+    IE_TRY(h->eng.build(problem, 1, h->cfg.num_temps * pops, &config->seed, config->force_f64 != 0));
     h->offset = problem->energy_offset;
     IE_TRY(h->d_inc_e.upload(std::vector<double>(1, std::numeric_limits<double>::infinity()), h->eng.stream));
     IE_TRY(h->d_inc_state.alloc(std::max<uint64_t>((problem->num_vars + 63) / 64, 1)));
@@ -1818,22 +1833,35 @@ ie_status ie_set_spins(ie_handle* h, const uint64_t* words) {
     return h->eng.write_words(0, words);
 }
 
+// A population handle's cells take temps[t % num_temps]: the ladder rows are
+// repeated once per population.
+static std::vector<double> ladder_rows(const Engine& E, const double* temps, uint64_t rows) {
+    const uint32_t L = E.pop_len ? E.pop_len : E.nt;
+    std::vector<double> out((size_t)rows * E.nt);
+    for (uint64_t s = 0; s < rows; s++)
+        for (uint32_t c = 0; c < E.nt; c++) out[(size_t)s * E.nt + c] = temps[(size_t)s * L + c % L];
+    return out;
+}
+
 ie_status ie_step(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t n_steps) {
     if (!h || !temps) return fail(IE_ERR_INVALID, "NULL argument");
-    if (n_temps != h->eng.nt) return fail(IE_ERR_INVALID, "n_temps must equal the handle's num_temps");
+    if (n_temps != h->cfg.num_temps) return fail(IE_ERR_INVALID, "n_temps must equal the handle's num_temps");
     IE_CUDA(cudaSetDevice(h->eng.device));
-    return h->eng.run_pt(temps, n_steps, false, h->cfg.exchange_interval);
+    if (!h->eng.pop_len) return h->eng.run_pt(temps, n_steps, false, h->cfg.exchange_interval);
+    return h->eng.run_pt(ladder_rows(h->eng, temps, 1).data(), n_steps, false, h->cfg.exchange_interval);
 }
 
 ie_status ie_run_schedule(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t n_steps) {
     if (!h || !temps) return fail(IE_ERR_INVALID, "NULL argument");
-    if (n_temps != h->eng.nt) return fail(IE_ERR_INVALID, "n_temps must equal the handle's num_temps");
+    if (n_temps != h->cfg.num_temps) return fail(IE_ERR_INVALID, "n_temps must equal the handle's num_temps");
     IE_CUDA(cudaSetDevice(h->eng.device));
-    return h->eng.run_pt(temps, n_steps, true, h->cfg.exchange_interval);
+    if (!h->eng.pop_len) return h->eng.run_pt(temps, n_steps, true, h->cfg.exchange_interval);
+    return h->eng.run_pt(ladder_rows(h->eng, temps, n_steps).data(), n_steps, true, h->cfg.exchange_interval);
 }
 
 ie_status ie_run_pt(ie_handle* h) {
     if (!h) return fail(IE_ERR_INVALID, "handle is NULL");
+    if (h->eng.pop_len) return fail(IE_ERR_INVALID, "a handle with num_pops > 1 runs ie_run_pa");
     IE_CUDA(cudaSetDevice(h->eng.device));
     std::vector<double> temps(h->eng.nt);
     IE_TRY(ie_geometric_temps(h->cfg.temp_max, h->cfg.temp_min, h->eng.nt, temps.data()));
@@ -1845,6 +1873,156 @@ ie_status ie_run_pt(ie_handle* h) {
     }
     IE_CUDA(cudaStreamSynchronize(h->eng.stream));
     h->have_incumbent = true;
+    return IE_OK;
+}
+
+// UltimateSolver::solve_population_annealing_diag (ultimate.rs:576-852) with
+// acceptance-uniform ladder tuning and no ICM. The steps, energies and
+// resampled configurations stay on the device; per stage the host reads the
+// cold-level energies (64 per population) for the weights and, on a
+// resampling event, takes the offset and shuffle draws from the master
+// stream at the device's position and advances it.
+ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
+    if (!h || !pc) return fail(IE_ERR_INVALID, "NULL argument");
+    Engine& E = h->eng;
+    if (!E.pop_len) return fail(IE_ERR_INVALID, "ie_run_pa needs a handle created with num_pops > 1");
+    if (pc->ladder_mode != 0) return fail(IE_ERR_UNSUPPORTED, "only the acceptance-uniform ladder tuning is on this path");
+    if (pc->use_icm) return fail(IE_ERR_UNSUPPORTED, "ICM cluster moves are not on this path");
+    if (std::isnan(pc->ess_threshold)) return fail(IE_ERR_INVALID, "ess_threshold is NaN");
+    IE_CUDA(cudaSetDevice(E.device));
+    const uint32_t L = E.pop_len, pops = E.nt / L, R = pops * (uint32_t)kReplicas;
+    const double tmax = h->cfg.temp_max, tmin = h->cfg.temp_min;
+    const uint32_t mode = E.desc[0].mode;
+    const uint64_t n = E.desc[0].n;
+    const size_t words = (size_t)E.nt * n;
+    cudaStream_t st = E.stream;
+    HostStream rng{};
+    std::copy(E.keys.begin(), E.keys.begin() + 8, rng.key);
+    auto run_steps = [&](const std::vector<double>& temps, uint64_t k) -> ie_status {
+        if (k == 0) return IE_OK;
+        return E.run_pt(ladder_rows(E, temps.data(), 1).data(), k, false, 1);
+    };
+    // StepScratch::for_field: a fresh scratch starts in the even DEO phase
+    auto fresh_scratch = [&]() -> ie_status {
+        IE_CUDA(cudaMemsetAsync(E.d_deo.p, 0, sizeof(int32_t), st));
+        return IE_OK;
+    };
+
+    // ladder shape alpha_t in log-temperature space, tuned on a throwaway field
+    const double denom = (double)std::max<uint32_t>(L - 1, 1);
+    std::vector<double> alphas(L), temps(L);
+    for (uint32_t t = 0; t < L; t++) alphas[t] = (double)t / denom;
+    if (L >= 3 && pc->ladder_tuning_iters > 0 && pc->ladder_tuning_steps > 0) {
+        IE_TRY(E.init_random());
+        IE_TRY(fresh_scratch());
+        std::vector<uint64_t> att(L - 1), acc(L - 1);
+        std::vector<double> rates(L - 1), sp(L - 1);
+        for (uint32_t it = 0; it < pc->ladder_tuning_iters; it++) {
+            for (uint32_t t = 0; t < L; t++) temps[t] = tmax * std::pow(tmin / tmax, alphas[t]);
+            IE_CUDA(cudaMemsetAsync(E.d_att.p, 0, (L - 1) * sizeof(uint64_t), st));
+            IE_CUDA(cudaMemsetAsync(E.d_acc.p, 0, (L - 1) * sizeof(uint64_t), st));
+            IE_TRY(run_steps(temps, pc->ladder_tuning_steps));
+            IE_CUDA(cudaMemcpyAsync(att.data(), E.d_att.p, (L - 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+            IE_CUDA(cudaMemcpyAsync(acc.data(), E.d_acc.p, (L - 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+            IE_CUDA(cudaStreamSynchronize(st));
+            for (uint32_t t = 0; t + 1 < L; t++) {
+                rates[t] = att[t] == 0 ? 0.0 : (double)acc[t] / (double)att[t];
+                sp[t] = alphas[t + 1] - alphas[t];
+            }
+            const std::vector<double> ns = pa::adapt_spacings(sp.data(), rates.data(), L - 1);
+            double a = 0.0;
+            for (uint32_t t = 0; t + 1 < L; t++) {
+                a += ns[t];
+                alphas[t + 1] = a;
+            }
+            alphas[L - 1] = 1.0;
+        }
+    }
+
+    // production population
+    IE_TRY(E.init_random());
+    IE_TRY(fresh_scratch());
+    IE_TRY(h->d_inc_e.upload(std::vector<double>(1, std::numeric_limits<double>::infinity()), st));
+    const uint32_t n_words = (uint32_t)h->d_inc_state.n;
+    const uint64_t K = std::max<uint64_t>(h->cfg.total_exchanges, 1);
+    const double cold_factor = K > 1 ? std::pow(tmin / tmax, 1.0 / (double)(K - 1)) : 1.0;
+    std::vector<double> log_w(R, 0.0), en(E.total_energy), ess_hist, rho_hist;
+    std::vector<uint64_t> family(R), fam_hist;
+    for (uint32_t i = 0; i < R; i++) family[i] = i;
+    double free_energy = 0.0;
+    uint64_t resamples = 0;
+    bool have_prev = false;
+    double beta_prev = 0.0;
+    DevBuf<uint64_t> old_spins;
+    DevBuf<int32_t> old_ei;
+    DevBuf<double> old_ef;
+    DevBuf<uint32_t> d_parents;
+    for (uint64_t k = 0; k < K; k++) {
+        const double t_cold = K > 1 ? tmax * powi_rt(cold_factor, (int)k) : tmin;
+        const double span = t_cold / tmax;
+        for (uint32_t t = 0; t < L; t++) temps[t] = tmax * std::pow(span, alphas[t]);
+        const double beta_cold = 1.0 / t_cold;
+        if (have_prev) {
+            IE_TRY(E.read_energies(en.data()));
+            const double db = beta_cold - beta_prev;
+            for (uint32_t p = 0; p < pops; p++)
+                for (uint32_t r = 0; r < (uint32_t)kReplicas; r++)
+                    log_w[p * kReplicas + r] -= db * en[((size_t)(L - 1) + (size_t)L * p) * kReplicas + r];
+            const std::vector<double> w = pa::normalized_weights(log_w.data(), R);
+            const double ess = pa::effective_sample_size(w.data(), R);
+            ess_hist.push_back(ess);
+            if (ess < pc->ess_threshold * (double)R) {
+                free_energy += pa::free_energy_increment(log_w.data(), R);
+                IE_CUDA(cudaMemcpyAsync(&rng.pos, E.d_pos.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+                IE_CUDA(cudaStreamSynchronize(st));
+                const double u = rng.unit_f64();
+                const std::vector<uint64_t> counts = pa::systematic_resample(w.data(), R, u);
+                const std::vector<uint32_t> parents = pa::shuffled_parents(counts, rng);
+                IE_CUDA(cudaMemcpyAsync(E.d_pos.p, &rng.pos, sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+                IE_TRY(old_spins.alloc(words));
+                IE_CUDA(cudaMemcpyAsync(old_spins.p, E.d_spins.p, words * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+                if (mode == kModeInt) {
+                    IE_TRY(old_ei.alloc(E.total_energy));
+                    IE_CUDA(cudaMemcpyAsync(old_ei.p, E.d_Ei.p, E.total_energy * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+                } else {
+                    IE_TRY(old_ef.alloc(E.total_energy));
+                    IE_CUDA(cudaMemcpyAsync(old_ef.p, E.d_Ef.p, E.total_energy * sizeof(double), cudaMemcpyDeviceToDevice, st));
+                }
+                IE_TRY(d_parents.upload(parents, st));
+                IE_CUDA(launch_resample(E.arrays(), 0, mode, (uint32_t)words, L, d_parents.p, old_spins.p, old_ei.p,
+                                        old_ef.p, g_sm_count, st));
+                const std::vector<uint64_t> before = family;
+                for (uint32_t d = 0; d < R; d++) family[d] = before[parents[d]];
+                double rho = 0.0;
+                uint64_t nf = 0;
+                pa::family_entropy(family.data(), R, rho, nf);
+                rho_hist.push_back(rho);
+                fam_hist.push_back(nf);
+                resamples++;
+                std::fill(log_w.begin(), log_w.end(), 0.0);
+                IE_TRY(run_steps(temps, pc->post_resample_relaxation));
+            }
+        }
+        have_prev = true;
+        beta_prev = beta_cold;
+        IE_TRY(run_steps(temps, h->cfg.sweeps_per_exchange));
+        // exact re-sync of every level, then the stage's incumbent
+        IE_CUDA(launch_energy(E.arrays(), 0, 1, st));
+        IE_CUDA(launch_incumbent(E.arrays(), 0, h->offset, h->d_inc_e.p, h->d_inc_state.p, n_words, st));
+    }
+    IE_CUDA(cudaStreamSynchronize(st));
+    h->have_incumbent = true;
+    if (rep) {
+        rep->free_energy = free_energy;
+        rep->resample_events = resamples;
+        rep->n_ess = ess_hist.size();
+        const uint64_t ne = std::min<uint64_t>(rep->capacity, ess_hist.size());
+        const uint64_t nr = std::min<uint64_t>(rep->capacity, rho_hist.size());
+        if (rep->ess_history) std::copy(ess_hist.begin(), ess_hist.begin() + ne, rep->ess_history);
+        if (rep->family_rho) std::copy(rho_hist.begin(), rho_hist.begin() + nr, rep->family_rho);
+        if (rep->family_count) std::copy(fam_hist.begin(), fam_hist.begin() + nr, rep->family_count);
+        if (rep->alphas) std::copy(alphas.begin(), alphas.end(), rep->alphas);
+    }
     return IE_OK;
 }
 
@@ -1863,7 +2041,8 @@ ie_status ie_read_energies(ie_handle* h, double* energies) {
 ie_status ie_read_swap_stats(ie_handle* h, uint64_t* attempts, uint64_t* accepts) {
     if (!h || !attempts || !accepts) return fail(IE_ERR_INVALID, "NULL argument");
     IE_CUDA(cudaSetDevice(h->eng.device));
-    const uint32_t np = h->eng.nt > 1 ? h->eng.nt - 1 : 0;
+    const uint32_t L = h->eng.pop_len ? h->eng.pop_len : h->eng.nt;
+    const uint32_t np = L > 1 ? L - 1 : 0;
     if (np) {
         IE_CUDA(cudaMemcpy(attempts, h->eng.d_att.p, np * sizeof(uint64_t), cudaMemcpyDeviceToHost));
         IE_CUDA(cudaMemcpy(accepts, h->eng.d_acc.p, np * sizeof(uint64_t), cudaMemcpyDeviceToHost));

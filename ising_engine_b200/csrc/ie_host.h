@@ -31,6 +31,30 @@ struct XTables {
 };
 ie_status build_xtables(const double* temps, uint32_t nt, XTables& X);
 
+// The master stream on the host, addressed by draw index (same draws as the
+// device's chacha8_draw), with rand 0.8.5's gen_range forms the population
+// annealing driver takes.
+uint64_t chacha8_draw_host(const uint32_t key[8], uint64_t k);
+struct HostStream {
+    uint32_t key[8];
+    uint64_t pos;
+    uint64_t next_u64();
+    double unit_f64();                    // gen_range(0.0..1.0)
+    uint64_t index_inclusive(uint64_t hi);  // gen_range(0..=hi) for usize
+};
+
+namespace pa {
+std::vector<double> normalized_weights(const double* lw, size_t r);
+double effective_sample_size(const double* w, size_t r);
+double free_energy_increment(const double* lw, size_t r);
+void family_entropy(const uint64_t* ids, size_t r, double& rho, uint64_t& families);
+std::vector<uint64_t> systematic_resample(const double* w, size_t r, double u);
+std::vector<double> adapt_spacings(const double* d, const double* acc, size_t k);
+// apply_resample's parent list: parent i repeated counts[i] times, then the
+// Fisher-Yates shuffle with gen_range(0..=k) for k = len - 1 down to 1.
+std::vector<uint32_t> shuffled_parents(const std::vector<uint64_t>& counts, HostStream& rng);
+}  // namespace pa
+
 }  // namespace ie
 
 #define IE_CUDA(call)                                                                      \

@@ -1289,7 +1289,8 @@ template __global__ void pt_kernel<kModeF64>(DevArrays, RunArgs, uint32_t, int);
 // with draws from pos + steps on (ballots give each replica's draw position),
 // energies are swapped in place and each pair's swap mask (0 for pairs not
 // exchanged) goes to A.xmask for swap_kernel; the phase toggles. Otherwise
-// only the stream position advances.
+// only the stream position advances. With populations (RunArgs::pop_len) the
+// populations' pairs are decided in population order (engine.rs:714-716).
 // ---------------------------------------------------------------------------
 template <uint32_t MODE>
 __global__ void __launch_bounds__(32) exchange_kernel(DevArrays A, RunArgs R, uint32_t steps, uint32_t exchange) {
@@ -1320,52 +1321,59 @@ __global__ void __launch_bounds__(32) exchange_kernel(DevArrays A, RunArgs R, ui
     };
     if (exchange) {
         if (nt > 1) {
-            for (int t = tid; t + 1 < nt; t += 32)
-                if ((t & 1) != deo) A.xmask[d.stat + t] = 0;
-            const unsigned lt = (1u << tid) - 1u;
-            for (int t = deo; t + 1 < nt; t += 2) {
-                const double db = R.dbeta[t];
-                const double dea = __dsub_rn(energy(t, tid), energy(t + 1, tid));
-                const double deb = __dsub_rn(energy(t, tid + 32), energy(t + 1, tid + 32));
-                const double exa = __dmul_rn(db, dea);
-                const double exb = __dmul_rn(db, deb);
-                const bool na = exa < 0.0, nb = exb < 0.0;
-                const unsigned ma = __ballot_sync(0xffffffffu, na);
-                const unsigned mb = __ballot_sync(0xffffffffu, nb);
-                bool aa = !na, ab = !nb;
-                if (na) {
-                    const uint64_t m = chacha8_draw(key, p + __popc(ma & lt)) >> 11;
-                    if constexpr (MODE == kModeInt) {
-                        const uint64_t ad = (uint64_t)fabs(dea);
-                        const uint64_t th = ad <= R.xdmax[t] ? R.xtab[R.xoff[t] + ad - 1]
-                                                             : (ad <= R.xdund[t] ? 1ULL : 0ULL);
-                        aa = m < th;
-                    } else {
-                        aa = __dmul_rn((double)m, 1.1102230246251565e-16) < exp(exa);
-                    }
-                }
-                if (nb) {
-                    const uint64_t m = chacha8_draw(key, p + __popc(ma) + __popc(mb & lt)) >> 11;
-                    if constexpr (MODE == kModeInt) {
-                        const uint64_t ad = (uint64_t)fabs(deb);
-                        const uint64_t th = ad <= R.xdmax[t] ? R.xtab[R.xoff[t] + ad - 1]
-                                                             : (ad <= R.xdund[t] ? 1ULL : 0ULL);
-                        ab = m < th;
-                    } else {
-                        ab = __dmul_rn((double)m, 1.1102230246251565e-16) < exp(exb);
-                    }
-                }
-                p += (uint64_t)(__popc(ma) + __popc(mb));
-                const unsigned Aa = __ballot_sync(0xffffffffu, aa);
-                const unsigned Ab = __ballot_sync(0xffffffffu, ab);
-                if (aa) swap_energy(t, tid);
-                if (ab) swap_energy(t, tid + 32);
-                if (tid == 0) {
-                    A.xmask[d.stat + t] = (uint64_t)Aa | ((uint64_t)Ab << 32);
-                    A.att[d.stat + t] += kReplicas;
-                    A.acc[d.stat + t] += (uint64_t)(__popc(Aa) + __popc(Ab));
-                }
+            // L cells per population; pairs (c, c + 1) with c = t + L * q
+            const int L = R.pop_len ? (int)R.pop_len : nt;
+            const int pops = nt / L;
+            for (int c = tid; c + 1 < nt; c += 32) {
+                const int t = c % L;
+                if ((t & 1) != deo || t + 1 >= L) A.xmask[d.stat + c] = 0;
             }
+            const unsigned lt = (1u << tid) - 1u;
+            for (int q = 0; q < pops; q++)
+                for (int t = deo; t + 1 < L; t += 2) {
+                    const int c = t + L * q;
+                    const double db = R.dbeta[t];
+                    const double dea = __dsub_rn(energy(c, tid), energy(c + 1, tid));
+                    const double deb = __dsub_rn(energy(c, tid + 32), energy(c + 1, tid + 32));
+                    const double exa = __dmul_rn(db, dea);
+                    const double exb = __dmul_rn(db, deb);
+                    const bool na = exa < 0.0, nb = exb < 0.0;
+                    const unsigned ma = __ballot_sync(0xffffffffu, na);
+                    const unsigned mb = __ballot_sync(0xffffffffu, nb);
+                    bool aa = !na, ab = !nb;
+                    if (na) {
+                        const uint64_t m = chacha8_draw(key, p + __popc(ma & lt)) >> 11;
+                        if constexpr (MODE == kModeInt) {
+                            const uint64_t ad = (uint64_t)fabs(dea);
+                            const uint64_t th = ad <= R.xdmax[t] ? R.xtab[R.xoff[t] + ad - 1]
+                                                                 : (ad <= R.xdund[t] ? 1ULL : 0ULL);
+                            aa = m < th;
+                        } else {
+                            aa = __dmul_rn((double)m, 1.1102230246251565e-16) < exp(exa);
+                        }
+                    }
+                    if (nb) {
+                        const uint64_t m = chacha8_draw(key, p + __popc(ma) + __popc(mb & lt)) >> 11;
+                        if constexpr (MODE == kModeInt) {
+                            const uint64_t ad = (uint64_t)fabs(deb);
+                            const uint64_t th = ad <= R.xdmax[t] ? R.xtab[R.xoff[t] + ad - 1]
+                                                                 : (ad <= R.xdund[t] ? 1ULL : 0ULL);
+                            ab = m < th;
+                        } else {
+                            ab = __dmul_rn((double)m, 1.1102230246251565e-16) < exp(exb);
+                        }
+                    }
+                    p += (uint64_t)(__popc(ma) + __popc(mb));
+                    const unsigned Aa = __ballot_sync(0xffffffffu, aa);
+                    const unsigned Ab = __ballot_sync(0xffffffffu, ab);
+                    if (aa) swap_energy(c, tid);
+                    if (ab) swap_energy(c, tid + 32);
+                    if (tid == 0) {
+                        A.xmask[d.stat + c] = (uint64_t)Aa | ((uint64_t)Ab << 32);
+                        A.att[d.stat + t] += kReplicas;
+                        A.acc[d.stat + t] += (uint64_t)(__popc(Aa) + __popc(Ab));
+                    }
+                }
         }
         deo ^= 1;
     }
@@ -1396,6 +1404,40 @@ __global__ void swap_kernel(DevArrays A, uint32_t inst) {
             w1[v] = a ^ dd;
             w2[v] = b ^ dd;
         }
+    }
+}
+
+// apply_resample (population_annealing.rs:240-287) on the device: member
+// (population q, replica r) of every level takes the configuration and tracked
+// energies of member parents[64 q + r], read from copies taken before.
+// Replica r sits at bit 8 (r % 8) + r / 8 of a lane-major spin word.
+template <uint32_t MODE>
+__global__ void resample_kernel(DevArrays A, uint32_t inst, uint32_t pop_len, const uint32_t* parents,
+                                const uint64_t* old_spins, const int32_t* old_ei, const double* old_ef) {
+    const InstDesc d = A.desc[inst];
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t words = (size_t)d.nt * d.n;
+    auto bitpos = [](uint32_t r) { return ((r & 7u) << 3) | (r >> 3); };
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) {
+        const uint32_t c = (uint32_t)(i / d.n), v = (uint32_t)(i % d.n);
+        const uint32_t t = c % pop_len, q = c / pop_len;
+        uint64_t w = 0;
+        for (uint32_t r = 0; r < (uint32_t)kReplicas; r++) {
+            const uint32_t src = parents[q * kReplicas + r];
+            const uint32_t sq = src / kReplicas, sr = src % kReplicas;
+            const uint64_t sw = old_spins[(size_t)(t + pop_len * sq) * d.n + v];
+            w |= ((sw >> bitpos(sr)) & 1ull) << bitpos(r);
+        }
+        A.spins[d.spin + i] = w;
+    }
+    const size_t ne = (size_t)d.nt * kReplicas;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += stride) {
+        const uint32_t c = (uint32_t)(i / kReplicas), r = (uint32_t)(i % kReplicas);
+        const uint32_t t = c % pop_len, q = c / pop_len;
+        const uint32_t src = parents[q * kReplicas + r];
+        const size_t o = (size_t)(t + pop_len * (src / kReplicas)) * kReplicas + src % kReplicas;
+        if constexpr (MODE == kModeInt) A.Ei[d.energy + i] = old_ei[o];
+        else A.Ef[d.energy + i] = old_ef[o];
     }
 }
 
@@ -1875,6 +1917,15 @@ cudaError_t launch_exchange(const DevArrays& A, const RunArgs& R, uint32_t ninst
 cudaError_t launch_swap(const DevArrays& A, uint32_t inst, uint32_t n_words, int sm_count, cudaStream_t st) {
     const int grid = (int)std::min<uint32_t>((n_words + 255) / 256, (uint32_t)(4 * sm_count));
     swap_kernel<<<std::max(grid, 1), 256, 0, st>>>(A, inst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_resample(const DevArrays& A, uint32_t inst, uint32_t mode, uint32_t n_words, uint32_t pop_len,
+                            const uint32_t* parents, const uint64_t* old_spins, const int32_t* old_ei,
+                            const double* old_ef, int sm_count, cudaStream_t st) {
+    const int grid = std::max(1, (int)std::min<uint32_t>((n_words + 255) / 256, (uint32_t)(4 * sm_count)));
+    if (mode == kModeInt) resample_kernel<kModeInt><<<grid, 256, 0, st>>>(A, inst, pop_len, parents, old_spins, old_ei, old_ef);
+    else resample_kernel<kModeF64><<<grid, 256, 0, st>>>(A, inst, pop_len, parents, old_spins, old_ei, old_ef);
     return cudaGetLastError();
 }
 

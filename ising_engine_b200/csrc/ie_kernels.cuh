@@ -113,6 +113,11 @@ struct RunArgs {
     // DEO phase and f64 resync to the exchange step (exchange_kernel)
     uint32_t cells;
     uint32_t ladder;
+    // populations (PA-PT): when nonzero, an instance's cells are populations
+    // of pop_len consecutive cells (cell t + pop_len * p); the exchange pairs
+    // stay inside a population and the exchange tables, dbeta and swap
+    // statistics are indexed by the pair t within it
+    uint32_t pop_len;
     // when set, the launch's step_base is read from device memory (so a
     // captured CUDA graph of the launch stays valid across runs)
     const uint64_t* step_base_dev;

@@ -19,6 +19,9 @@ cudaError_t launch_chain(const DevArrays& A, const RunArgs& R, uint32_t mode, ui
 cudaError_t launch_exchange(const DevArrays& A, const RunArgs& R, uint32_t ninst, uint32_t mode, uint32_t steps,
                             bool exchange, cudaStream_t st);
 cudaError_t launch_swap(const DevArrays& A, uint32_t inst, uint32_t n_words, int sm_count, cudaStream_t st);
+cudaError_t launch_resample(const DevArrays& A, uint32_t inst, uint32_t mode, uint32_t n_words, uint32_t pop_len,
+                            const uint32_t* parents, const uint64_t* old_spins, const int32_t* old_ei,
+                            const double* old_ef, int sm_count, cudaStream_t st);
 cudaError_t launch_pt(const DevArrays& A, const RunArgs& R, uint32_t inst0, uint32_t ninst, uint32_t mode,
                       int block, int tab_stride, size_t smem, cudaStream_t st);
 cudaError_t launch_init(const DevArrays& A, uint32_t inst0, uint32_t ninst, const uint32_t* draw_idx,

@@ -1,6 +1,7 @@
 // engine_v2 (S2) state backend on the device: the integer bit-sliced state of
 // src/engine_v2/backends/sparse_bitslice.rs:19-346 with the MetropolisSweep
-// (src/engine_v2/operators/metropolis_sweep.rs:95-146) and ReplicaExchange
+// (src/engine_v2/operators/metropolis_sweep.rs:95-146), GibbsColorSweep
+// (src/engine_v2/operators/gibbs_color_sweep.rs:119-165) and ReplicaExchange
 // (src/engine_v2/operators/replica_exchange.rs:61-110) operators, behind the
 // per-sweep seam ie_v2_* of include/ising_b200.h.
 //
@@ -114,6 +115,121 @@ __global__ void __launch_bounds__(128) v2_metropolis_color(V2Dev D, Key key, uin
     if (lane == 0 && acc_count) atomicAdd(D.counter, acc_count);
 }
 
+// GibbsColorSweep thresholds of one temperature: P(x = 1) = 1 / (1 + exp(b h))
+// as ceil(P * 2^53) for integer fields h, so that u < P <=> (draw >> 11) < T.
+struct GParam {
+    int64_t lo;      // field of tab entry 0
+    uint64_t off;    // first entry in the table
+    uint64_t len;    // entries
+    uint64_t below;  // T for h < lo
+    uint64_t above;  // T for lo + len <= h <= und
+    int64_t und;     // h > und: P == 0, T == 0
+};
+
+__device__ __forceinline__ uint64_t gibbs_threshold(const GParam& P, const uint64_t* tab, int32_t h) {
+    const int64_t rel = (int64_t)h - P.lo;
+    if (rel < 0) return P.below;
+    if ((uint64_t)rel < P.len) return tab[P.off + rel];
+    return h <= P.und ? P.above : 0ull;
+}
+
+// One colour of one Gibbs sweep, same decomposition as v2_metropolis_color:
+// replica's new spin is 1 iff its draw is below the threshold of its field.
+__global__ void __launch_bounds__(128) v2_gibbs_color(V2Dev D, const GParam* gp, const uint64_t* gtab, Key key,
+                                                      uint32_t p_begin, uint32_t p_end, uint64_t draw0) {
+    const uint32_t g = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t rep = g * 32 + lane;
+    const bool valid = rep < D.r;
+    const uint32_t* planes = reinterpret_cast<const uint32_t*>(D.spins);
+    uint32_t* own = reinterpret_cast<uint32_t*>(D.spins);
+    GParam P = gp[valid ? rep % D.n_temps : 0];
+    constexpr uint64_t kOne = 1ull << 53;
+    long long eacc = 0;
+    unsigned long long acc_count = 0;
+    for (uint32_t p = p_begin + warp; p < p_end; p += nwarps) {
+        const uint32_t site = D.order[p];
+        int32_t h = D.lin[site];
+        const uint32_t e1 = D.row[site + 1];
+        for (uint32_t e = D.row[site]; e < e1; e++) {
+            const uint32_t word = planes[(size_t)D.col[e] * D.w2 + g];
+            h += ((word >> lane) & 1u) ? D.wt[e] : 0;
+        }
+        const uint32_t ownw = planes[(size_t)site * D.w2 + g];
+        const bool x = (ownw >> lane) & 1u;
+        bool flip = false;
+        if (valid) {
+            const uint64_t th = gibbs_threshold(P, gtab, h);
+            // u < 1 always: T == 2^53 needs no draw, nor T == 0
+            const bool one = th >= kOne ? true
+                             : (th == 0 ? false : (chacha8_draw(key.k, draw0 + (uint64_t)p * D.r + rep) >> 11) < th);
+            flip = one != x;
+        }
+        const uint32_t mask = __ballot_sync(0xffffffffu, flip);
+        if (lane == 0) {
+            own[(size_t)site * D.w2 + g] = ownw ^ mask;
+            acc_count += __popc(mask);
+        }
+        if (flip) eacc += x ? -h : h;
+    }
+    if (valid && eacc) atomicAdd(D.energies + rep, (unsigned long long)eacc);
+    if (lane == 0 && acc_count) atomicAdd(D.counter, acc_count);
+}
+
+// Host tables for v2_gibbs_color. For t > 0 the fields |h| <= 40 t + 1 are
+// tabulated with libm exp (the reference's function); beyond, exp(h / t) is
+// below 2^-54 (P rounds to 1, T = 2^53) or above 2^57 (0 < P < 2^-53, T = 1)
+// until exp overflows (P = 0). t <= 0 or NaN: bh = sign(h) * inf, the
+// reference's greedy limit (P = 0, 1/2, 1); t = +inf: bh = 0, P = 1/2.
+ie_status gibbs_tables(const double* temps, uint32_t nt, int64_t hb, std::vector<GParam>& P,
+                       std::vector<uint64_t>& tab) {
+    constexpr uint64_t kOne = 1ull << 53;
+    P.assign(nt, GParam{});
+    tab.clear();
+    for (uint32_t ti = 0; ti < nt; ti++) {
+        const double t = temps[ti];
+        GParam& g = P[ti];
+        g.off = tab.size();
+        if (!(t > 0.0)) {
+            g.lo = 0;
+            g.len = 1;
+            tab.push_back(kOne / 2);
+            g.below = kOne;
+            g.above = 0;
+            g.und = 0;
+            continue;
+        }
+        if (std::isinf(t)) {
+            g.lo = hb + 1;
+            g.len = 0;
+            g.below = kOne / 2;
+            g.above = 0;
+            g.und = hb;
+            continue;
+        }
+        const double m = std::ceil(40.0 * t) + 1.0;
+        const int64_t hi = m >= (double)hb ? hb : (int64_t)m;
+        g.lo = -hi;
+        g.len = (uint64_t)(2 * hi + 1);
+        if (tab.size() + g.len > (1u << 24)) return fail(IE_ERR_UNSUPPORTED, "temperatures too high for the threshold tables");
+        for (int64_t h = -hi; h <= hi; h++)
+            tab.push_back((uint64_t)std::ceil(std::ldexp(1.0 / (1.0 + std::exp((double)h / t)), 53)));
+        g.below = kOne;
+        g.above = 1;
+        int64_t a = hi, b = hb + 1;  // largest h <= hb with exp(h / t) finite
+        if (std::isinf(std::exp((double)hi / t))) b = hi + 1;
+        while (b - a > 1) {
+            const int64_t mid = a + (b - a) / 2;
+            if (std::isfinite(std::exp((double)mid / t))) a = mid;
+            else b = mid;
+        }
+        g.und = a;
+    }
+    return IE_OK;
+}
+
 // One exchange round's decisions: pairs (k, k+1), k = start, start + 2, ...;
 // pair p takes draw draw0 + p. Energies of swapped pairs are exchanged and
 // the pair's bit set in pmask for v2_swap_pairs.
@@ -200,6 +316,8 @@ struct ie_v2 {
     DevBuf<int32_t> d_wt, d_lin;
     DevBuf<uint64_t> d_spins, d_thr, d_thr_off, d_thr_max, d_thr_und, d_xtab, d_xoff, d_xdmax, d_xdund, d_pmask;
     DevBuf<double> d_dbeta;
+    DevBuf<GParam> d_gp;
+    DevBuf<uint64_t> d_gtab;
     DevBuf<unsigned long long> d_E, d_cnt;
 
     ~ie_v2() {
@@ -387,6 +505,40 @@ struct ie_v2 {
         return IE_OK;
     }
 
+    ie_status gibbs(const double* temps, uint32_t nt, uint64_t sweeps, uint64_t seed, uint64_t draw_offset,
+                    uint64_t* proposed, uint64_t* accepted) {
+        if (!temps || nt == 0) return fail(IE_ERR_INVALID, "GibbsColorSweep needs a temperature");
+        std::vector<GParam> gp;
+        std::vector<uint64_t> gtab;
+        IE_TRY(gibbs_tables(temps, nt, hbound, gp, gtab));
+        IE_CUDA(cudaSetDevice(device));
+        IE_TRY(d_gp.upload(gp, stream));
+        IE_TRY(d_gtab.upload(gtab.empty() ? std::vector<uint64_t>(1, 0) : gtab, stream));
+        IE_CUDA(cudaMemsetAsync(d_cnt.p, 0, sizeof(unsigned long long), stream));
+        Key key;
+        chacha_key_from_u64(seed, key.k);
+        V2Dev D = dev();
+        D.n_temps = nt;
+        const uint32_t ng = (r + 31) / 32;
+        if (ng > 65535) return fail(IE_ERR_UNSUPPORTED, "too many replicas");
+        for (uint64_t sw = 0; sw < sweeps; sw++) {
+            const uint64_t draw0 = draw_offset + sw * (uint64_t)n * r;
+            for (size_t c = 0; c + 1 < color_off.size(); c++) {
+                const uint32_t cnt = color_off[c + 1] - color_off[c];
+                const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((cnt + 3) / 4, 1184 / ng + 1));
+                v2_gibbs_color<<<dim3(blocks, ng), 128, 0, stream>>>(D, d_gp.p, d_gtab.p, key, color_off[c],
+                                                                    color_off[c + 1], draw0);
+                IE_CUDA(cudaGetLastError());
+            }
+        }
+        unsigned long long a = 0;
+        IE_CUDA(cudaMemcpyAsync(&a, d_cnt.p, sizeof(a), cudaMemcpyDeviceToHost, stream));
+        IE_CUDA(cudaStreamSynchronize(stream));
+        if (proposed) *proposed = sweeps * (uint64_t)n * r;
+        if (accepted) *accepted = a;
+        return IE_OK;
+    }
+
     ie_status exchange(const double* temps, uint32_t nt, uint64_t rounds, uint64_t seed, uint64_t draw_offset,
                        uint64_t* proposed, uint64_t* accepted) {
         if (proposed) *proposed = 0;
@@ -475,6 +627,12 @@ ie_status ie_v2_metropolis(ie_v2* h, const double* temps, uint32_t n_temps, uint
                            uint64_t draw_offset, uint64_t* proposed, uint64_t* accepted) {
     if (!h) return fail(IE_ERR_INVALID, "handle is NULL");
     return h->metropolis(temps, n_temps, sweeps, seed, draw_offset, proposed, accepted);
+}
+
+ie_status ie_v2_gibbs(ie_v2* h, const double* temps, uint32_t n_temps, uint64_t sweeps, uint64_t seed,
+                      uint64_t draw_offset, uint64_t* proposed, uint64_t* accepted) {
+    if (!h) return fail(IE_ERR_INVALID, "handle is NULL");
+    return h->gibbs(temps, n_temps, sweeps, seed, draw_offset, proposed, accepted);
 }
 
 ie_status ie_v2_exchange(ie_v2* h, const double* temps, uint32_t n_temps, uint64_t rounds, uint64_t seed,

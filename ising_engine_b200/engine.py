@@ -36,20 +36,23 @@ def _p(a: np.ndarray):
 
 
 class Engine:
-    """One problem, ``num_temps`` cells x 64 replicas, resident on the device."""
+    """One problem, ``num_temps`` x ``num_pops`` cells x 64 replicas, resident
+    on the device (cell t + num_temps * p)."""
 
     def __init__(self, model: QuboModel, num_temps: int = 10, seed: int = 0,
                  exchange_interval: int = 1, temp_max: float = 1.0, temp_min: float = 0.1,
                  sweeps_per_exchange: int = 1, total_exchanges: int = 1, force_f64: bool = False,
-                 device: int = 0, pt_path: int = 0):
+                 device: int = 0, pt_path: int = 0, num_pops: int = 1):
         self._L = _ffi.lib()
         self.model = model
         self.num_temps = int(num_temps)
+        self.num_pops = int(num_pops)
+        self.cells = self.num_temps * self.num_pops  # cell t + num_temps * p
         self.n = model.num_vars
         keep: list = []
         prob = _problem(model, keep)
         cfg = _ffi.ie_config(temp_max, temp_min, sweeps_per_exchange, total_exchanges,
-                             seed & 0xFFFFFFFFFFFFFFFF, self.num_temps, 1, 1, exchange_interval,
+                             seed & 0xFFFFFFFFFFFFFFFF, self.num_temps, self.num_pops, 1, exchange_interval,
                              int(force_f64), device, pt_path)
         h = C.c_void_p()
         _ffi.check(self._L.ie_create(C.byref(prob), C.byref(cfg), C.byref(h)))
@@ -85,8 +88,8 @@ class Engine:
 
     def set_spins(self, words) -> None:
         w = np.ascontiguousarray(words, dtype=np.uint64).reshape(-1)
-        if w.size != self.num_temps * self.n:
-            raise ValueError("words must have num_temps * num_vars entries")
+        if w.size != self.cells * self.n:
+            raise ValueError("words must have num_temps * num_pops * num_vars entries")
         _ffi.check(self._L.ie_set_spins(self._h, _p(w)))
 
     def step(self, temps, n_steps: int = 1) -> None:
@@ -102,13 +105,32 @@ class Engine:
     def run_pt(self) -> None:
         _ffi.check(self._L.ie_run_pt(self._h))
 
+    def run_pa(self, config=None):
+        """Population annealing with PT equilibration (ultimate.rs:576-852) on a
+        handle with num_pops > 1, from a fresh master stream; returns the
+        ``PaDiagnostics``. ``best`` and ``one_opt`` finish the solve."""
+        from .population_annealing import PaConfig, PaDiagnostics
+        cfg = (config or PaConfig()).to_c()
+        cap = 1 << 16
+        ess = np.zeros(cap, dtype=np.float64)
+        rho = np.zeros(cap, dtype=np.float64)
+        fam = np.zeros(cap, dtype=np.uint64)
+        alphas = np.zeros(self.num_temps, dtype=np.float64)
+        rep = _ffi.ie_pa_report(0.0, 0, 0, ess.ctypes.data, rho.ctypes.data, fam.ctypes.data, cap,
+                                alphas.ctypes.data)
+        _ffi.check(self._L.ie_run_pa(self._h, C.byref(cfg), C.byref(rep)))
+        ne = min(int(rep.n_ess), cap)
+        nr = min(int(rep.resample_events), cap)
+        return PaDiagnostics(rep.free_energy, ess[:ne].tolist(),
+                             [(float(rho[i]), int(fam[i])) for i in range(nr)], int(rep.resample_events), alphas)
+
     def spins(self) -> np.ndarray:
-        w = np.zeros((self.num_temps, self.n), dtype=np.uint64)
+        w = np.zeros((self.cells, self.n), dtype=np.uint64)
         _ffi.check(self._L.ie_read_spins(self._h, _p(w)))
         return w
 
     def energies(self) -> np.ndarray:
-        e = np.zeros((self.num_temps, NUM_REPLICAS), dtype=np.float64)
+        e = np.zeros((self.cells, NUM_REPLICAS), dtype=np.float64)
         _ffi.check(self._L.ie_read_energies(self._h, _p(e)))
         return e
 

@@ -6,8 +6,10 @@ total_exchanges x sweeps_per_exchange calls of engine::step with energy
 resync every 1000 steps, update_incumbent after every exchange block, best
 replica extraction, then the 1-opt polish of src/solver/local_search.rs:19-57.
 
-Presolve and component decomposition (ultimate.rs:161-218) are host-side
-reductions before this path; ``solve`` accepts their result as clamps.
+With num_pops > 1 the solve is population annealing with PT equilibration
+(ultimate.rs:576-852, run by ``Engine.run_pa``). Presolve and component
+decomposition (ultimate.rs:161-218) are host-side reductions before either
+path; ``solve`` accepts their result as clamps.
 """
 from __future__ import annotations
 
@@ -54,8 +56,9 @@ def steepest_descent_1opt(model: QuboModel, state, is_clamped=None) -> float:
 
 
 class UltimateSolver:
-    """Configuration of the reference's UltimateSolver (ultimate.rs:18-57) for
-    the PT path: num_pops = num_slices = 1."""
+    """Configuration of the reference's UltimateSolver (ultimate.rs:18-87):
+    the PT path (num_pops = 1) and population annealing with PT
+    equilibration (num_pops > 1, ultimate.rs:576-852); num_slices = 1."""
 
     def __init__(self, temp_max: float, temp_min: float, sweeps: int, exchanges: int,
                  seed: int | None, num_temps: int = 10, exchange_interval: int = 1,
@@ -71,31 +74,64 @@ class UltimateSolver:
         self.num_pops = 1
         self.exchange_interval = int(exchange_interval)
         self.device = device
+        # population-annealing knobs (ultimate.rs:29-52, defaults :77-86)
+        self.ess_threshold = 0.5
+        self.ladder_tuning_iters = 8
+        self.ladder_tuning_steps = 10
+        self.post_resample_relaxation = 5
 
     @staticmethod
     def new(temp_max, temp_min, sweeps, exchanges, seed):
         return UltimateSolver(temp_max, temp_min, sweeps, exchanges, seed)
 
     def with_quantum_dims(self, slices: int, temps: int, pops: int) -> "UltimateSolver":
-        if slices != 1 or pops != 1:
-            raise NotImplementedError("only num_slices = num_pops = 1 is on the device path")
+        """ultimate.rs:126-131."""
+        if slices != 1:
+            raise NotImplementedError("only num_slices = 1 is on the device path")
         self.num_temps = int(temps)
+        self.num_pops = int(pops)
         return self
 
-    def engine(self, model: QuboModel) -> Engine:
+    def pa_config(self):
+        from .population_annealing import PaConfig
+        return PaConfig(self.ess_threshold, self.ladder_tuning_iters, self.ladder_tuning_steps,
+                        self.post_resample_relaxation)
+
+    def engine(self, model: QuboModel, num_pops: int | None = None) -> Engine:
         return Engine(model, num_temps=self.num_temps, seed=self.seed,
                       exchange_interval=self.exchange_interval, temp_max=self.temp_max,
                       temp_min=self.temp_min, sweeps_per_exchange=self.sweeps_per_exchange,
-                      total_exchanges=self.total_exchanges, device=self.device)
+                      total_exchanges=self.total_exchanges, device=self.device,
+                      num_pops=self.num_pops if num_pops is None else num_pops)
 
-    def solve(self, model: QuboModel, clamped=()) -> np.ndarray:
-        """PT path of UltimateSolver::solve for `model` with `clamped` fixings."""
+    def _clamps(self, model: QuboModel, clamped):
         n = model.num_vars
         is_clamped = np.zeros(n, dtype=np.uint8)
         cval = np.zeros(n, dtype=np.int8)
         for idx, val in clamped:
             is_clamped[idx] = 1
             cval[idx] = val
+        return is_clamped, cval
+
+    def solve_with_pa_diagnostics(self, model: QuboModel, clamped=()):
+        """ultimate.rs:858-890: population annealing with num_pops >= 2 (no
+        presolve), then best extraction and 1-opt (ultimate.rs:806-845);
+        returns (state, PaDiagnostics)."""
+        is_clamped, cval = self._clamps(model, clamped)
+        with self.engine(model, num_pops=max(self.num_pops, 2)) as eng:
+            if len(clamped):
+                eng.set_clamps(is_clamped, cval)
+            diag = eng.run_pa(self.pa_config())
+            _, best = eng.best()
+            eng.one_opt(best, is_clamped)
+        return best, diag
+
+    def solve(self, model: QuboModel, clamped=()) -> np.ndarray:
+        """UltimateSolver::solve for `model` with `clamped` fixings: the PT
+        path, or population annealing when num_pops > 1 (ultimate.rs:220-232)."""
+        if self.num_pops > 1:
+            return self.solve_with_pa_diagnostics(model, clamped)[0]
+        is_clamped, cval = self._clamps(model, clamped)
         with self.engine(model) as eng:
             if len(clamped):
                 eng.set_clamps(is_clamped, cval)

@@ -5,7 +5,8 @@ Mirrors the reference's S2 seam: ``ProblemIR`` (src/engine_v2/ir.rs:14-148),
 the ``SpinState`` queries of the bit-sliced backend
 (src/engine_v2/backends/sparse_bitslice.rs:238-347) and ``Operator::apply``
 (src/engine_v2/operator.rs:72-86) of ``MetropolisSweep``
-(src/engine_v2/operators/metropolis_sweep.rs:95-146) and ``ReplicaExchange``
+(src/engine_v2/operators/metropolis_sweep.rs:95-146), ``GibbsColorSweep``
+(src/engine_v2/operators/gibbs_color_sweep.rs:119-165) and ``ReplicaExchange``
 (src/engine_v2/operators/replica_exchange.rs:61-110). The operators' shared
 ``ChaCha8Rng`` is a ``ChaChaStream``: its seed and the number of 64-bit draws
 consumed so far; each apply advances it by exactly the draws the reference's
@@ -188,6 +189,20 @@ class MetropolisSweep:
         p, a = C.c_uint64(), C.c_uint64()
         _ffi.check(state._L.ie_v2_metropolis(state._h, _p(t), len(t), int(sweeps), rng.seed & 0xFFFFFFFFFFFFFFFF,
                                              rng.position, C.byref(p), C.byref(a)))
+        rng.position += p.value
+        return Report(p.value, a.value, float(state.ir.n * state.r * sweeps))
+
+
+class GibbsColorSweep:
+    """gibbs_color_sweep.rs:119-165 on the device: heat-bath resampling, one
+    draw per (site, replica) in chromatic order; T <= 0 is the greedy limit."""
+    NAME = "gibbs_color_sweep"
+
+    def apply(self, state: GpuBitSlice, temperatures, rng: ChaChaStream, sweeps: int) -> Report:
+        t = np.ascontiguousarray(temperatures, dtype=np.float64)
+        p, a = C.c_uint64(), C.c_uint64()
+        _ffi.check(state._L.ie_v2_gibbs(state._h, _p(t), len(t), int(sweeps), rng.seed & 0xFFFFFFFFFFFFFFFF,
+                                        rng.position, C.byref(p), C.byref(a)))
         rng.position += p.value
         return Report(p.value, a.value, float(state.ir.n * state.r * sweeps))
 

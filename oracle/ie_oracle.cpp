@@ -21,6 +21,7 @@
 #include <deque>
 #include <functional>
 #include <limits>
+#include <map>
 #include <thread>
 #include <vector>
 
@@ -905,6 +906,267 @@ static std::vector<int8_t> solve(const Qubo& m, const Assign& clamped, const Sol
     return best;
 }
 
+// ---------------------------------------------------------------------------
+// Population annealing with PT equilibration (num_pops > 1):
+// src/solver/population_annealing.rs:51-287 (weights, ESS, free energy,
+// family entropy, systematic resampling, spacing adaptation, apply_resample)
+// and UltimateSolver::solve_population_annealing_diag (ultimate.rs:576-852)
+// in its defaults: acceptance-uniform ladder tuning, ICM, GNN warm start and
+// 2-opt off. Entered as solve_with_pa_diagnostics does (ultimate.rs:858-890):
+// no presolve or decomposition.
+// ---------------------------------------------------------------------------
+
+// rand 0.8.5 UniformInt<usize>::sample_single_inclusive (gen_range(0..=hi) on
+// a 64-bit target): range = hi + 1, zone = (range << lz(range)) - 1; draws
+// u64 v until the low half of the 128-bit v * range is <= zone and returns
+// the high half.
+static uint64_t gen_index_inclusive(ChaCha8Rng& rng, uint64_t hi) {
+    const uint64_t range = hi + 1;
+    if (range == 0) return rng.next_u64();
+    const uint64_t zone = (range << __builtin_clzll(range)) - 1;
+    for (;;) {
+        const unsigned __int128 m = (unsigned __int128)rng.next_u64() * range;
+        if ((uint64_t)m <= zone) return (uint64_t)(m >> 64);
+    }
+}
+
+// population_annealing.rs:51-56
+static std::vector<double> pa_normalized_weights(const std::vector<double>& lw) {
+    double m = -std::numeric_limits<double>::infinity();
+    for (double x : lw) m = std::max(m, x);
+    std::vector<double> e(lw.size());
+    double z = 0.0;
+    for (size_t i = 0; i < lw.size(); i++) {
+        e[i] = std::exp(lw[i] - m);
+        z += e[i];
+    }
+    for (double& x : e) x /= z;
+    return e;
+}
+
+// population_annealing.rs:60-63
+static double pa_ess(const std::vector<double>& w) {
+    double s2 = 0.0;
+    for (double x : w) s2 += x * x;
+    return 1.0 / s2;
+}
+
+// population_annealing.rs:70-78
+static double pa_free_energy_increment(const std::vector<double>& lw) {
+    const double r = (double)lw.size();
+    double m = -std::numeric_limits<double>::infinity();
+    for (double x : lw) m = std::max(m, x);
+    if (!std::isfinite(m)) return 0.0;
+    double s = 0.0;
+    for (double x : lw) s += std::exp(x - m);
+    return m + std::log(s) - std::log(r);
+}
+
+// population_annealing.rs:84-101; families summed in ascending id order (the
+// reference sums in its hash map's order, which is unspecified).
+static std::pair<double, int64_t> pa_family_entropy(const std::vector<int64_t>& ids) {
+    if (ids.empty()) return {0.0, 0};
+    std::map<int64_t, int64_t> cnt;
+    for (int64_t f : ids) cnt[f]++;
+    const double r = (double)ids.size();
+    double rho = 0.0;
+    for (auto& kv : cnt) {
+        const double frac = (double)kv.second / r;
+        rho += frac * frac;
+    }
+    return {rho * r, (int64_t)cnt.size()};
+}
+
+// population_annealing.rs:106-127
+static std::vector<int64_t> pa_systematic_resample(const std::vector<double>& w, double u) {
+    const size_t R = w.size();
+    std::vector<int64_t> counts(R, 0);
+    double cum = 0.0;
+    size_t j = 0;
+    for (size_t i = 0; i < R; i++) {
+        cum += w[i];
+        while (j < R && (((double)j + u) / (double)R) < cum) {
+            counts[i]++;
+            j++;
+        }
+    }
+    if (j < R) counts[R - 1] += (int64_t)(R - j);
+    return counts;
+}
+
+// population_annealing.rs:141-152
+static std::vector<double> pa_adapt_spacings(const std::vector<double>& d, const std::vector<double>& a) {
+    std::vector<double> raw(d.size());
+    double old_total = 0.0, new_total = 0.0;
+    for (size_t k = 0; k < d.size(); k++) raw[k] = d[k] * std::sqrt(std::max(a[k], 0.02));
+    for (double x : d) old_total += x;
+    for (double x : raw) new_total += x;
+    for (double& x : raw) x = x * old_total / new_total;
+    return raw;
+}
+
+// population_annealing.rs:240-287: parents per offspring slot, Fisher-Yates
+// shuffled with gen_range(0..=k), then every level's configuration and
+// tracked energies of member dst = parent member src.
+static std::vector<int64_t> pa_apply_resample(Field& f, const std::vector<int64_t>& counts, ChaCha8Rng& rng) {
+    const int64_t R = (int64_t)f.np * NR;
+    std::vector<int64_t> parents;
+    for (int64_t i = 0; i < R; i++)
+        for (int64_t c = 0; c < counts[i]; c++) parents.push_back(i);
+    for (int64_t k = (int64_t)parents.size() - 1; k >= 1; k--) {
+        const int64_t j = (int64_t)gen_index_inclusive(rng, (uint64_t)k);
+        std::swap(parents[k], parents[j]);
+    }
+    const std::vector<int8_t> old = f.spins;
+    const auto old_e = f.energies;
+    for (int64_t dst = 0; dst < R; dst++) {
+        const int64_t src = parents[dst];
+        if (dst == src) continue;
+        const int64_t dp = dst / NR, dr = dst % NR, sp = src / NR, sr = src % NR;
+        for (int t = 0; t < f.nt; t++) {
+            const size_t dc = (size_t)(t + f.nt * dp) * f.n, sc = (size_t)(t + f.nt * sp) * f.n;
+            for (int64_t v = 0; v < f.n; v++) f.spins[(dc + v) * NR + dr] = old[(sc + v) * NR + sr];
+            f.energies[t + f.nt * dp][dr] = old_e[t + f.nt * sp][sr];
+        }
+    }
+    return parents;
+}
+
+struct PaCfg {
+    double tmax, tmin;
+    int64_t sweeps, exchanges;
+    uint64_t seed;
+    int nt, pops;
+    double ess_threshold;
+    int64_t tuning_iters, tuning_steps, relax;
+    int threads;
+};
+
+struct PaOut {
+    std::vector<double> alphas, ess, rho;
+    std::vector<int64_t> families;
+    double free_energy = 0.0;
+    int64_t resamples = 0;
+    std::vector<int8_t> best_pre, best;
+    double incumbent_e = 0.0;
+};
+
+static void all_energies(const Qubo& m, Field& f) {
+    for (int c = 0; c < f.nt * f.np; c++) replica_energies(m, f.cell(c), f.energies[c].data());
+}
+
+// ultimate.rs:576-852 (defaults as above; num_slices = 1)
+static Field pa_run(const Qubo& m, const std::vector<uint8_t>& is_clamped, const std::vector<int8_t>& cval,
+                    const PaCfg& cfg, PaOut& out, ChaCha8Rng& rng) {
+    const int64_t n = m.n;
+    const int nt = std::max(cfg.nt, 1), pops = cfg.pops;
+    const int64_t R = (int64_t)pops * NR;
+    std::vector<int64_t> family(R);
+    for (int64_t i = 0; i < R; i++) family[i] = i;
+    const double denom = (double)std::max(nt - 1, 1);
+    std::vector<double> alphas(nt);
+    for (int t = 0; t < nt; t++) alphas[t] = (double)t / denom;
+    std::vector<double> temps(nt);
+    if (nt >= 3 && cfg.tuning_iters > 0 && cfg.tuning_steps > 0) {
+        Field tf(n, nt, pops);
+        init_field(tf, is_clamped, cval, rng);
+        all_energies(m, tf);
+        StepScratch sc;
+        sc.attempts.assign(nt - 1, 0);
+        sc.accepts.assign(nt - 1, 0);
+        for (int64_t it = 0; it < cfg.tuning_iters; it++) {
+            for (int t = 0; t < nt; t++) temps[t] = cfg.tmax * std::pow(cfg.tmin / cfg.tmax, alphas[t]);
+            std::fill(sc.attempts.begin(), sc.attempts.end(), 0);
+            std::fill(sc.accepts.begin(), sc.accepts.end(), 0);
+            for (int64_t s = 0; s < cfg.tuning_steps; s++)
+                step(tf, m, temps.data(), is_clamped, sc, rng, true, true, cfg.threads, nullptr);
+            std::vector<double> rates(nt - 1), sp(nt - 1);
+            for (int t = 0; t + 1 < nt; t++) {
+                rates[t] = sc.attempts[t] == 0 ? 0.0 : (double)sc.accepts[t] / (double)sc.attempts[t];
+                sp[t] = alphas[t + 1] - alphas[t];
+            }
+            const std::vector<double> ns = pa_adapt_spacings(sp, rates);
+            double acc = 0.0;
+            for (int t = 0; t + 1 < nt; t++) {
+                acc += ns[t];
+                alphas[t + 1] = acc;
+            }
+            alphas[nt - 1] = 1.0;
+        }
+    }
+    out.alphas = alphas;
+    Field f(n, nt, pops);
+    init_field(f, is_clamped, cval, rng);
+    all_energies(m, f);
+    const int64_t K = std::max<int64_t>(cfg.exchanges, 1);
+    const double cold_factor = K > 1 ? std::pow(cfg.tmin / cfg.tmax, 1.0 / (double)(K - 1)) : 1.0;
+    StepScratch sc;
+    sc.attempts.assign(std::max(nt - 1, 0), 0);
+    sc.accepts.assign(std::max(nt - 1, 0), 0);
+    std::vector<double> log_w(R, 0.0);
+    bool have_prev = false;
+    double beta_prev = 0.0;
+    double inc_e = std::numeric_limits<double>::infinity();
+    std::vector<int8_t> inc(n, 0), buf(n, 0);
+    for (int64_t k = 0; k < K; k++) {
+        const double t_cold = K > 1 ? cfg.tmax * powi(cold_factor, (int)k) : cfg.tmin;
+        const double span = t_cold / cfg.tmax;
+        for (int t = 0; t < nt; t++) temps[t] = cfg.tmax * std::pow(span, alphas[t]);
+        const double beta_cold = 1.0 / t_cold;
+        if (have_prev) {
+            const double db = beta_cold - beta_prev;
+            const int cold = nt - 1;
+            for (int p = 0; p < pops; p++)
+                for (int r = 0; r < NR; r++) log_w[p * NR + r] -= db * f.energies[cold + nt * p][r];
+            const std::vector<double> w = pa_normalized_weights(log_w);
+            const double ess = pa_ess(w);
+            out.ess.push_back(ess);
+            if (ess < cfg.ess_threshold * (double)R) {
+                out.free_energy += pa_free_energy_increment(log_w);
+                const double u = rng.gen_range(0.0, 1.0);
+                const std::vector<int64_t> counts = pa_systematic_resample(w, u);
+                const std::vector<int64_t> parents = pa_apply_resample(f, counts, rng);
+                const std::vector<int64_t> old = family;
+                for (int64_t d = 0; d < R; d++) family[d] = old[parents[d]];
+                const auto fe = pa_family_entropy(family);
+                out.rho.push_back(fe.first);
+                out.families.push_back(fe.second);
+                out.resamples++;
+                std::fill(log_w.begin(), log_w.end(), 0.0);
+                for (int64_t s = 0; s < cfg.relax; s++)
+                    step(f, m, temps.data(), is_clamped, sc, rng, true, false, cfg.threads, nullptr);
+            }
+        }
+        have_prev = true;
+        beta_prev = beta_cold;
+        for (int64_t s = 0; s < cfg.sweeps; s++)
+            step(f, m, temps.data(), is_clamped, sc, rng, true, false, cfg.threads, nullptr);
+        all_energies(m, f);
+        update_incumbent(m, f, inc_e, inc, buf);
+    }
+    // best member by true model energy (p, t, r order), then the incumbent
+    std::vector<int8_t> best(n, 0), rb((size_t)NR * n);
+    double best_e = std::numeric_limits<double>::infinity();
+    for (int c = 0; c < nt * pops; c++) {
+        const int8_t* s = f.cell(c);
+        for (int64_t v = 0; v < n; v++)
+            for (int r = 0; r < NR; r++) rb[(size_t)r * n + v] = s[v * NR + r];
+        for (int r = 0; r < NR; r++) {
+            const double e = total_energy(m, rb.data() + (size_t)r * n);
+            if (e < best_e) {
+                best_e = e;
+                std::copy(rb.begin() + (size_t)r * n, rb.begin() + (size_t)(r + 1) * n, best.begin());
+            }
+        }
+    }
+    if (inc_e < best_e) best = inc;
+    out.incumbent_e = inc_e;
+    out.best_pre = best;
+    one_opt(m, best.data(), is_clamped);
+    out.best = best;
+    return f;
+}
+
 static void pack_words(const Field& f, uint64_t* words) {
     const int cells = f.nt * f.np;
     for (int c = 0; c < cells; c++)
@@ -939,7 +1201,8 @@ namespace {
 // (src/engine_v2/backends/sparse_bitslice.rs:19-346), the default
 // swap_replicas of the SpinState trait (src/engine_v2/state.rs:126-140),
 // ProblemIR::greedy_coloring (src/engine_v2/ir.rs:114-139), MetropolisSweep
-// (src/engine_v2/operators/metropolis_sweep.rs:40-146) and ReplicaExchange
+// (src/engine_v2/operators/metropolis_sweep.rs:40-146), GibbsColorSweep
+// (src/engine_v2/operators/gibbs_color_sweep.rs:55-165) and ReplicaExchange
 // (src/engine_v2/operators/replica_exchange.rs:61-110).
 // ---------------------------------------------------------------------------
 struct V2State {
@@ -1064,6 +1327,44 @@ static void v2_metropolis(V2State& s, const double* temps, int nt, int64_t sweep
                 }
                 proposed++;
                 if (acc) {
+                    mask[rep / 64] |= 1ull << (rep % 64);
+                    accepted++;
+                    any = true;
+                }
+            }
+            if (any) s.apply_flips(site, mask);
+        }
+}
+
+// gibbs_color_sweep.rs:55-74 (order) and :119-165 (apply): heat-bath
+// resampling P(x = 1) = 1 / (1 + exp(h / t)), the greedy limit for t <= 0,
+// one draw per (site, replica) in chromatic order.
+static void v2_gibbs(V2State& s, const double* temps, int nt, int64_t sweeps, ChaCha8Rng& rng, int64_t& proposed,
+                     int64_t& accepted) {
+    const std::vector<uint32_t> colors = v2_greedy_coloring(s);
+    uint32_t ncol = 0;
+    for (uint32_t c : colors) ncol = std::max(ncol, c + 1);
+    std::vector<int64_t> order;
+    for (uint32_t c = 0; c < ncol; c++)
+        for (int64_t i = 0; i < s.n; i++)
+            if (colors[i] == c) order.push_back(i);
+    std::vector<double> de(s.r);
+    std::vector<uint64_t> mask(s.w);
+    const double inf = std::numeric_limits<double>::infinity();
+    for (int64_t sw = 0; sw < sweeps; sw++)
+        for (int64_t site : order) {
+            s.delta_e_into(site, de);
+            std::fill(mask.begin(), mask.end(), 0);
+            bool any = false;
+            for (int64_t rep = 0; rep < s.r; rep++) {
+                const bool x = s.bit(site, rep) != 0;
+                const double h = x ? -de[rep] : de[rep];
+                const double t = temps[rep % nt];
+                const double bh = t > 0.0 ? h / t : (h > 0.0 ? inf : (h < 0.0 ? -inf : 0.0));
+                const double p1 = 1.0 / (1.0 + std::exp(bh));
+                const bool one = rng.gen_f64() < p1;
+                proposed++;
+                if (one != x) {
                     mask[rep / 64] |= 1ull << (rep % 64);
                     accepted++;
                     any = true;
@@ -1288,10 +1589,68 @@ int or_run_sa_batch(int64_t count, const int64_t* ns, const double* const* lins,
     return 0;
 }
 
+// UltimateSolver with num_temps = nt, num_pops = pops >= 2 and the PA knobs,
+// run through solve_with_pa_diagnostics(model, clamped). Outputs: final
+// words [nt * pops][n] (cell t + nt p), tracked energies [nt * pops][64],
+// master-stream position, tuned alphas [nt], ESS per stage [exchanges - 1],
+// family (rho, count) per resampling event, free energy, resampling events,
+// the best member before 1-opt, the incumbent energy and the solution.
+int or_pa_run(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,
+              double offset, double tmax, double tmin, int64_t sweeps, int64_t exchanges, uint64_t seed, int nt,
+              int pops, double ess_threshold, int64_t tuning_iters, int64_t tuning_steps, int64_t relax,
+              const uint8_t* clamped, const int8_t* clamp_val, int threads, uint64_t* words_out,
+              double* energies_out, uint64_t* draws_out, double* alphas_out, double* ess_out, int64_t* n_ess,
+              double* rho_out, int64_t* fam_out, int64_t* n_res, double* free_energy_out, int8_t* best_pre_out,
+              double* incumbent_out, int8_t* state_out) {
+    Qubo m = make_qubo(n, lin, row, col, val, offset);
+    std::vector<uint8_t> cl(n, 0);
+    std::vector<int8_t> cv(n, 0);
+    for (int64_t i = 0; i < n; i++) {
+        cl[i] = clamped ? clamped[i] : 0;
+        cv[i] = clamp_val ? clamp_val[i] : 0;
+    }
+    PaCfg cfg{tmax, tmin, sweeps, exchanges, seed, nt, pops, ess_threshold, tuning_iters, tuning_steps, relax, threads};
+    ChaCha8Rng rng(seed);
+    PaOut o;
+    Field f = pa_run(m, cl, cv, cfg, o, rng);
+    pack_words(f, words_out);
+    for (size_t c = 0; c < f.energies.size(); c++)
+        for (int r = 0; r < NR; r++) energies_out[c * NR + r] = f.energies[c][r];
+    *draws_out = rng.draws;
+    std::copy(o.alphas.begin(), o.alphas.end(), alphas_out);
+    std::copy(o.ess.begin(), o.ess.end(), ess_out);
+    *n_ess = (int64_t)o.ess.size();
+    std::copy(o.rho.begin(), o.rho.end(), rho_out);
+    std::copy(o.families.begin(), o.families.end(), fam_out);
+    *n_res = o.resamples;
+    *free_energy_out = o.free_energy;
+    std::copy(o.best_pre.begin(), o.best_pre.end(), best_pre_out);
+    *incumbent_out = o.incumbent_e;
+    std::copy(o.best.begin(), o.best.end(), state_out);
+    return 0;
+}
+
+// population_annealing.rs primitives for the host tests.
+void or_pa_normalized_weights(const double* lw, int64_t r, double* out) {
+    const auto w = pa_normalized_weights(std::vector<double>(lw, lw + r));
+    std::copy(w.begin(), w.end(), out);
+}
+void or_pa_systematic_resample(const double* w, int64_t r, double u, int64_t* counts) {
+    const auto c = pa_systematic_resample(std::vector<double>(w, w + r), u);
+    std::copy(c.begin(), c.end(), counts);
+}
+// gen_range(0..=hi[i]) in sequence on ChaCha8Rng::seed_from_u64(seed).
+void or_gen_index_inclusive(uint64_t seed, const uint64_t* hi, int64_t count, uint64_t* out, uint64_t* draws) {
+    ChaCha8Rng rng(seed);
+    for (int64_t i = 0; i < count; i++) out[i] = gen_index_inclusive(rng, hi[i]);
+    *draws = rng.draws;
+}
+
 // A program of S2 operator applications on one state with one master stream
 // (ChaCha8Rng::seed_from_u64(seed) after skip_draws draws): op i is
-// MetropolisSweep (kinds[i] == 0) for counts[i] sweeps or ReplicaExchange
-// (kinds[i] == 1) for counts[i] rounds, all at temps[nt]. Outputs the planes
+// MetropolisSweep (kinds[i] == 0) for counts[i] sweeps, ReplicaExchange
+// (kinds[i] == 1) for counts[i] rounds or GibbsColorSweep (kinds[i] == 2) for
+// counts[i] sweeps, all at temps[nt]. Outputs the planes
 // [n * ceil(r/64)], the ledger energies [r], (proposed, accepted) per op, the
 // largest ledger drift against a rebuild and the stream position.
 int or_v2_program(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,
@@ -1325,7 +1684,8 @@ int or_v2_program(int64_t n, const double* lin, const int64_t* row, const int64_
     for (int64_t i = 0; i < nops; i++) {
         int64_t p = 0, a = 0;
         if (kinds[i] == 0) v2_metropolis(s, temps, nt, counts[i], rng, p, a);
-        else v2_exchange(s, temps, nt, counts[i], rng, p, a);
+        else if (kinds[i] == 1) v2_exchange(s, temps, nt, counts[i], rng, p, a);
+        else v2_gibbs(s, temps, nt, counts[i], rng, p, a);
         stats_out[2 * i] = p;
         stats_out[2 * i + 1] = a;
     }

@@ -74,6 +74,13 @@ def lib():
         L.or_v2_program.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, C.c_int64, _u8p,
                                     C.c_uint64, C.c_uint64, C.c_int64, C.c_void_p, _i64p, _f64p, C.c_int32,
                                     _u64p, _f64p, _i64p, _f64p, _u64p]
+        L.or_pa_run.argtypes = [
+            C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int64,
+            C.c_uint64, C.c_int, C.c_int, C.c_double, C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+            C.c_int, _u64p, _f64p, _u64p, _f64p, _f64p, _i64p, _f64p, _i64p, _i64p, _f64p, _i8p, _f64p, _i8p]
+        L.or_pa_normalized_weights.argtypes = [_f64p, C.c_int64, _f64p]
+        L.or_pa_systematic_resample.argtypes = [_f64p, C.c_int64, C.c_double, _i64p]
+        L.or_gen_index_inclusive.argtypes = [C.c_uint64, _u64p, C.c_int64, _u64p, _u64p]
         _lib = L
     return _lib
 
@@ -242,13 +249,13 @@ def run_sa_batch(models, seeds, temps, threads=1, want_words=True):
 
 def v2_program(model, r, init, seed, ops, temps, skip_draws=0):
     """S2 operators on one bit-sliced state with one master stream: ops is a
-    list of ("metropolis", sweeps) / ("exchange", rounds), all at per-replica
+    list of ("metropolis", sweeps) / ("exchange", rounds) / ("gibbs", sweeps), all at per-replica
     temperatures temps (replica k uses temps[k % len]). Returns (planes
     [n, ceil(r/64)], energies [r], [(proposed, accepted)] per op, ledger drift,
     stream position)."""
     n, lin, row, col, val = _csr(model)
     w = (r + 63) // 64
-    kinds = np.array([0 if k == "metropolis" else 1 for k, _ in ops], dtype=np.int32)
+    kinds = np.array([{"metropolis": 0, "exchange": 1, "gibbs": 2}[k] for k, _ in ops], dtype=np.int32)
     counts = np.array([c for _, c in ops], dtype=np.int64)
     temps = np.ascontiguousarray(temps, dtype=np.float64)
     planes = np.zeros(n * w, dtype=np.uint64)
@@ -262,3 +269,63 @@ def v2_program(model, r, init, seed, ops, temps, skip_draws=0):
                         drift, draws)
     return (planes.reshape(n, w), en, [(int(stats[2 * i]), int(stats[2 * i + 1])) for i in range(len(ops))],
             float(drift[0]), int(draws[0]))
+
+
+def pa_run(model, temp_max, temp_min, sweeps, exchanges, seed, num_temps, num_pops, ess_threshold=0.5,
+           tuning_iters=8, tuning_steps=10, relax=5, clamped=None, clamp_val=None, threads=1, offset=0.0):
+    """UltimateSolver::new(temp_max, temp_min, sweeps, exchanges, Some(seed)) with
+    num_temps, num_pops and the PA knobs, through solve_with_pa_diagnostics
+    (ultimate.rs:576-890). Returns a dict: words [nt*pops, n], energies
+    [nt*pops, 64], draws, alphas, ess, rho, families, free_energy, resamples,
+    best_pre (before 1-opt), incumbent, state."""
+    n, lin, row, col, val = _csr(model)
+    cells = num_temps * num_pops
+    words = np.zeros(cells * n, dtype=np.uint64)
+    en = np.zeros(cells * 64, dtype=np.float64)
+    draws = np.zeros(1, dtype=np.uint64)
+    alphas = np.zeros(num_temps, dtype=np.float64)
+    k = max(exchanges, 1)
+    ess = np.zeros(k, dtype=np.float64)
+    n_ess = np.zeros(1, dtype=np.int64)
+    rho = np.zeros(k, dtype=np.float64)
+    fam = np.zeros(k, dtype=np.int64)
+    n_res = np.zeros(1, dtype=np.int64)
+    fe = np.zeros(1, dtype=np.float64)
+    best_pre = np.zeros(n, dtype=np.int8)
+    inc = np.zeros(1, dtype=np.float64)
+    state = np.zeros(n, dtype=np.int8)
+    cl = None if clamped is None else np.ascontiguousarray(clamped, dtype=np.uint8)
+    cv = None if clamp_val is None else np.ascontiguousarray(clamp_val, dtype=np.int8)
+    L = lib()
+    L.or_pa_run(n, lin, row, col, val, float(offset), float(temp_max), float(temp_min), int(sweeps), int(exchanges),
+                int(seed), int(num_temps), int(num_pops), float(ess_threshold), int(tuning_iters), int(tuning_steps),
+                int(relax), _ptr(cl), _ptr(cv), int(threads), words, en, draws, alphas, ess, n_ess, rho, fam, n_res, fe, best_pre,
+                inc, state)
+    ne, nr = int(n_ess[0]), int(n_res[0])
+    return dict(words=words.reshape(cells, n), energies=en.reshape(cells, 64), draws=int(draws[0]), alphas=alphas,
+                ess=ess[:ne], rho=rho[:nr], families=fam[:nr], free_energy=float(fe[0]), resamples=nr,
+                best_pre=best_pre, incumbent=float(inc[0]), state=state)
+
+
+def pa_normalized_weights(log_w) -> np.ndarray:
+    lw = np.ascontiguousarray(log_w, dtype=np.float64)
+    out = np.zeros(len(lw), dtype=np.float64)
+    lib().or_pa_normalized_weights(lw, len(lw), out)
+    return out
+
+
+def pa_systematic_resample(w, u: float) -> np.ndarray:
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    out = np.zeros(len(w), dtype=np.int64)
+    lib().or_pa_systematic_resample(w, len(w), float(u), out)
+    return out
+
+
+def gen_index_inclusive(seed: int, his):
+    """gen_range(0..=hi) for each hi in sequence on seed_from_u64(seed);
+    returns (values, draws consumed)."""
+    hi = np.ascontiguousarray(his, dtype=np.uint64)
+    out = np.zeros(len(hi), dtype=np.uint64)
+    draws = np.zeros(1, dtype=np.uint64)
+    lib().or_gen_index_inclusive(int(seed), hi, len(hi), out, draws)
+    return out, int(draws[0])

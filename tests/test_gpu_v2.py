@@ -1,13 +1,14 @@
 """engine_v2 (S2) on the device against the oracle's restatement, through
 the C ABI: planes, ledger energies, (proposed, accepted) per operator and
-stream positions equal after sequences of MetropolisSweep and
-ReplicaExchange applications; the audit finds no drift (integer state)."""
+stream positions equal after sequences of MetropolisSweep, GibbsColorSweep
+and ReplicaExchange applications; the audit finds no drift (integer state)."""
 import numpy as np
 import pytest
 
 from ising_engine_b200 import _ffi
 from ising_engine_b200 import instances as I
-from ising_engine_b200.v2 import ChaChaStream, GpuBitSlice, MetropolisSweep, ProblemIR, ReplicaExchange
+from ising_engine_b200.v2 import (ChaChaStream, GibbsColorSweep, GpuBitSlice, MetropolisSweep, ProblemIR,
+                                  ReplicaExchange)
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -24,7 +25,7 @@ def run_gpu(ir, r, init, seed, ops, temps, skip=0):
     rng = ChaChaStream(seed, skip)
     stats = []
     for kind, count in ops:
-        op = MetropolisSweep() if kind == "metropolis" else ReplicaExchange()
+        op = {"metropolis": MetropolisSweep, "exchange": ReplicaExchange, "gibbs": GibbsColorSweep}[kind]()
         rep = op.apply(st, temps, rng, count)
         stats.append((rep.proposed, rep.accepted))
     out = st.planes(), st.energies(), stats, st.audit(), rng.position
@@ -65,6 +66,45 @@ def test_lattice_short_ladder_and_zero_temperature():
     init = np.zeros(ir.n, np.uint8)
     check(ir, 96, init, 3, [("metropolis", 20), ("exchange", 4)], [2.0, 1.0, 0.5])
     check(ir, 40, init, 4, [("metropolis", 5)], [0.0, 0.7])  # T = 0: pure descent
+
+
+def test_gibbs_reference_case_and_scorer():
+    """gibbs_color_sweep.rs:197-252: r = 100, temps 0.2 + 0.05 k, 30 sweeps,
+    seed 7; every replica's ledger energy equals ProblemIR::energy of its
+    extracted configuration."""
+    ir = frustrated()
+    r = 100
+    init = np.array([1, 0, 1, 0, 0, 1, 0], np.uint8)
+    temps = [0.2 + 0.05 * k for k in range(r)]
+    check(ir, r, init, 7, [("gibbs", 30)], temps)
+    st = GpuBitSlice(ir, r, init)
+    GibbsColorSweep().apply(st, temps, ChaChaStream(7), 30)
+    en = st.energies()
+    for k in range(r):
+        assert ir.energy(st.extract(k)) == en[k]
+    st.close()
+
+
+@pytest.mark.parametrize("r", [64, 97])
+def test_gibbs_sequences_and_special_temperatures(r):
+    m = I.maxcut_gnm(400, 3000, seed=9)
+    ir = ProblemIR.from_model(m)
+    init = (np.random.default_rng(r + 1).random(ir.n) < 0.5).astype(np.uint8)
+    temps = list(I.geometric_beta_ladder(r - 6, 0.2, 4.0)) + [0.0, -1.0, float("nan"), float("inf"), 1e-300, 0.01]
+    ops = [("gibbs", 6), ("exchange", 2), ("metropolis", 3), ("gibbs", 4)]
+    check(ir, r, init, 13, [("gibbs", 6)], temps, skip=3)
+    finite = [t for t in temps if t > 0.0 and np.isfinite(t)]
+    check(ir, r, init, 13, ops, finite)
+
+
+def test_gibbs_cold_is_monotone_descent():
+    """gibbs_color_sweep.rs:255-291."""
+    ir = frustrated()
+    st = GpuBitSlice(ir, 8, np.zeros(7, np.uint8))
+    e0 = st.energies()
+    GibbsColorSweep().apply(st, [1e-9] * 8, ChaChaStream(1), 5)
+    assert (st.energies() <= e0).all() and st.audit() == 0.0
+    st.close()
 
 
 def test_rejects_non_integral():

@@ -66,7 +66,7 @@ def py_program(ir, r, init, seed, ops, temps):
     x = [[int(init[s]) for _ in range(r)] for s in range(n)]
     colors = py_coloring(ir)
     order = [s for c in range(max(colors) + 1) for s in range(n) if colors[s] == c]
-    total = sum(c * (n * r if k == "metropolis" else r) for k, c in ops)
+    total = sum(c * (r if k == "exchange" else n * r) for k, c in ops)
     draws = O.chacha8_u64(seed, total + 8)
     pos = 0
 
@@ -106,6 +106,25 @@ def py_program(ir, r, init, seed, ops, temps):
                             flips.append(k)
                     for k in flips:
                         x[s][k] ^= 1
+        elif kind == "gibbs":
+            for _ in range(count):
+                for s in order:
+                    flips = []
+                    for k in range(r):
+                        h = float(field(s, k))
+                        t = temps[k % len(temps)]
+                        bh = h / t if t > 0.0 else (math.inf if h > 0 else (-math.inf if h < 0 else 0.0))
+                        try:
+                            ex = math.exp(bh)
+                        except OverflowError:
+                            ex = math.inf
+                        one = u() < 1.0 / (1.0 + ex)
+                        p += 1
+                        if one != bool(x[s][k]):
+                            a += 1
+                            flips.append(k)
+                    for k in flips:
+                        x[s][k] ^= 1
         else:
             for rnd in range(count):
                 e = [float(energy(k)) for k in range(r)]
@@ -137,10 +156,33 @@ def test_oracle_v2_matches_python_restatement(r):
     ir = frustrated()
     init = np.array([1, 0, 1, 0, 0, 1, 0], np.uint8)
     temps = [0.2 + 0.05 * k for k in range(r)]
-    ops = [("metropolis", 3), ("exchange", 2), ("metropolis", 2), ("exchange", 1)]
+    ops = [("metropolis", 3), ("exchange", 2), ("gibbs", 2), ("metropolis", 2), ("exchange", 1), ("gibbs", 1)]
     pl, en, st, drift, draws = O.v2_program(ir.model(), r, init, 11, ops, temps)
     ppl, pen, pst, ppos = py_program(ir, r, init, 11, ops, temps)
     assert (pl == ppl).all()
     assert en.tolist() == pen.tolist()
     assert st == pst
     assert drift == 0.0 and draws == ppos
+
+
+def test_oracle_gibbs_special_temperatures():
+    """T <= 0 and NaN take the greedy limit, T = inf resamples with P = 1/2
+    (gibbs_color_sweep.rs:139-149); the fields of this instance reach +-10,
+    so T = 0.01 overflows exp for the uphill ones."""
+    ir = frustrated()
+    init = np.array([0, 1, 1, 0, 1, 0, 1], np.uint8)
+    temps = [0.0, -1.0, math.nan, math.inf, 0.01, 1e-300, 3.0]
+    r = 21
+    pl, en, st, drift, draws = O.v2_program(ir.model(), r, init, 5, [("gibbs", 4)], temps)
+    ppl, pen, pst, ppos = py_program(ir, r, init, 5, [("gibbs", 4)], temps)
+    assert (pl == ppl).all() and en.tolist() == pen.tolist() and st == pst and draws == ppos
+
+
+def test_oracle_gibbs_cold_is_monotone_descent():
+    """gibbs_color_sweep.rs:255-291: at T = 1e-9 no replica's energy rises."""
+    ir = frustrated()
+    r = 8
+    init = np.zeros(7, np.uint8)
+    _, e0, _, _, _ = O.v2_program(ir.model(), r, init, 1, [], [1e-9] * r)
+    _, e1, _, drift, _ = O.v2_program(ir.model(), r, init, 1, [("gibbs", 5)], [1e-9] * r)
+    assert (e1 <= e0).all() and drift == 0.0
