@@ -4,8 +4,8 @@ Restates the reference's readers: the engine_v2 frontend
 (src/engine_v2/frontend.rs:11-98: ``qubo_model_to_ir``, ``parse_rudy``,
 ``maxcut_to_qubo``, ``rudy_maxcut_ir``) and the benchmark family parsers
 (src/benchmark/instances.rs:60-231: ``assemble``, ``parse_rudy_maxcut``,
-``parse_orlib_bqp``, ``parse_biqmac_sparse``). Errors raise ``ValueError``
-with the reference's message. The QPLIB reader is not restated.
+``parse_orlib_bqp``, ``parse_biqmac_sparse``, ``parse_qplib``). Errors raise
+``ValueError`` with the reference's message.
 """
 from __future__ import annotations
 
@@ -212,3 +212,79 @@ def parse_biqmac_sparse(text: str, name: str) -> Instance:
         else:
             edges.append((i, j, 2.0 * v))
     return Instance(name, "biqmac_sparse", assemble(n, edges, linear), False)
+
+
+def _as_usize(x: float) -> int:
+    """Rust's saturating `f64 as usize`: NaN and negatives give 0, toward zero."""
+    if x != x or x <= 0.0:
+        return 0
+    return int(min(x, 2.0 ** 64 - 1))
+
+
+def parse_qplib(text: str, name: str) -> Instance:
+    """instances.rs:227-345 (QPLIB, the unconstrained binary subset): one
+    logical line per field, numeric fields first and free text after; type
+    code `?B N` only; objective 1/2 sum of the listed q_ij x_i x_j (each listed
+    entry once, diagonal into the linear term) + b'x + c, negated for a
+    maximization so that the energy is always minimized."""
+    lines = [l.split() for l in text.splitlines()]
+    lines = iter([t for t in lines if t])
+
+    def next_line(what: str):
+        t = next(lines, None)
+        if t is None:
+            raise ValueError(f"qplib: missing {what}")
+        return t
+
+    def parse1(t, w: str) -> float:
+        if not t:
+            raise ValueError(f"qplib: empty {w}")
+        try:
+            return float(t[0])
+        except ValueError:
+            raise ValueError(f"qplib: bad {w}") from None
+
+    next_line("name")
+    ptype = next_line("type")[0]
+    if len(ptype) < 2 or ptype[1].upper() != "B":
+        raise ValueError(f"{name}: QPLIB type {ptype} not binary-variable (unsupported)")
+    if len(ptype) < 3 or ptype[2].upper() != "N":
+        raise ValueError(f"{name}: QPLIB type {ptype} is constrained; only unconstrained instances supported")
+    maximize = next_line("sense")[0].lower() == "maximize"
+    n = _as_usize(parse1(next_line("n"), "n"))
+    sign = -1.0 if maximize else 1.0
+    nq = _as_usize(parse1(next_line("nq"), "nq"))
+    edges, linear = [], [0.0] * n
+    for _ in range(nq):
+        t = next_line("quad term")
+        if len(t) < 3:
+            raise ValueError(f"{name}: short quad line")
+        i = _as_usize(parse1(t[0:1], "qi"))
+        j = _as_usize(parse1(t[1:2], "qj"))
+        q = parse1(t[2:3], "qv")
+        if i == 0 or j == 0 or i > n or j > n:
+            raise ValueError(f"{name}: quad index out of range")
+        i, j = i - 1, j - 1
+        if i == j:
+            linear[i] += sign * 0.5 * q
+        else:
+            edges.append((i, j, sign * 0.5 * q))
+    b_default = parse1(next_line("b_default"), "b_default")
+    linear = [v + sign * b_default for v in linear]
+    nb = _as_usize(parse1(next_line("nb"), "nb"))
+    for _ in range(nb):
+        t = next_line("linear term")
+        if len(t) < 2:
+            raise ValueError(f"{name}: short linear line")
+        i = _as_usize(parse1(t[0:1], "bi"))
+        v = parse1(t[1:2], "bv")
+        if i == 0 or i > n:
+            raise ValueError(f"{name}: linear index out of range")
+        linear[i - 1] += sign * (v - b_default)
+    try:
+        c = parse1(next_line("c"), "c")
+    except ValueError:
+        c = 0.0
+    m = assemble(n, edges, linear)
+    m.energy_offset = sign * c
+    return Instance(name, "qplib", m, maximize)

@@ -5,7 +5,7 @@ of the QuboModel -> ProblemIR bridge, and the readers' errors."""
 import numpy as np
 import pytest
 
-from ising_engine_b200.formats import (assemble, parse_biqmac_sparse, parse_orlib_bqp, parse_rudy,
+from ising_engine_b200.formats import (assemble, parse_biqmac_sparse, parse_orlib_bqp, parse_qplib, parse_rudy,
                                        parse_rudy_maxcut, qubo_model_to_ir, rudy_maxcut_ir, tokens)
 
 
@@ -109,3 +109,53 @@ def test_bridge_preserves_energy_bitwise():
 def test_tokens_strip_comments():
     assert tokens("1 2 3 # c") == ["1", "2", "3"]
     assert tokens("% only a comment") == []
+
+
+def brute(inst):
+    n = inst.model.num_vars
+    best = min(inst.model.calculate_total_energy(np.array([(b >> v) & 1 for v in range(n)], np.int8))
+               for b in range(1 << n))
+    return best, -best if inst.maximize else best
+
+
+def test_qplib_unconstrained_binary():
+    """test_benchmark.rs:84-123: pair coefficient -6/2, minimum -1 at (1, 1);
+    constrained and continuous types refused."""
+    text = ("toy            name\nQBN            type\nminimize       sense\n2              n\n"
+            "1              nq\n1 2 -6         q12\n0              b_default\n2              nb\n"
+            "1 1            b1\n2 1            b2\n0              c\n")
+    inst = parse_qplib(text, "toy")
+    assert not inst.maximize and inst.family == "qplib"
+    e, native = brute(inst)
+    assert abs(e + 1.0) < 1e-9 and abs(native + 1.0) < 1e-9
+    with pytest.raises(ValueError, match="is constrained"):
+        parse_qplib("c name\nQBL type\nminimize sense\n2 n\n", "c")
+    with pytest.raises(ValueError, match="not binary-variable"):
+        parse_qplib("c name\nQCN type\nminimize sense\n2 n\n", "c")
+
+
+def test_qplib_maximize_defaults_and_offset():
+    """A maximization: energy = -objective; the diagonal entry and b_default
+    reach every variable, listed b entries replace the default, c is the
+    offset (and may be missing)."""
+    rng = np.random.default_rng(4)
+    n = 5
+    quad = [(1, 1, 4.0), (1, 3, -2.0), (2, 5, 6.0), (4, 4, -8.0)]
+    bdef, blist, c = 1.5, [(2, -3.0), (5, 0.5)], 7.0
+    lines = ["q name", "QBN type", "maximize sense", f"{n} n", f"{len(quad)} nq"]
+    lines += [f"{i} {j} {q}" for i, j, q in quad] + [f"{bdef} b_default", f"{len(blist)} nb"]
+    lines += [f"{i} {v}" for i, v in blist]
+    inst = parse_qplib("\n".join(lines + [f"{c} c"]), "q")
+    inst2 = parse_qplib("\n".join(lines), "q")
+    b = [bdef] * n
+    for i, v in blist:
+        b[i - 1] = v
+    for _ in range(20):
+        x = rng.integers(0, 2, size=n).astype(np.int8)
+        obj = sum(0.5 * q * x[i - 1] * x[j - 1] for i, j, q in quad) + sum(bi * xi for bi, xi in zip(b, x))
+        assert inst.model.calculate_total_energy(x) == pytest.approx(-(obj + c), abs=1e-12)
+        assert inst2.model.calculate_total_energy(x) == pytest.approx(-obj, abs=1e-12)
+    with pytest.raises(ValueError, match="q: quad index out of range"):
+        parse_qplib("q name\nQBN type\nminimize sense\n2 n\n1 nq\n1 3 1\n", "q")
+    with pytest.raises(ValueError, match="qplib: missing nb"):
+        parse_qplib("q name\nQBN type\nminimize sense\n2 n\n0 nq\n0 b_default\n", "q")
