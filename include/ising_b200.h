@@ -341,6 +341,19 @@ ie_status ie_pa_family_entropy(const uint64_t* family_ids, uint64_t r, double* r
 ie_status ie_pa_systematic_resample(const double* w, uint64_t r, double u, uint64_t* counts);
 ie_status ie_pa_adapt_spacings(const double* spacings, const double* acceptance, uint64_t k, double* out);
 
+/* ---- presolve and decomposition (host only) ----
+ * full_presolve (src/presolve/mod.rs:279-324): roof-duality strong
+ * persistencies (src/presolve/qpbo.rs) of the clamp-reduced model unioned
+ * with probing weak persistencies; writes the fixings beyond the user's
+ * clamps (out_idx / out_val: [num_vars] capacity, may be NULL to count). */
+ie_status ie_presolve(const ie_problem* problem, const uint64_t* clamp_idx, const int8_t* clamp_val,
+                      uint64_t n_clamps, uint64_t* out_idx, int8_t* out_val, uint64_t* n_out);
+/* connected_components (mod.rs:189-218) of the graph of nonzero couplings
+ * among active variables: component[v] = its component (numbered by
+ * smallest vertex) or UINT64_MAX for inactive v. */
+ie_status ie_connected_components(const ie_problem* problem, const uint8_t* active, uint64_t* component,
+                                  uint64_t* n_components);
+
 /* ---- measurement helper (no reference counterpart) ----
  * Measured roofline denominators on `device`: int32 LOP3/IADD3 throughput
  * (ops/s) and Xoshiro256++ step+compare throughput (outputs/s), the per-attempt

@@ -8,10 +8,12 @@ replica extraction, then the 1-opt polish of src/solver/local_search.rs:19-57.
 
 With num_pops > 1 the solve is population annealing with PT equilibration
 (ultimate.rs:576-852, run by ``Engine.run_pa``). Presolve and component
-decomposition (ultimate.rs:161-218) are host-side reductions before either
-path; ``solve`` accepts their result as clamps.
+decomposition (ultimate.rs:161-218) run first on the host
+(``ising_engine_b200.presolve``), as in the reference.
 """
 from __future__ import annotations
+
+import copy
 
 import numpy as np
 
@@ -79,6 +81,10 @@ class UltimateSolver:
         self.ladder_tuning_iters = 8
         self.ladder_tuning_steps = 10
         self.post_resample_relaxation = 5
+        # presolve and decomposition before annealing (ultimate.rs:161-218); an
+        # extension may switch them off, e.g. where probing's O(n^2 nnz) cost
+        # is too high
+        self.use_presolve = True
 
     @staticmethod
     def new(temp_max, temp_min, sweeps, exchanges, seed):
@@ -117,6 +123,9 @@ class UltimateSolver:
         """ultimate.rs:858-890: population annealing with num_pops >= 2 (no
         presolve), then best extraction and 1-opt (ultimate.rs:806-845);
         returns (state, PaDiagnostics)."""
+        return self._solve_pa(model, clamped)
+
+    def _solve_pa(self, model: QuboModel, clamped):
         is_clamped, cval = self._clamps(model, clamped)
         with self.engine(model, num_pops=max(self.num_pops, 2)) as eng:
             if len(clamped):
@@ -127,10 +136,28 @@ class UltimateSolver:
         return best, diag
 
     def solve(self, model: QuboModel, clamped=()) -> np.ndarray:
-        """UltimateSolver::solve for `model` with `clamped` fixings: the PT
-        path, or population annealing when num_pops > 1 (ultimate.rs:220-232)."""
+        """UltimateSolver::solve (ultimate.rs:138-387) for `model` with
+        `clamped` fixings: presolve fixings join the clamps; a free-variable
+        graph of several components is solved component by component (seed +
+        index + 1, ultimate.rs:173-218); otherwise the PT path, or population
+        annealing when num_pops > 1 (ultimate.rs:220-232)."""
+        clamped = [(int(i), int(v)) for i, v in clamped]
+        if self.use_presolve:
+            from .presolve import connected_components, extract_component, full_presolve
+            clamped = clamped + full_presolve(model, clamped)
+            is_clamped, cval = self._clamps(model, clamped)
+            comps = connected_components(model, is_clamped == 0)
+            if len(comps) > 1:
+                result = np.where(is_clamped != 0, cval, 0).astype(np.int8)
+                fixed_one = (is_clamped != 0) & (cval == 1)
+                for ci, comp in enumerate(comps):
+                    sub, gmap = extract_component(model, comp, fixed_one)
+                    child = copy.copy(self)
+                    child.seed = (self.seed + ci + 1) & 0xFFFFFFFFFFFFFFFF
+                    result[gmap] = child.solve(sub)
+                return result
         if self.num_pops > 1:
-            return self.solve_with_pa_diagnostics(model, clamped)[0]
+            return self._solve_pa(model, clamped)[0]
         is_clamped, cval = self._clamps(model, clamped)
         with self.engine(model) as eng:
             if len(clamped):
