@@ -81,7 +81,8 @@ typedef struct ie_pa_config {
     uint32_t ladder_tuning_iters;      /* 8 by default; 0 keeps the geometric ladder */
     uint32_t ladder_tuning_steps;      /* 10 by default */
     uint32_t post_resample_relaxation; /* 5 by default */
-    int32_t ladder_mode;               /* 0: LadderMode::AcceptanceUniform (the default; the only mode here) */
+    int32_t ladder_mode;               /* 0: LadderMode::AcceptanceUniform (the default);
+                                          1: LadderMode::FeedbackOptimized (round-trip tracking) */
     int32_t use_icm;                   /* must be 0 (the default) */
 } ie_pa_config;
 
@@ -340,6 +341,8 @@ ie_status ie_pa_free_energy_increment(const double* log_w, uint64_t r, double* o
 ie_status ie_pa_family_entropy(const uint64_t* family_ids, uint64_t r, double* rho, uint64_t* families);
 ie_status ie_pa_systematic_resample(const double* w, uint64_t r, double u, uint64_t* counts);
 ie_status ie_pa_adapt_spacings(const double* spacings, const double* acceptance, uint64_t k, double* out);
+ie_status ie_pa_feedback_optimized_alphas(const double* alphas, const double* flow, uint64_t nt, double damping,
+                                          double* out);
 
 /* ---- presolve and decomposition (host only) ----
  * full_presolve (src/presolve/mod.rs:279-324): roof-duality strong

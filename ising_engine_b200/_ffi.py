@@ -90,6 +90,7 @@ _SIGS = {
     "ie_pa_family_entropy": ([_vp, C.c_uint64, _vp, _vp], C.c_int),
     "ie_pa_systematic_resample": ([_vp, C.c_uint64, C.c_double, _vp], C.c_int),
     "ie_pa_adapt_spacings": ([_vp, _vp, C.c_uint64, _vp], C.c_int),
+    "ie_pa_feedback_optimized_alphas": ([_vp, _vp, C.c_uint64, C.c_double, _vp], C.c_int),
     "ie_read_spins": ([_vp, _vp], C.c_int),
     "ie_read_energies": ([_vp, _vp], C.c_int),
     "ie_read_swap_stats": ([_vp, _vp, _vp], C.c_int),

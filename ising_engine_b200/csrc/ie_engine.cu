@@ -395,6 +395,10 @@ struct Engine {
     // re-syncs energies itself, so the PT loop's periodic re-sync is off
     uint32_t pop_len = 0;
     bool periodic_resync = true;
+    // round-trip tracking of the exchange (feedback-optimized ladder tuning)
+    bool track_roundtrips = false;
+    DevBuf<int8_t> d_labels;
+    DevBuf<unsigned long long> d_rt;
 
     ~Engine() {
         if (device >= 0) cudaSetDevice(device);
@@ -1233,6 +1237,10 @@ struct Engine {
             X.xdund = d_xdund.p;
             X.dbeta = d_dbeta.p;
             X.pop_len = pop_len;
+            if (track_roundtrips) {
+                X.labels = d_labels.p;
+                X.rt = d_rt.p;
+            }
             return run_pt_cells(steps, per_step, X);
         }
         const int block = (int)(((nt * 8) + 31) / 32 * 32);
@@ -1877,7 +1885,7 @@ ie_status ie_run_pt(ie_handle* h) {
 }
 
 // UltimateSolver::solve_population_annealing_diag (ultimate.rs:576-852) with
-// acceptance-uniform ladder tuning and no ICM. The steps, energies and
+// either ladder mode and no ICM. The steps, energies and
 // resampled configurations stay on the device; per stage the host reads the
 // cold-level energies (64 per population) for the weights and, on a
 // resampling event, takes the offset and shuffle draws from the master
@@ -1886,7 +1894,7 @@ ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
     if (!h || !pc) return fail(IE_ERR_INVALID, "NULL argument");
     Engine& E = h->eng;
     if (!E.pop_len) return fail(IE_ERR_INVALID, "ie_run_pa needs a handle created with num_pops > 1");
-    if (pc->ladder_mode != 0) return fail(IE_ERR_UNSUPPORTED, "only the acceptance-uniform ladder tuning is on this path");
+    if (pc->ladder_mode != 0 && pc->ladder_mode != 1) return fail(IE_ERR_INVALID, "ladder_mode must be 0 or 1");
     if (pc->use_icm) return fail(IE_ERR_UNSUPPORTED, "ICM cluster moves are not on this path");
     if (std::isnan(pc->ess_threshold)) return fail(IE_ERR_INVALID, "ess_threshold is NaN");
     IE_CUDA(cudaSetDevice(E.device));
@@ -1917,8 +1925,40 @@ ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
         IE_TRY(fresh_scratch());
         std::vector<uint64_t> att(L - 1), acc(L - 1);
         std::vector<double> rates(L - 1), sp(L - 1);
+        const bool feedback = pc->ladder_mode == 1;
+        std::vector<unsigned long long> rt(1 + 2 * (size_t)L);
+        if (feedback) {
+            IE_TRY(E.d_labels.alloc(E.total_energy));
+            IE_TRY(E.d_rt.alloc(rt.size()));
+            E.track_roundtrips = true;
+        }
         for (uint32_t it = 0; it < pc->ladder_tuning_iters; it++) {
             for (uint32_t t = 0; t < L; t++) temps[t] = tmax * std::pow(tmin / tmax, alphas[t]);
+            if (feedback) {
+                // reset_roundtrip_stats (engine.rs:529-536): counts and labels to zero
+                IE_CUDA(cudaMemsetAsync(E.d_labels.p, 0, E.total_energy, st));
+                IE_CUDA(cudaMemsetAsync(E.d_rt.p, 0, rt.size() * sizeof(unsigned long long), st));
+                const ie_status rs = run_steps(temps, pc->ladder_tuning_steps);
+                if (rs != IE_OK) {
+                    E.track_roundtrips = false;
+                    return rs;
+                }
+                IE_CUDA(cudaMemcpyAsync(rt.data(), E.d_rt.p, rt.size() * sizeof(unsigned long long),
+                                        cudaMemcpyDeviceToHost, st));
+                IE_CUDA(cudaStreamSynchronize(st));
+                // KTHT redistribution only with enough round trips (ultimate.rs:662-677)
+                if (rt[0] >= (unsigned long long)L) {
+                    std::vector<double> flow(L);
+                    for (uint32_t t = 0; t < L; t++) {
+                        const unsigned long long u = rt[1 + t], dn = rt[1 + L + t];
+                        flow[t] = u + dn == 0 ? 0.0 : (double)u / (double)(u + dn);
+                    }
+                    alphas = pa::feedback_optimized_alphas(alphas, flow, 0.5);
+                    alphas[0] = 0.0;
+                    alphas[L - 1] = 1.0;
+                }
+                continue;
+            }
             IE_CUDA(cudaMemsetAsync(E.d_att.p, 0, (L - 1) * sizeof(uint64_t), st));
             IE_CUDA(cudaMemsetAsync(E.d_acc.p, 0, (L - 1) * sizeof(uint64_t), st));
             IE_TRY(run_steps(temps, pc->ladder_tuning_steps));
@@ -1939,7 +1979,8 @@ ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
         }
     }
 
-    // production population
+    // production population (a fresh scratch: no round-trip tracking)
+    E.track_roundtrips = false;
     IE_TRY(E.init_random());
     IE_TRY(fresh_scratch());
     IE_TRY(h->d_inc_e.upload(std::vector<double>(1, std::numeric_limits<double>::infinity()), st));

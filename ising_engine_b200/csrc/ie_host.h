@@ -50,6 +50,8 @@ double free_energy_increment(const double* lw, size_t r);
 void family_entropy(const uint64_t* ids, size_t r, double& rho, uint64_t& families);
 std::vector<uint64_t> systematic_resample(const double* w, size_t r, double u);
 std::vector<double> adapt_spacings(const double* d, const double* acc, size_t k);
+std::vector<double> feedback_optimized_alphas(const std::vector<double>& alphas, const std::vector<double>& flow,
+                                              double damping);
 // apply_resample's parent list: parent i repeated counts[i] times, then the
 // Fisher-Yates shuffle with gen_range(0..=k) for k = len - 1 down to 1.
 std::vector<uint32_t> shuffled_parents(const std::vector<uint64_t>& counts, HostStream& rng);

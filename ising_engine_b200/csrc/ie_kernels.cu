@@ -1368,12 +1368,53 @@ __global__ void __launch_bounds__(32) exchange_kernel(DevArrays A, RunArgs R, ui
                     const unsigned Ab = __ballot_sync(0xffffffffu, ab);
                     if (aa) swap_energy(c, tid);
                     if (ab) swap_energy(c, tid + 32);
+                    if (R.labels) {
+                        int8_t* lab = R.labels + d.energy + (size_t)c * kReplicas;
+                        if (aa) {
+                            const int8_t x = lab[tid];
+                            lab[tid] = lab[kReplicas + tid];
+                            lab[kReplicas + tid] = x;
+                        }
+                        if (ab) {
+                            const int8_t x = lab[tid + 32];
+                            lab[tid + 32] = lab[kReplicas + tid + 32];
+                            lab[kReplicas + tid + 32] = x;
+                        }
+                    }
                     if (tid == 0) {
                         A.xmask[d.stat + c] = (uint64_t)Aa | ((uint64_t)Ab << 32);
                         A.att[d.stat + t] += kReplicas;
                         A.acc[d.stat + t] += (uint64_t)(__popc(Aa) + __popc(Ab));
                     }
                 }
+            if (R.labels && L >= 2) {
+                // the hot end's up-labels complete round trips; relabel both
+                // ends, then count labels per ladder position
+                for (int q = 0; q < pops; q++) {
+                    int8_t* hot = R.labels + d.energy + (size_t)(L * q) * kReplicas;
+                    int8_t* cold = R.labels + d.energy + (size_t)(L - 1 + L * q) * kReplicas;
+                    const unsigned done = __ballot_sync(0xffffffffu, hot[tid] == 1);
+                    const unsigned done2 = __ballot_sync(0xffffffffu, hot[tid + 32] == 1);
+                    hot[tid] = -1;
+                    hot[tid + 32] = -1;
+                    cold[tid] = 1;
+                    cold[tid + 32] = 1;
+                    __syncwarp();
+                    if (tid == 0) R.rt[0] += (unsigned long long)(__popc(done) + __popc(done2));
+                    for (int t = 0; t < L; t++) {
+                        const int8_t* lab = R.labels + d.energy + (size_t)(t + L * q) * kReplicas;
+                        const unsigned up = __ballot_sync(0xffffffffu, lab[tid] == 1);
+                        const unsigned up2 = __ballot_sync(0xffffffffu, lab[tid + 32] == 1);
+                        const unsigned dn = __ballot_sync(0xffffffffu, lab[tid] == -1);
+                        const unsigned dn2 = __ballot_sync(0xffffffffu, lab[tid + 32] == -1);
+                        if (tid == 0) {
+                            R.rt[1 + t] += (unsigned long long)(__popc(up) + __popc(up2));
+                            R.rt[1 + L + t] += (unsigned long long)(__popc(dn) + __popc(dn2));
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
         }
         deo ^= 1;
     }

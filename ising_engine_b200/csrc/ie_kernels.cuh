@@ -118,6 +118,12 @@ struct RunArgs {
     // stay inside a population and the exchange tables, dbeta and swap
     // statistics are indexed by the pair t within it
     uint32_t pop_len;
+    // round-trip tracking (engine.rs:794-816), on when labels is set: a
+    // direction label per (cell, replica) at the energy index, swapped with
+    // the replicas; rt[0] completed round trips, rt[1 + t] up-labels and
+    // rt[1 + L + t] down-labels counted at ladder position t after each exchange
+    int8_t* labels;
+    unsigned long long* rt;
     // when set, the launch's step_base is read from device memory (so a
     // captured CUDA graph of the launch stays valid across runs)
     const uint64_t* step_base_dev;

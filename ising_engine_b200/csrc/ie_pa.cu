@@ -1,7 +1,8 @@
 // Population-annealing primitives on the host (src/solver/population_annealing.rs:
 // normalized_weights :51-56, effective_sample_size :60-63,
 // free_energy_increment :70-78, family_entropy :84-101, systematic_resample
-// :106-127, adapt_spacings :141-152, the shuffle of apply_resample :240-260)
+// :106-127, adapt_spacings :141-152, feedback_optimized_alphas :172-232, the
+// shuffle of apply_resample :240-260)
 // and the master-stream draws they take: rand 0.8.5's gen_range on
 // rand_chacha 0.3.1's ChaCha8Rng, addressed by draw index like the device's
 // chacha8_draw.
@@ -139,6 +140,41 @@ std::vector<double> adapt_spacings(const double* d, const double* acc, size_t k)
     return out;
 }
 
+std::vector<double> feedback_optimized_alphas(const std::vector<double>& alphas, const std::vector<double>& flow,
+                                              double damping) {
+    const size_t nt = alphas.size();
+    if (nt < 3) return alphas;
+    constexpr double kEps = 1e-6;
+    std::vector<double> f(flow);  // cumulative max from the hot end
+    for (size_t k = 1; k < nt; k++) f[k] = f[k] < f[k - 1] ? f[k - 1] : f[k];
+    std::vector<double> mass(nt - 1), cum(nt, 0.0);
+    double total = 0.0;
+    for (size_t k = 0; k + 1 < nt; k++) {
+        mass[k] = std::sqrt(std::max(std::fabs(f[k + 1] - f[k]), kEps) *
+                            std::max(std::fabs(alphas[k + 1] - alphas[k]), kEps));
+        total += mass[k];
+    }
+    if (total <= 0.0 || !std::isfinite(total)) return alphas;
+    for (size_t k = 0; k + 1 < nt; k++) cum[k + 1] = cum[k] + mass[k];
+    std::vector<double> out(nt, 0.0);
+    out[0] = alphas[0];
+    out[nt - 1] = alphas[nt - 1];
+    size_t k = 0;
+    for (size_t i = 1; i + 1 < nt; i++) {
+        const double target = (double)i / (double)(nt - 1) * total;
+        k = 0;
+        while (k < nt - 2 && cum[k + 1] < target) k++;
+        const double frac = mass[k] > 0.0 ? (target - cum[k]) / mass[k] : 0.0;
+        out[i] = damping * (alphas[k] + frac * (alphas[k + 1] - alphas[k])) + (1.0 - damping) * alphas[i];
+    }
+    for (size_t i = 1; i < nt; i++)
+        if (out[i] <= out[i - 1]) out[i] = out[i - 1] + kEps;
+    const double base = out[0], span = out[nt - 1] - out[0], old_span = alphas[nt - 1] - alphas[0];
+    if (span > 0.0)
+        for (double& a : out) a = alphas[0] + (a - base) / span * old_span;
+    return out;
+}
+
 std::vector<uint32_t> shuffled_parents(const std::vector<uint64_t>& counts, HostStream& rng) {
     std::vector<uint32_t> parents;
     parents.reserve(counts.size());
@@ -183,6 +219,15 @@ ie_status ie_pa_systematic_resample(const double* w, uint64_t r, double u, uint6
     if ((!w || !counts) && r) return fail(IE_ERR_INVALID, "NULL argument");
     const std::vector<uint64_t> c = pa::systematic_resample(w, r, u);
     std::copy(c.begin(), c.end(), counts);
+    return IE_OK;
+}
+
+ie_status ie_pa_feedback_optimized_alphas(const double* alphas, const double* flow, uint64_t nt, double damping,
+                                          double* out) {
+    if ((!alphas || !flow || !out) && nt) return fail(IE_ERR_INVALID, "NULL argument");
+    const std::vector<double> a = pa::feedback_optimized_alphas(std::vector<double>(alphas, alphas + nt),
+                                                                std::vector<double>(flow, flow + nt), damping);
+    std::copy(a.begin(), a.end(), out);
     return IE_OK;
 }
 

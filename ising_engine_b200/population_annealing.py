@@ -3,7 +3,8 @@
 Mirrors src/solver/population_annealing.rs: the reweighting / resampling
 primitives (``normalized_weights`` :51-56, ``effective_sample_size`` :60-63,
 ``free_energy_increment`` :70-78, ``family_entropy`` :84-101,
-``systematic_resample`` :106-127, ``adapt_spacings`` :141-152) computed by the
+``systematic_resample`` :106-127, ``adapt_spacings`` :141-152,
+``feedback_optimized_alphas`` :172-232) computed by the
 library's host code, and ``PaDiagnostics`` (:34-45). The annealing driver
 (ultimate.rs:576-852) runs on the device through ``Engine.run_pa``.
 """
@@ -31,6 +32,12 @@ class PaDiagnostics:
     alphas: np.ndarray | None = None
 
 
+# LadderMode (ultimate.rs): acceptance uniformization (default) or the
+# feedback-optimized ladder of Katzgraber, Trebst, Huse and Troyer
+ACCEPTANCE_UNIFORM = 0
+FEEDBACK_OPTIMIZED = 1
+
+
 @dataclass
 class PaConfig:
     """The PA knobs of UltimateSolver (ultimate.rs:29-52) with their defaults
@@ -39,10 +46,12 @@ class PaConfig:
     ladder_tuning_iters: int = 8
     ladder_tuning_steps: int = 10
     post_resample_relaxation: int = 5
+    ladder_mode: int = ACCEPTANCE_UNIFORM
 
     def to_c(self) -> _ffi.ie_pa_config:
         return _ffi.ie_pa_config(float(self.ess_threshold), int(self.ladder_tuning_iters),
-                                 int(self.ladder_tuning_steps), int(self.post_resample_relaxation), 0, 0)
+                                 int(self.ladder_tuning_steps), int(self.post_resample_relaxation),
+                                 int(self.ladder_mode), 0)
 
 
 def normalized_weights(log_w) -> np.ndarray:
@@ -88,4 +97,15 @@ def adapt_spacings(spacings, acceptance) -> np.ndarray:
         raise ValueError("spacings and acceptance must have the same length")
     out = np.zeros(len(d), dtype=np.float64)
     _ffi.check(_ffi.lib().ie_pa_adapt_spacings(_p(d), _p(a), len(d), _p(out)))
+    return out
+
+
+def feedback_optimized_alphas(alphas, flow, damping: float) -> np.ndarray:
+    """population_annealing.rs:172-232."""
+    a = np.ascontiguousarray(alphas, dtype=np.float64)
+    f = np.ascontiguousarray(flow, dtype=np.float64)
+    if a.shape != f.shape:
+        raise ValueError("alphas and flow must have the same length")
+    out = np.zeros(len(a), dtype=np.float64)
+    _ffi.check(_ffi.lib().ie_pa_feedback_optimized_alphas(_p(a), _p(f), len(a), float(damping), _p(out)))
     return out

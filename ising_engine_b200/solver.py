@@ -81,6 +81,7 @@ class UltimateSolver:
         self.ladder_tuning_iters = 8
         self.ladder_tuning_steps = 10
         self.post_resample_relaxation = 5
+        self.ladder_mode = 0  # 0 acceptance-uniform, 1 feedback-optimized (LadderMode)
         # presolve and decomposition before annealing (ultimate.rs:161-218); an
         # extension may switch them off, e.g. where probing's O(n^2 nnz) cost
         # is too high
@@ -101,7 +102,7 @@ class UltimateSolver:
     def pa_config(self):
         from .population_annealing import PaConfig
         return PaConfig(self.ess_threshold, self.ladder_tuning_iters, self.ladder_tuning_steps,
-                        self.post_resample_relaxation)
+                        self.post_resample_relaxation, self.ladder_mode)
 
     def engine(self, model: QuboModel, num_pops: int | None = None) -> Engine:
         return Engine(model, num_temps=self.num_temps, seed=self.seed,

@@ -285,6 +285,13 @@ static void replica_energies(const Qubo& m, const int8_t* spins, double* en) {
 struct StepScratch {
     std::vector<uint64_t> attempts, accepts;
     bool deo_odd = false;
+    // round-trip tracking (engine.rs:454-536, opt-in): direction label per
+    // (cell, replica) (+1 up, -1 down, 0 none), up/down histograms per
+    // temperature, completed round trips
+    bool track = false;
+    std::vector<std::array<int8_t, NR>> labels;
+    std::vector<uint64_t> n_up, n_down;
+    uint64_t rt = 0;
 };
 
 // A tiny fork/join pool standing in for Rayon's par_chunks_mut (engine.rs:603-608).
@@ -364,7 +371,10 @@ static void exchange(Field& f, const double* temps, StepScratch& sc, ChaCha8Rng&
                         c2[v * NR + r] ^= dd;
                     }
                 for (int r = 0; r < NR; r++)
-                    if (mask[r]) std::swap(e1[r], e2[r]);
+                    if (mask[r]) {
+                        std::swap(e1[r], e2[r]);
+                        if (sc.track) std::swap(sc.labels[t + nt * p][r], sc.labels[t + 1 + nt * p][r]);
+                    }
             }
         }
     }
@@ -386,6 +396,21 @@ static void step(Field& f, const Qubo& m, const double* temps, const std::vector
     });
     if (do_exchange) {
         exchange(f, temps, sc, rng, stats);
+        // engine.rs:794-816: relabel the ends, count round trips, histogram
+        if (sc.track && f.nt >= 2)
+            for (int p = 0; p < f.np; p++) {
+                const int hot = f.nt * p, cold = f.nt - 1 + f.nt * p;
+                for (int r = 0; r < NR; r++) {
+                    if (sc.labels[hot][r] == 1) sc.rt++;
+                    sc.labels[hot][r] = -1;
+                    sc.labels[cold][r] = 1;
+                }
+                for (int t = 0; t < f.nt; t++)
+                    for (int r = 0; r < NR; r++) {
+                        if (sc.labels[t + f.nt * p][r] == 1) sc.n_up[t]++;
+                        else if (sc.labels[t + f.nt * p][r] == -1) sc.n_down[t]++;
+                    }
+            }
         sc.deo_odd = !sc.deo_odd;
     }
 }
@@ -911,8 +936,8 @@ static std::vector<int8_t> solve(const Qubo& m, const Assign& clamped, const Sol
 // src/solver/population_annealing.rs:51-287 (weights, ESS, free energy,
 // family entropy, systematic resampling, spacing adaptation, apply_resample)
 // and UltimateSolver::solve_population_annealing_diag (ultimate.rs:576-852)
-// in its defaults: acceptance-uniform ladder tuning, ICM, GNN warm start and
-// 2-opt off. Entered as solve_with_pa_diagnostics does (ultimate.rs:858-890):
+// with either ladder mode (acceptance-uniform, the default, or feedback-
+// optimized with round-trip tracking); ICM, GNN warm start and 2-opt off. Entered as solve_with_pa_diagnostics does (ultimate.rs:858-890):
 // no presolve or decomposition.
 // ---------------------------------------------------------------------------
 
@@ -1032,6 +1057,44 @@ static std::vector<int64_t> pa_apply_resample(Field& f, const std::vector<int64_
     return parents;
 }
 
+// population_annealing.rs:172-232: monotone flow, interval masses
+// sqrt(max(|df|, 1e-6) * max(|da|, 1e-6)), interior points equidistributed
+// in cumulative mass (damped), strict order enforced, endpoints rescaled.
+static std::vector<double> pa_feedback_alphas(const std::vector<double>& alphas, const std::vector<double>& flow,
+                                              double damping) {
+    const size_t nt = alphas.size();
+    if (nt < 3) return alphas;
+    std::vector<double> f = flow;
+    for (size_t k = 1; k < nt; k++)
+        if (f[k] < f[k - 1]) f[k] = f[k - 1];
+    const double eps = 1e-6;
+    std::vector<double> mass(nt - 1);
+    for (size_t k = 0; k + 1 < nt; k++)
+        mass[k] = std::sqrt(std::max(std::fabs(f[k + 1] - f[k]), eps) * std::max(std::fabs(alphas[k + 1] - alphas[k]), eps));
+    double total = 0.0;
+    for (double x : mass) total += x;
+    if (total <= 0.0 || !std::isfinite(total)) return alphas;
+    std::vector<double> cum(nt, 0.0);
+    for (size_t k = 0; k + 1 < nt; k++) cum[k + 1] = cum[k] + mass[k];
+    std::vector<double> na(nt, 0.0);
+    na[0] = alphas[0];
+    na[nt - 1] = alphas[nt - 1];
+    for (size_t i = 1; i + 1 < nt; i++) {
+        const double target = (double)i / (double)(nt - 1) * total;
+        size_t k = 0;
+        while (k < nt - 2 && cum[k + 1] < target) k++;
+        const double frac = mass[k] > 0.0 ? (target - cum[k]) / mass[k] : 0.0;
+        const double interp = alphas[k] + frac * (alphas[k + 1] - alphas[k]);
+        na[i] = damping * interp + (1.0 - damping) * alphas[i];
+    }
+    for (size_t i = 1; i < nt; i++)
+        if (na[i] <= na[i - 1]) na[i] = na[i - 1] + eps;
+    const double base = na[0], span = na[nt - 1] - na[0], old_span = alphas[nt - 1] - alphas[0];
+    if (span > 0.0)
+        for (double& a : na) a = alphas[0] + (a - base) / span * old_span;
+    return na;
+}
+
 struct PaCfg {
     double tmax, tmin;
     int64_t sweeps, exchanges;
@@ -1040,6 +1103,7 @@ struct PaCfg {
     double ess_threshold;
     int64_t tuning_iters, tuning_steps, relax;
     int threads;
+    int ladder_mode;  // 0 acceptance-uniform, 1 feedback-optimized
 };
 
 struct PaOut {
@@ -1074,12 +1138,37 @@ static Field pa_run(const Qubo& m, const std::vector<uint8_t>& is_clamped, const
         StepScratch sc;
         sc.attempts.assign(nt - 1, 0);
         sc.accepts.assign(nt - 1, 0);
+        const bool feedback = cfg.ladder_mode == 1;
+        sc.track = feedback;
+        sc.labels.assign((size_t)nt * pops, {});
+        sc.n_up.assign(nt, 0);
+        sc.n_down.assign(nt, 0);
         for (int64_t it = 0; it < cfg.tuning_iters; it++) {
             for (int t = 0; t < nt; t++) temps[t] = cfg.tmax * std::pow(cfg.tmin / cfg.tmax, alphas[t]);
-            std::fill(sc.attempts.begin(), sc.attempts.end(), 0);
-            std::fill(sc.accepts.begin(), sc.accepts.end(), 0);
+            if (feedback) {
+                std::fill(sc.n_up.begin(), sc.n_up.end(), 0);
+                std::fill(sc.n_down.begin(), sc.n_down.end(), 0);
+                sc.rt = 0;
+                for (auto& l : sc.labels) l.fill(0);
+            } else {
+                std::fill(sc.attempts.begin(), sc.attempts.end(), 0);
+                std::fill(sc.accepts.begin(), sc.accepts.end(), 0);
+            }
             for (int64_t s = 0; s < cfg.tuning_steps; s++)
-                step(tf, m, temps.data(), is_clamped, sc, rng, true, true, cfg.threads, nullptr);
+                step(tf, m, temps.data(), is_clamped, sc, rng, true, !feedback, cfg.threads, nullptr);
+            if (feedback) {
+                if (sc.rt >= (uint64_t)nt) {
+                    std::vector<double> flow(nt);
+                    for (int t = 0; t < nt; t++) {
+                        const uint64_t u = sc.n_up[t], d = sc.n_down[t];
+                        flow[t] = u + d == 0 ? 0.0 : (double)u / (double)(u + d);
+                    }
+                    alphas = pa_feedback_alphas(alphas, flow, 0.5);
+                    alphas[0] = 0.0;
+                    alphas[nt - 1] = 1.0;
+                }
+                continue;
+            }
             std::vector<double> rates(nt - 1), sp(nt - 1);
             for (int t = 0; t + 1 < nt; t++) {
                 rates[t] = sc.attempts[t] == 0 ? 0.0 : (double)sc.accepts[t] / (double)sc.attempts[t];
@@ -1598,7 +1687,7 @@ int or_run_sa_batch(int64_t count, const int64_t* ns, const double* const* lins,
 int or_pa_run(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,
               double offset, double tmax, double tmin, int64_t sweeps, int64_t exchanges, uint64_t seed, int nt,
               int pops, double ess_threshold, int64_t tuning_iters, int64_t tuning_steps, int64_t relax,
-              const uint8_t* clamped, const int8_t* clamp_val, int threads, uint64_t* words_out,
+              int ladder_mode, const uint8_t* clamped, const int8_t* clamp_val, int threads, uint64_t* words_out,
               double* energies_out, uint64_t* draws_out, double* alphas_out, double* ess_out, int64_t* n_ess,
               double* rho_out, int64_t* fam_out, int64_t* n_res, double* free_energy_out, int8_t* best_pre_out,
               double* incumbent_out, int8_t* state_out) {
@@ -1609,7 +1698,8 @@ int or_pa_run(int64_t n, const double* lin, const int64_t* row, const int64_t* c
         cl[i] = clamped ? clamped[i] : 0;
         cv[i] = clamp_val ? clamp_val[i] : 0;
     }
-    PaCfg cfg{tmax, tmin, sweeps, exchanges, seed, nt, pops, ess_threshold, tuning_iters, tuning_steps, relax, threads};
+    PaCfg cfg{tmax, tmin, sweeps, exchanges, seed, nt, pops, ess_threshold, tuning_iters, tuning_steps, relax, threads,
+              ladder_mode};
     ChaCha8Rng rng(seed);
     PaOut o;
     Field f = pa_run(m, cl, cv, cfg, o, rng);
@@ -1638,6 +1728,11 @@ void or_pa_normalized_weights(const double* lw, int64_t r, double* out) {
 void or_pa_systematic_resample(const double* w, int64_t r, double u, int64_t* counts) {
     const auto c = pa_systematic_resample(std::vector<double>(w, w + r), u);
     std::copy(c.begin(), c.end(), counts);
+}
+void or_pa_feedback_alphas(const double* alphas, const double* flow, int64_t nt, double damping, double* out) {
+    const auto a = pa_feedback_alphas(std::vector<double>(alphas, alphas + nt), std::vector<double>(flow, flow + nt),
+                                      damping);
+    std::copy(a.begin(), a.end(), out);
 }
 // gen_range(0..=hi[i]) in sequence on ChaCha8Rng::seed_from_u64(seed).
 void or_gen_index_inclusive(uint64_t seed, const uint64_t* hi, int64_t count, uint64_t* out, uint64_t* draws) {

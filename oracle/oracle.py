@@ -76,10 +76,11 @@ def lib():
                                     _u64p, _f64p, _i64p, _f64p, _u64p]
         L.or_pa_run.argtypes = [
             C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int64,
-            C.c_uint64, C.c_int, C.c_int, C.c_double, C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
-            C.c_int, _u64p, _f64p, _u64p, _f64p, _f64p, _i64p, _f64p, _i64p, _i64p, _f64p, _i8p, _f64p, _i8p]
+            C.c_uint64, C.c_int, C.c_int, C.c_double, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_void_p,
+            C.c_void_p, C.c_int, _u64p, _f64p, _u64p, _f64p, _f64p, _i64p, _f64p, _i64p, _i64p, _f64p, _i8p, _f64p, _i8p]
         L.or_pa_normalized_weights.argtypes = [_f64p, C.c_int64, _f64p]
         L.or_pa_systematic_resample.argtypes = [_f64p, C.c_int64, C.c_double, _i64p]
+        L.or_pa_feedback_alphas.argtypes = [_f64p, _f64p, C.c_int64, C.c_double, _f64p]
         L.or_gen_index_inclusive.argtypes = [C.c_uint64, _u64p, C.c_int64, _u64p, _u64p]
         _lib = L
     return _lib
@@ -272,7 +273,8 @@ def v2_program(model, r, init, seed, ops, temps, skip_draws=0):
 
 
 def pa_run(model, temp_max, temp_min, sweeps, exchanges, seed, num_temps, num_pops, ess_threshold=0.5,
-           tuning_iters=8, tuning_steps=10, relax=5, clamped=None, clamp_val=None, threads=1, offset=0.0):
+           tuning_iters=8, tuning_steps=10, relax=5, clamped=None, clamp_val=None, threads=1, offset=0.0,
+           ladder_mode=0):
     """UltimateSolver::new(temp_max, temp_min, sweeps, exchanges, Some(seed)) with
     num_temps, num_pops and the PA knobs, through solve_with_pa_diagnostics
     (ultimate.rs:576-890). Returns a dict: words [nt*pops, n], energies
@@ -299,7 +301,7 @@ def pa_run(model, temp_max, temp_min, sweeps, exchanges, seed, num_temps, num_po
     L = lib()
     L.or_pa_run(n, lin, row, col, val, float(offset), float(temp_max), float(temp_min), int(sweeps), int(exchanges),
                 int(seed), int(num_temps), int(num_pops), float(ess_threshold), int(tuning_iters), int(tuning_steps),
-                int(relax), _ptr(cl), _ptr(cv), int(threads), words, en, draws, alphas, ess, n_ess, rho, fam, n_res, fe, best_pre,
+                int(relax), int(ladder_mode), _ptr(cl), _ptr(cv), int(threads), words, en, draws, alphas, ess, n_ess, rho, fam, n_res, fe, best_pre,
                 inc, state)
     ne, nr = int(n_ess[0]), int(n_res[0])
     return dict(words=words.reshape(cells, n), energies=en.reshape(cells, 64), draws=int(draws[0]), alphas=alphas,
@@ -329,3 +331,11 @@ def gen_index_inclusive(seed: int, his):
     draws = np.zeros(1, dtype=np.uint64)
     lib().or_gen_index_inclusive(int(seed), hi, len(hi), out, draws)
     return out, int(draws[0])
+
+
+def pa_feedback_alphas(alphas, flow, damping) -> np.ndarray:
+    a = np.ascontiguousarray(alphas, dtype=np.float64)
+    f = np.ascontiguousarray(flow, dtype=np.float64)
+    out = np.zeros(len(a), dtype=np.float64)
+    lib().or_pa_feedback_alphas(a, f, len(a), float(damping), out)
+    return out

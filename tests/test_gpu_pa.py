@@ -22,7 +22,8 @@ pytestmark = pytest.mark.gpu
 
 def check_pa(m, tmax, tmin, sweeps, exchanges, seed, nt, pops, cfg, clamped=None, cval=None):
     ref = O.pa_run(m, tmax, tmin, sweeps, exchanges, seed, nt, pops, cfg.ess_threshold, cfg.ladder_tuning_iters,
-                   cfg.ladder_tuning_steps, cfg.post_resample_relaxation, clamped=clamped, clamp_val=cval, threads=8)
+                   cfg.ladder_tuning_steps, cfg.post_resample_relaxation, clamped=clamped, clamp_val=cval, threads=8,
+                   ladder_mode=cfg.ladder_mode)
     with Engine(m, num_temps=nt, num_pops=pops, seed=seed, temp_max=tmax, temp_min=tmin,
                 sweeps_per_exchange=sweeps, total_exchanges=exchanges) as eng:
         if clamped is not None:
@@ -76,6 +77,28 @@ def test_two_level_ladder_without_tuning_and_one_stage():
     m = random_qubo(40, 0.3, 3, integral=True)
     check_pa(m, 3.0, 0.5, 5, 6, 12, 2, 2, PaConfig(ess_threshold=0.95))
     check_pa(m, 3.0, 0.5, 7, 1, 13, 3, 3, PaConfig())
+
+
+@pytest.mark.parametrize("integral", [True, False])
+def test_feedback_optimized_ladder(integral):
+    """LadderMode::FeedbackOptimized: round-trip labels travel with the
+    replicas through the exchanges, the flow histogram moves the ladder
+    (enough tuning steps for round trips) — all bit for bit."""
+    m = I.maxcut_gnm(150, 900, seed=6) if integral else random_qubo(100, 0.08, 6)
+    ref = check_pa(m, 5.0, 0.5 if integral else 0.1, 3, 6, 17, 7, 2, PaConfig(ess_threshold=0.9, ladder_tuning_iters=4,
+                                                         ladder_tuning_steps=120, ladder_mode=1))
+    assert not np.allclose(ref["alphas"], np.arange(7) / 6)
+
+
+def test_feedback_ladder_solver_optimal():
+    """test_feedback_ladder.rs:108-131 on the device."""
+    for trial in range(2):
+        m = random_qubo(14, 0.4, 3 + trial)
+        s = UltimateSolver(10.0, 0.05, 5, 15, 700 + trial).with_quantum_dims(1, 8, 2)
+        s.ladder_mode = 1
+        a = s.solve(m)
+        assert np.array_equal(a, s.solve(m))
+        assert abs(m.calculate_total_energy(a) - brute_force(m)) < 1e-9
 
 
 def test_device_pa_finds_optimum_honors_clamps_is_deterministic():

@@ -175,3 +175,44 @@ def test_oracle_pa_diagnostics():
     assert ((r["rho"] >= 1 - 1e-6) & (r["rho"] <= R + 1e-6)).all() and (r["families"] >= 1).all()
     a = r["alphas"]
     assert a[0] == 0.0 and a[-1] == 1.0 and (np.diff(a) > 0).all()
+
+
+def test_feedback_optimized_alphas():
+    """test_feedback_ladder.rs:11-59 on the library's function, and bit for
+    bit against the oracle's on random profiles."""
+    nt = 8
+    a = np.arange(nt) / (nt - 1)
+    out = P.feedback_optimized_alphas(a, a.copy(), 1.0)
+    assert np.allclose(out, a, atol=1e-9, rtol=0)
+    nt = 9
+    a = np.arange(nt) / (nt - 1)
+    flow = 1.0 / (1.0 + np.exp(-20.0 * (a - 0.5)))
+    out = P.feedback_optimized_alphas(a, flow, 1.0)
+    c = nt // 2
+    assert out[c] - out[c - 1] < out[1] - out[0]
+    assert abs(out[0]) < 1e-9 and abs(out[-1] - 1.0) < 1e-9 and (np.diff(out) > 0).all()
+    rng = np.random.default_rng(8)
+    for k in (2, 3, 5, 12):
+        a = np.sort(rng.random(k))
+        f = rng.random(k)
+        for damp in (0.5, 1.0):
+            assert np.array_equal(P.feedback_optimized_alphas(a, f, damp), O.pa_feedback_alphas(a, f, damp))
+    assert np.array_equal(P.feedback_optimized_alphas([0, 0.5, 1], [0, 0, 0], 0.5),
+                          O.pa_feedback_alphas([0, 0.5, 1], [0, 0, 0], 0.5))
+
+
+def test_oracle_feedback_ladder_solver():
+    """test_feedback_ladder.rs:108-131 on the oracle: deterministic, reaches
+    the exhaustive optimum, and the tuned ladder moved off the geometric one."""
+    for trial in range(3):
+        m = random_qubo(14, 0.4, 3 + trial)
+        a = O.pa_run(m, 10.0, 0.05, 5, 15, 700 + trial, 8, 2, ladder_mode=1, threads=4)
+        b = O.pa_run(m, 10.0, 0.05, 5, 15, 700 + trial, 8, 2, ladder_mode=1, threads=4)
+        assert np.array_equal(a["state"], b["state"]) and a["draws"] == b["draws"]
+        assert abs(m.calculate_total_energy(a["state"]) - brute_force(m)) < 1e-9
+    # 10 tuning steps per iteration give fewer round trips than levels (the
+    # shape stays geometric, ultimate.rs:662-669); 120 steps move it
+    assert np.array_equal(a["alphas"], np.arange(8) / 7)
+    c = O.pa_run(m, 10.0, 0.05, 5, 15, 9, 8, 2, tuning_steps=120, ladder_mode=1, threads=4)
+    assert not np.allclose(c["alphas"], np.arange(8) / 7)
+    assert c["alphas"][0] == 0.0 and c["alphas"][-1] == 1.0 and (np.diff(c["alphas"]) > 0).all()
