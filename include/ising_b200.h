@@ -69,6 +69,8 @@ typedef struct ie_config {
     int32_t pt_path;     /* 0: chosen by size; 1: one CTA runs all cells of the instance;
                             2: every cell is its own work item of the batched kernels, the
                             exchange runs between their launches (same results) */
+    int32_t use_icm;     /* UltimateSolver::use_icm: an ICM sweep (src/solver/icm.rs) after every
+                            exchange block of ie_run_pt; 0 by default */
 } ie_config;
 
 typedef struct ie_handle ie_handle;
@@ -83,7 +85,7 @@ typedef struct ie_pa_config {
     uint32_t post_resample_relaxation; /* 5 by default */
     int32_t ladder_mode;               /* 0: LadderMode::AcceptanceUniform (the default);
                                           1: LadderMode::FeedbackOptimized (round-trip tracking) */
-    int32_t use_icm;                   /* must be 0 (the default) */
+    int32_t use_icm;                   /* ICM sweep after every stage (ultimate.rs:800-808); 0 by default */
 } ie_pa_config;
 
 /* PaDiagnostics (population_annealing.rs:34-45) plus the frozen ladder

@@ -37,7 +37,8 @@ class ie_config(C.Structure):
                 ("sweeps_per_exchange", C.c_uint64), ("total_exchanges", C.c_uint64),
                 ("seed", C.c_uint64), ("num_temps", C.c_uint32), ("num_pops", C.c_uint32),
                 ("num_slices", C.c_uint32), ("exchange_interval", C.c_uint32),
-                ("force_f64", C.c_int32), ("device", C.c_int32), ("pt_path", C.c_int32)]
+                ("force_f64", C.c_int32), ("device", C.c_int32), ("pt_path", C.c_int32),
+                ("use_icm", C.c_int32)]
 
 
 class ie_problem_device(C.Structure):

@@ -399,6 +399,25 @@ struct Engine {
     bool track_roundtrips = false;
     DevBuf<int8_t> d_labels;
     DevBuf<unsigned long long> d_rt;
+    DevBuf<uint32_t> d_icm_count, d_icm_rank, d_icm_stack;
+    DevBuf<uint8_t> d_icm_flags;
+
+    // icm_sweep (src/solver/icm.rs:161-185) on instance 0: up to 256 MiB of
+    // scratch (9 bytes per site per concurrent pair)
+    ie_status icm_sweep() {
+        const InstDesc& d = desc[0];
+        if (d.n == 0) return IE_OK;
+        const uint32_t pairs = nt * 32u;
+        const uint64_t per = 9ull * d.n;
+        const uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(pairs, (256ull << 20) / per));
+        IE_TRY(d_icm_count.alloc(pairs));
+        IE_TRY(d_icm_rank.alloc(pairs));
+        IE_TRY(d_icm_flags.alloc((size_t)slots * d.n));
+        IE_TRY(d_icm_stack.alloc((size_t)slots * 2 * d.n));
+        IE_CUDA(launch_icm(arrays(), 0, d.mode, nt, d_icm_count.p, d_icm_rank.p, d_icm_flags.p, d_icm_stack.p, slots,
+                           stream));
+        return IE_OK;
+    }
 
     ~Engine() {
         if (device >= 0) cudaSetDevice(device);
@@ -1876,6 +1895,7 @@ ie_status ie_run_pt(ie_handle* h) {
     const uint32_t n_words = (uint32_t)h->d_inc_state.n;
     for (uint64_t ex = 0; ex < h->cfg.total_exchanges; ex++) {
         IE_TRY(h->eng.run_pt(temps.data(), h->cfg.sweeps_per_exchange, false, h->cfg.exchange_interval));
+        if (h->cfg.use_icm) IE_TRY(h->eng.icm_sweep());  // ultimate.rs:326-328
         IE_CUDA(launch_incumbent(h->eng.arrays(), 0, h->offset, h->d_inc_e.p, h->d_inc_state.p, n_words,
                                  h->eng.stream));
     }
@@ -1885,7 +1905,7 @@ ie_status ie_run_pt(ie_handle* h) {
 }
 
 // UltimateSolver::solve_population_annealing_diag (ultimate.rs:576-852) with
-// either ladder mode and no ICM. The steps, energies and
+// either ladder mode and optional ICM. The steps, energies and
 // resampled configurations stay on the device; per stage the host reads the
 // cold-level energies (64 per population) for the weights and, on a
 // resampling event, takes the offset and shuffle draws from the master
@@ -1895,7 +1915,6 @@ ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
     Engine& E = h->eng;
     if (!E.pop_len) return fail(IE_ERR_INVALID, "ie_run_pa needs a handle created with num_pops > 1");
     if (pc->ladder_mode != 0 && pc->ladder_mode != 1) return fail(IE_ERR_INVALID, "ladder_mode must be 0 or 1");
-    if (pc->use_icm) return fail(IE_ERR_UNSUPPORTED, "ICM cluster moves are not on this path");
     if (std::isnan(pc->ess_threshold)) return fail(IE_ERR_INVALID, "ess_threshold is NaN");
     IE_CUDA(cudaSetDevice(E.device));
     const uint32_t L = E.pop_len, pops = E.nt / L, R = pops * (uint32_t)kReplicas;
@@ -2047,8 +2066,12 @@ ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
         have_prev = true;
         beta_prev = beta_cold;
         IE_TRY(run_steps(temps, h->cfg.sweeps_per_exchange));
-        // exact re-sync of every level, then the stage's incumbent
+        // exact re-sync of every level (again after ICM), then the stage's incumbent
         IE_CUDA(launch_energy(E.arrays(), 0, 1, st));
+        if (pc->use_icm) {
+            IE_TRY(E.icm_sweep());
+            IE_CUDA(launch_energy(E.arrays(), 0, 1, st));
+        }
         IE_CUDA(launch_incumbent(E.arrays(), 0, h->offset, h->d_inc_e.p, h->d_inc_state.p, n_words, st));
     }
     IE_CUDA(cudaStreamSynchronize(st));

@@ -1483,6 +1483,139 @@ __global__ void resample_kernel(DevArrays A, uint32_t inst, uint32_t pop_len, co
 }
 
 // ---------------------------------------------------------------------------
+// Isoenergetic cluster moves (src/solver/icm.rs:91-185) on lane pairs
+// (r, r + 32) of every cell of instance `inst`, pair k = 32 * cell + r.
+// Pairs touch disjoint lanes, so they are independent except for the
+// master-stream draws of their seeds, which follow pair order:
+//  icm_count_kernel  one warp per cell, lane r counts pair r's disagreements
+//                    (the cell's words are read once, broadcast);
+//  icm_draw_kernel   one thread walks the pairs in order and takes each
+//                    seed rank with rand's gen_range(0..count) from the
+//                    stream (no draw when the replicas agree everywhere);
+//  icm_move_kernel   one thread per pair: the rank-th disagreeing site,
+//                    the depth-first cluster along the CSR rows, delta_a in
+//                    cluster order, the cluster flipped in both lanes
+//                    (atomic XOR: other pairs flip other bits of the same
+//                    words) and the tracked energies moved by +-delta_a.
+// Scratch per concurrent pair: n flag bytes and 2n u32 (stack, cluster).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t lane_bit(uint32_t r) { return ((r & 7u) << 3) | (r >> 3); }
+
+__global__ void __launch_bounds__(32) icm_count_kernel(DevArrays A, uint32_t inst, uint32_t* count) {
+    const InstDesc d = A.desc[inst];
+    const uint32_t c = blockIdx.x, r = threadIdx.x;
+    const uint64_t* w = A.spins + d.spin + (size_t)c * d.n;
+    const uint32_t pa = lane_bit(r), pb = lane_bit(r + 32);
+    uint32_t k = 0;
+    for (uint32_t v = 0; v < d.n; v++) {
+        const uint64_t x = w[v];
+        k += (uint32_t)(((x >> pa) ^ (x >> pb)) & 1ull);
+    }
+    count[(size_t)c * 32 + r] = k;
+}
+
+__global__ void icm_draw_kernel(DevArrays A, uint32_t inst, const uint32_t* count, uint32_t* rank) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const InstDesc d = A.desc[inst];
+    uint32_t key[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) key[i] = A.keys[8 * (size_t)inst + i];
+    uint64_t pos = A.pos[inst];
+    const uint32_t pairs = d.nt * 32u;
+    for (uint32_t k = 0; k < pairs; k++) {
+        const uint32_t m = count[k];
+        if (m == 0) {
+            rank[k] = 0xFFFFFFFFu;
+            continue;
+        }
+        // rand 0.8.5 sample_single_inclusive(0, m - 1): zone = (m << lz(m)) - 1
+        const uint64_t range = m;
+        const uint64_t zone = (range << __clzll((long long)range)) - 1;
+        for (;;) {
+            const uint64_t v = chacha8_draw(key, pos++);
+            if (v * range <= zone) {
+                rank[k] = (uint32_t)__umul64hi(v, range);
+                break;
+            }
+        }
+    }
+    A.pos[inst] = pos;
+}
+
+template <uint32_t MODE>
+__global__ void __launch_bounds__(64) icm_move_kernel(DevArrays A, uint32_t inst, const uint32_t* rank, uint8_t* flags,
+                                                      uint32_t* stack, uint32_t slots) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= slots) return;
+    const InstDesc d = A.desc[inst];
+    const uint32_t n = d.n;
+    const uint32_t* rows = A.rows + d.row;
+    const uint32_t* cols = A.cols + d.ent;
+    const double* vals = A.vals + d.ent;
+    const double* lin = A.lin + d.site;
+    uint8_t* fl = flags + (size_t)slot * n;       // bit 0 visited, bit 1 in cluster
+    uint32_t* st = stack + (size_t)slot * 2 * n;  // [0, n) stack, [n, 2n) cluster
+    uint32_t* cl = st + n;
+    for (uint32_t k = slot; k < d.nt * 32u; k += slots) {
+        const uint32_t seed_rank = rank[k];
+        if (seed_rank == 0xFFFFFFFFu) continue;
+        const uint32_t c = k / 32, a = k % 32, b = a + 32;
+        const uint32_t pa = lane_bit(a), pb = lane_bit(b);
+        unsigned long long* w = reinterpret_cast<unsigned long long*>(A.spins + d.spin + (size_t)c * n);
+        uint32_t seed = 0, seen = 0;
+        for (uint32_t v = 0; v < n; v++) {
+            const uint64_t x = w[v];
+            const bool dis = ((x >> pa) ^ (x >> pb)) & 1ull;
+            fl[v] = dis ? 0 : 1;
+            if (dis) {
+                if (seen == seed_rank) seed = v;
+                seen++;
+            }
+        }
+        uint32_t sp = 0, nc = 0;
+        st[sp++] = seed;
+        fl[seed] = 3;
+        while (sp) {
+            const uint32_t i = st[--sp];
+            cl[nc++] = i;
+            for (uint32_t e = rows[i]; e < rows[i + 1]; e++) {
+                const uint32_t j = cols[e];
+                if (!(fl[j] & 1)) {
+                    fl[j] = 3;
+                    st[sp++] = j;
+                }
+            }
+        }
+        // icm.rs:55-89 in cluster order; every product is by 0 or +-1 (exact)
+        double delta = 0.0;
+        for (uint32_t q = 0; q < nc; q++) {
+            const uint32_t i = cl[q];
+            const double xi = (double)((w[i] >> pa) & 1ull);
+            delta = __dadd_rn(delta, __dmul_rn(lin[i], 1.0 - 2.0 * xi));
+            for (uint32_t e = rows[i]; e < rows[i + 1]; e++) {
+                const uint32_t j = cols[e];
+                const double xj = (double)((w[j] >> pa) & 1ull);
+                if (fl[j] & 2) {
+                    if (i < j) delta = __dadd_rn(delta, __dmul_rn(vals[e], (1.0 - xi) * (1.0 - xj) - xi * xj));
+                } else {
+                    delta = __dadd_rn(delta, __dmul_rn(__dmul_rn(vals[e], xj), 1.0 - 2.0 * xi));
+                }
+            }
+        }
+        const unsigned long long m = (1ull << pa) | (1ull << pb);
+        for (uint32_t q = 0; q < nc; q++) atomicXor(w + cl[q], m);
+        const size_t ea = d.energy + (size_t)c * kReplicas + a, eb = ea + 32;
+        if constexpr (MODE == kModeInt) {
+            A.Ei[ea] += (int32_t)delta;
+            A.Ei[eb] -= (int32_t)delta;
+        } else {
+            A.Ef[ea] = __dadd_rn(A.Ef[ea], delta);
+            A.Ef[eb] = __dsub_rn(A.Ef[eb], delta);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Random init (ultimate.rs:248-280): one gen::<u64>() word per unclamped
 // (cell, site) in cell-major, site-minor order; clamped sites take their value
 // in every replica. One CTA per instance. draw_idx[site] = number of unclamped
@@ -1967,6 +2100,16 @@ cudaError_t launch_resample(const DevArrays& A, uint32_t inst, uint32_t mode, ui
     const int grid = std::max(1, (int)std::min<uint32_t>((n_words + 255) / 256, (uint32_t)(4 * sm_count)));
     if (mode == kModeInt) resample_kernel<kModeInt><<<grid, 256, 0, st>>>(A, inst, pop_len, parents, old_spins, old_ei, old_ef);
     else resample_kernel<kModeF64><<<grid, 256, 0, st>>>(A, inst, pop_len, parents, old_spins, old_ei, old_ef);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_icm(const DevArrays& A, uint32_t inst, uint32_t mode, uint32_t cells, uint32_t* count,
+                       uint32_t* rank, uint8_t* flags, uint32_t* stack, uint32_t slots, cudaStream_t st) {
+    icm_count_kernel<<<cells, 32, 0, st>>>(A, inst, count);
+    icm_draw_kernel<<<1, 32, 0, st>>>(A, inst, count, rank);
+    const int grid = (int)((slots + 63) / 64);
+    if (mode == kModeInt) icm_move_kernel<kModeInt><<<grid, 64, 0, st>>>(A, inst, rank, flags, stack, slots);
+    else icm_move_kernel<kModeF64><<<grid, 64, 0, st>>>(A, inst, rank, flags, stack, slots);
     return cudaGetLastError();
 }
 

@@ -19,6 +19,8 @@ cudaError_t launch_chain(const DevArrays& A, const RunArgs& R, uint32_t mode, ui
 cudaError_t launch_exchange(const DevArrays& A, const RunArgs& R, uint32_t ninst, uint32_t mode, uint32_t steps,
                             bool exchange, cudaStream_t st);
 cudaError_t launch_swap(const DevArrays& A, uint32_t inst, uint32_t n_words, int sm_count, cudaStream_t st);
+cudaError_t launch_icm(const DevArrays& A, uint32_t inst, uint32_t mode, uint32_t cells, uint32_t* count,
+                       uint32_t* rank, uint8_t* flags, uint32_t* stack, uint32_t slots, cudaStream_t st);
 cudaError_t launch_resample(const DevArrays& A, uint32_t inst, uint32_t mode, uint32_t n_words, uint32_t pop_len,
                             const uint32_t* parents, const uint64_t* old_spins, const int32_t* old_ei,
                             const double* old_ef, int sm_count, cudaStream_t st);

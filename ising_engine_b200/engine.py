@@ -42,7 +42,7 @@ class Engine:
     def __init__(self, model: QuboModel, num_temps: int = 10, seed: int = 0,
                  exchange_interval: int = 1, temp_max: float = 1.0, temp_min: float = 0.1,
                  sweeps_per_exchange: int = 1, total_exchanges: int = 1, force_f64: bool = False,
-                 device: int = 0, pt_path: int = 0, num_pops: int = 1):
+                 device: int = 0, pt_path: int = 0, num_pops: int = 1, use_icm: bool = False):
         self._L = _ffi.lib()
         self.model = model
         self.num_temps = int(num_temps)
@@ -53,7 +53,7 @@ class Engine:
         prob = _problem(model, keep)
         cfg = _ffi.ie_config(temp_max, temp_min, sweeps_per_exchange, total_exchanges,
                              seed & 0xFFFFFFFFFFFFFFFF, self.num_temps, self.num_pops, 1, exchange_interval,
-                             int(force_f64), device, pt_path)
+                             int(force_f64), device, pt_path, int(use_icm))
         h = C.c_void_p()
         _ffi.check(self._L.ie_create(C.byref(prob), C.byref(cfg), C.byref(h)))
         self._h = h

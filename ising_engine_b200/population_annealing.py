@@ -47,11 +47,12 @@ class PaConfig:
     ladder_tuning_steps: int = 10
     post_resample_relaxation: int = 5
     ladder_mode: int = ACCEPTANCE_UNIFORM
+    use_icm: bool = False
 
     def to_c(self) -> _ffi.ie_pa_config:
         return _ffi.ie_pa_config(float(self.ess_threshold), int(self.ladder_tuning_iters),
                                  int(self.ladder_tuning_steps), int(self.post_resample_relaxation),
-                                 int(self.ladder_mode), 0)
+                                 int(self.ladder_mode), int(self.use_icm))
 
 
 def normalized_weights(log_w) -> np.ndarray:

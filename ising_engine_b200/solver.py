@@ -82,6 +82,7 @@ class UltimateSolver:
         self.ladder_tuning_steps = 10
         self.post_resample_relaxation = 5
         self.ladder_mode = 0  # 0 acceptance-uniform, 1 feedback-optimized (LadderMode)
+        self.use_icm = False  # isoenergetic cluster moves after every exchange block / stage
         # presolve and decomposition before annealing (ultimate.rs:161-218); an
         # extension may switch them off, e.g. where probing's O(n^2 nnz) cost
         # is too high
@@ -102,14 +103,14 @@ class UltimateSolver:
     def pa_config(self):
         from .population_annealing import PaConfig
         return PaConfig(self.ess_threshold, self.ladder_tuning_iters, self.ladder_tuning_steps,
-                        self.post_resample_relaxation, self.ladder_mode)
+                        self.post_resample_relaxation, self.ladder_mode, self.use_icm)
 
     def engine(self, model: QuboModel, num_pops: int | None = None) -> Engine:
         return Engine(model, num_temps=self.num_temps, seed=self.seed,
                       exchange_interval=self.exchange_interval, temp_max=self.temp_max,
                       temp_min=self.temp_min, sweeps_per_exchange=self.sweeps_per_exchange,
                       total_exchanges=self.total_exchanges, device=self.device,
-                      num_pops=self.num_pops if num_pops is None else num_pops)
+                      num_pops=self.num_pops if num_pops is None else num_pops, use_icm=self.use_icm)
 
     def _clamps(self, model: QuboModel, clamped):
         n = model.num_vars

@@ -463,6 +463,85 @@ static void update_incumbent(const Qubo& m, Field& f, double& best_e, std::vecto
     }
 }
 
+// rand 0.8.5 UniformInt<usize>::sample_single_inclusive (gen_range(0..=hi) on
+// a 64-bit target): range = hi + 1, zone = (range << lz(range)) - 1; draws
+// u64 v until the low half of the 128-bit v * range is <= zone and returns
+// the high half. gen_range(0..len) is the same with hi = len - 1.
+static uint64_t gen_index_inclusive(ChaCha8Rng& rng, uint64_t hi) {
+    const uint64_t range = hi + 1;
+    if (range == 0) return rng.next_u64();
+    const uint64_t zone = (range << __builtin_clzll(range)) - 1;
+    for (;;) {
+        const unsigned __int128 m = (unsigned __int128)rng.next_u64() * range;
+        if ((uint64_t)m <= zone) return (uint64_t)(m >> 64);
+    }
+}
+
+// Houdayer / ICM move on lanes (a, b) of cell c (src/solver/icm.rs:91-158):
+// the disagreement sites, a seed among them by gen_range(0..len), the
+// connected disagreement cluster grown depth-first along the CSR rows,
+// delta_a in cluster order (icm.rs:55-89), the cluster flipped in both lanes,
+// the tracked energies moved by +-delta_a.
+static void icm_pair_move(Field& f, const Qubo& m, int c, int a, int b, ChaCha8Rng& rng) {
+    const int64_t n = f.n;
+    int8_t* s = f.cell(c);
+    std::vector<char> vis(n), in_c(n, 0);
+    std::vector<int64_t> dis;
+    for (int64_t v = 0; v < n; v++) {
+        vis[v] = (s[v * NR + a] ^ s[v * NR + b]) == 0;
+        if (!vis[v]) dis.push_back(v);
+    }
+    if (dis.empty()) return;
+    const int64_t seed = dis[gen_index_inclusive(rng, dis.size() - 1)];
+    std::vector<int64_t> stack{seed}, cluster;
+    vis[seed] = 1;
+    in_c[seed] = 1;
+    while (!stack.empty()) {
+        const int64_t i = stack.back();
+        stack.pop_back();
+        cluster.push_back(i);
+        for (int64_t e = m.row[i]; e < m.row[i + 1]; e++) {
+            const int64_t j = m.col[e];
+            if (!vis[j]) {
+                vis[j] = 1;
+                in_c[j] = 1;
+                stack.push_back(j);
+            }
+        }
+    }
+    double delta = 0.0;
+    for (int64_t i : cluster) {
+        const double xi = (double)s[i * NR + a];
+        delta += m.linear[i] * (1.0 - 2.0 * xi);
+        for (int64_t e = m.row[i]; e < m.row[i + 1]; e++) {
+            const int64_t j = m.col[e];
+            const double w = m.val[e];
+            if (in_c[j]) {
+                if (i < j) {
+                    const double xj = (double)s[j * NR + a];
+                    delta += w * ((1.0 - xi) * (1.0 - xj) - xi * xj);
+                }
+            } else {
+                const double xj = (double)s[j * NR + a];
+                delta += w * xj * (1.0 - 2.0 * xi);
+            }
+        }
+    }
+    for (int64_t i : cluster) {
+        s[i * NR + a] ^= 1;
+        s[i * NR + b] ^= 1;
+    }
+    f.energies[c][a] += delta;
+    f.energies[c][b] -= delta;
+}
+
+// icm.rs:161-185: lanes (r, r + 32) of every cell, p then t then r.
+static void icm_sweep(Field& f, const Qubo& m, ChaCha8Rng& rng) {
+    for (int p = 0; p < f.np; p++)
+        for (int t = 0; t < f.nt; t++)
+            for (int r = 0; r < NR / 2; r++) icm_pair_move(f, m, t + f.nt * p, r, r + NR / 2, rng);
+}
+
 // ---------------------------------------------------------------------------
 // Presolve (src/presolve/mod.rs, src/presolve/qpbo.rs) and 1-opt polish
 // (src/solver/local_search.rs:19-57): needed only to reproduce the end-to-end
@@ -854,6 +933,7 @@ struct SolverCfg {
     uint64_t seed;
     int nt;
     int threads;
+    bool icm = false;  // UltimateSolver::use_icm (pairwise QUBO input: always applicable)
 };
 
 // UltimateSolver::solve, ultimate.rs:138-387, PT path (num_pops = 1,
@@ -910,6 +990,7 @@ static std::vector<int8_t> solve(const Qubo& m, const Assign& clamped, const Sol
             if (counter % 1000 == 0)
                 for (int t = 0; t < cfg.nt; t++) replica_energies(m, f.cell(t), f.energies[t].data());
         }
+        if (cfg.icm) icm_sweep(f, m, rng);  // ultimate.rs:326-328
         update_incumbent(m, f, inc_e, inc, buf);
     }
     std::vector<int8_t> best(n, 0), rb((size_t)NR * n);
@@ -937,23 +1018,10 @@ static std::vector<int8_t> solve(const Qubo& m, const Assign& clamped, const Sol
 // family entropy, systematic resampling, spacing adaptation, apply_resample)
 // and UltimateSolver::solve_population_annealing_diag (ultimate.rs:576-852)
 // with either ladder mode (acceptance-uniform, the default, or feedback-
-// optimized with round-trip tracking); ICM, GNN warm start and 2-opt off. Entered as solve_with_pa_diagnostics does (ultimate.rs:858-890):
+// optimized with round-trip tracking) and optional ICM; GNN warm start and
+// 2-opt off. Entered as solve_with_pa_diagnostics does (ultimate.rs:858-890):
 // no presolve or decomposition.
 // ---------------------------------------------------------------------------
-
-// rand 0.8.5 UniformInt<usize>::sample_single_inclusive (gen_range(0..=hi) on
-// a 64-bit target): range = hi + 1, zone = (range << lz(range)) - 1; draws
-// u64 v until the low half of the 128-bit v * range is <= zone and returns
-// the high half.
-static uint64_t gen_index_inclusive(ChaCha8Rng& rng, uint64_t hi) {
-    const uint64_t range = hi + 1;
-    if (range == 0) return rng.next_u64();
-    const uint64_t zone = (range << __builtin_clzll(range)) - 1;
-    for (;;) {
-        const unsigned __int128 m = (unsigned __int128)rng.next_u64() * range;
-        if ((uint64_t)m <= zone) return (uint64_t)(m >> 64);
-    }
-}
 
 // population_annealing.rs:51-56
 static std::vector<double> pa_normalized_weights(const std::vector<double>& lw) {
@@ -1104,6 +1172,7 @@ struct PaCfg {
     int64_t tuning_iters, tuning_steps, relax;
     int threads;
     int ladder_mode;  // 0 acceptance-uniform, 1 feedback-optimized
+    bool icm = false;
 };
 
 struct PaOut {
@@ -1231,6 +1300,10 @@ static Field pa_run(const Qubo& m, const std::vector<uint8_t>& is_clamped, const
         for (int64_t s = 0; s < cfg.sweeps; s++)
             step(f, m, temps.data(), is_clamped, sc, rng, true, false, cfg.threads, nullptr);
         all_energies(m, f);
+        if (cfg.icm) {  // ultimate.rs:800-808
+            icm_sweep(f, m, rng);
+            all_energies(m, f);
+        }
         update_incumbent(m, f, inc_e, inc, buf);
     }
     // best member by true model energy (p, t, r order), then the incumbent
@@ -1548,11 +1621,11 @@ double or_total_energy(int64_t n, const double* lin, const int64_t* row, const i
 int or_solve(int64_t n, const double* lin, const int64_t* row, const int64_t* col,
              const double* val, double offset, double tmax, double tmin, int64_t sweeps,
              int64_t exchanges, uint64_t seed, int nt, const int64_t* clamp_idx,
-             const int8_t* clamp_val, int64_t n_clamps, int threads, int8_t* state_out) {
+             const int8_t* clamp_val, int64_t n_clamps, int threads, int8_t* state_out, int use_icm) {
     Qubo m = make_qubo(n, lin, row, col, val, offset);
     Assign cl;
     for (int64_t i = 0; i < n_clamps; i++) cl.push_back({clamp_idx[i], clamp_val[i]});
-    SolverCfg cfg{tmax, tmin, sweeps, exchanges, seed, nt, threads};
+    SolverCfg cfg{tmax, tmin, sweeps, exchanges, seed, nt, threads, use_icm != 0};
     auto s = solve(m, cl, cfg);
     std::copy(s.begin(), s.end(), state_out);
     return 0;
@@ -1587,6 +1660,8 @@ double or_one_opt(int64_t n, const double* lin, const int64_t* row, const int64_
 //               init (the master stream then draws nothing for the init).
 //   exchange_interval: phase 2 runs after every k-th step (k = 1 is the reference).
 //   incumbent_every: if > 0, update_incumbent after every that many steps.
+//   icm_every: if > 0, icm_sweep after every that many steps (before the
+//              incumbent, as the PT loop orders them).
 // Outputs: words [nt][n], energies [nt][64] (tracked), swap attempts/accepts
 // [nt-1], draws = master-stream u64 position, base_seeds [steps] (optional),
 // incumbent energy and state (optional).
@@ -1596,7 +1671,7 @@ int or_run_schedule(int64_t n, const double* lin, const int64_t* row, const int6
                     int64_t exchange_interval, int collect_stats, int64_t incumbent_every,
                     int threads, uint64_t* words_out, double* energies_out, uint64_t* attempts_out,
                     uint64_t* accepts_out, uint64_t* draws_out, uint64_t* base_seeds_out,
-                    double* inc_energy_out, int8_t* inc_state_out) {
+                    double* inc_energy_out, int8_t* inc_state_out, int64_t icm_every) {
     Qubo m = make_qubo(n, lin, row, col, val, 0.0);
     std::vector<uint8_t> isc(n, 0);
     std::vector<int8_t> cv(n, 0);
@@ -1623,6 +1698,7 @@ int or_run_schedule(int64_t n, const double* lin, const int64_t* row, const int6
              base_seeds_out ? base_seeds_out + s : nullptr);
         if ((uint64_t)(s + 1) % 1000 == 0)
             for (int t = 0; t < nt; t++) replica_energies(m, f.cell(t), f.energies[t].data());
+        if (icm_every > 0 && (s + 1) % icm_every == 0) icm_sweep(f, m, rng);
         if (incumbent_every > 0 && (s + 1) % incumbent_every == 0) update_incumbent(m, f, inc_e, inc, buf);
     }
     if (words_out) pack_words(f, words_out);
@@ -1687,7 +1763,8 @@ int or_run_sa_batch(int64_t count, const int64_t* ns, const double* const* lins,
 int or_pa_run(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,
               double offset, double tmax, double tmin, int64_t sweeps, int64_t exchanges, uint64_t seed, int nt,
               int pops, double ess_threshold, int64_t tuning_iters, int64_t tuning_steps, int64_t relax,
-              int ladder_mode, const uint8_t* clamped, const int8_t* clamp_val, int threads, uint64_t* words_out,
+              int ladder_mode, int use_icm, const uint8_t* clamped, const int8_t* clamp_val, int threads,
+              uint64_t* words_out,
               double* energies_out, uint64_t* draws_out, double* alphas_out, double* ess_out, int64_t* n_ess,
               double* rho_out, int64_t* fam_out, int64_t* n_res, double* free_energy_out, int8_t* best_pre_out,
               double* incumbent_out, int8_t* state_out) {
@@ -1699,7 +1776,7 @@ int or_pa_run(int64_t n, const double* lin, const int64_t* row, const int64_t* c
         cv[i] = clamp_val ? clamp_val[i] : 0;
     }
     PaCfg cfg{tmax, tmin, sweeps, exchanges, seed, nt, pops, ess_threshold, tuning_iters, tuning_steps, relax, threads,
-              ladder_mode};
+              ladder_mode, use_icm != 0};
     ChaCha8Rng rng(seed);
     PaOut o;
     Field f = pa_run(m, cl, cv, cfg, o, rng);

@@ -55,7 +55,7 @@ def lib():
         L.or_total_energy.restype = C.c_double
         L.or_solve.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, C.c_double,
                                C.c_double, C.c_int64, C.c_int64, C.c_uint64, C.c_int, _i64p, _i8p,
-                               C.c_int64, C.c_int, _i8p]
+                               C.c_int64, C.c_int, _i8p, C.c_int]
         L.or_full_presolve.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, _i64p, _i8p,
                                        C.c_int64, _i64p, _i8p]
         L.or_full_presolve.restype = C.c_int64
@@ -65,7 +65,7 @@ def lib():
             C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_int, _f64p, C.c_int64, C.c_uint64,
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int64, C.c_int,
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-            C.c_void_p, C.c_void_p]
+            C.c_void_p, C.c_void_p, C.c_int64]
         L.or_replica_energies.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_int, _u64p,
                                           _f64p]
         L.or_run_sa_batch.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -76,8 +76,8 @@ def lib():
                                     _u64p, _f64p, _i64p, _f64p, _u64p]
         L.or_pa_run.argtypes = [
             C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int64,
-            C.c_uint64, C.c_int, C.c_int, C.c_double, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_void_p,
-            C.c_void_p, C.c_int, _u64p, _f64p, _u64p, _f64p, _f64p, _i64p, _f64p, _i64p, _i64p, _f64p, _i8p, _f64p, _i8p]
+            C.c_uint64, C.c_int, C.c_int, C.c_double, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int,
+            C.c_void_p, C.c_void_p, C.c_int, _u64p, _f64p, _u64p, _f64p, _f64p, _i64p, _f64p, _i64p, _i64p, _f64p, _i8p, _f64p, _i8p]
         L.or_pa_normalized_weights.argtypes = [_f64p, C.c_int64, _f64p]
         L.or_pa_systematic_resample.argtypes = [_f64p, C.c_int64, C.c_double, _i64p]
         L.or_pa_feedback_alphas.argtypes = [_f64p, _f64p, C.c_int64, C.c_double, _f64p]
@@ -146,7 +146,7 @@ def total_energy(model, state, offset: float = 0.0) -> float:
 
 
 def solve(model, temp_max, temp_min, sweeps, exchanges, seed, num_temps=10, clamped=(),
-          threads=1, offset=0.0) -> np.ndarray:
+          threads=1, offset=0.0, use_icm=False) -> np.ndarray:
     """UltimateSolver::new(temp_max, temp_min, sweeps, exchanges, Some(seed))
     with num_temps, then .solve(model, clamped) (ultimate.rs:60-87, 138-387)."""
     n, lin, row, col, val = _csr(model)
@@ -154,7 +154,7 @@ def solve(model, temp_max, temp_min, sweeps, exchanges, seed, num_temps=10, clam
     cv = np.array([c[1] for c in clamped], dtype=np.int8)
     out = np.zeros(n, dtype=np.int8)
     lib().or_solve(n, lin, row, col, val, offset, temp_max, temp_min, sweeps, exchanges, seed,
-                   num_temps, ci, cv, len(clamped), threads, out)
+                   num_temps, ci, cv, len(clamped), threads, out, int(use_icm))
     return out
 
 
@@ -186,7 +186,7 @@ class RunResult:
 
 def run_schedule(model, temps, seed, init_words=None, clamped=None, clamp_val=None,
                  exchange_interval=1, collect_stats=False, incumbent_every=0, threads=1,
-                 want_base_seeds=False) -> RunResult:
+                 want_base_seeds=False, icm_every=0) -> RunResult:
     """The step loop of ultimate.rs:248-336 under temps[steps][nt]."""
     n, lin, row, col, val = _csr(model)
     temps = np.ascontiguousarray(temps, dtype=np.float64)
@@ -207,7 +207,7 @@ def run_schedule(model, temps, seed, init_words=None, clamped=None, clamp_val=No
     lib().or_run_schedule(n, lin, row, col, val, nt, temps.reshape(-1), steps, seed, _ptr(iw),
                           _ptr(cl), _ptr(cv), exchange_interval, int(collect_stats),
                           incumbent_every, threads, _ptr(words), _ptr(en), _ptr(att), _ptr(acc),
-                          _ptr(draws), _ptr(bs), _ptr(inc_e), _ptr(inc_s))
+                          _ptr(draws), _ptr(bs), _ptr(inc_e), _ptr(inc_s), int(icm_every))
     return RunResult(words=words, energies=en, swap_attempts=att[:nt - 1],
                      swap_accepts=acc[:nt - 1], draws=int(draws[0]), base_seeds=bs,
                      incumbent_energy=float(inc_e[0]), incumbent_state=inc_s)
@@ -274,7 +274,7 @@ def v2_program(model, r, init, seed, ops, temps, skip_draws=0):
 
 def pa_run(model, temp_max, temp_min, sweeps, exchanges, seed, num_temps, num_pops, ess_threshold=0.5,
            tuning_iters=8, tuning_steps=10, relax=5, clamped=None, clamp_val=None, threads=1, offset=0.0,
-           ladder_mode=0):
+           ladder_mode=0, use_icm=False):
     """UltimateSolver::new(temp_max, temp_min, sweeps, exchanges, Some(seed)) with
     num_temps, num_pops and the PA knobs, through solve_with_pa_diagnostics
     (ultimate.rs:576-890). Returns a dict: words [nt*pops, n], energies
@@ -301,7 +301,7 @@ def pa_run(model, temp_max, temp_min, sweeps, exchanges, seed, num_temps, num_po
     L = lib()
     L.or_pa_run(n, lin, row, col, val, float(offset), float(temp_max), float(temp_min), int(sweeps), int(exchanges),
                 int(seed), int(num_temps), int(num_pops), float(ess_threshold), int(tuning_iters), int(tuning_steps),
-                int(relax), int(ladder_mode), _ptr(cl), _ptr(cv), int(threads), words, en, draws, alphas, ess, n_ess, rho, fam, n_res, fe, best_pre,
+                int(relax), int(ladder_mode), int(use_icm), _ptr(cl), _ptr(cv), int(threads), words, en, draws, alphas, ess, n_ess, rho, fam, n_res, fe, best_pre,
                 inc, state)
     ne, nr = int(n_ess[0]), int(n_res[0])
     return dict(words=words.reshape(cells, n), energies=en.reshape(cells, 64), draws=int(draws[0]), alphas=alphas,

@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 def check_pa(m, tmax, tmin, sweeps, exchanges, seed, nt, pops, cfg, clamped=None, cval=None):
     ref = O.pa_run(m, tmax, tmin, sweeps, exchanges, seed, nt, pops, cfg.ess_threshold, cfg.ladder_tuning_iters,
                    cfg.ladder_tuning_steps, cfg.post_resample_relaxation, clamped=clamped, clamp_val=cval, threads=8,
-                   ladder_mode=cfg.ladder_mode)
+                   ladder_mode=cfg.ladder_mode, use_icm=cfg.use_icm)
     with Engine(m, num_temps=nt, num_pops=pops, seed=seed, temp_max=tmax, temp_min=tmin,
                 sweeps_per_exchange=sweeps, total_exchanges=exchanges) as eng:
         if clamped is not None:
