@@ -57,6 +57,18 @@ def steepest_descent_1opt(model: QuboModel, state, is_clamped=None) -> float:
             gains[j] += (1.0 - 2.0 * float(state[j])) * float(va[k]) * dirn
 
 
+def luby(i: int) -> int:
+    """The Luby sequence 1, 1, 2, 1, 1, 2, 4, ... (src/solver/tts.rs:95-112),
+    1-indexed."""
+    if i < 1:
+        raise ValueError("luby is 1-indexed")
+    while True:
+        k = i.bit_length()  # 2^(k-1) <= i <= 2^k - 1
+        if i == (1 << k) - 1:
+            return 1 << (k - 1)
+        i -= (1 << (k - 1)) - 1
+
+
 class UltimateSolver:
     """Configuration of the reference's UltimateSolver (ultimate.rs:18-87):
     the PT path (num_pops = 1) and population annealing with PT
@@ -120,6 +132,21 @@ class UltimateSolver:
             is_clamped[idx] = 1
             cval[idx] = val
         return is_clamped, cval
+
+    def solve_with_luby_restarts(self, model: QuboModel, clamped=(), num_restarts: int = 1) -> np.ndarray:
+        """ultimate.rs:95-120: restart i (0-based) solves with total_exchanges *
+        luby(i + 1) exchanges and seed + 0x9e3779b97f4a7c15 * (i + 1) (mod 2^64);
+        the first state of lowest true energy wins."""
+        best_e, best = None, None
+        for i in range(max(int(num_restarts), 1)):
+            r = copy.copy(self)
+            r.total_exchanges = self.total_exchanges * luby(i + 1)
+            r.seed = (self.seed + 0x9E3779B97F4A7C15 * (i + 1)) & 0xFFFFFFFFFFFFFFFF
+            x = r.solve(model, clamped)
+            e = model.calculate_total_energy(x)
+            if best_e is None or e < best_e:
+                best_e, best = e, x
+        return best
 
     def solve_with_pa_diagnostics(self, model: QuboModel, clamped=()):
         """ultimate.rs:858-890: population annealing with num_pops >= 2 (no
