@@ -1946,6 +1946,12 @@ ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
         std::vector<double> rates(L - 1), sp(L - 1);
         const bool feedback = pc->ladder_mode == 1;
         std::vector<unsigned long long> rt(1 + 2 * (size_t)L);
+        // tracking belongs to the throwaway tuning field only: off again on
+        // every way out of this block
+        struct TrackingOff {
+            Engine& e;
+            ~TrackingOff() { e.track_roundtrips = false; }
+        } tracking_off{E};
         if (feedback) {
             IE_TRY(E.d_labels.alloc(E.total_energy));
             IE_TRY(E.d_rt.alloc(rt.size()));
@@ -1957,11 +1963,7 @@ ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
                 // reset_roundtrip_stats (engine.rs:529-536): counts and labels to zero
                 IE_CUDA(cudaMemsetAsync(E.d_labels.p, 0, E.total_energy, st));
                 IE_CUDA(cudaMemsetAsync(E.d_rt.p, 0, rt.size() * sizeof(unsigned long long), st));
-                const ie_status rs = run_steps(temps, pc->ladder_tuning_steps);
-                if (rs != IE_OK) {
-                    E.track_roundtrips = false;
-                    return rs;
-                }
+                IE_TRY(run_steps(temps, pc->ladder_tuning_steps));
                 IE_CUDA(cudaMemcpyAsync(rt.data(), E.d_rt.p, rt.size() * sizeof(unsigned long long),
                                         cudaMemcpyDeviceToHost, st));
                 IE_CUDA(cudaStreamSynchronize(st));
@@ -1999,7 +2001,6 @@ ie_status ie_run_pa(ie_handle* h, const ie_pa_config* pc, ie_pa_report* rep) {
     }
 
     // production population (a fresh scratch: no round-trip tracking)
-    E.track_roundtrips = false;
     IE_TRY(E.init_random());
     IE_TRY(fresh_scratch());
     IE_TRY(h->d_inc_e.upload(std::vector<double>(1, std::numeric_limits<double>::infinity()), st));
