@@ -33,7 +33,7 @@ extern "C" {
 typedef enum ie_status {
     IE_OK = 0,
     IE_ERR_INVALID = 1,     /* bad shape, index out of range, bad config */
-    IE_ERR_UNSUPPORTED = 2, /* e.g. num_slices != 1 or num_pops != 1 */
+    IE_ERR_UNSUPPORTED = 2, /* e.g. num_slices != 1, more than 64 populations */
     IE_ERR_OOM = 3,         /* device allocation failed */
     IE_ERR_CUDA = 4,        /* CUDA runtime error */
     IE_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
@@ -121,14 +121,16 @@ ie_status ie_set_clamps(ie_handle* h, const uint8_t* is_clamped, const int8_t* c
  * calculate_replica_energies for every cell. */
 ie_status ie_init_random(ie_handle* h);
 
-/* Sets spin words [num_temps][num_vars] directly (no master-stream draws) and
- * recomputes the tracked energies. */
+/* Sets spin words [num_temps * num_pops][num_vars] (cell t + num_temps * p)
+ * directly (no master-stream draws) and recomputes the tracked energies. */
 ie_status ie_set_spins(ie_handle* h, const uint64_t* words);
 
 /* engine::step (engine.rs:573-819) n_steps times with a constant temperature
- * ladder temps[num_temps]: base_seed draw, index-order sweep of every cell,
- * DEO exchange (every exchange_interval-th step), phase toggle. Energies are
- * re-synced every 1000 steps as ultimate.rs:316-324 does. */
+ * ladder temps[num_temps] (every population's ladder): base_seed draw,
+ * index-order sweep of every cell, DEO exchange (every exchange_interval-th
+ * step; population by population), phase toggle. Energies are re-synced
+ * every 1000 steps as ultimate.rs:316-324 does (not on population handles,
+ * whose driver re-syncs per stage). */
 ie_status ie_step(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t n_steps);
 
 /* Per-step temperature schedule temps[n_steps][num_temps] (SA schedules). */
@@ -136,12 +138,13 @@ ie_status ie_run_schedule(ie_handle* h, const double* temps, uint32_t n_temps, u
 
 /* The UltimateSolver PT loop (ultimate.rs:234-336) with the geometric ladder
  * of the config: total_exchanges x sweeps_per_exchange steps, resync every
- * 1000 steps, update_incumbent after every exchange block (ultimate.rs:397-430).
- * Requires ie_init_random (or ie_set_spins) first. */
+ * 1000 steps, the ICM sweep when use_icm, update_incumbent after every
+ * exchange block (ultimate.rs:397-430). Requires ie_init_random (or
+ * ie_set_spins) first; num_pops must be 1 (population handles run ie_run_pa). */
 ie_status ie_run_pt(ie_handle* h);
 
-ie_status ie_read_spins(ie_handle* h, uint64_t* words /* [num_temps][num_vars] */);
-ie_status ie_read_energies(ie_handle* h, double* energies /* [num_temps][64] */);
+ie_status ie_read_spins(ie_handle* h, uint64_t* words /* [num_temps * num_pops][num_vars] */);
+ie_status ie_read_energies(ie_handle* h, double* energies /* [num_temps * num_pops][64] */);
 /* swap attempts / accepts per adjacent pair [num_temps - 1] (engine.rs:545-551). */
 ie_status ie_read_swap_stats(ie_handle* h, uint64_t* attempts, uint64_t* accepts);
 /* Master-stream position (number of u64 draws so far) and DEO phase. */
