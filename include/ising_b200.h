@@ -349,6 +349,14 @@ ie_status ie_pa_adapt_spacings(const double* spacings, const double* acceptance,
 ie_status ie_pa_feedback_optimized_alphas(const double* alphas, const double* flow, uint64_t nt, double damping,
                                           double* out);
 
+/* ---- the 2-opt escape finisher (host only) ----
+ * steepest_descent_2opt_escapes (src/solver/local_search.rs:123-143): 1-opt
+ * descent, then the steepest improving 2-flip along the coupling graph's
+ * edges, repeated until neither improves; free variables only (is_clamped may
+ * be NULL). state [num_vars] 0/1 is polished in place; *improvement (may be
+ * NULL) = max(0, E_before - E_after). */
+ie_status ie_two_opt(const ie_problem* problem, int8_t* state, const uint8_t* is_clamped, double* improvement);
+
 /* ---- presolve and decomposition (host only) ----
  * full_presolve (src/presolve/mod.rs:279-324): roof-duality strong
  * persistencies (src/presolve/qpbo.rs) of the clamp-reduced model unioned

@@ -14,11 +14,13 @@ decomposition (ultimate.rs:161-218) run first on the host
 from __future__ import annotations
 
 import copy
+import ctypes as C
 
 import numpy as np
 
+from . import _ffi
 from .core import QuboModel
-from .engine import Engine
+from .engine import Engine, _p, _problem
 
 NUM_REPLICAS = 64
 
@@ -69,6 +71,20 @@ def luby(i: int) -> int:
         i -= (1 << (k - 1)) - 1
 
 
+def steepest_descent_2opt_escapes(model: QuboModel, state, is_clamped=None) -> float:
+    """local_search.rs:123-143 (the library's host code): polishes ``state``
+    (contiguous int8 0/1) in place to a 1-opt minimum with no improving 2-flip
+    along a coupling; returns the improvement."""
+    if not (isinstance(state, np.ndarray) and state.dtype == np.int8 and state.flags.c_contiguous):
+        raise TypeError("state must be a contiguous int8 array")
+    keep: list = []
+    prob = _problem(model, keep)
+    c = None if is_clamped is None else np.ascontiguousarray(is_clamped, dtype=np.uint8)
+    imp = C.c_double()
+    _ffi.check(_ffi.lib().ie_two_opt(C.byref(prob), _p(state), None if c is None else _p(c), C.byref(imp)))
+    return imp.value
+
+
 class UltimateSolver:
     """Configuration of the reference's UltimateSolver (ultimate.rs:18-87):
     the PT path (num_pops = 1) and population annealing with PT
@@ -95,6 +111,7 @@ class UltimateSolver:
         self.post_resample_relaxation = 5
         self.ladder_mode = 0  # 0 acceptance-uniform, 1 feedback-optimized (LadderMode)
         self.use_icm = False  # isoenergetic cluster moves after every exchange block / stage
+        self.use_2opt = False  # edge-restricted 2-opt escapes after the 1-opt polish
         # presolve and decomposition before annealing (ultimate.rs:161-218); an
         # extension may switch them off, e.g. where probing's O(n^2 nnz) cost
         # is too high
@@ -110,6 +127,11 @@ class UltimateSolver:
             raise NotImplementedError("only num_slices = 1 is on the device path")
         self.num_temps = int(temps)
         self.num_pops = int(pops)
+        return self
+
+    def with_2opt(self, enabled: bool) -> "UltimateSolver":
+        """ultimate.rs:133-136."""
+        self.use_2opt = bool(enabled)
         return self
 
     def pa_config(self):
@@ -162,6 +184,8 @@ class UltimateSolver:
             diag = eng.run_pa(self.pa_config())
             _, best = eng.best()
             eng.one_opt(best, is_clamped)
+        if self.use_2opt:
+            steepest_descent_2opt_escapes(model, best, is_clamped)
         return best, diag
 
     def solve(self, model: QuboModel, clamped=()) -> np.ndarray:
@@ -195,4 +219,6 @@ class UltimateSolver:
             eng.run_pt()
             _, best = eng.best()
             eng.one_opt(best, is_clamped)
+        if self.use_2opt:
+            steepest_descent_2opt_escapes(model, best, is_clamped)
         return best

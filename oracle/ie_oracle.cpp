@@ -927,6 +927,45 @@ static double one_opt(const Qubo& m, int8_t* state, const std::vector<uint8_t>& 
     }
 }
 
+// local_search.rs:123-143 with find_steepest_2opt_edge_flip (:83-121):
+// 1-opt, fresh gains, the steepest improving edge 2-flip (strict <, first
+// found on ties), repeated; returns max(0, E_before - E_after).
+static double two_opt(const Qubo& m, int8_t* state, const std::vector<uint8_t>& clamped) {
+    const int64_t n = m.n;
+    const double e0 = total_energy(m, state);
+    std::vector<double> g(n);
+    for (;;) {
+        one_opt(m, state, clamped);
+        for (int64_t i = 0; i < n; i++) {
+            double field = m.linear[i];
+            for (int64_t k = m.row[i]; k < m.row[i + 1]; k++) field += m.val[k] * (double)state[m.col[k]];
+            g[i] = (1.0 - 2.0 * (double)state[i]) * field;
+        }
+        int64_t bu = -1, bv = -1;
+        double bd = 0.0;
+        for (int64_t u = 0; u < n; u++) {
+            if (clamped[u]) continue;
+            const double su = 1.0 - 2.0 * (double)state[u];
+            for (int64_t k = m.row[u]; k < m.row[u + 1]; k++) {
+                const int64_t v = m.col[k];
+                if (v > u && !clamped[v]) {
+                    const double sv = 1.0 - 2.0 * (double)state[v];
+                    const double d = g[u] + g[v] + m.val[k] * su * sv;
+                    if (d < -1e-12 && (bu < 0 || d < bd)) {
+                        bu = u;
+                        bv = v;
+                        bd = d;
+                    }
+                }
+            }
+        }
+        if (bu < 0) break;
+        state[bu] = (int8_t)(1 - state[bu]);
+        state[bv] = (int8_t)(1 - state[bv]);
+    }
+    return std::max(0.0, e0 - total_energy(m, state));
+}
+
 struct SolverCfg {
     double tmax, tmin;
     int64_t sweeps, exchanges;
@@ -1644,6 +1683,13 @@ int64_t or_full_presolve(int64_t n, const double* lin, const int64_t* row, const
         out_val[i] = d[i].second;
     }
     return (int64_t)d.size();
+}
+
+double or_two_opt(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,
+                  double offset, int8_t* state, const uint8_t* clamped) {
+    Qubo m = make_qubo(n, lin, row, col, val, offset);
+    std::vector<uint8_t> cl(clamped, clamped + n);
+    return two_opt(m, state, cl);
 }
 
 double or_one_opt(int64_t n, const double* lin, const int64_t* row, const int64_t* col,

@@ -61,6 +61,8 @@ def lib():
         L.or_full_presolve.restype = C.c_int64
         L.or_one_opt.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, _i8p, _u8p]
         L.or_one_opt.restype = C.c_double
+        L.or_two_opt.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, _i8p, _u8p]
+        L.or_two_opt.restype = C.c_double
         L.or_run_schedule.argtypes = [
             C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_int, _f64p, C.c_int64, C.c_uint64,
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int64, C.c_int,
@@ -339,3 +341,13 @@ def pa_feedback_alphas(alphas, flow, damping) -> np.ndarray:
     out = np.zeros(len(a), dtype=np.float64)
     lib().or_pa_feedback_alphas(a, f, len(a), float(damping), out)
     return out
+
+
+def two_opt(model, state, clamped=None, offset=0.0):
+    """steepest_descent_2opt_escapes (local_search.rs:123-143) on a copy of
+    state; returns (state, improvement)."""
+    n, lin, row, col, val = _csr(model)
+    x = np.array(state, dtype=np.int8)
+    cl = np.zeros(n, dtype=np.uint8) if clamped is None else np.ascontiguousarray(clamped, dtype=np.uint8)
+    imp = lib().or_two_opt(n, lin, row, col, val, float(offset), x, cl)
+    return x, imp
