@@ -349,13 +349,22 @@ ie_status ie_pa_adapt_spacings(const double* spacings, const double* acceptance,
 ie_status ie_pa_feedback_optimized_alphas(const double* alphas, const double* flow, uint64_t nt, double damping,
                                           double* out);
 
-/* ---- the 2-opt escape finisher (host only) ----
+/* ---- finishers after the anneal (host only) ----
  * steepest_descent_2opt_escapes (src/solver/local_search.rs:123-143): 1-opt
  * descent, then the steepest improving 2-flip along the coupling graph's
  * edges, repeated until neither improves; free variables only (is_clamped may
  * be NULL). state [num_vars] 0/1 is polished in place; *improvement (may be
  * NULL) = max(0, E_before - E_after). */
 ie_status ie_two_opt(const ie_problem* problem, int8_t* state, const uint8_t* is_clamped, double* improvement);
+/* The path-relinking finisher (ultimate.rs:436-479, src/solver/elite.rs):
+ * the current state and every replica of words [cells][num_vars] (the layout
+ * ie_read_spins returns: bit r = replica r) feed an elite archive (8 entries,
+ * Hamming radius max(num_vars / 10, 1)); every pair of elites is relinked
+ * greedily and polished by 1-opt; the best state (strictly better than the
+ * current one, else the current one) is written back to `state`, its model
+ * energy to *energy (may be NULL). Host only. */
+ie_status ie_path_relink(const ie_problem* problem, const uint64_t* words, uint64_t cells,
+                         const uint8_t* is_clamped, int8_t* state, double* energy);
 
 /* ---- presolve and decomposition (host only) ----
  * full_presolve (src/presolve/mod.rs:279-324): roof-duality strong

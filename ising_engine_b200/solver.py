@@ -85,6 +85,24 @@ def steepest_descent_2opt_escapes(model: QuboModel, state, is_clamped=None) -> f
     return imp.value
 
 
+def path_relink_finish(model: QuboModel, words, state, is_clamped=None) -> float:
+    """ultimate.rs:436-479 (the library's host code): an elite archive of
+    ``state`` and every replica of the field ``words`` [cells, n] (bit r =
+    replica r, as ``Engine.spins`` returns them), greedy path relinking of
+    every elite pair, each polished by 1-opt; the best state replaces
+    ``state`` (contiguous int8) when strictly better. Returns its energy."""
+    if not (isinstance(state, np.ndarray) and state.dtype == np.int8 and state.flags.c_contiguous):
+        raise TypeError("state must be a contiguous int8 array")
+    keep: list = []
+    prob = _problem(model, keep)
+    w = np.ascontiguousarray(words, dtype=np.uint64).reshape(-1)
+    c = None if is_clamped is None else np.ascontiguousarray(is_clamped, dtype=np.uint8)
+    e = C.c_double()
+    _ffi.check(_ffi.lib().ie_path_relink(C.byref(prob), _p(w), w.size // max(model.num_vars, 1),
+                                         None if c is None else _p(c), _p(state), C.byref(e)))
+    return e.value
+
+
 class UltimateSolver:
     """Configuration of the reference's UltimateSolver (ultimate.rs:18-87):
     the PT path (num_pops = 1) and population annealing with PT
@@ -112,6 +130,7 @@ class UltimateSolver:
         self.ladder_mode = 0  # 0 acceptance-uniform, 1 feedback-optimized (LadderMode)
         self.use_icm = False  # isoenergetic cluster moves after every exchange block / stage
         self.use_2opt = False  # edge-restricted 2-opt escapes after the 1-opt polish
+        self.use_path_relinking = False  # elite path relinking after the polish (PT path)
         # presolve and decomposition before annealing (ultimate.rs:161-218); an
         # extension may switch them off, e.g. where probing's O(n^2 nnz) cost
         # is too high
@@ -219,6 +238,9 @@ class UltimateSolver:
             eng.run_pt()
             _, best = eng.best()
             eng.one_opt(best, is_clamped)
+            words = eng.spins() if self.use_path_relinking else None
         if self.use_2opt:
             steepest_descent_2opt_escapes(model, best, is_clamped)
+        if self.use_path_relinking:  # ultimate.rs:382-385
+            path_relink_finish(model, words, best, is_clamped)
         return best

@@ -966,6 +966,113 @@ static double two_opt(const Qubo& m, int8_t* state, const std::vector<uint8_t>& 
     return std::max(0.0, e0 - total_energy(m, state));
 }
 
+// src/solver/elite.rs:21-123 (EliteArchive) and :133-181 (path_relink), and
+// the finisher of ultimate.rs:436-479.
+struct EliteArchive {
+    size_t cap, min_h;
+    std::vector<std::pair<double, std::vector<int8_t>>> entries;
+
+    static size_t hamming(const std::vector<int8_t>& a, const std::vector<int8_t>& b) {
+        size_t d = 0;
+        for (size_t i = 0; i < a.size(); i++) d += a[i] != b[i];
+        return d;
+    }
+    void sort_and_trim() {
+        std::stable_sort(entries.begin(), entries.end(),
+                         [](const auto& a, const auto& b) { return a.first < b.first; });
+        if (entries.size() > cap) entries.resize(cap);
+    }
+    void insert(const std::vector<int8_t>& x, double e) {
+        for (size_t i = 0; i < entries.size(); i++)
+            if (hamming(entries[i].second, x) < std::max<size_t>(min_h, 1)) {
+                if (e < entries[i].first - 1e-12) {
+                    entries[i] = {e, x};
+                    sort_and_trim();
+                }
+                return;
+            }
+        if (entries.size() < cap) {
+            entries.push_back({e, x});
+            sort_and_trim();
+            return;
+        }
+        const double worst = entries.empty() ? std::numeric_limits<double>::infinity() : entries.back().first;
+        if (e < worst - 1e-12) {
+            entries.push_back({e, x});
+            sort_and_trim();
+        }
+    }
+};
+
+static std::vector<int8_t> path_relink(const Qubo& m, const std::vector<int8_t>& source,
+                                       const std::vector<int8_t>& target) {
+    const int64_t n = m.n;
+    std::vector<int8_t> x = source, best = source;
+    double e = total_energy(m, x.data()), be = e;
+    std::vector<double> g(n);
+    for (int64_t i = 0; i < n; i++) {
+        double field = m.linear[i];
+        for (int64_t k = m.row[i]; k < m.row[i + 1]; k++) field += m.val[k] * (double)x[m.col[k]];
+        g[i] = (1.0 - 2.0 * (double)x[i]) * field;
+    }
+    std::vector<int64_t> differing;
+    for (int64_t i = 0; i < n; i++)
+        if (source[i] != target[i]) differing.push_back(i);
+    while (!differing.empty()) {
+        size_t pick = 0;
+        double bg = std::numeric_limits<double>::infinity();
+        for (size_t k = 0; k < differing.size(); k++)
+            if (g[differing[k]] < bg - 1e-15) {
+                bg = g[differing[k]];
+                pick = k;
+            }
+        const int64_t i = differing[pick];
+        differing[pick] = differing.back();
+        differing.pop_back();
+        const double dir = 1.0 - 2.0 * (double)x[i];
+        e += g[i];
+        x[i] = (int8_t)(1 - x[i]);
+        g[i] = -g[i];
+        for (int64_t k = m.row[i]; k < m.row[i + 1]; k++) {
+            const int64_t j = m.col[k];
+            g[j] += (1.0 - 2.0 * (double)x[j]) * m.val[k] * dir;
+        }
+        if (e < be) {
+            be = e;
+            best = x;
+        }
+    }
+    return best;
+}
+
+static std::vector<int8_t> path_relink_finish(const Qubo& m, const std::vector<uint64_t>& words, int64_t cells,
+                                              const std::vector<uint8_t>& clamped, std::vector<int8_t> current,
+                                              double current_e, double& best_e_out) {
+    const int64_t n = m.n;
+    EliteArchive arch{8, (size_t)std::max<int64_t>(n / 10, 1), {}};
+    arch.insert(current, current_e);
+    std::vector<int8_t> buf(n);
+    for (int64_t c = 0; c < cells; c++)
+        for (int r = 0; r < NR; r++) {
+            for (int64_t v = 0; v < n; v++) buf[v] = (int8_t)((words[c * n + v] >> r) & 1);
+            arch.insert(buf, total_energy(m, buf.data()));
+        }
+    std::vector<int8_t> best = current;
+    double be = current_e;
+    for (size_t i = 0; i < arch.entries.size(); i++)
+        for (size_t j = i + 1; j < arch.entries.size(); j++) {
+            std::vector<int8_t> x = path_relink(m, arch.entries[i].second, arch.entries[j].second);
+            one_opt(m, x.data(), clamped);
+            const double e = total_energy(m, x.data());
+            if (e < be) {
+                be = e;
+                best = x;
+            }
+        }
+    best_e_out = be;
+    return best;
+}
+
 struct SolverCfg {
     double tmax, tmin;
     int64_t sweeps, exchanges;
@@ -1683,6 +1790,18 @@ int64_t or_full_presolve(int64_t n, const double* lin, const int64_t* row, const
         out_val[i] = d[i].second;
     }
     return (int64_t)d.size();
+}
+
+double or_path_relink(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,
+                      double offset, const uint64_t* words, int64_t cells, const uint8_t* clamped, int8_t* state) {
+    Qubo m = make_qubo(n, lin, row, col, val, offset);
+    std::vector<uint8_t> cl(clamped, clamped + n);
+    std::vector<int8_t> cur(state, state + n);
+    double be = 0.0;
+    const std::vector<int8_t> best = path_relink_finish(m, std::vector<uint64_t>(words, words + cells * n), cells, cl,
+                                                        cur, total_energy(m, state), be);
+    std::copy(best.begin(), best.end(), state);
+    return be;
 }
 
 double or_two_opt(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,

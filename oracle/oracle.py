@@ -63,6 +63,9 @@ def lib():
         L.or_one_opt.restype = C.c_double
         L.or_two_opt.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, _i8p, _u8p]
         L.or_two_opt.restype = C.c_double
+        L.or_path_relink.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, _u64p, C.c_int64, _u8p,
+                                     _i8p]
+        L.or_path_relink.restype = C.c_double
         L.or_run_schedule.argtypes = [
             C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_int, _f64p, C.c_int64, C.c_uint64,
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int64, C.c_int,
@@ -351,3 +354,14 @@ def two_opt(model, state, clamped=None, offset=0.0):
     cl = np.zeros(n, dtype=np.uint8) if clamped is None else np.ascontiguousarray(clamped, dtype=np.uint8)
     imp = lib().or_two_opt(n, lin, row, col, val, float(offset), x, cl)
     return x, imp
+
+
+def path_relink_finish(model, words, state, clamped=None, offset=0.0):
+    """ultimate.rs:436-479 on a copy of state with the field's words
+    [cells, n] (bit r = replica r); returns (state, energy)."""
+    n, lin, row, col, val = _csr(model)
+    w = np.ascontiguousarray(words, dtype=np.uint64).reshape(-1)
+    x = np.array(state, dtype=np.int8)
+    cl = np.zeros(n, dtype=np.uint8) if clamped is None else np.ascontiguousarray(clamped, dtype=np.uint8)
+    e = lib().or_path_relink(n, lin, row, col, val, float(offset), w, w.size // max(n, 1), cl, x)
+    return x, e

@@ -54,3 +54,31 @@ def test_two_opt_respects_clamps():
 def test_with_2opt_flag():
     s = UltimateSolver(1.0, 0.1, 1, 1, 0)
     assert s.use_2opt is False and s.with_2opt(True) is s and s.use_2opt
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_path_relink_finisher_equals_oracle(seed):
+    """ultimate.rs:436-479: the library's finisher returns the oracle's state
+    and energy bit for bit on fields of random and near-duplicate replicas
+    (the archive's diversity rule and replacement both fire), never worse
+    than the current state."""
+    from ising_engine_b200.solver import path_relink_finish
+    n = [12, 30, 50][seed % 3]
+    m = random_qubo(n, 0.3, 900 + seed, integral=seed % 2 == 1)
+    rng = np.random.default_rng(seed)
+    cells = 3
+    base = rng.integers(0, 2, size=n).astype(np.int8)
+    words = np.zeros((cells, n), dtype=np.uint64)
+    for c in range(cells):
+        for r in range(64):
+            x = base.copy() if r % 3 else rng.integers(0, 2, size=n).astype(np.int8)
+            x[rng.integers(0, n, size=r % 4)] ^= 1  # near duplicates of the base
+            words[c] |= x.astype(np.uint64) << np.uint64(r)
+    cl = np.zeros(n, np.uint8)
+    cl[[0, n // 2]] = 1
+    cur = rng.integers(0, 2, size=n).astype(np.int8)
+    ref, re = O.path_relink_finish(m, words, cur, cl)
+    got = cur.copy()
+    e = path_relink_finish(m, words, got, cl)
+    assert got.tolist() == ref.tolist() and e == re
+    assert e <= m.calculate_total_energy(cur) and e == m.calculate_total_energy(got)
