@@ -121,6 +121,18 @@ ie_status ie_set_clamps(ie_handle* h, const uint8_t* is_clamped, const int8_t* c
  * calculate_replica_energies for every cell. */
 ie_status ie_init_random(ie_handle* h);
 
+/* UltimateSolver::with_gnn_heuristic (ultimate.rs:121-124, 256-263): from now
+ * on the initial state (ie_init_random, and the fields ie_run_pa initializes)
+ * is drawn per replica: replica r of an unclamped site v is one when its
+ * gen_range(0.0..1.0) draw is below probs[v] (64 draws per cell and site);
+ * probs [num_vars] is copied; NULL restores the random init. */
+ie_status ie_set_init_probs(ie_handle* h, const double* probs);
+/* The same initial words on the host (reference layout, bit r = replica r)
+ * for `cells` cells from ChaCha8Rng::seed_from_u64(seed) after draw_offset
+ * draws; *draws = the position after them. */
+ie_status ie_warm_start_words(uint64_t seed, uint64_t draw_offset, const double* probs, const uint8_t* is_clamped,
+                              const int8_t* clamp_val, uint64_t n, uint64_t cells, uint64_t* words, uint64_t* draws);
+
 /* Sets spin words [num_temps * num_pops][num_vars] (cell t + num_temps * p)
  * directly (no master-stream draws) and recomputes the tracked energies. */
 ie_status ie_set_spins(ie_handle* h, const uint64_t* words);

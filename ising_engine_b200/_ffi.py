@@ -85,6 +85,8 @@ _SIGS = {
     "ie_run_pa": ([_vp, _vp, _vp], C.c_int),
     "ie_presolve": ([_vp, _vp, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
     "ie_two_opt": ([_vp, _vp, _vp, _vp], C.c_int),
+    "ie_set_init_probs": ([_vp, _vp], C.c_int),
+    "ie_warm_start_words": ([C.c_uint64, C.c_uint64, _vp, _vp, _vp, C.c_uint64, C.c_uint64, _vp, _vp], C.c_int),
     "ie_path_relink": ([_vp, _vp, C.c_uint64, _vp, _vp, _vp], C.c_int),
     "ie_connected_components": ([_vp, _vp, _vp, _vp], C.c_int),
     "ie_pa_normalized_weights": ([_vp, C.c_uint64, _vp], C.c_int),

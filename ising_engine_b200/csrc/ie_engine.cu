@@ -648,7 +648,27 @@ struct Engine {
         return IE_OK;
     }
 
+    // warm-start probabilities per site (single-instance handles); empty:
+    // the random init
+    std::vector<double> init_probs;
+
     ie_status init_random() {
+        if (!init_probs.empty()) {
+            // the warm start is drawn on the host at the stream's position
+            // and uploaded like ie_set_spins; the position advances past it
+            const InstDesc& d = desc[0];
+            HostStream rng{};
+            std::copy(keys.begin(), keys.begin() + 8, rng.key);
+            IE_CUDA(cudaMemcpyAsync(&rng.pos, d_pos.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+            IE_CUDA(cudaStreamSynchronize(stream));
+            std::vector<uint64_t> w((size_t)d.nt * d.n);
+            warm_start_words(rng, init_probs.data(), clampf.data() + d.site, clampv.data() + d.site, d.n, d.nt,
+                             w.data());
+            IE_TRY(write_words(0, w.data()));
+            IE_CUDA(cudaMemcpyAsync(d_pos.p, &rng.pos, sizeof(uint64_t), cudaMemcpyHostToDevice, stream));
+            IE_CUDA(cudaStreamSynchronize(stream));
+            return IE_OK;
+        }
         const DevArrays A = arrays();
         IE_CUDA(launch_init(A, 0, count, d_draw_idx.p, d_unclamped.p, stream));
         IE_CUDA(launch_energy(A, 0, count, stream));
@@ -1846,6 +1866,16 @@ ie_status ie_set_clamps(ie_handle* h, const uint8_t* is_clamped, const int8_t* c
     if (!h) return fail(IE_ERR_INVALID, "handle is NULL");
     IE_CUDA(cudaSetDevice(h->eng.device));
     return h->eng.set_clamps(0, is_clamped, clamp_val);
+}
+
+ie_status ie_set_init_probs(ie_handle* h, const double* probs) {
+    if (!h) return fail(IE_ERR_INVALID, "handle is NULL");
+    if (!probs) {
+        h->eng.init_probs.clear();
+        return IE_OK;
+    }
+    h->eng.init_probs.assign(probs, probs + h->eng.desc[0].n);
+    return IE_OK;
 }
 
 ie_status ie_init_random(ie_handle* h) {

@@ -43,6 +43,11 @@ struct HostStream {
     uint64_t index_inclusive(uint64_t hi);  // gen_range(0..=hi) for usize
 };
 
+// The warm-start initial words (reference layout, bit r = replica r) of
+// `cells` cells of n sites from the stream at rng.pos; rng.pos advances.
+void warm_start_words(HostStream& rng, const double* probs, const uint8_t* clampf, const int8_t* clampv, uint64_t n,
+                      uint64_t cells, uint64_t* words);
+
 namespace pa {
 std::vector<double> normalized_weights(const double* lw, size_t r);
 double effective_sample_size(const double* w, size_t r);

@@ -73,6 +73,26 @@ uint64_t HostStream::index_inclusive(uint64_t hi) {
     }
 }
 
+// UltimateSolver's warm start (ultimate.rs:256-263, the same policy for every
+// field geometry at :481-518): for cell c (cell-major) and site v, a clamped
+// site takes its value in every replica and draws nothing; otherwise replica
+// r is one when its gen_range(0.0..1.0) draw is below probs[v], 64 draws per
+// site in replica order. Words in the reference layout (bit r = replica r).
+void warm_start_words(HostStream& rng, const double* probs, const uint8_t* clampf, const int8_t* clampv, uint64_t n,
+                      uint64_t cells, uint64_t* words) {
+    for (uint64_t c = 0; c < cells; c++)
+        for (uint64_t v = 0; v < n; v++) {
+            uint64_t w = 0;
+            if (clampf && clampf[v]) {
+                w = clampv && clampv[v] == 1 ? ~0ull : 0ull;
+            } else {
+                for (int r = 0; r < 64; r++)
+                    if (rng.unit_f64() < probs[v]) w |= 1ull << r;
+            }
+            words[c * n + v] = w;
+        }
+}
+
 namespace pa {
 
 std::vector<double> normalized_weights(const double* lw, size_t r) {
@@ -189,6 +209,17 @@ std::vector<uint32_t> shuffled_parents(const std::vector<uint64_t>& counts, Host
 using namespace ie;
 
 extern "C" {
+
+ie_status ie_warm_start_words(uint64_t seed, uint64_t draw_offset, const double* probs, const uint8_t* is_clamped,
+                              const int8_t* clamp_val, uint64_t n, uint64_t cells, uint64_t* words, uint64_t* draws) {
+    if ((n && (!probs || !words)) || !draws) return fail(IE_ERR_INVALID, "NULL argument");
+    HostStream rng{};
+    chacha_key_from_u64(seed, rng.key);
+    rng.pos = draw_offset;
+    warm_start_words(rng, probs, is_clamped, clamp_val, n, cells, words);
+    *draws = rng.pos;
+    return IE_OK;
+}
 
 ie_status ie_pa_normalized_weights(const double* log_w, uint64_t r, double* w_out) {
     if ((!log_w || !w_out) && r) return fail(IE_ERR_INVALID, "NULL argument");

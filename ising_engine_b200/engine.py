@@ -83,6 +83,17 @@ class Engine:
         v = np.ascontiguousarray(np.zeros(self.n) if clamp_val is None else clamp_val, dtype=np.int8)
         _ffi.check(self._L.ie_set_clamps(self._h, _p(f), _p(v)))
 
+    def set_init_probs(self, probs) -> None:
+        """Warm start (ultimate.rs:121-124, 256-263): later inits draw replica
+        r of site v as one with probability probs[v]; None: random init."""
+        if probs is None:
+            _ffi.check(self._L.ie_set_init_probs(self._h, None))
+            return
+        p = np.ascontiguousarray(probs, dtype=np.float64)
+        if p.shape != (self.n,):
+            raise ValueError("probs must have num_vars entries")
+        _ffi.check(self._L.ie_set_init_probs(self._h, _p(p)))
+
     def init_random(self) -> None:
         _ffi.check(self._L.ie_init_random(self._h))
 

@@ -131,6 +131,7 @@ class UltimateSolver:
         self.use_icm = False  # isoenergetic cluster moves after every exchange block / stage
         self.use_2opt = False  # edge-restricted 2-opt escapes after the 1-opt polish
         self.use_path_relinking = False  # elite path relinking after the polish (PT path)
+        self.gnn_heuristic_probs = None  # warm-start probabilities per variable
         # presolve and decomposition before annealing (ultimate.rs:161-218); an
         # extension may switch them off, e.g. where probing's O(n^2 nnz) cost
         # is too high
@@ -148,6 +149,11 @@ class UltimateSolver:
         self.num_pops = int(pops)
         return self
 
+    def with_gnn_heuristic(self, probs) -> "UltimateSolver":
+        """ultimate.rs:121-124: the initial replicas are drawn with P(x_v = 1) = probs[v]."""
+        self.gnn_heuristic_probs = np.asarray(probs, dtype=np.float64).copy()
+        return self
+
     def with_2opt(self, enabled: bool) -> "UltimateSolver":
         """ultimate.rs:133-136."""
         self.use_2opt = bool(enabled)
@@ -159,11 +165,14 @@ class UltimateSolver:
                         self.post_resample_relaxation, self.ladder_mode, self.use_icm)
 
     def engine(self, model: QuboModel, num_pops: int | None = None) -> Engine:
-        return Engine(model, num_temps=self.num_temps, seed=self.seed,
-                      exchange_interval=self.exchange_interval, temp_max=self.temp_max,
-                      temp_min=self.temp_min, sweeps_per_exchange=self.sweeps_per_exchange,
-                      total_exchanges=self.total_exchanges, device=self.device,
-                      num_pops=self.num_pops if num_pops is None else num_pops, use_icm=self.use_icm)
+        eng = Engine(model, num_temps=self.num_temps, seed=self.seed,
+                     exchange_interval=self.exchange_interval, temp_max=self.temp_max,
+                     temp_min=self.temp_min, sweeps_per_exchange=self.sweeps_per_exchange,
+                     total_exchanges=self.total_exchanges, device=self.device,
+                     num_pops=self.num_pops if num_pops is None else num_pops, use_icm=self.use_icm)
+        if self.gnn_heuristic_probs is not None:
+            eng.set_init_probs(self.gnn_heuristic_probs)
+        return eng
 
     def _clamps(self, model: QuboModel, clamped):
         n = model.num_vars
@@ -226,6 +235,8 @@ class UltimateSolver:
                     sub, gmap = extract_component(model, comp, fixed_one)
                     child = copy.copy(self)
                     child.seed = (self.seed + ci + 1) & 0xFFFFFFFFFFFFFFFF
+                    if self.gnn_heuristic_probs is not None:  # ultimate.rs:200-203
+                        child.gnn_heuristic_probs = self.gnn_heuristic_probs[gmap]
                     result[gmap] = child.solve(sub)
                 return result
         if self.num_pops > 1:

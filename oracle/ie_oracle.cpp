@@ -415,9 +415,12 @@ static void step(Field& f, const Qubo& m, const double* temps, const std::vector
     }
 }
 
-// ultimate.rs:248-280 (random branch; the GNN warm start is not on the path).
+// ultimate.rs:248-280: clamped sites take their value; with warm-start
+// probabilities (with_gnn_heuristic) each replica is one when its
+// gen_range(0.0..1.0) draw is below probs[v]; otherwise one gen::<u64>()
+// word per site.
 static void init_field(Field& f, const std::vector<uint8_t>& clamped,
-                       const std::vector<int8_t>& cval, ChaCha8Rng& rng) {
+                       const std::vector<int8_t>& cval, ChaCha8Rng& rng, const double* probs = nullptr) {
     for (int p = 0; p < f.np; p++)
         for (int t = 0; t < f.nt; t++) {
             int8_t* s = f.cell(t + f.nt * p);
@@ -425,6 +428,8 @@ static void init_field(Field& f, const std::vector<uint8_t>& clamped,
                 if (clamped[v]) {
                     int8_t val = cval[v] == 1 ? 1 : 0;
                     for (int r = 0; r < NR; r++) s[v * NR + r] = val;
+                } else if (probs) {
+                    for (int r = 0; r < NR; r++) s[v * NR + r] = rng.gen_range(0.0, 1.0) < probs[v] ? 1 : 0;
                 } else {
                     uint64_t w = rng.next_u64();
                     for (int r = 0; r < NR; r++) s[v * NR + r] = (int8_t)((w >> r) & 1);
@@ -1802,6 +1807,20 @@ double or_path_relink(int64_t n, const double* lin, const int64_t* row, const in
                                                         cur, total_energy(m, state), be);
     std::copy(best.begin(), best.end(), state);
     return be;
+}
+
+// Warm-start words of `cells` cells (ultimate.rs:256-263) from
+// seed_from_u64(seed) after `skip` draws; returns the position after them.
+uint64_t or_warm_start_words(uint64_t seed, uint64_t skip, const double* probs, const uint8_t* clamped,
+                             const int8_t* clamp_val, int64_t n, int cells, uint64_t* words_out) {
+    ChaCha8Rng rng(seed);
+    for (uint64_t k = 0; k < skip; k++) rng.next_u64();
+    Field f(n, cells, 1);
+    std::vector<uint8_t> cl(clamped, clamped + n);
+    std::vector<int8_t> cv(clamp_val, clamp_val + n);
+    init_field(f, cl, cv, rng, probs);
+    pack_words(f, words_out);
+    return rng.draws;
 }
 
 double or_two_opt(int64_t n, const double* lin, const int64_t* row, const int64_t* col, const double* val,

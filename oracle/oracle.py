@@ -63,6 +63,8 @@ def lib():
         L.or_one_opt.restype = C.c_double
         L.or_two_opt.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, _i8p, _u8p]
         L.or_two_opt.restype = C.c_double
+        L.or_warm_start_words.argtypes = [C.c_uint64, C.c_uint64, _f64p, _u8p, _i8p, C.c_int64, C.c_int, _u64p]
+        L.or_warm_start_words.restype = C.c_uint64
         L.or_path_relink.argtypes = [C.c_int64, _f64p, _i64p, _i64p, _f64p, C.c_double, _u64p, C.c_int64, _u8p,
                                      _i8p]
         L.or_path_relink.restype = C.c_double
@@ -365,3 +367,15 @@ def path_relink_finish(model, words, state, clamped=None, offset=0.0):
     cl = np.zeros(n, dtype=np.uint8) if clamped is None else np.ascontiguousarray(clamped, dtype=np.uint8)
     e = lib().or_path_relink(n, lin, row, col, val, float(offset), w, w.size // max(n, 1), cl, x)
     return x, e
+
+
+def warm_start_words(seed, skip, probs, cells, clamped=None, clamp_val=None):
+    """The warm-start init (ultimate.rs:256-263): words [cells, n] and the
+    stream position after them."""
+    p = np.ascontiguousarray(probs, dtype=np.float64)
+    n = len(p)
+    cl = np.zeros(n, np.uint8) if clamped is None else np.ascontiguousarray(clamped, dtype=np.uint8)
+    cv = np.zeros(n, np.int8) if clamp_val is None else np.ascontiguousarray(clamp_val, dtype=np.int8)
+    out = np.zeros(cells * n, dtype=np.uint64)
+    d = lib().or_warm_start_words(int(seed), int(skip), p, cl, cv, n, int(cells), out)
+    return out.reshape(cells, n), int(d)

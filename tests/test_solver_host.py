@@ -31,3 +31,34 @@ def test_luby_restart_driver(monkeypatch):
     assert all(c[2] == [(2, 0)] for c in calls)
     # energies: 1, -2, -1.5, -2, -0.5, 0: the first -2 wins
     assert x.tolist() == [0, 1, 0] and base.total_exchanges == 3 and base.seed == 2 ** 64 - 5
+
+
+def test_warm_start_words_equal_oracle():
+    """with_gnn_heuristic's init (ultimate.rs:256-263): the library's host
+    generator gives the oracle's words and stream position (clamped sites
+    draw nothing; probabilities 0, 1, NaN and out of range included)."""
+    import ctypes as C
+    from ising_engine_b200 import _ffi
+    from oracle import oracle as O
+    rng = np.random.default_rng(4)
+    n, cells = 37, 5
+    probs = rng.random(n)
+    probs[[0, 1, 2, 3]] = [0.0, 1.0, np.nan, 1.7]
+    cl = np.zeros(n, np.uint8)
+    cl[[5, 20]] = 1
+    cv = np.zeros(n, np.int8)
+    cv[20] = 1
+    for seed, skip in ((1, 0), (77, 13)):
+        ref, rd = O.warm_start_words(seed, skip, probs, cells, cl, cv)
+        w = np.zeros(cells * n, dtype=np.uint64)
+        d = C.c_uint64()
+        _ffi.check(_ffi.lib().ie_warm_start_words(seed, skip, probs.ctypes.data, cl.ctypes.data, cv.ctypes.data, n,
+                                                  cells, w.ctypes.data, C.byref(d)))
+        assert np.array_equal(w.reshape(cells, n), ref) and d.value == rd == skip + cells * (n - 2) * 64
+        assert (ref[:, 0] == 0).all() and (ref[:, 1] == np.uint64(2 ** 64 - 1)).all() and (ref[:, 2] == 0).all()
+        assert (ref[:, 20] == np.uint64(2 ** 64 - 1)).all() and (ref[:, 5] == 0).all()
+
+
+def test_with_gnn_heuristic_flag():
+    s = S.UltimateSolver(1.0, 0.1, 1, 1, 0)
+    assert s.with_gnn_heuristic([0.2, 0.8]) is s and s.gnn_heuristic_probs.tolist() == [0.2, 0.8]
