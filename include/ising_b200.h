@@ -225,19 +225,20 @@ ie_status ie_batch_class_report(ie_batch* b, uint32_t max_classes, uint32_t* n_c
 ie_status ie_batch_last_launches(ie_batch* b, uint64_t* launches);
 
 /* ---- one SA run with no device allocation (no reference counterpart) ----
- * For callers that cannot allocate device memory: code that runs while a CUDA
- * graph is being captured, hosts whose framework owns a fixed device pool and
- * forbids other allocators, services that must not block or fail on an
- * allocation mid-request. The problem and the outputs are in device memory the
+ * For callers that cannot allocate device memory: hosts whose framework owns
+ * a fixed device pool and forbids other allocators, and services that must
+ * not block or fail on an allocation mid-request. The problem and the outputs are in device memory the
  * caller already owns; all scratch lives in one file-scope device array of
  * 12 MiB that every GPU loading this library holds until process exit.
  * Limits: num_vars <= 16384, nnz <= 262144 (both triangles), n_steps <= 65536;
  * larger inputs return IE_ERR_INVALID. The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
- * Calls share the array, so calls that overlap on the GPU (other threads or
- * streams) race; serialize them. The run is the f64 mode of the batched sweep
- * (same spins and energies as ie_batch_run_schedule for the same problem, seed
- * and temperatures); it returns after the stream has finished the run. */
+ * array's device address (kept for the life of that device's CUDA context);
+ * make that first call before any stream capture. The caller's current device
+ * is restored before the call returns. Calls share the array, so calls that
+ * overlap on the GPU (other threads or streams) race; serialize them. The run
+ * is the f64 mode of the batched sweep (same spins and energies as
+ * ie_batch_run_schedule for the same problem, seed and temperatures); it
+ * returns after the stream has finished the run. */
 typedef struct ie_problem_device {
     uint32_t num_vars;
     uint32_t nnz;

@@ -1,10 +1,9 @@
 // Simulated-annealing run of one problem with no device allocation.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA graph is
-// being captured (allocation is not a capturable operation), hosts that hand
-// the GPU to a framework with its own fixed memory pool and forbid other
-// allocators, and latency-critical services that must not risk a blocking or
-// failing allocation mid-request. ie_sa_run_static serves them: the caller
+// Some callers cannot call cudaMalloc: hosts that hand the GPU to a framework
+// with its own fixed memory pool and forbid other allocators, and
+// latency-critical services that must not risk a blocking or failing
+// allocation mid-request. ie_sa_run_static serves them: the caller
 // provides the problem and the output buffers in device memory it already
 // owns, and every byte of scratch the run needs (the site-record stream, the
 // instance descriptor, the master-stream key and position, the work-queue
@@ -48,12 +47,27 @@ static_assert(kOffRecs + (size_t)64 * 1024 * 4 < kStaticScratchBytes, "record ar
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
+// Checks the caller's CSR on many threads before anything reads it through
+// the row offsets: rows[0] == 0, rows[n] <= nnz, monotone row offsets, and
+// every stored column below n. A violation sets *err = 4. Every index used
+// here is below n + 1 (rows) or nnz (cols), the sizes the caller declared.
+__global__ void static_check_kernel(const uint32_t* rows, const uint32_t* cols, uint32_t n, uint32_t nnz,
+                                    int32_t* err) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0 && (rows[0] != 0 || rows[n] > nnz)) atomicExch(err, 4);
+    for (uint32_t v = t; v < n; v += stride)
+        if (rows[v + 1] < rows[v]) atomicExch(err, 4);
+    for (uint32_t e = t; e < nnz; e += stride)
+        if (cols[e] >= n) atomicExch(err, 4);
+}
+
 // Packs the f64 site-record stream (layout in ie_kernels.cuh) of the problem
-// into the scratch record area. One thread: chunk packing is sequential. The
-// caller's CSR is checked first (monotone row offsets within nnz, columns
-// below n); every write is bounds-checked. On a bad CSR (*err = 4) or too
-// little room (*err = 3) the descriptor gets n = 0, so the later kernels of
-// the call touch nothing.
+// into the scratch record area. One thread: chunk packing is sequential (about
+// 1M words at the coupling limit). It runs only on a CSR that
+// static_check_kernel passed; every write is bounds-checked. On a bad CSR
+// (*err = 4) or too little room (*err = 3) the descriptor gets n = 0, so the
+// later kernels of the call touch nothing.
 __global__ void static_records_kernel(const uint32_t* rows, const uint32_t* cols, const double* vals,
                                       const double* lin, uint32_t n, uint32_t nnz, uint32_t* recs, uint64_t cap,
                                       InstDesc* desc, int32_t* err) {
@@ -62,23 +76,9 @@ __global__ void static_records_kernel(const uint32_t* rows, const uint32_t* cols
     bad.mode = kModeF64;
     bad.nt = 1;
     bad.rec_len = 0;
-    if (rows[0] != 0 || rows[n] > nnz) {
-        *err = 4;
+    if (*err != 0) {
         *desc = bad;
         return;
-    }
-    for (uint32_t v = 0; v < n; v++) {
-        if (rows[v + 1] < rows[v]) {
-            *err = 4;
-            *desc = bad;
-            return;
-        }
-        for (uint32_t e = rows[v]; e < rows[v + 1]; e++)
-            if (cols[e] >= n) {
-                *err = 4;
-                *desc = bad;
-                return;
-            }
     }
     uint64_t w = 0;   // words written
     uint32_t c = 0;   // position in the current chunk
@@ -159,7 +159,20 @@ __global__ void static_export_kernel(const uint64_t* spins, uint32_t n, uint64_t
 namespace {
 
 std::mutex g_static_mu;
+// Device address of the scratch array per device ordinal, looked up on the
+// first call on that device and valid for the life of its CUDA context.
 void* g_static_ptr[64] = {nullptr};
+
+// Restores the caller's current device on every return path.
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
 
 ie_status static_fail(ie_status s, const char* msg) {
     ie::set_last_error(msg);
@@ -194,6 +207,7 @@ extern "C" ie_status ie_sa_run_static(const ie_problem_device* problem, uint64_t
     if (device < 0 || device >= 64) return static_fail(IE_ERR_INVALID, "ie_sa_run_static: bad device ordinal");
     for (uint64_t i = 0; i < n_steps; i++)
         if (!(temps[i] > 0.0)) return static_fail(IE_ERR_INVALID, "ie_sa_run_static: temperatures must be positive");
+    DeviceGuard guard;
     if (cudaSetDevice(device) != cudaSuccess) return static_fail(IE_ERR_CUDA, "cudaSetDevice failed");
     unsigned char* base = nullptr;
     {
@@ -236,6 +250,7 @@ extern "C" ie_status ie_sa_run_static(const ie_problem_device* problem, uint64_t
         return static_fail(IE_ERR_CUDA, "copy into the static scratch failed");
 
     const uint32_t n = problem->num_vars;
+    static_check_kernel<<<64, 256, 0, st>>>(problem->row_offsets, problem->col_indices, n, problem->nnz, d_err);
     static_records_kernel<<<1, 1, 0, st>>>(problem->row_offsets, problem->col_indices, problem->values,
                                            problem->linear, n, problem->nnz, d_recs, kStaticRecWords, d_desc,
                                            d_err);
