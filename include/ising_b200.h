@@ -68,9 +68,14 @@ typedef struct ie_config {
     int32_t device;      /* CUDA device ordinal */
     int32_t pt_path;     /* 0: chosen by size; 1: one CTA runs all cells of the instance;
                             2: every cell is its own work item of the batched kernels, the
-                            exchange runs between their launches (same results) */
+                            exchange runs between their launches (same results);
+                            3: as 2, but one launch (one CTA) per cell, one after another:
+                            the plain per-temperature method (level kernel only) */
     int32_t use_icm;     /* UltimateSolver::use_icm: an ICM sweep (src/solver/icm.rs) after every
                             exchange block of ie_run_pt; 0 by default */
+    int32_t kernel_form; /* 0: integer-mode cells run on the level kernel (generator and
+                            decision phases, all cells of the ladder in flight); 1: the
+                            per-lane kernels only (same results) */
 } ie_config;
 
 typedef struct ie_handle ie_handle;
@@ -189,6 +194,13 @@ typedef struct ie_batch_config {
     int32_t use_graph;          /* nonzero: ie_batch_run_schedule replays one CUDA graph holding
                                    the launches of every work class (captured on first use and
                                    again when the classes or the schedule length change) */
+    int32_t kernel_form;        /* 0: the level kernel (default); 1: the per-lane kernels.
+                                   Same spins; f64 energies are the FP64 recompute of the final
+                                   state on the level kernel, the tracked sum on the others */
+    uint32_t item_sites;        /* level kernel: spin words per CTA work item (0: 4096) */
+    uint32_t tie_shift;         /* test hook, 0 in normal use: level-kernel decisions compare only
+                                   the top 32 - tie_shift bits of the stored outputs, so the exact
+                                   path (outputs recomputed from the lane seed) runs often */
 } ie_batch_config;
 
 /* count problems, each run as one cell of 64 replicas with its own seed. */
@@ -223,6 +235,16 @@ ie_status ie_batch_class_report(ie_batch* b, uint32_t max_classes, uint32_t* n_c
                                 double* ms);
 /* Number of kernel launches the last run call issued. */
 ie_status ie_batch_last_launches(ie_batch* b, uint64_t* launches);
+/* Level kernel: number of decisions taken on its exact path (output
+ * recomputed from the lane seed) since the batch was created. */
+ie_status ie_batch_exact_decisions(ie_batch* b, uint64_t* count);
+
+/* Coefficients of x^steps mod P(x), P the characteristic polynomial of the
+ * Xoshiro256 state transition (engine.rs:115-121): bit i of out[i / 64] is the
+ * coefficient of x^i. The state after `steps` more steps is the XOR of the
+ * states after i steps over the set coefficients i < 256 (the jump the level
+ * kernel uses to start a lane's stream mid-sweep). out: [4]. */
+ie_status ie_xoshiro_jump_poly(uint64_t steps, uint64_t* out);
 
 /* ---- one SA run with no device allocation (no reference counterpart) ----
  * For callers that cannot allocate device memory: hosts whose framework owns

@@ -8,8 +8,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libising_b200.so")
-SOURCES = ["ie_kernels.cu", "ie_engine.cu", "ie_static.cu", "ie_v2.cu", "ie_pa.cu", "ie_presolve.cu", "ie_local.cu"]
-HEADERS = ["ie_device.cuh", "ie_kernels.cuh", "ie_launch.h", "ie_host.h",
+SOURCES = ["ie_kernels.cu", "ie_level.cu", "ie_level_host.cu", "ie_engine.cu", "ie_static.cu", "ie_v2.cu",
+           "ie_pa.cu", "ie_presolve.cu", "ie_local.cu"]
+HEADERS = ["ie_device.cuh", "ie_kernels.cuh", "ie_sweep.cuh", "ie_level.cuh", "ie_level_host.h", "ie_launch.h",
+           "ie_host.h",
            os.path.join("..", "..", "include", "ising_b200.h")]
 
 NVCC_FLAGS = [

@@ -38,7 +38,7 @@ class ie_config(C.Structure):
                 ("seed", C.c_uint64), ("num_temps", C.c_uint32), ("num_pops", C.c_uint32),
                 ("num_slices", C.c_uint32), ("exchange_interval", C.c_uint32),
                 ("force_f64", C.c_int32), ("device", C.c_int32), ("pt_path", C.c_int32),
-                ("use_icm", C.c_int32)]
+                ("use_icm", C.c_int32), ("kernel_form", C.c_int32)]
 
 
 class ie_problem_device(C.Structure):
@@ -61,7 +61,8 @@ class ie_pa_report(C.Structure):
 class ie_batch_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("force_f64", C.c_int32),
                 ("threads_per_block", C.c_uint32), ("blocks_per_sm", C.c_uint32),
-                ("disable_windows", C.c_int32), ("use_graph", C.c_int32)]
+                ("disable_windows", C.c_int32), ("use_graph", C.c_int32),
+                ("kernel_form", C.c_int32), ("item_sites", C.c_uint32), ("tie_shift", C.c_uint32)]
 
 
 class ie_serve_config(C.Structure):
@@ -118,6 +119,8 @@ _SIGS = {
     "ie_batch_autotune": ([_vp, _vp, C.c_uint64, _vp], C.c_int),
     "ie_batch_class_report": ([_vp, C.c_uint32, _vp, _vp, _vp], C.c_int),
     "ie_batch_last_launches": ([_vp, _vp], C.c_int),
+    "ie_batch_exact_decisions": ([_vp, _vp], C.c_int),
+    "ie_xoshiro_jump_poly": ([C.c_uint64, _vp], C.c_int),
     "ie_probe_peaks": ([C.c_int32, _vp, _vp], C.c_int),
     "ie_sa_run_static": ([_vp, C.c_uint64, _vp, C.c_uint64, _vp, _vp, C.c_int32, _vp], C.c_int),
     "ie_serve_create": ([_vp, _vp], C.c_int),

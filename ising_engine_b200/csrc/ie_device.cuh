@@ -110,6 +110,46 @@ struct Xoshiro {
         advance();
         return result;
     }
+    // Top 32 bits of the next output (the output's uniform is determined to
+    // within 2^-32 by them).
+    __device__ __forceinline__ uint32_t next_hi() {
+        const uint64_t s0 = ((uint64_t)a1 << 32) | a0, s3 = ((uint64_t)d1 << 32) | d0;
+        const uint64_t result = rotl64(s0 + s3, 23) + s0;
+        advance();
+        return (uint32_t)(result >> 32);
+    }
+    // Jump: the state after D more steps, given the coefficients (bit i of
+    // poly[i / 64] = coefficient of x^i) of x^D mod P(x), P the characteristic
+    // polynomial of the state transition M: M^D s = sum of r_i M^i s over the
+    // set coefficients r_i (Cayley-Hamilton), accumulated over 256 steps.
+    __device__ __forceinline__ void jump(const uint64_t* __restrict__ poly) {
+        uint32_t j[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+        for (int w = 0; w < 8; w++) {
+            const uint32_t p = (uint32_t)(__ldg(poly + (w >> 1)) >> (32 * (w & 1)));
+#pragma unroll 4
+            for (int b = 0; b < 32; b++) {
+                const uint32_t m = 0u - ((p >> b) & 1u);
+                j[0] ^= a0 & m;
+                j[1] ^= a1 & m;
+                j[2] ^= b0 & m;
+                j[3] ^= b1 & m;
+                j[4] ^= c0 & m;
+                j[5] ^= c1 & m;
+                j[6] ^= d0 & m;
+                j[7] ^= d1 & m;
+                advance();
+            }
+        }
+        a0 = j[0];
+        a1 = j[1];
+        b0 = j[2];
+        b1 = j[3];
+        c0 = j[4];
+        c1 = j[5];
+        d0 = j[6];
+        d1 = j[7];
+    }
 };
 
 // ---------------------------------------------------------------------------

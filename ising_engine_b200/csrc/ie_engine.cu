@@ -22,6 +22,7 @@
 #include "ie_device.cuh"
 #include "ie_host.h"
 #include "ie_launch.h"
+#include "ie_level_host.h"
 
 using namespace ie;
 
@@ -643,6 +644,7 @@ struct Engine {
         IE_TRY(d_wtab.upload(wt, stream));
         quads_built = false;
         IE_CUDA(cudaMemcpyAsync(d_desc.p, desc.data(), desc.size() * sizeof(InstDesc), cudaMemcpyHostToDevice, stream));
+        if (kernel_form == 0) IE_TRY(build_level_data());
         IE_CUDA(cudaStreamSynchronize(stream));
         recs_dirty = false;
         return IE_OK;
@@ -699,7 +701,15 @@ struct Engine {
         double site_steps = 0; // sites summed over the class (per sweep)
         DevBuf<uint32_t> items;
         DevBuf<int32_t> itemh;
+        // level-kernel class: items of the shared item arrays in launch order
+        bool level = false;
+        bool gsp = false;
+        uint32_t ntab = 1;
+        int grid = 0;
+        uint64_t keystride = 0, keyoff = 0;
+        DevBuf<uint32_t> order;
     };
+    static constexpr int kLevelForm = 32;  // tpl tag of a level-kernel class
     std::vector<std::unique_ptr<WorkClass>> classes;
     std::vector<cudaStream_t> cstreams;
     std::vector<cudaEvent_t> cevents, cstart, cjoin;
@@ -743,6 +753,68 @@ struct Engine {
     bool use_windows = true;
     std::vector<uint8_t> active;  // instances in the work classes (empty: all)
 
+    // Level kernel (ie_level.cu): kernel_form 0 runs batched instances and
+    // integer-mode PT cells on it; 1 keeps the per-lane kernels.
+    int kernel_form = 0;
+    uint32_t lvl_cap = 4096;  // spin words per item (shared memory)
+    int lvl_threads = 256;
+    uint32_t lvl_tie_shift = 0;
+    bool serving = false;     // serving launches: one threshold table per member
+    std::vector<std::vector<uint32_t>> lv_sites, lv_off;  // per instance: sites by level, level starts
+    DevBuf<uint32_t> d_lrecs, d_recoff, d_lent, d_llvl, d_lseg, d_keybuf;
+    DevBuf<LvlItem> d_litems;
+    DevBuf<LvlMember> d_lmem;
+    DevBuf<uint64_t> d_jpoly;
+    DevBuf<int32_t> d_exact;
+    DevBuf<uint32_t> d_plainq;  // queue counters of the one-launch-per-cell path
+    uint32_t jpoly_count = 0;
+    LvlHost lvh;
+
+    bool level_ok(const InstDesc& d, bool cells_view) const {
+        if (kernel_form != 0) return false;
+        return !cells_view || d.mode == kModeInt;
+    }
+
+    static LvlSource lvl_source(const HostInst& h, const uint8_t* clampf) {
+        LvlSource s;
+        s.n = h.n;
+        s.mode = h.mode;
+        s.rows = h.rows.data();
+        s.cols = h.cols.data();
+        s.vals = h.vals.data();
+        s.lin = h.lin.data();
+        s.ents = h.ents.data();
+        s.linp = h.linp.data();
+        s.clampf = clampf;
+        return s;
+    }
+
+    // Level records (recoff indexed by InstDesc::site + v) and dependency
+    // levels of every instance, built on host threads.
+    ie_status build_level_data() {
+        std::vector<std::vector<uint32_t>> lrec(count);
+        std::vector<uint32_t> recoff(std::max<size_t>(total_sites, 1), 0);
+        lv_sites.assign(count, {});
+        lv_off.assign(count, {});
+        parallel_for(count, [&](uint32_t i) {
+            const LvlSource src = lvl_source(insts[i], clampf.data() + desc[i].site);
+            level_records(src, lrec[i], recoff.data() + desc[i].site);
+            site_levels(src, lv_sites[i], lv_off[i]);
+        });
+        std::vector<uint64_t> base(count + 1, 0);
+        for (uint32_t i = 0; i < count; i++) base[i + 1] = base[i] + lrec[i].size();
+        if (base[count] / 4 >= (1ull << 32)) return fail(IE_ERR_UNSUPPORTED, "level records exceed 64 GiB");
+        std::vector<uint32_t> recs(std::max<uint64_t>(base[count], 4), 0);
+        parallel_for(count, [&](uint32_t i) {
+            std::copy(lrec[i].begin(), lrec[i].end(), recs.begin() + base[i]);
+            const uint32_t b16 = (uint32_t)(base[i] / 4);
+            for (uint32_t v = 0; v < desc[i].n; v++) recoff[desc[i].site + v] += b16;
+        });
+        IE_TRY(d_lrecs.upload(recs, stream));
+        IE_TRY(d_recoff.upload(recoff, stream));
+        return IE_OK;
+    }
+
     // CUDA graph of one batched run (use_graph): valid for the classes it was
     // captured with and for runs of g_steps steps; the step base is read from
     // d_stepbase so replays continue the trajectory.
@@ -769,6 +841,96 @@ struct Engine {
         return (n + 63u) & ~63u;
     }
 
+    // Level-kernel classes over an instance view: one class per (mode,
+    // spins in shared / global memory); items of up to lvl_cap spin words
+    // (a PT cell of 512 sites or more is an item of its own, so a ladder
+    // spreads over as many CTAs as it has cells). Each class's grid and
+    // per-CTA output buffer are fixed here.
+    template <typename Live>
+    ie_status build_level_classes(const std::vector<InstDesc>& D, const std::vector<HostInst>& HI, bool cells_view,
+                                  Live live) {
+        lvh.clear();
+        std::vector<uint64_t> nnz_of(D.size());
+        for (size_t i = 0; i < D.size(); i++) nnz_of[i] = HI[i].nnz;
+        const bool own = cells_view || serving;
+        std::vector<uint32_t> mem[2][2];
+        for (uint32_t i = 0; i < (uint32_t)D.size(); i++) {
+            if (!live(i) || !level_ok(D[i], cells_view)) continue;
+            const bool gsp = D[i].n > lvl_cap;
+            mem[D[i].mode == kModeF64 ? 1 : 0][gsp ? 1 : 0].push_back(i);
+        }
+        uint64_t keytotal = 0;
+        for (int m = 0; m < 2; m++)
+            for (int g = 0; g < 2; g++) {
+                if (mem[m][g].empty()) continue;
+                std::unique_ptr<WorkClass> wc(new WorkClass());
+                wc->level = true;
+                wc->mode = m ? kModeF64 : kModeInt;
+                wc->gsp = g != 0;
+                wc->tpl = kLevelForm;
+                wc->cap = g ? 0u : lvl_cap;
+                uint32_t cap = lvl_cap, maxn = 0;
+                for (uint32_t i : mem[m][g]) maxn = std::max(maxn, D[i].n);
+                if (cells_view && maxn >= 512) cap = std::min(cap, maxn);
+                const uint32_t maxmem = own ? kLvlMaxOwnTables : kLvlMaxMembers;
+                std::vector<uint32_t> order;
+                double longest = 0;
+                build_level_items(D, nnz_of, lv_sites, lv_off, mem[m][g], g != 0, cap, maxmem, lvh, order, longest);
+                wc->nitems = (uint32_t)order.size();
+                wc->work = longest;
+                for (uint32_t i : mem[m][g]) wc->site_steps += (double)D[i].n;
+                wc->ntab = own ? maxmem : 1u;
+                const size_t smem = level_smem(wc->mode, wc->ntab, g ? 0 : lvl_cap);
+                int occ = level_occupancy(wc->mode, g != 0, lvl_threads, smem);
+                if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "level kernel does not fit on an SM");
+                if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
+                wc->grid = std::max(1, std::min<int>((int)wc->nitems, occ * g_sm_count));
+                wc->keystride = 64ull * (g ? maxn : lvl_cap);
+                wc->keyoff = keytotal;
+                keytotal += wc->keystride * (uint64_t)wc->grid;
+                IE_TRY(wc->order.upload(order, stream));
+                classes.push_back(std::move(wc));
+            }
+        if (lvh.items.empty()) return IE_OK;
+        IE_TRY(d_litems.upload(lvh.items, stream));
+        IE_TRY(d_lmem.upload(lvh.members, stream));
+        IE_TRY(d_lent.upload(lvh.entries.empty() ? std::vector<uint32_t>(1, 0) : lvh.entries, stream));
+        IE_TRY(d_llvl.upload(lvh.lvloff, stream));
+        IE_TRY(d_lseg.upload(lvh.segs, stream));
+        IE_TRY(d_keybuf.alloc(std::max<uint64_t>(keytotal, 1)));
+        if (lvh.max_segs > jpoly_count) {
+            std::vector<uint64_t> tab;
+            if (!xoshiro_segment_polys(lvh.max_segs, tab))
+                return fail(IE_ERR_DEVICE, "Xoshiro jump polynomial could not be derived");
+            IE_TRY(d_jpoly.upload(tab, stream));
+            jpoly_count = lvh.max_segs;
+        }
+        if (!d_exact.p) IE_TRY(d_exact.upload(std::vector<int32_t>(1, 0), stream));
+        return IE_OK;
+    }
+
+    LvlArgs level_args(const WorkClass& wc, uint32_t* queue) const {
+        LvlArgs L{};
+        L.items = d_litems.p;
+        L.order = wc.order.p;
+        L.nitems = wc.nitems;
+        L.queue = queue;
+        L.members = d_lmem.p;
+        L.entries = d_lent.p;
+        L.lvloff = d_llvl.p;
+        L.segs = d_lseg.p;
+        L.jpoly = d_jpoly.p;
+        L.recoff = d_recoff.p;
+        L.lrecs = d_lrecs.p;
+        L.keybuf = d_keybuf.p + wc.keyoff;
+        L.keystride = wc.keystride;
+        L.spin_cap = wc.gsp ? 0u : lvl_cap;
+        L.ntab = wc.ntab;
+        L.tie_shift = lvl_tie_shift;
+        L.exact_count = d_exact.p;
+        return L;
+    }
+
     // Per class: instances ordered by degree then size into items of 4/TPL
     // (the groups of a warp stay in step sweep by sweep), items ordered by
     // work, longest first; classes ordered by their longest item.
@@ -782,7 +944,9 @@ struct Engine {
         cells_built = false;
         graph_valid = false;
         std::vector<std::tuple<uint32_t, int, uint32_t>> keys;
-        auto live = [&](uint32_t i) { return Dp || active.empty() || active[i] != 0; };
+        auto live0 = [&](uint32_t i) { return Dp || active.empty() || active[i] != 0; };
+        IE_TRY(build_level_classes(D, HI, Dp != nullptr, live0));
+        auto live = [&](uint32_t i) { return live0(i) && !level_ok(D[i], Dp != nullptr); };
         for (uint32_t i = 0; i < N; i++) {
             if (!live(i)) continue;
             auto k = std::make_tuple(D[i].mode, tpl_of(D[i], HI[i]), class_cap(D[i]));
@@ -850,7 +1014,7 @@ struct Engine {
     bool use_cells() const {
         if (pop_len) return true;
         if (pt_path == 1) return false;
-        if (pt_path == 2) return true;
+        if (pt_path >= 2) return true;
         return desc[0].n >= 256;
     }
 
@@ -986,6 +1150,10 @@ struct Engine {
         for (size_t k = 0; k < classes.size(); k++) {
             WorkClass& wc = *classes[k];
             if (!wc.nitems) continue;
+            if (wc.level) {
+                grids[k] = wc.grid;
+                continue;
+            }
             int occ = wc.tpl == 8       ? window_occupancy(wc.mode, wc.cap)
                       : wc.tpl == kChain ? chain_occupancy(wc.mode, wc.cap)
                                          : batch_occupancy(wc.mode, wc.tpl, wc.cap, base.serve != 0 || base.cells != 0);
@@ -1003,6 +1171,13 @@ struct Engine {
         const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
         launches = 0;
         IE_CUDA(cudaMemsetAsync(d_queue.p, 0, classes.size() * sizeof(uint32_t), stream));
+        uint32_t plain_base = 0;
+        if (pt_path == 3 && base.cells) {
+            uint32_t total = 0;
+            for (auto& c : classes) total += c->level ? c->nitems : 0u;
+            IE_TRY(d_plainq.alloc(std::max<uint32_t>(total, 1)));
+            IE_CUDA(cudaMemsetAsync(d_plainq.p, 0, d_plainq.n * sizeof(uint32_t), stream));
+        }
         IE_CUDA(cudaEventRecord(evfork, stream));
         for (size_t k = 0; k < classes.size(); k++) {
             WorkClass& wc = *classes[k];
@@ -1014,7 +1189,22 @@ struct Engine {
             R.nquads = wc.nitems;
             R.queue = d_queue.p + k;
             IE_CUDA(cudaEventRecordWithFlags(cstart[k], cstreams[k], rec));
-            if (wc.tpl == 8) IE_CUDA(launch_window(A, R, wc.mode, wc.cap, grids[k], cstreams[k]));
+            if (wc.level && pt_path == 3 && base.cells) {
+                // the plain per-temperature method: one launch (one CTA) per
+                // cell, one after another
+                for (uint32_t it = 0; it < wc.nitems; it++) {
+                    LvlArgs L = level_args(wc, d_plainq.p + plain_base + it);
+                    L.order = wc.order.p + it;
+                    L.nitems = 1;
+                    IE_CUDA(launch_level(A, R, L, wc.mode, wc.gsp, lvl_threads, 1, cstreams[k]));
+                    launches++;
+                }
+                plain_base += wc.nitems;
+                launches--;
+            } else if (wc.level)
+                IE_CUDA(launch_level(A, R, level_args(wc, d_queue.p + k), wc.mode, wc.gsp, lvl_threads, grids[k],
+                                     cstreams[k]));
+            else if (wc.tpl == 8) IE_CUDA(launch_window(A, R, wc.mode, wc.cap, grids[k], cstreams[k]));
             else if (wc.tpl == kChain) IE_CUDA(launch_chain(A, R, wc.mode, wc.cap, grids[k], cstreams[k]));
             else IE_CUDA(launch_batch(A, R, wc.mode, wc.tpl, wc.cap, grids[k], cstreams[k]));
             IE_CUDA(cudaEventRecordWithFlags(cevents[k], cstreams[k], rec));
@@ -1192,6 +1382,37 @@ struct Engine {
         if (recs_dirty) IE_TRY(build_record_streams());
         std::vector<double> t(temps, temps + steps);
         IE_TRY(d_temps.upload(t, stream));
+        if (kernel_form == 0) {
+            // the level kernel, one launch (one CTA) per instance in sequence
+            quads_built = false;
+            graph_valid = false;
+            classes.clear();
+            IE_TRY(build_level_classes(desc, insts, false,
+                                       [&](uint32_t j) { return j >= first && j < first + n_inst; }));
+            DevBuf<uint32_t> counters;
+            IE_TRY(counters.upload(std::vector<uint32_t>(n_inst, 0), stream));
+            IE_CUDA(cudaEventRecord(ev0, stream));
+            uint32_t launched = 0;
+            for (auto& wcp : classes) {
+                const WorkClass& wc = *wcp;
+                for (uint32_t k = 0; k < wc.nitems; k++) {
+                    RunArgs R = sa_args(steps);
+                    LvlArgs L = level_args(wc, counters.p + launched);
+                    L.order = wc.order.p + k;
+                    L.nitems = 1;
+                    IE_CUDA(launch_level(arrays(), R, L, wc.mode, wc.gsp, lvl_threads, 1, stream));
+                    launched++;
+                }
+            }
+            IE_CUDA(cudaEventRecord(ev1, stream));
+            IE_CUDA(cudaEventSynchronize(ev1));
+            float ms = 0;
+            IE_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+            last_ms = ms;
+            last_launches = launched;
+            classes.clear();
+            return IE_OK;
+        }
         std::vector<uint32_t> quads((size_t)4 * n_inst, 0xffffffffu);
         std::vector<int32_t> qh(n_inst);
         for (uint32_t i = 0; i < n_inst; i++) {
@@ -1474,6 +1695,7 @@ struct ServeEngine {
         if (cfg.max_sites >= (1ull << 32) || cfg.max_couplings >= (1ull << 32))
             return fail(IE_ERR_INVALID, "max_sites and max_couplings must be below 2^32");
         IE_TRY(eng.setup_device(cfg.device));
+        eng.kernel_form = 1;
         const uint32_t S = cfg.max_requests;
         eng.nt = 1;
         eng.count = S;
@@ -1837,9 +2059,13 @@ ie_status ie_create(const ie_problem* problem, const ie_config* config, ie_handl
     if (h->cfg.num_temps == 0) h->cfg.num_temps = 10;
     if (h->cfg.exchange_interval == 0) h->cfg.exchange_interval = 1;
     if (h->cfg.num_temps > 128) return fail(IE_ERR_UNSUPPORTED, "at most 128 temperatures");
-    if (h->cfg.pt_path < 0 || h->cfg.pt_path > 2) return fail(IE_ERR_INVALID, "pt_path must be 0, 1 or 2");
+    if (h->cfg.pt_path < 0 || h->cfg.pt_path > 3) return fail(IE_ERR_INVALID, "pt_path must be 0, 1, 2 or 3");
+    if (h->cfg.kernel_form < 0 || h->cfg.kernel_form > 1) return fail(IE_ERR_INVALID, "kernel_form must be 0 or 1");
+    if (h->cfg.pt_path == 3 && h->cfg.kernel_form != 0)
+        return fail(IE_ERR_INVALID, "pt_path 3 (one launch per cell) runs on the level kernel (kernel_form 0)");
     IE_TRY(h->eng.setup_device(config->device));
     h->eng.pt_path = h->cfg.pt_path;
+    h->eng.kernel_form = h->cfg.kernel_form;
     const uint32_t pops = std::max<uint32_t>(h->cfg.num_pops, 1);
     if (pops > 1) {
         // QuantumField::new(n, 1, num_temps, num_pops): cell t + num_temps * p,
@@ -2249,6 +2475,15 @@ ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint
     b->eng.blocks_per_sm = cfg.blocks_per_sm;
     b->eng.use_windows = cfg.disable_windows == 0;
     b->eng.use_graph = cfg.use_graph != 0;
+    if (cfg.kernel_form < 0 || cfg.kernel_form > 1) return fail(IE_ERR_INVALID, "kernel_form must be 0 or 1");
+    b->eng.kernel_form = cfg.kernel_form;
+    if (cfg.item_sites) {
+        if (cfg.item_sites < 64 || cfg.item_sites > 16384)
+            return fail(IE_ERR_INVALID, "item_sites must be in [64, 16384]");
+        b->eng.lvl_cap = cfg.item_sites;
+    }
+    if (cfg.tie_shift > 31) return fail(IE_ERR_INVALID, "tie_shift must be below 32");
+    b->eng.lvl_tie_shift = cfg.tie_shift;
     if (cfg.threads_per_block && (cfg.threads_per_block % 32 || cfg.threads_per_block > 256))
         return fail(IE_ERR_INVALID, "threads_per_block must be a multiple of 32, at most 256");
     IE_TRY(b->eng.build(problems, count, 1, seeds, cfg.force_f64 != 0));
@@ -2333,6 +2568,15 @@ ie_status ie_batch_class_report(ie_batch* b, uint32_t max_classes, uint32_t* n_c
         }
         if (ms) ms[k] = k < E.class_ms.size() ? E.class_ms[k] : 0.0;
     }
+    return IE_OK;
+}
+
+ie_status ie_batch_exact_decisions(ie_batch* b, uint64_t* count) {
+    if (!b || !count) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(b->eng.device));
+    int32_t c = 0;
+    if (b->eng.d_exact.p) IE_CUDA(cudaMemcpy(&c, b->eng.d_exact.p, sizeof(c), cudaMemcpyDeviceToHost));
+    *count = (uint64_t)(uint32_t)c;
     return IE_OK;
 }
 

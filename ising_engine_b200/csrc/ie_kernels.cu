@@ -27,6 +27,7 @@
 
 #include "ie_device.cuh"
 #include "ie_kernels.cuh"
+#include "ie_sweep.cuh"
 
 namespace ie {
 
@@ -181,41 +182,6 @@ __device__ __forceinline__ void energies_f64(const DevArrays& A, const InstDesc&
 
 __device__ __forceinline__ unsigned group_mask(int tid) { return 0xFFu << (8 * ((tid >> 3) & 3)); }
 
-// Number of exchange phases executed in global steps (base, base + steps].
-__device__ __forceinline__ uint32_t exchanges_in(uint64_t base, uint32_t steps, uint32_t k) {
-    return (uint32_t)((base + steps) / k - base / k);
-}
-
-// The steps one instance runs in a batched launch: the launch's own schedule,
-// or in a serving launch the instance's schedule from its next unexecuted
-// step, at most max(1, site_budget / n) steps. Step s of the launch is global
-// step base + s of the instance and runs at temperature temps[tstride * s].
-struct StepPlan {
-    uint64_t base;
-    uint32_t steps;
-    uint32_t tstride;
-    const double* temps;
-};
-
-__device__ __forceinline__ StepPlan step_plan(const DevArrays& A, const RunArgs& R, const InstDesc& d,
-                                              uint32_t inst) {
-    StepPlan P;
-    if (R.serve) {
-        P.base = A.done[d.owner];
-        const uint64_t left = d.sched_len > P.base ? d.sched_len - P.base : 0;
-        const uint64_t want = max(1u, R.site_budget / max(d.n, 1u));
-        P.steps = (uint32_t)min(left, want);
-        P.tstride = 1;
-        P.temps = R.temps + d.sched + P.base;
-    } else {
-        P.base = R.step_base_dev ? *R.step_base_dev : R.step_base;
-        P.steps = R.steps;
-        P.tstride = R.temps_per_step ? (R.cells ? R.ladder : 1u) : 0u;
-        P.temps = R.temps + (R.cells ? d.cell : 0u);
-    }
-    return P;
-}
-
 // ---------------------------------------------------------------------------
 // Batched single-cell kernel.
 //
@@ -255,32 +221,6 @@ __device__ __forceinline__ void ring_fetch(uint32_t* ring, const uint32_t* strea
         for (int i = 0; i < 32 / G; i++) cp_async16(dst + 4 * (t + G * i), src + 4 * (t + G * i));
     }
     cp_async_commit();
-}
-
-// f32 evaluation of fast_exp, every operation rounded separately (no fused
-// multiply-add), used only to pre-decide u < fast_exp(x) outside a relative
-// band of 2^-10 around the f64 value; the worst relative gap between this and
-// the f64 evaluation over [-20, 0] is below 6e-6.
-__device__ __forceinline__ float fast_exp_f32(float x) {
-    x = fminf(fmaxf(x, -20.0f), 0.0f);
-    const float r = __fmul_rn(x, 0.0625f);
-    const float r2 = __fmul_rn(r, r);
-    const float r3 = __fmul_rn(r2, r);
-    float p = __fadd_rn(1.0f, r);
-    p = __fadd_rn(p, __fmul_rn(0.5f, r2));
-    p = __fadd_rn(p, __fmul_rn(1.0f / 6.0f, r3));
-    p = __fadd_rn(p, __fmul_rn(__fmul_rn(1.0f / 24.0f, r2), r2));
-    p = __fadd_rn(p, __fmul_rn(__fmul_rn(1.0f / 120.0f, r2), r3));
-    p = __fadd_rn(p, __fmul_rn(__fmul_rn(1.0f / 720.0f, r3), r3));
-    const float p2 = __fmul_rn(p, p);
-    const float p4 = __fmul_rn(p2, p2);
-    const float p8 = __fmul_rn(p4, p4);
-    return __fmul_rn(p8, p8);
-}
-
-// Exact f64 decision, out of line: only reached inside the f32 band.
-__device__ __noinline__ bool metropolis_exact_f64(double x, uint64_t m) {
-    return __dmul_rn((double)m, 2.220446049250313e-16) < fast_exp_rn(x);
 }
 
 // The reference decision dE <= 0 || u < fast_exp(-dE * beta) (engine.rs:665-666),
@@ -621,7 +561,7 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
         // step and the warp fills the table. Own tables: each active group runs
         // its own steps and fills its own table.
         for (uint32_t s = 0; s < P.steps; s++) {
-            const double beta = __ddiv_rn(1.0, P.temps[P.tstride ? s : 0]);
+            const double beta = __ddiv_rn(1.0, P.temps[(size_t)P.tstride * s]);
             if constexpr (MODE == kModeInt) {
                 if (own_tab) {
                     __syncwarp(gmask);
@@ -734,7 +674,7 @@ __global__ void __launch_bounds__(64, 1) chain_kernel(DevArrays A, RunArgs R, ui
         }
         __syncthreads();
         for (uint32_t s = 0; s < P.steps; s++) {
-            const double beta = __ddiv_rn(1.0, P.temps[P.tstride ? s : 0]);
+            const double beta = __ddiv_rn(1.0, P.temps[(size_t)P.tstride * s]);
             const uint64_t base = chacha8_draw(key, pos0 + s) + d.cell;
             if (producer) {
                 produce_windows(base, d.n, rngb, t, 64);
@@ -1014,7 +954,7 @@ __global__ void __launch_bounds__(WsCfg<MODE>::THREADS, 1) window_kernel(DevArra
         const uint32_t* stream = A.recs + d.wrec;
         for (uint32_t s = 0; s < P.steps; s++) {
             __syncthreads();
-            const double beta = __ddiv_rn(1.0, P.temps[P.tstride ? s : 0]);
+            const double beta = __ddiv_rn(1.0, P.temps[(size_t)P.tstride * s]);
             if constexpr (MODE == kModeInt) {
                 for (int i = tid; i < 2 * H + 1; i += NT) tab[i] = metropolis_threshold(i - H, beta);
                 __syncthreads();

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "ie_kernels.cuh"
+#include "ie_level.cuh"
 
 namespace ie {
 cudaError_t set_smem_limits(size_t pt_bytes);
@@ -38,6 +39,10 @@ cudaError_t launch_best_extract(const DevArrays& A, uint32_t inst, const double*
                                 double* best, int32_t* found, cudaStream_t st);
 cudaError_t launch_one_opt(const DevArrays& A, uint32_t inst, int8_t* state, const uint8_t* clamped, double* gains,
                            double* improvement, uint64_t* flips, uint64_t max_flips, cudaStream_t st);
+size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap);
+int level_occupancy(uint32_t mode, bool gsp, int threads, size_t smem);
+cudaError_t launch_level(const DevArrays& A, const RunArgs& R, const LvlArgs& L, uint32_t mode, bool gsp, int threads,
+                         int grid, cudaStream_t st);
 void set_last_error(const char* msg);
 cudaError_t probe_peaks(int sm_count, double* int_ops_per_s, double* xoshiro_per_s);
 }  // namespace ie

@@ -1,0 +1,506 @@
+// Level kernel: the sweep of a group of instances ("item") by a whole CTA,
+// generator phase then decision phase (data model in ie_level.cuh).
+//
+// Why: the reference's sweep is a chain over sites, and each of a cell's 8
+// Xoshiro lanes is a chain over its 8n calls per sweep. Run as such, a few
+// threads per instance do dependent work and the SMs idle. Here both chains
+// are cut: the lane streams by GF(2) jumps into segments that threads
+// generate side by side, the site chain by dependency levels whose sites the
+// CTA decides side by side. The values are the reference's, bit for bit: the
+// same Xoshiro outputs at the same stream positions, the same neighbour
+// values at every decision.
+//
+// Generator phase: thread (segment, lane) seeds its lane (engine.rs:87-103),
+// jumps to the segment's first call and stores the top 32 bits of each output
+// at keys[site][lane][call] (lane l's call k at site v is replica l + 8k,
+// engine.rs:145-151, 617-621). Decision phase: level by level, thread (site,
+// lane) computes dE of its 8 replicas and decides with those 32 bits; the
+// decision is certain unless the 32 bits equal the threshold's (probability
+// 2^-32 per attempt), in which case the full output is recomputed from the
+// lane's seed (lane_output) and decided exactly.
+//
+// Integer mode: dE by SWAR byte sums (as the batched kernel) and a table of
+// the top 32 bits of the thresholds m < ceil(fast_exp(-dE beta) 2^52), m the
+// output's 52-bit mantissa (engine.rs:665-666). f64 mode: dE in the
+// reference's f64 order (engine.rs:218-271), then u < fast_exp(x) decided by
+// an ex2 estimate, the f32 form, or exactly in f64.
+//
+// Energies are not tracked through the sweep: at the end of a launch (or of a
+// request's schedule) they are computed from the spins, integer exactly and
+// f64 in the reference's summation order (engine.rs:333-368), which is the
+// value the reference's periodic re-sync (ultimate.rs:316-324) takes.
+#include <cuda_runtime.h>
+
+#include "ie_device.cuh"
+#include "ie_kernels.cuh"
+#include "ie_level.cuh"
+#include "ie_sweep.cuh"
+
+namespace ie {
+
+struct LvlMem {
+    const double* temps;
+    uint64_t site, spin, energy, pos0, step0, base;
+    double beta;
+    uint32_t key[8];
+    uint32_t inst, flat, n, steps, tstride, cell, owner, fin;
+};
+
+// Top 32 bits of the integer threshold: accept iff m < T with T =
+// ceil(fast_exp(-de beta) 2^52) (metropolis_threshold returns (T << 12) - 1);
+// every m whose top 32 bits are below Q = T >> 20 accepts, above it rejects.
+// 0xffffffff: every m accepts (dE <= 0, or T = 2^52).
+__device__ __forceinline__ uint32_t q_threshold(int de, double beta) {
+    if (de <= 0) return 0xFFFFFFFFu;
+    const uint64_t U = metropolis_threshold(de, beta);
+    if (U == ~0ULL) return 0xFFFFFFFFu;
+    return (uint32_t)(((U + 1) >> 12) >> 20);
+}
+
+// Output `8 (v - segment start) + k` of the segment of lane `lane` that holds
+// site v, recomputed from the lane's seed and the segment's jump.
+__device__ __noinline__ uint64_t lane_output(uint64_t base, int lane, uint32_t v, int k, const uint64_t* jpoly) {
+    Xoshiro x;
+    x.seed_lane(base, lane);
+    const uint32_t seg = v / kLvlSeg;
+    if (seg) x.jump(jpoly + 4ull * seg);
+    const uint32_t skip = 8u * (v - seg * kLvlSeg) + (uint32_t)k;
+    for (uint32_t i = 0; i < skip; i++) x.advance();
+    return x.next();
+}
+
+__device__ __forceinline__ float ex2_approx(float a) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+
+// f64 decision for dE > 0 knowing the top bits of the output: 1 accept,
+// -1 reject, 0 undecided (the bits equal the threshold's). The uniform u =
+// m 2^-52 lies in [lo 2^-32, (lo + 2^sh) 2^-32), lo = mh with its low sh bits
+// cleared. fast_exp(x) >= exp(x) (the alternating Taylor tail is negative) and
+// <= 1.054 exp(x) on [-20, 0]; ex2.approx is within 3e-6 of exp here.
+__device__ __forceinline__ int f64_decide(double de, double beta, uint32_t mh, uint32_t sh) {
+    const double x = __dmul_rn(-de, beta);
+    const uint32_t lo = (mh >> sh) << sh;
+    const float s32 = 2.3283064365386963e-10f;  // 2^-32
+    const float ulo = __fmul_rn(__uint2float_rd(lo), s32);
+    const float uhi = __fmul_rn(__fadd_ru(__uint2float_ru(lo), (float)(1u << sh)), s32);
+    const float xf = __double2float_rn(fmax(x, -20.0));
+    const float ex = ex2_approx(__fmul_rn(xf, 1.4426950408889634f));
+    if (uhi <= __fmul_rn(ex, 0.99998f)) return 1;
+    if (ulo >= __fmul_rn(ex, 1.0625f)) return -1;
+    const float f = fast_exp_f32(__double2float_rn(x));
+    if (uhi < __fmul_rn(f, 0.9990234375f)) return 1;
+    if (ulo > __fmul_rn(f, 1.0009765625f)) return -1;
+    const uint64_t T = (uint64_t)ceil(__dmul_rn(fast_exp_rn(x), 4503599627370496.0));
+    const uint64_t mlo = (uint64_t)lo << 20, mhi = ((uint64_t)lo + (1ull << sh)) << 20;
+    if (mhi <= T) return 1;
+    if (mlo >= T) return -1;
+    return 0;
+}
+
+// Exact decisions of the undecided calls (bit k of `ties`): the outputs are
+// recomputed and decided as the reference does.
+__device__ __noinline__ uint32_t exact_flips_int(uint32_t ties, uint64_t base, int lane, uint32_t v, uint32_t iL,
+                                                 uint32_t iH, int H, double beta, const uint64_t* jpoly) {
+    uint32_t f = 0;
+    for (int k = 0; k < 8; k++) {
+        if (!((ties >> k) & 1u)) continue;
+        const int idx = (int)(((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu);
+        const uint64_t res = lane_output(base, lane, v, k, jpoly);
+        if (res <= metropolis_threshold(idx - H, beta)) f |= 1u << k;
+    }
+    return f;
+}
+
+__device__ __noinline__ uint32_t exact_flips_f64(uint32_t ties, uint64_t base, int lane, uint32_t v,
+                                                 const double* dl, double beta, const uint64_t* jpoly) {
+    uint32_t f = 0;
+    for (int k = 0; k < 8; k++) {
+        if (!((ties >> k) & 1u)) continue;
+        const uint64_t res = lane_output(base, lane, v, k, jpoly);
+        if (metropolis_exact_f64(__dmul_rn(-dl[k], beta), res >> 12)) f |= 1u << k;
+    }
+    return f;
+}
+
+// Integer energies of one member (hubo.rs:176-189 restricted to QUBO, each
+// edge once from its lower end): thread (site, lane) adds x_v (lin_v +
+// sum_{j > v} w x_j) for its 8 replicas, by SWAR byte sums as in the sweep.
+__device__ __forceinline__ void member_energy_int(const LvlArgs& L, const LvlMem& m, const uint8_t* spb,
+                                                  const uint2* lut, int tid, int T, int32_t* sE) {
+    int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t i = tid; i < 8u * m.n; i += T) {
+        const uint32_t v = i >> 3;
+        const uint32_t f = m.flat + v;
+        const uint32_t xb = spb[8u * f];
+        if (!xb) continue;
+        const uint32_t* rec = L.lrecs + 4ull * __ldg(L.recoff + m.site + v);
+        const uint4 hd = __ldg(reinterpret_cast<const uint4*>(rec));
+        const uint32_t deg = hd.x & 0x7FFFFFFFu;
+        const int lin = (int)hd.z;
+        uint32_t aL = 0, aH = 0;
+        int nsum = 0;
+        const uint4* e4p = reinterpret_cast<const uint4*>(rec + 4);
+        for (uint32_t q = 0; q < deg; q += 4) {
+            const uint4 e4 = __ldg(e4p + (q >> 2));
+            const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const uint32_t col = en[e] & 0xFFFFFFu;
+                const uint32_t w = (en[e] >> 24) & 0x7Fu;
+                if (col > v && w) {
+                    const uint2 sv = lut[spb[8u * (m.flat + col)] | ((en[e] >> 23) & 0x100u)];
+                    aL += w * sv.x;
+                    aH += w * sv.y;
+                    if (en[e] >> 31) nsum += (int)w;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if ((xb >> k) & 1u) acc[k] += lin + (int)(((k < 4 ? aL : aH) >> (8 * (k & 3))) & 0xFFu) - nsum;
+    }
+    const int lane = tid & 7;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        if (acc[k]) atomicAdd(sE + lane + 8 * k, acc[k]);
+}
+
+// f64 energies of one (member, lane): calculate_replica_energies_local
+// (engine.rs:333-368) in its order: site order, lin then the CSR entries with
+// v < j, each added with one rounding.
+__device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uint8_t* spb, double* out) {
+    const InstDesc d = A.desc[m.inst];
+    const uint32_t* rows = A.rows + d.row;
+    const uint32_t* cols = A.cols + d.ent;
+    const double* vals = A.vals + d.ent;
+    const double* lin = A.lin + d.site;
+    double E[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) E[k] = 0.0;
+    for (uint32_t v = 0; v < d.n; v++) {
+        const uint32_t xb = spb[8u * (m.flat + v)];
+        if (!xb) continue;
+        const double wl = lin[v];
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if ((xb >> k) & 1u) E[k] = __dadd_rn(E[k], wl);
+        for (uint32_t e = rows[v]; e < rows[v + 1]; e++) {
+            const uint32_t j = cols[e];
+            if (v < j) {
+                const uint32_t mk = xb & spb[8u * (m.flat + j)];
+                if (mk) {
+                    const double w = vals[e];
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        if ((mk >> k) & 1u) E[k] = __dadd_rn(E[k], w);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) out[8 * k] = E[k];
+}
+
+template <uint32_t MODE, bool GSP>
+__global__ void __launch_bounds__(512) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
+    extern __shared__ __align__(16) uint64_t dsm[];
+    __shared__ LvlMem ms[kLvlMaxMembers];
+    __shared__ uint32_t s_item, s_steps;
+    __shared__ int32_t sE[kReplicas];
+    const int tid = threadIdx.x;
+    const int T = blockDim.x;  // a multiple of 8: thread tid always serves lane tid % 8
+    const int lane = tid & 7;
+    const bool own_tab = R.serve != 0 || R.cells != 0;
+    uint32_t* const tabs = reinterpret_cast<uint32_t*>(dsm);
+    uint2* const lut = reinterpret_cast<uint2*>(tabs + (size_t)L.ntab * kLvlTab);
+    uint64_t* const ssw = reinterpret_cast<uint64_t*>(lut + (MODE == kModeInt ? 512 : 0));
+    uint32_t* const kb = L.keybuf + (size_t)blockIdx.x * L.keystride;
+    if constexpr (MODE == kModeInt) {
+        // spread table: entry b (256 + b for a negative coupling, which
+        // contributes |w| (1 - x_j)) holds bit k of b (~b) in byte k
+        for (int i = tid; i < 512; i += T) {
+            const uint32_t b = (i < 256 ? (uint32_t)i : (uint32_t)(i - 256) ^ 0xFFu);
+            lut[i] = make_uint2(spread4(b), spread4(b >> 4));
+        }
+    }
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t q = atomicAdd(L.queue, 1u);
+            s_item = q < L.nitems ? L.order[q] : 0xffffffffu;
+        }
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it == 0xffffffffu) break;
+        const LvlItem I = L.items[it];
+        if ((!GSP && I.sites > L.spin_cap) || I.nmem > kLvlMaxMembers || I.nmem == 0 ||
+            (own_tab && I.nmem > L.ntab) || (uint64_t)I.sites * 64 > L.keystride || (GSP && I.nmem != 1)) {
+            if (tid == 0) atomicExch(A.err, 2);  // host sizing error: report, skip the item
+            continue;
+        }
+        if (tid == 0) s_steps = 0;
+        __syncthreads();
+        for (uint32_t k = tid; k < I.nmem; k += T) {
+            const LvlMember mb = L.members[I.mem0 + k];
+            const InstDesc d = A.desc[mb.inst];
+            const StepPlan P = step_plan(A, R, d, mb.inst);
+            LvlMem& m = ms[k];
+            m.temps = P.temps;
+            m.tstride = P.tstride;
+            m.steps = P.steps;
+            m.step0 = P.base;
+            m.site = d.site;
+            m.spin = d.spin;
+            m.energy = d.energy;
+            m.n = d.n;
+            m.flat = mb.flat;
+            m.inst = mb.inst;
+            m.cell = d.cell;
+            m.owner = d.owner;
+            m.pos0 = A.pos[d.owner];
+            // energies at the end: every batched / PT launch, a request when
+            // its schedule is done
+            m.fin = !R.serve || P.base + P.steps >= d.sched_len;
+#pragma unroll
+            for (int i = 0; i < 8; i++) m.key[i] = A.keys[8 * (size_t)d.owner + i];
+            atomicMax(&s_steps, P.steps);
+        }
+        __syncthreads();
+        const uint32_t nsteps = s_steps;
+        uint64_t* const sw = GSP ? A.spins + ms[0].spin : ssw;
+        uint8_t* const spb = reinterpret_cast<uint8_t*>(sw) + lane;
+        if (!GSP) {
+            for (uint32_t k = 0; k < I.nmem; k++) {
+                const uint64_t* gw = A.spins + ms[k].spin;
+                for (uint32_t i = tid; i < ms[k].n; i += T) ssw[ms[k].flat + i] = gw[i];
+            }
+        }
+        for (uint32_t s = 0; s < nsteps; s++) {
+            __syncthreads();
+            for (uint32_t k = tid; k < I.nmem; k += T) {
+                LvlMem& m = ms[k];
+                if (s < m.steps) {
+                    m.base = chacha8_draw(m.key, m.pos0 + s) + m.cell;
+                    m.beta = __ddiv_rn(1.0, m.temps[(size_t)m.tstride * s]);
+                }
+            }
+            __syncthreads();
+            if constexpr (MODE == kModeInt) {
+                const int H = I.H, W = 2 * H + 1;
+                const uint32_t nt = own_tab ? I.nmem : 1u;
+                for (uint32_t i = tid; i < nt * (uint32_t)W; i += T) {
+                    const uint32_t k = i / (uint32_t)W, idx = i % (uint32_t)W;
+                    if (s < ms[k].steps) tabs[k * kLvlTab + idx] = q_threshold((int)idx - H, ms[k].beta);
+                }
+            }
+            // generator phase: chain c = (segment c / 8, lane c % 8)
+            for (uint32_t c = tid; c < 8u * I.nseg; c += T) {
+                const uint32_t sd = __ldg(L.segs + I.seg0 + (c >> 3));
+                const uint32_t slot = sd >> 24, seg = sd & 0xFFFFFFu;
+                const LvlMem& m = ms[slot];
+                if (s >= m.steps) continue;
+                Xoshiro x;
+                x.seed_lane(m.base, lane);
+                if (seg) x.jump(L.jpoly + 4ull * seg);
+                const uint32_t v0 = seg * kLvlSeg, v1 = min(m.n, v0 + kLvlSeg);
+                uint4* out = reinterpret_cast<uint4*>(kb + (size_t)(m.flat + v0) * 64 + lane * 8);
+                for (uint32_t v = v0; v < v1; v++) {
+                    uint32_t h[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) h[k] = x.next_hi();
+                    out[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                    out[1] = make_uint4(h[4], h[5], h[6], h[7]);
+                    out += 16;
+                }
+            }
+            __syncthreads();
+            // decision phase, level by level
+            const uint32_t sh = L.tie_shift;
+            for (uint32_t l = 0; l < I.nlvl; l++) {
+                const uint32_t e0 = __ldg(L.lvloff + I.lvl0 + l), e1 = __ldg(L.lvloff + I.lvl0 + l + 1);
+                for (uint32_t i = tid; i < 8u * (e1 - e0); i += T) {
+                    const uint32_t ent = __ldg(L.entries + I.ent0 + e0 + (i >> 3));
+                    const uint32_t slot = ent >> kLvlFlatBits, f = ent & ((1u << kLvlFlatBits) - 1u);
+                    const LvlMem& m = ms[slot];
+                    if (s >= m.steps) continue;
+                    const uint32_t v = f - m.flat;
+                    const uint32_t* rec = L.lrecs + 4ull * __ldg(L.recoff + m.site + v);
+                    const uint4 hd = __ldg(reinterpret_cast<const uint4*>(rec));
+                    const uint32_t deg = hd.x & 0x7FFFFFFFu;
+                    const uint32_t fb = m.flat;
+                    const uint32_t xb = spb[8u * f];
+                    const uint4* kp = reinterpret_cast<const uint4*>(kb + (size_t)f * 64 + lane * 8);
+                    const uint4 k0 = kp[0], k1 = kp[1];
+                    const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+                    uint32_t flips = 0, ties = 0;
+                    if constexpr (MODE == kModeInt) {
+                        const int lp = (int)hd.y;
+                        uint32_t aL = 0, aH = 0;
+                        const uint4* e4p = reinterpret_cast<const uint4*>(rec + 4);
+                        for (uint32_t q = 0; q < deg; q += 4) {
+                            const uint4 e4 = __ldg(e4p + (q >> 2));
+                            const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
+                            uint32_t li[4];
+#pragma unroll
+                            for (int e = 0; e < 4; e++)
+                                li[e] = spb[8u * (fb + (en[e] & 0xFFFFFFu))] | ((en[e] >> 23) & 0x100u);
+#pragma unroll
+                            for (int e = 0; e < 4; e++) {
+                                const uint2 sv = lut[li[e]];
+                                const uint32_t w = (en[e] >> 24) & 0x7Fu;
+                                aL += w * sv.x;
+                                aH += w * sv.y;
+                            }
+                        }
+                        const int H = I.H;
+                        const uint32_t cA = (uint32_t)(H + lp) * 0x01010101u;
+                        const uint32_t cB = (uint32_t)(H - lp) * 0x01010101u;
+                        const uint32_t xL = spread4(xb) * 0xFFu;
+                        const uint32_t xH = spread4(xb >> 4) * 0xFFu;
+                        // byte k of iL / iH = dE_k + H for replica lane + 8k
+                        const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
+                        const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
+                        const uint32_t* tb = tabs + (own_tab ? slot * kLvlTab : 0u);
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
+                            const uint32_t a = mh[k] >> sh, b = tb[idx] >> sh;
+                            flips |= (uint32_t)(a < b) << k;
+                            ties |= (uint32_t)(a == b) << k;
+                        }
+                        if (ties) {
+                            flips |= exact_flips_int(ties, m.base, lane, v, iL, iH, H, m.beta, L.jpoly);
+                            if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
+                        }
+                    } else {
+                        const double wl = __hiloint2double((int)hd.w, (int)hd.z);
+                        const uint32_t deg4 = (deg + 3u) & ~3u;
+                        const uint4* c4p = reinterpret_cast<const uint4*>(rec + 4);
+                        const double2* w2p = reinterpret_cast<const double2*>(rec + 4 + deg4);
+                        double dl[8], tp[8];
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            const bool xv = (xb >> k) & 1u;
+                            tp[k] = xv ? -1.0 : 1.0;
+                            dl[k] = xv ? -wl : wl;
+                        }
+                        for (uint32_t q = 0; q < deg; q += 4) {
+                            const uint4 c4 = __ldg(c4p + (q >> 2));
+                            const double2 w01 = __ldg(w2p + (q >> 1));
+                            const double2 w23 = __ldg(w2p + (q >> 1) + 1);
+                            const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+                            const double ww[4] = {w01.x, w01.y, w23.x, w23.y};
+                            uint32_t bj[4];
+#pragma unroll
+                            for (int e = 0; e < 4; e++) bj[e] = spb[8u * (fb + cc[e])];
+#pragma unroll
+                            for (int e = 0; e < 4; e++) {
+                                if (q + e < deg) {
+#pragma unroll
+                                    for (int k = 0; k < 8; k++) {
+                                        // t = (x_j ^ x_v) - x_v; w * t is exact, so
+                                        // fma(w, t, dE) is the reference's dE + w * t
+                                        const double tt = ((bj[e] >> k) & 1u) ? tp[k] : 0.0;
+                                        dl[k] = __fma_rn(ww[e], tt, dl[k]);
+                                    }
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            if (dl[k] <= 0.0) {
+                                flips |= 1u << k;
+                                continue;
+                            }
+                            const int r = f64_decide(dl[k], m.beta, mh[k], sh);
+                            flips |= (uint32_t)(r > 0) << k;
+                            ties |= (uint32_t)(r == 0) << k;
+                        }
+                        if (ties) {
+                            flips |= exact_flips_f64(ties, m.base, lane, v, dl, m.beta, L.jpoly);
+                            if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
+                        }
+                    }
+                    spb[8u * f] = (uint8_t)(xb ^ flips);
+                }
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+        // energies, spins and stream state of every member
+        for (uint32_t k = 0; k < I.nmem; k++) {
+            const LvlMem& m = ms[k];
+            if (!m.fin || m.steps == 0) continue;
+            if constexpr (MODE == kModeInt) {
+                if (tid < kReplicas) sE[tid] = 0;
+                __syncthreads();
+                member_energy_int(L, m, spb, lut, tid, T, sE);
+                __syncthreads();
+                if (tid < kReplicas) A.Ei[m.energy + tid] = sE[tid];
+            }
+        }
+        if constexpr (MODE == kModeF64) {
+            for (uint32_t p = tid; p < 8u * I.nmem; p += T) {
+                const LvlMem& m = ms[p >> 3];
+                if (!m.fin || m.steps == 0) continue;
+                member_energy_f64(A, m, reinterpret_cast<const uint8_t*>(sw) + (p & 7), A.Ef + m.energy + (p & 7));
+            }
+        }
+        if (!GSP) {
+            for (uint32_t k = 0; k < I.nmem; k++) {
+                uint64_t* gw = A.spins + ms[k].spin;
+                for (uint32_t i = tid; i < ms[k].n; i += T) gw[i] = ssw[ms[k].flat + i];
+            }
+        }
+        if (!R.cells) {
+            for (uint32_t k = tid; k < I.nmem; k += T) {
+                const LvlMem& m = ms[k];
+                A.pos[m.owner] = m.pos0 + m.steps;
+                A.deo[m.owner] ^= (int32_t)(exchanges_in(m.step0, m.steps, R.exchange_interval) & 1u);
+                if (R.serve) A.done[m.owner] = m.step0 + m.steps;
+            }
+        }
+    }
+}
+
+template __global__ void level_kernel<kModeInt, false>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeInt, true>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeF64, false>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeF64, true>(DevArrays, RunArgs, LvlArgs);
+
+size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap) {
+    return (size_t)ntab * kLvlTab * 4 + (mode == kModeInt ? 512 * 8 : 0) + (size_t)spin_cap * 8;
+}
+
+template <uint32_t MODE, bool GSP>
+static int level_occ_of(int threads, size_t smem) {
+    auto k = level_kernel<MODE, GSP>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) return 0;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess) return 0;
+    return occ;
+}
+
+int level_occupancy(uint32_t mode, bool gsp, int threads, size_t smem) {
+    if (mode == kModeInt)
+        return gsp ? level_occ_of<kModeInt, true>(threads, smem) : level_occ_of<kModeInt, false>(threads, smem);
+    return gsp ? level_occ_of<kModeF64, true>(threads, smem) : level_occ_of<kModeF64, false>(threads, smem);
+}
+
+cudaError_t launch_level(const DevArrays& A, const RunArgs& R, const LvlArgs& L, uint32_t mode, bool gsp, int threads,
+                         int grid, cudaStream_t st) {
+    const size_t smem = level_smem(mode, L.ntab, gsp ? 0 : L.spin_cap);
+    if (mode == kModeInt) {
+        if (gsp) level_kernel<kModeInt, true><<<grid, threads, smem, st>>>(A, R, L);
+        else level_kernel<kModeInt, false><<<grid, threads, smem, st>>>(A, R, L);
+    } else {
+        if (gsp) level_kernel<kModeF64, true><<<grid, threads, smem, st>>>(A, R, L);
+        else level_kernel<kModeF64, false><<<grid, threads, smem, st>>>(A, R, L);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace ie

@@ -42,7 +42,8 @@ class Engine:
     def __init__(self, model: QuboModel, num_temps: int = 10, seed: int = 0,
                  exchange_interval: int = 1, temp_max: float = 1.0, temp_min: float = 0.1,
                  sweeps_per_exchange: int = 1, total_exchanges: int = 1, force_f64: bool = False,
-                 device: int = 0, pt_path: int = 0, num_pops: int = 1, use_icm: bool = False):
+                 device: int = 0, pt_path: int = 0, num_pops: int = 1, use_icm: bool = False,
+                 kernel_form: int = 0):
         self._L = _ffi.lib()
         self.model = model
         self.num_temps = int(num_temps)
@@ -53,7 +54,7 @@ class Engine:
         prob = _problem(model, keep)
         cfg = _ffi.ie_config(temp_max, temp_min, sweeps_per_exchange, total_exchanges,
                              seed & 0xFFFFFFFFFFFFFFFF, self.num_temps, self.num_pops, 1, exchange_interval,
-                             int(force_f64), device, pt_path, int(use_icm))
+                             int(force_f64), device, pt_path, int(use_icm), int(kernel_form))
         h = C.c_void_p()
         _ffi.check(self._L.ie_create(C.byref(prob), C.byref(cfg), C.byref(h)))
         self._h = h
@@ -190,8 +191,9 @@ class BatchEngine:
 
     def __init__(self, models, seeds, device: int = 0, force_f64: bool = False,
                  threads_per_block: int = 0, blocks_per_sm: int = 0, windows: bool = True,
-                 graph: bool = False):
+                 graph: bool = False, kernel_form: int = 0, item_sites: int = 0, tie_shift: int = 0):
         self._L = _ffi.lib()
+        self.kernel_form = int(kernel_form)
         self.models = list(models)
         self.count = len(self.models)
         keep: list = []
@@ -200,7 +202,8 @@ class BatchEngine:
         if self.seeds.shape != (self.count,):
             raise ValueError("one seed per problem")
         cfg = _ffi.ie_batch_config(device, int(force_f64), threads_per_block, blocks_per_sm,
-                                   0 if windows else 1, 1 if graph else 0)
+                                   0 if windows else 1, 1 if graph else 0, int(kernel_form),
+                                   int(item_sites), int(tie_shift))
         h = C.c_void_p()
         _ffi.check(self._L.ie_batch_create(probs, self.count, _p(self.seeds), C.byref(cfg),
                                            C.byref(h)))
@@ -287,6 +290,12 @@ class BatchEngine:
     def last_launches(self) -> int:
         n = np.zeros(1, dtype=np.uint64)
         _ffi.check(self._L.ie_batch_last_launches(self._h, _p(n)))
+        return int(n[0])
+
+    def exact_decisions(self) -> int:
+        """Level-kernel decisions taken on the exact path so far."""
+        n = np.zeros(1, dtype=np.uint64)
+        _ffi.check(self._L.ie_batch_exact_decisions(self._h, _p(n)))
         return int(n[0])
 
 

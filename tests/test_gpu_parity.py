@@ -39,6 +39,24 @@ def assert_same_run(eng: Engine, ref, check_stats=True):
         assert (acc == ref.swap_accepts).all()
 
 
+def assert_batch_energies(b: BatchEngine, models, ref_e, words=None):
+    """Energies of a batched run. The level kernel (the default form) reports
+    the FP64 recompute of the final state in the reference's order
+    (engine.rs:333-368): bit-identical to the oracle's recompute of the same
+    words, and within FP64_REL_TOL of the oracle's tracked sum (equal for
+    integer couplings). The per-lane forms report the tracked sum itself."""
+    e = b.energies()
+    ref_e = np.asarray(ref_e).reshape(e.shape)
+    if b.kernel_form == 1:
+        assert e.tobytes() == ref_e.tobytes(), np.argwhere(e != ref_e)[:8]
+        return
+    w = b.spins() if words is None else words
+    rec = np.stack([O.replica_energies(m, w[b.offsets[i]:b.offsets[i + 1]])[0] for i, m in enumerate(models)])
+    assert e.tobytes() == rec.tobytes(), np.argwhere(e != rec)[:8]
+    rel = np.abs(e - ref_e) / np.maximum(np.abs(ref_e), 1.0)
+    assert rel.max() <= FP64_REL_TOL
+
+
 def test_lattice_2d_single_cell_1000_sweeps():
     """2D periodic +-J, L=32, one cell at beta=1, random init, 1000 sweeps."""
     m = I.pm_j_lattice(32, 2, seed=2024)
@@ -51,7 +69,7 @@ def test_lattice_2d_single_cell_1000_sweeps():
     b.init_random()
     b.run_schedule(np.ones(1000))
     assert (b.spins() == ref.words.reshape(-1)).all()
-    assert b.energies().tobytes() == ref.energies.tobytes()
+    assert_batch_energies(b, [m], ref.energies)
     assert int(b.draws()[0]) == ref.draws
     b.close()
 
@@ -179,7 +197,7 @@ def test_windowed_global_spins_random_graphs():
     b.run_schedule(temps[:5])
     b.run_schedule(temps[5:])
     assert (b.spins() == words_ref).all()
-    assert b.energies().tobytes() == ref_e.tobytes()
+    assert_batch_energies(b, models, ref_e)
     b.close()
 
 
@@ -228,7 +246,7 @@ def test_uneven_batch_bit_exact_and_plain_equal():
     w = b.spins()
     e = b.energies()
     assert (w == words_ref).all()
-    assert e.tobytes() == ref_e.tobytes()
+    assert_batch_energies(b, models, ref_e)
     assert (b.draws() == np.array([m.num_vars + 60 for m in models], np.uint64)).all()
     rec = b.recompute_energies()
     rel = np.abs(rec - e) / np.maximum(np.abs(rec), 1.0)
@@ -255,7 +273,8 @@ def test_f64_resync_across_1000_steps():
     b = BatchEngine([m], [31])
     b.init_random()
     b.run_schedule(temps)
-    assert b.energies().tobytes() == ref.energies.tobytes()
+    assert (b.spins() == ref.words.reshape(-1)).all()
+    assert_batch_energies(b, [m], ref.energies)
     b.close()
 
 
@@ -315,7 +334,7 @@ def test_batch_long_rows_and_thread_classes():
     b.run_schedule(temps[:11])
     b.run_schedule(temps[11:])
     assert (b.spins() == words_ref).all()
-    assert b.energies().tobytes() == ref_e.tobytes()
+    assert_batch_energies(b, models, ref_e)
     b.close()
 
 
@@ -331,7 +350,7 @@ def test_autotune_restores_state():
     assert len(chosen) == 4
     b.run_schedule(temps)
     assert (b.spins() == words_ref).all()
-    assert b.energies().tobytes() == ref_e.tobytes()
+    assert_batch_energies(b, models, ref_e)
     assert (b.draws() == np.array([m.num_vars + 24 for m in models], np.uint64)).all()
     b.close()
 
@@ -354,7 +373,7 @@ def test_windowed_kernel_large_instances():
     b.run_schedule(temps[:13])
     b.run_schedule(temps[13:])
     assert (b.spins() == words_ref).all()
-    assert b.energies().tobytes() == ref_e.tobytes()
+    assert_batch_energies(b, models, ref_e)
     b.close()
 
 
@@ -383,7 +402,7 @@ def test_windowed_kernel_degree_17_to_32():
     b.init_random()
     b.run_schedule(temps)
     assert (b.spins() == words_ref).all()
-    assert b.energies().tobytes() == ref_e.tobytes()
+    assert_batch_energies(b, models, ref_e)
     b.close()
 
 
@@ -404,7 +423,7 @@ def test_batched_runs_replayed_from_cuda_graph():
     b.run_schedule(temps[600:1200])
     b.run_schedule(temps[1200:])
     assert (b.spins() == words_ref).all()
-    assert b.energies().tobytes() == ref_e.tobytes()
+    assert_batch_energies(b, models, ref_e)
     assert len(b.class_report()) >= 2 and all(c[4] > 0 for c in b.class_report())
     b.close()
 
@@ -418,5 +437,5 @@ def test_windowed_kernel_f64_resync():
     b.init_random()
     b.run_schedule(temps)
     assert (b.spins() == words_ref).all()
-    assert b.energies().tobytes() == ref_e.tobytes()
+    assert_batch_energies(b, [m], ref_e)
     b.close()
