@@ -848,7 +848,7 @@ struct Engine {
     // per-CTA output buffer are fixed here.
     template <typename Live>
     ie_status build_level_classes(const std::vector<InstDesc>& D, const std::vector<HostInst>& HI, bool cells_view,
-                                  Live live) {
+                                  Live live, bool one_per_item = false) {
         lvh.clear();
         std::vector<uint64_t> nnz_of(D.size());
         for (size_t i = 0; i < D.size(); i++) nnz_of[i] = HI[i].nnz;
@@ -872,14 +872,14 @@ struct Engine {
                 uint32_t cap = lvl_cap, maxn = 0;
                 for (uint32_t i : mem[m][g]) maxn = std::max(maxn, D[i].n);
                 if (cells_view && maxn >= 512) cap = std::min(cap, maxn);
-                const uint32_t maxmem = own ? kLvlMaxOwnTables : kLvlMaxMembers;
+                const uint32_t maxmem = one_per_item ? 1u : own ? kLvlMaxOwnTables : kLvlMaxMembers;
                 std::vector<uint32_t> order;
                 double longest = 0;
                 build_level_items(D, nnz_of, lv_sites, lv_off, mem[m][g], g != 0, cap, maxmem, lvh, order, longest);
                 wc->nitems = (uint32_t)order.size();
                 wc->work = longest;
                 for (uint32_t i : mem[m][g]) wc->site_steps += (double)D[i].n;
-                wc->ntab = own ? maxmem : 1u;
+                wc->ntab = own ? std::max<uint32_t>(maxmem, 1u) : 1u;
                 const size_t smem = level_smem(wc->mode, wc->ntab, g ? 0 : lvl_cap);
                 int occ = level_occupancy(wc->mode, g != 0, lvl_threads, smem);
                 if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "level kernel does not fit on an SM");
@@ -1388,7 +1388,7 @@ struct Engine {
             graph_valid = false;
             classes.clear();
             IE_TRY(build_level_classes(desc, insts, false,
-                                       [&](uint32_t j) { return j >= first && j < first + n_inst; }));
+                                       [&](uint32_t j) { return j >= first && j < first + n_inst; }, true));
             DevBuf<uint32_t> counters;
             IE_TRY(counters.upload(std::vector<uint32_t>(n_inst, 0), stream));
             IE_CUDA(cudaEventRecord(ev0, stream));
