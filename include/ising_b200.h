@@ -215,10 +215,13 @@ ie_status ie_batch_run_schedule(ie_batch* b, const double* temps, uint64_t n_ste
 /* Same schedule, one launch per instance in sequence (the plain method). */
 ie_status ie_batch_run_schedule_plain(ie_batch* b, const double* temps, uint64_t n_steps,
                                       uint32_t first, uint32_t count);
-/* Autotuner: times trial_steps of the schedule temps[] for a grid of
- * thread-class thresholds (instances above a size threshold get 2 or 4 threads
- * per generator lane), restoring the device state after every trial, and keeps
- * the fastest. chosen[4] (may be NULL) receives {n4_int, n2_int, n4_f64, n2_f64}. */
+/* Autotuner: times trial_steps of the schedule temps[] for a grid of launch
+ * shapes, restoring the device state after every trial, and keeps the fastest.
+ * Level kernel (kernel_form 0): spin words per CTA work item in {1024, 2048,
+ * 4096, 8192} x threads per CTA in {128, 256, 512}; chosen[4] (may be NULL)
+ * receives {item_sites, threads, 0, 0}. Per-lane kernels: the thread-class
+ * thresholds (instances above a size threshold get 2 or 4 threads per
+ * generator lane); chosen receives {n4_int, n2_int, n4_f64, n2_f64}. */
 ie_status ie_batch_autotune(ie_batch* b, const double* temps, uint64_t trial_steps, uint32_t* chosen);
 /* Spin words of instance i at words + offsets[i] (offsets = prefix sums of n). */
 ie_status ie_batch_read_spins(ie_batch* b, uint64_t* words);

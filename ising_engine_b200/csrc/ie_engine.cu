@@ -1307,6 +1307,44 @@ struct Engine {
         };
         IE_TRY(copy_all(true));
         const uint64_t saved_steps = steps_done;
+        if (kernel_form == 0) {
+            // Level kernel: the CTA work tile (spin words per item, i.e. 64
+            // replica bytes per word) and the CTA size; the fastest of each
+            // pair on the best of two trials wins.
+            const uint32_t caps[4] = {1024, 2048, 4096, 8192};
+            const int thrs[3] = {128, 256, 512};
+            double best = 1e300;
+            uint32_t bc = lvl_cap;
+            int bt = lvl_threads;
+            for (uint32_t c : caps)
+                for (int t : thrs) {
+                    lvl_cap = c;
+                    lvl_threads = t;
+                    quads_built = false;
+                    double ms_best = 1e300;
+                    for (int rep = 0; rep < 2; rep++) {
+                        IE_TRY(run_batch(temps, trial_steps));
+                        IE_TRY(copy_all(false));
+                        steps_done = saved_steps;
+                        ms_best = std::min(ms_best, last_ms);
+                    }
+                    if (ms_best < best) {
+                        best = ms_best;
+                        bc = c;
+                        bt = t;
+                    }
+                }
+            lvl_cap = bc;
+            lvl_threads = bt;
+            quads_built = false;
+            IE_TRY(build_quads());
+            if (out) {
+                out[0] = bc;
+                out[1] = (uint32_t)bt;
+                out[2] = out[3] = 0;
+            }
+            return IE_OK;
+        }
         // Coordinate search: the (n4, n2) pair of one mode over its grid with
         // the other mode's pair held, integer then f64, two passes; each trial
         // is timed on the same state (restored after it).

@@ -233,9 +233,9 @@ class BatchEngine:
         return self.last_ms()
 
     def autotune(self, temps, trial_steps: int = 16):
-        """Chooses the thread-class thresholds by timing short trials of the
-        schedule (state restored after each); returns (n4_int, n2_int,
-        n4_f64, n2_f64)."""
+        """Chooses the launch shape by timing short trials of the schedule
+        (state restored after each). Level kernel: returns (item_sites,
+        threads, 0, 0); per-lane kernels: (n4_int, n2_int, n4_f64, n2_f64)."""
         t = np.ascontiguousarray(temps, dtype=np.float64).reshape(-1)
         out = np.zeros(4, dtype=np.uint32)
         _ffi.check(self._L.ie_batch_autotune(self._h, _p(t), min(int(trial_steps), len(t)), _p(out)))
