@@ -13,8 +13,12 @@ all in one persistent launch. Attempts = sum_i N_i * 64 * sweeps.
   e2e   : the same metric through the public API from host buffers: create
           (host->device copy of the problems), init, run, read spins and
           energies back (device->host), wall clock.
+  parity: the e2e run's spins and energies against the oracle on every 64th
+          instance over the full schedule, and the plain arm's against the
+          batched run's on its instances.
   --impl reference : the CPU restatement of the reference's Rayon path (the
-          oracle), all host threads, on a bounded sample of the workload.
+          oracle), all host threads, on a bounded sample of the workload:
+          all instances over a strided subset of the schedule's sweeps.
 
 Multi-GPU: replicas only; every rank runs its own batch (weak scaling), no
 collective on the data path.
@@ -37,6 +41,7 @@ sys.path.insert(0, ROOT)
 METRIC = "spin-flip attempts/s: batched vs plain GPU, same energies; serve p50/p99 ms"
 UNIT = "attempts/s"
 OPS_PER_ATTEMPT = 22  # algorithmic int32 ops per attempt: Xoshiro256++ step (20) + 64-bit compare (2)
+CPU_SWEEPS = 32       # sweeps of the strided schedule sample timed on the host
 WORKLOAD = ("uneven batch: 4096 random-regular QUBO instances, N log-uniform [64,4096], degree "
             "3..16, half integer couplings [-8,8], half float32 N(0,1); SA beta 0.1->5.0 over 2000 "
             "sweeps; 64 replicas per instance")
@@ -201,7 +206,8 @@ def run_ours(args):
     eng = BatchEngine(models, seeds, device=local, threads_per_block=args.threads_per_block,
                       blocks_per_sm=args.blocks_per_sm, graph=True)
     eng.init_random()
-    tuned = eng.autotune(temps, 160) if not args.no_autotune else None
+    tuned = eng.autotune(temps, 100) if not args.no_autotune else None
+    shape = dict(item_sites=tuned[0], threads_per_block=tuned[1]) if tuned else {}
     for _ in range(args.warmup):
         eng.run_schedule(temps)
     dist.barrier()
@@ -251,47 +257,66 @@ def run_ours(args):
         except Exception:
             traffic = None
 
-    plain = None
-    if not args.no_plain and rank == 0:
-        order = np.argsort([m.num_vars for m in models])
-        pick = [int(order[i]) for i in np.linspace(0, len(order) - 1, 12).astype(int)]
-        sub = [models[i] for i in pick]
-        pe = BatchEngine(sub, seeds[pick], device=local)
-        pe.init_random()
-        pt = temps[:100]
-        pe.run_schedule_plain(pt[:5])
-        ms = pe.run_schedule_plain(pt)
-        plain = {"value": attempts_of(sub, len(pt)) / (ms / 1e3), "unit": UNIT,
-                 "sample": f"{len(sub)} instances spread over the size range, {len(pt)} sweeps each, "
-                           "one launch per instance in sequence",
-                 "launches": pe.last_launches()}
-        pe.close()
-
+    # e2e: one fresh run of the full schedule through the public API from
+    # host buffers; its results are the ones the parity checks read
     e2e = None
+    w_run = e_run = None
+    offs = np.zeros(len(models) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([m.num_vars for m in models])
     if not args.no_e2e:
         ts = []
         for _ in range(max(1, min(args.steps, 2))):
             dist.barrier()
             t1 = time.perf_counter()
-            b = BatchEngine(models, seeds, device=local)
+            b = BatchEngine(models, seeds, device=local, **shape)
             b.init_random()
             b.run_schedule(temps)
             w = b.spins()
             e = b.energies()
             b.close()
             ts.append(time.perf_counter() - t1)
+            w_run, e_run = w, e
         e2e_s = dist.max(float(np.mean(ts)))
         e2e = {"value": dist.sum(attempts) / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(host_bytes(models)),
                "d2h_bytes_per_step": int(w.nbytes + e.nbytes)}
 
+    plain = None
+    plain_pick = []
+    plain_mismatch = None
+    if not args.no_plain and rank == 0:
+        order = np.argsort([m.num_vars for m in models])
+        plain_pick = [int(order[i]) for i in np.linspace(0, len(order) - 1, 12).astype(int)]
+        sub = [models[i] for i in plain_pick]
+        pe = BatchEngine(sub, seeds[plain_pick], device=local, **shape)
+        pe.init_random()
+        ms = pe.run_schedule_plain(temps)
+        plain = {"value": attempts_of(sub, len(temps)) / (ms / 1e3), "unit": UNIT,
+                 "sample": f"{len(sub)} instances spread over the size range, full {len(temps)}-sweep "
+                           "schedule, one launch (one CTA of the batched run's kernel) per instance in sequence",
+                 "launches": pe.last_launches()}
+        if w_run is not None:
+            pw, pen = pe.spins(), pe.energies()
+            plain_mismatch = 0
+            for j, i in enumerate(plain_pick):
+                same = (pw[pe.offsets[j]:pe.offsets[j + 1]] == w_run[offs[i]:offs[i + 1]]).all()
+                same = same and pen[j].tobytes() == e_run[i].tobytes()
+                plain_mismatch += 0 if same else 1
+        pe.close()
+
+    parity = None
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(models, seeds, temps)
+        if w_run is not None:
+            parity = check_parity(models, seeds, temps, w_run, e_run, offs)
+            if plain_mismatch is not None:
+                parity["plain_instances"] = len(plain_pick)
+                parity["plain_mismatched"] = plain_mismatch
+
     serve = None
     if not args.no_serve and rank == 0:
         serve = run_serve(args, local)
-
-    cpu = None
-    if not args.no_cpu and rank == 0 and ws == 1:
-        cpu = cpu_baseline(models, seeds, temps)
 
     if rank == 0:
         line = {
@@ -304,10 +329,13 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (problem data %.0f MB per GPU)" % (host_bytes(models) / 1e6),
                        "parallelism": f"replicas x{ws}",
                        "launch": "one persistent launch per work class, replayed from a CUDA graph",
-                       "thread_classes": ({"n4_int": tuned[0], "n2_int": tuned[1], "n4_f64": tuned[2],
-                                           "n2_f64": tuned[3]} if tuned else "default")},
+                       "launch_shape": ({"item_sites": tuned[0], "threads_per_cta": tuned[1],
+                                         "source": "autotuner (ie_batch_autotune)"} if tuned else "default")},
             "roofline": {"bound": "alu", "achieved": achieved_ops / 1e9, "peak": ip.value / 1e9,
-                         "unit": "Gop/s", "frac": achieved_ops / ip.value, "traffic": traffic, "traffic_source": "profiles/batched_step_traffic.json (ncu, bytes per attempt x attempts per step)" if traffic else None,
+                         "unit": "Gop/s", "frac": achieved_ops / ip.value, "traffic": traffic,
+                         "traffic_source": ("scaled: ncu DRAM bytes per attempt of a smaller capture "
+                                            "(profiles/batched_step_traffic.json) x attempts per step")
+                         if traffic else None,
                          "ops_per_attempt": OPS_PER_ATTEMPT,
                          "peak_source": "measured in-run: int32 LOP3/IADD3 microkernel (ie_probe_peaks)",
                          "per": "step: one group of concurrent class launches",
@@ -325,6 +353,8 @@ def run_ours(args):
             "classes": [{"mode": c[0], "threads_per_lane": c[1], "cap": c[2], "items": c[3],
                          "ms": round(c[4], 1)} for c in classes],
         }
+        if parity:
+            line["parity"] = parity
         if serve:
             line["serve"] = serve
         if cpu:
@@ -362,26 +392,70 @@ def run_serve(args, device):
                       f"SA {lo}..{hi} sweeps (beta 0.1 -> 5.0), Poisson arrivals"}
 
 
-def cpu_sample(models, seeds, temps):
-    order = np.arange(len(models))
+def parity_sample(models):
+    """Every 64th instance (64 of 4096): checked over the full schedule."""
     stride = max(1, len(models) // 64)
-    return [int(i) for i in order[::stride]]
+    return list(range(0, len(models), stride))
+
+
+def strided_temps(temps):
+    """CPU_SWEEPS sweeps taken at evenly spaced steps of the schedule, so the
+    sample spans its whole temperature range."""
+    idx = np.linspace(0, len(temps) - 1, min(CPU_SWEEPS, len(temps))).astype(int)
+    return np.ascontiguousarray(temps[idx])
+
+
+def cpu_sample_desc(models, temps):
+    return (f"all {len(models)} instances, {min(CPU_SWEEPS, len(temps))} of the {len(temps)} sweeps "
+            f"(every {max(1, len(temps) // CPU_SWEEPS)}th temperature of the schedule), parallel over "
+            "instances; attempts/s = attempts of the sample / its time")
 
 
 def cpu_baseline(models, seeds, temps):
     """The oracle (C++ restatement of the reference's Rayon path) on a bounded
-    sample of the workload (every 64th instance, full schedule), dynamically
-    scheduled over instances on every host core."""
+    sample of the workload (every instance, a strided subset of the sweeps),
+    dynamically scheduled over instances on every host core."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    pick = cpu_sample(models, seeds, temps)
+    ts = strided_temps(temps)
+    t0 = time.perf_counter()
+    O.run_sa_batch(models, seeds, ts, threads=cores, want_words=False)
+    dt = time.perf_counter() - t0
+    return {"value": attempts_of(models, len(ts)) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": cpu_sample_desc(models, temps)}
+
+
+def check_parity(models, seeds, temps, words, energies, offs):
+    """The run's spins and energies against the oracle on every 64th instance
+    over the full schedule: spin words bit for bit; energies equal to the
+    oracle's FP64 recompute of the same words (the level kernel reports the
+    recompute) and, for integer couplings, to the oracle's tracked sum; for
+    f64 couplings the largest relative gap to the tracked sum."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    pick = parity_sample(models)
     sub = [models[i] for i in pick]
     t0 = time.perf_counter()
-    O.run_sa_batch(sub, seeds[pick], temps, threads=cores, want_words=False)
+    wref, roff, eref = O.run_sa_batch(sub, seeds[pick], temps, threads=cores, want_words=True)
     dt = time.perf_counter() - t0
-    return {"value": attempts_of(sub, len(temps)) / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{len(sub)} of {len(models)} instances (every {len(models) // len(pick)}th), full "
-                      f"{len(temps)}-sweep schedule, parallel over instances"}
+    bad_w = bad_e = 0
+    max_rel = 0.0
+    for j, i in enumerate(pick):
+        m = models[i]
+        w = words[offs[i]:offs[i + 1]]
+        if not (w == wref[roff[j]:roff[j] + m.num_vars]).all():
+            bad_w += 1
+        e = energies[i]
+        rec = O.replica_energies(m, w)[0]
+        ok = e.tobytes() == rec.tobytes()
+        if m.is_integral():
+            ok = ok and e.tobytes() == eref[j].tobytes()
+        else:
+            max_rel = max(max_rel, float((np.abs(e - eref[j]) / np.maximum(np.abs(eref[j]), 1.0)).max()))
+        bad_e += 0 if ok else 1
+    return {"instances": len(pick), "sweeps": len(temps), "mismatched_words": bad_w,
+            "mismatched_energies": bad_e, "max_rel_fp64": max_rel, "fp64_rel_tol": 1e-6,
+            "oracle_s": dt, "sample": f"every {len(models) // len(pick)}th instance, full schedule"}
 
 
 def run_reference(args):
@@ -391,20 +465,17 @@ def run_reference(args):
     models, seeds, temps = make_workload(args.count, args.seed, args.sweeps)
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    pick = cpu_sample(models, seeds, temps)
-    # one step = a fixed sample sized to about a few seconds of host work
-    per_step = pick[: max(cores, min(len(pick), 2 * cores))]
-    sub = [models[i] for i in per_step]
-    ss = seeds[per_step]
+    # one step = every instance over a strided subset of the sweeps (a few
+    # seconds of host work), so no single large instance sets the time
+    ts = strided_temps(temps)
     for _ in range(args.warmup):
-        O.run_sa_batch(sub, ss, temps, threads=cores, want_words=False)
+        O.run_sa_batch(models, seeds, ts, threads=cores, want_words=False)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.run_sa_batch(sub, ss, temps, threads=cores, want_words=False)
+        O.run_sa_batch(models, seeds, ts, threads=cores, want_words=False)
     dt = time.perf_counter() - t0
-    value = attempts_of(sub, len(temps)) * args.steps / dt
-    sample = (f"{len(sub)} of {len(models)} instances (every {len(models) // len(pick)}th), full "
-              f"{len(temps)}-sweep schedule per step, parallel over instances")
+    value = attempts_of(models, len(ts)) * args.steps / dt
+    sample = cpu_sample_desc(models, temps) + "; per step"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "i32+f64", "data": "synthetic (seeded)",

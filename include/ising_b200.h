@@ -188,7 +188,7 @@ ie_status ie_suggested_temp_range(const ie_problem* problem, double* temp_max, d
 typedef struct ie_batch_config {
     int32_t device;
     int32_t force_f64;
-    uint32_t threads_per_block; /* reserved, 0 */
+    uint32_t threads_per_block; /* level kernel: threads per CTA (multiple of 32, <= 512; 0: 256) */
     uint32_t blocks_per_sm;     /* cap on resident CTAs per SM per class, 0 = as many as fit */
     int32_t disable_windows;    /* nonzero: never use the windowed kernel for large instances */
     int32_t use_graph;          /* nonzero: ie_batch_run_schedule replays one CUDA graph holding
