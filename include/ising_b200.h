@@ -188,7 +188,7 @@ ie_status ie_suggested_temp_range(const ie_problem* problem, double* temp_max, d
 typedef struct ie_batch_config {
     int32_t device;
     int32_t force_f64;
-    uint32_t threads_per_block; /* level kernel: threads per CTA (multiple of 32, <= 512; 0: 256) */
+    uint32_t threads_per_block; /* level kernel: threads per CTA (multiple of 32, <= 256; 0: 256) */
     uint32_t blocks_per_sm;     /* cap on resident CTAs per SM per class, 0 = as many as fit */
     int32_t disable_windows;    /* nonzero: never use the windowed kernel for large instances */
     int32_t use_graph;          /* nonzero: ie_batch_run_schedule replays one CUDA graph holding
@@ -218,7 +218,7 @@ ie_status ie_batch_run_schedule_plain(ie_batch* b, const double* temps, uint64_t
 /* Autotuner: times trial_steps of the schedule temps[] for a grid of launch
  * shapes, restoring the device state after every trial, and keeps the fastest.
  * Level kernel (kernel_form 0): spin words per CTA work item in {1024, 2048,
- * 4096, 8192} x threads per CTA in {128, 256, 512}; chosen[4] (may be NULL)
+ * 4096, 8192} x threads per CTA in {128, 256}; chosen[4] (may be NULL)
  * receives {item_sites, threads, 0, 0}. Per-lane kernels: the thread-class
  * thresholds (instances above a size threshold get 2 or 4 threads per
  * generator lane); chosen receives {n4_int, n2_int, n4_f64, n2_f64}. */

@@ -1312,7 +1312,7 @@ struct Engine {
             // replica bytes per word) and the CTA size; the fastest of each
             // pair on the best of two trials wins.
             const uint32_t caps[4] = {1024, 2048, 4096, 8192};
-            const int thrs[3] = {128, 256, 512};
+            const int thrs[2] = {128, 256};
             double best = 1e300;
             uint32_t bc = lvl_cap;
             int bt = lvl_threads;
@@ -2522,8 +2522,8 @@ ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint
     }
     if (cfg.tie_shift > 31) return fail(IE_ERR_INVALID, "tie_shift must be below 32");
     b->eng.lvl_tie_shift = cfg.tie_shift;
-    if (cfg.threads_per_block && (cfg.threads_per_block % 32 || cfg.threads_per_block > 512))
-        return fail(IE_ERR_INVALID, "threads_per_block must be a multiple of 32, at most 512");
+    if (cfg.threads_per_block && (cfg.threads_per_block % 32 || cfg.threads_per_block > 256))
+        return fail(IE_ERR_INVALID, "threads_per_block must be a multiple of 32, at most 256");
     if (cfg.threads_per_block) b->eng.lvl_threads = (int)cfg.threads_per_block;
     IE_TRY(b->eng.build(problems, count, 1, seeds, cfg.force_f64 != 0));
     *out = b.release();

@@ -205,7 +205,7 @@ __device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uin
 }
 
 template <uint32_t MODE, bool GSP>
-__global__ void __launch_bounds__(512) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
+__global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
     extern __shared__ __align__(16) uint64_t dsm[];
     __shared__ LvlMem ms[kLvlMaxMembers];
     __shared__ uint32_t s_item, s_steps;
@@ -380,13 +380,14 @@ __global__ void __launch_bounds__(512) level_kernel(DevArrays A, RunArgs R, LvlA
                         const uint32_t deg4 = (deg + 3u) & ~3u;
                         const uint4* c4p = reinterpret_cast<const uint4*>(rec + 4);
                         const double2* w2p = reinterpret_cast<const double2*>(rec + 4 + deg4);
-                        double dl[8], tp[8];
+                        // dE_k = s_k (lin + sum of w over the neighbours with x_j = 1, in
+                        // CSR order), s_k = 1 - 2 x_v: the reference adds w ((x_j ^ x_v) -
+                        // x_v) = s_k w or a zero term, and round-to-nearest is symmetric
+                        // (fl(-a - b) = -fl(a + b)), so the sum of signed terms is s_k
+                        // times the sum of the weights; zero terms change no nonzero sum.
+                        double dl[8];
 #pragma unroll
-                        for (int k = 0; k < 8; k++) {
-                            const bool xv = (xb >> k) & 1u;
-                            tp[k] = xv ? -1.0 : 1.0;
-                            dl[k] = xv ? -wl : wl;
-                        }
+                        for (int k = 0; k < 8; k++) dl[k] = wl;
                         for (uint32_t q = 0; q < deg; q += 4) {
                             const uint4 c4 = __ldg(c4p + (q >> 2));
                             const double2 w01 = __ldg(w2p + (q >> 1));
@@ -400,17 +401,14 @@ __global__ void __launch_bounds__(512) level_kernel(DevArrays A, RunArgs R, LvlA
                             for (int e = 0; e < 4; e++) {
                                 if (q + e < deg) {
 #pragma unroll
-                                    for (int k = 0; k < 8; k++) {
-                                        // t = (x_j ^ x_v) - x_v; w * t is exact, so
-                                        // fma(w, t, dE) is the reference's dE + w * t
-                                        const double tt = ((bj[e] >> k) & 1u) ? tp[k] : 0.0;
-                                        dl[k] = __fma_rn(ww[e], tt, dl[k]);
-                                    }
+                                    for (int k = 0; k < 8; k++)
+                                        if ((bj[e] >> k) & 1u) dl[k] = __dadd_rn(dl[k], ww[e]);
                                 }
                             }
                         }
 #pragma unroll
                         for (int k = 0; k < 8; k++) {
+                            if ((xb >> k) & 1u) dl[k] = -dl[k];
                             if (dl[k] <= 0.0) {
                                 flips |= 1u << k;
                                 continue;
