@@ -761,7 +761,9 @@ struct Engine {
     uint32_t lvl_tie_shift = 0;
     bool serving = false;     // serving launches: one threshold table per member
     std::vector<std::vector<uint32_t>> lv_sites, lv_off;  // per instance: sites by level, level starts
-    DevBuf<uint32_t> d_lrecs, d_recoff, d_lent, d_llvl, d_lseg, d_keybuf;
+    std::vector<uint32_t> h_recoff;                       // level-record offset per site
+    DevBuf<uint32_t> d_lrecs, d_recoff, d_llvl, d_lseg, d_keybuf;
+    DevBuf<LvlEntry> d_lent;
     DevBuf<LvlItem> d_litems;
     DevBuf<LvlMember> d_lmem;
     DevBuf<uint64_t> d_jpoly;
@@ -812,6 +814,7 @@ struct Engine {
         });
         IE_TRY(d_lrecs.upload(recs, stream));
         IE_TRY(d_recoff.upload(recoff, stream));
+        h_recoff = std::move(recoff);
         return IE_OK;
     }
 
@@ -875,7 +878,8 @@ struct Engine {
                 const uint32_t maxmem = one_per_item ? 1u : own ? kLvlMaxOwnTables : kLvlMaxMembers;
                 std::vector<uint32_t> order;
                 double longest = 0;
-                build_level_items(D, nnz_of, lv_sites, lv_off, mem[m][g], g != 0, cap, maxmem, lvh, order, longest);
+                build_level_items(D, nnz_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem, lvh, order,
+                                  longest);
                 wc->nitems = (uint32_t)order.size();
                 wc->work = longest;
                 for (uint32_t i : mem[m][g]) wc->site_steps += (double)D[i].n;
@@ -894,7 +898,7 @@ struct Engine {
         if (lvh.items.empty()) return IE_OK;
         IE_TRY(d_litems.upload(lvh.items, stream));
         IE_TRY(d_lmem.upload(lvh.members, stream));
-        IE_TRY(d_lent.upload(lvh.entries.empty() ? std::vector<uint32_t>(1, 0) : lvh.entries, stream));
+        IE_TRY(d_lent.upload(lvh.entries.empty() ? std::vector<LvlEntry>(1, LvlEntry{0, 0}) : lvh.entries, stream));
         IE_TRY(d_llvl.upload(lvh.lvloff, stream));
         IE_TRY(d_lseg.upload(lvh.segs, stream));
         IE_TRY(d_keybuf.alloc(std::max<uint64_t>(keytotal, 1)));

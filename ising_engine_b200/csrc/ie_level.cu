@@ -69,6 +69,15 @@ __device__ __noinline__ uint64_t lane_output(uint64_t base, int lane, uint32_t v
     return x.next();
 }
 
+__device__ __forceinline__ LvlEntry load_entry(const LvlEntry* p) {
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
+    return LvlEntry{u.x, u.y};
+}
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ float ex2_approx(float a) {
     float r;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
@@ -317,17 +326,22 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                 }
             }
             __syncthreads();
-            // decision phase, level by level
+            // decision phase, level by level; before each level barrier a
+            // thread loads its first entry of the next level and prefetches
+            // that site's record and outputs (read-only during the phase)
             const uint32_t sh = L.tie_shift;
+            uint32_t e1 = I.nlvl ? __ldg(L.lvloff + I.lvl0) : 0u;
+            LvlEntry nxt{0, 0};
             for (uint32_t l = 0; l < I.nlvl; l++) {
-                const uint32_t e0 = __ldg(L.lvloff + I.lvl0 + l), e1 = __ldg(L.lvloff + I.lvl0 + l + 1);
+                const uint32_t e0 = e1;
+                e1 = __ldg(L.lvloff + I.lvl0 + l + 1);
                 for (uint32_t i = tid; i < 8u * (e1 - e0); i += T) {
-                    const uint32_t ent = __ldg(L.entries + I.ent0 + e0 + (i >> 3));
-                    const uint32_t slot = ent >> kLvlFlatBits, f = ent & ((1u << kLvlFlatBits) - 1u);
+                    const LvlEntry en = (i == (uint32_t)tid && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + (i >> 3));
+                    const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
                     const LvlMem& m = ms[slot];
                     if (s >= m.steps) continue;
                     const uint32_t v = f - m.flat;
-                    const uint32_t* rec = L.lrecs + 4ull * __ldg(L.recoff + m.site + v);
+                    const uint32_t* rec = L.lrecs + 4ull * en.rec;
                     const uint4 hd = __ldg(reinterpret_cast<const uint4*>(rec));
                     const uint32_t deg = hd.x & 0x7FFFFFFFu;
                     const uint32_t fb = m.flat;
@@ -423,6 +437,14 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                         }
                     }
                     spb[8u * f] = (uint8_t)(xb ^ flips);
+                }
+                if (l + 1 < I.nlvl) {
+                    const uint32_t e2 = __ldg(L.lvloff + I.lvl0 + l + 2);
+                    if ((uint32_t)tid < 8u * (e2 - e1)) {
+                        nxt = load_entry(L.entries + I.ent0 + e1 + (tid >> 3));
+                        prefetch_l1(L.lrecs + 4ull * nxt.rec);
+                        prefetch_l1(kb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64 + lane * 8);
+                    }
                 }
                 __syncthreads();
             }

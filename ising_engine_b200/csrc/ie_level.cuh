@@ -42,6 +42,13 @@ struct LvlMember {
     uint32_t flat;  // first flat spin word of the member
 };
 
+// One site of a level: slot << 26 | flat site index, and its level record's
+// offset in 16-byte units (one load gives both).
+struct alignas(8) LvlEntry {
+    uint32_t site;
+    uint32_t rec;
+};
+
 // Level-record stream: one record per site, 16-byte aligned.
 //  integer: [deg | clamp << 31, linp, lin, 0, e_0 .. e_{deg-1}, 0-padding to 4],
 //           e = col | |w| << 24 | (w < 0) << 31 (padding entries are 0: no effect)
@@ -52,7 +59,7 @@ struct LvlArgs {
     uint32_t nitems;
     uint32_t* queue;
     const LvlMember* members;
-    const uint32_t* entries;
+    const LvlEntry* entries;
     const uint32_t* lvloff;
     const uint32_t* segs;
     const uint64_t* jpoly;     // [j][4]: x^(8 kLvlSeg j) mod P(x), bit i = coefficient of x^i

@@ -220,7 +220,8 @@ void site_levels(const LvlSource& s, std::vector<uint32_t>& sites, std::vector<u
 
 void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_t>& nnz_of,
                        const std::vector<std::vector<uint32_t>>& lv_sites,
-                       const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& mem,
+                       const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& recoff,
+                       const std::vector<uint32_t>& mem,
                        bool gsp, uint32_t cap, uint32_t max_mem, LvlHost& out, std::vector<uint32_t>& order,
                        double& longest) {
     std::vector<uint32_t> m = mem;
@@ -277,7 +278,7 @@ void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_
                 const std::vector<uint32_t>& st = lv_sites[d.owner];
                 const uint32_t f0 = out.members[it.mem0 + slot].flat;
                 for (uint32_t q = off[l]; q < off[l + 1]; q++)
-                    out.entries.push_back(slot << kLvlFlatBits | (f0 + st[q]));
+                    out.entries.push_back(LvlEntry{slot << kLvlFlatBits | (f0 + st[q]), recoff[d.site + st[q]]});
             }
         }
         out.lvloff.push_back((uint32_t)(out.entries.size() - it.ent0));

@@ -43,12 +43,14 @@ void site_levels(const LvlSource& s, std::vector<uint32_t>& sites, std::vector<u
 // Items of one launch class: members (indices into the view of InstDesc `D`)
 // grouped into items of at most cap spin words and max_mem members (gsp: one
 // member per item, spins in global memory). Level lists of member i are
-// lv_sites / lv_off of instance D[i].owner. Appends to the item arrays and
+// lv_sites / lv_off of instance D[i].owner; recoff[D[i].site + v] is site v's
+// level-record offset. Appends to the item arrays and
 // returns the class's item ids ordered longest first.
 struct LvlHost {
     std::vector<LvlItem> items;
     std::vector<LvlMember> members;
-    std::vector<uint32_t> entries, lvloff, segs;
+    std::vector<LvlEntry> entries;
+    std::vector<uint32_t> lvloff, segs;
     uint32_t max_segs = 1;  // largest segment count of any member
     void clear() {
         items.clear();
@@ -61,7 +63,8 @@ struct LvlHost {
 };
 void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_t>& nnz_of,
                        const std::vector<std::vector<uint32_t>>& lv_sites,
-                       const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& mem,
+                       const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& recoff,
+                       const std::vector<uint32_t>& mem,
                        bool gsp, uint32_t cap, uint32_t max_mem, LvlHost& out, std::vector<uint32_t>& order,
                        double& longest);
 
