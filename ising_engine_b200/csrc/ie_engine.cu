@@ -1076,6 +1076,9 @@ struct Engine {
         while (done < steps) {
             const uint64_t g0 = steps_done + done;
             uint64_t k = kx - g0 % kx;
+            // a single cell has no exchange pairs: its exchange steps only
+            // toggle the DEO phase, so one launch runs every step
+            if (nt == 1) k = std::min<uint64_t>(steps - done, 1u << 20);
             if (mode == kModeF64 && periodic_resync) k = std::min<uint64_t>(k, kResyncEvery - g0 % kResyncEvery);
             k = std::min<uint64_t>(k, steps - done);
             R.steps = (uint32_t)k;
@@ -1083,7 +1086,7 @@ struct Engine {
             R.temps = d_temps.p + (per_step ? done * nt : 0);
             IE_TRY(launch_classes(R, AC));
             launches += last_launches;
-            const bool ex = (g0 + k) % kx == 0;
+            const bool ex = nt == 1 ? (((g0 + k) / kx - g0 / kx) & 1u) != 0 : (g0 + k) % kx == 0;
             IE_CUDA(launch_exchange(A, R, count, mode, (uint32_t)k, ex, stream));
             launches++;
             if (ex && nt > 1)
