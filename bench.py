@@ -307,12 +307,14 @@ def run_ours(args):
     parity = None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_baseline(models, seeds, temps)
+        # the parity run (oracle, full schedule) comes first and warms the
+        # host code, as the reference arm's warm-up steps do
         if w_run is not None:
             parity = check_parity(models, seeds, temps, w_run, e_run, offs)
             if plain_mismatch is not None:
                 parity["plain_instances"] = len(plain_pick)
                 parity["plain_mismatched"] = plain_mismatch
+        cpu = cpu_baseline(models, seeds, temps)
 
     serve = None
     if not args.no_serve and rank == 0:

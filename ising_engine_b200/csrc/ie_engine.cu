@@ -613,10 +613,15 @@ struct Engine {
     // Record streams and window tables, built per instance on host threads
     // (each stream a whole number of chunks) and concatenated.
     ie_status build_record_streams() {
+        // the per-lane kernels' streams: needed unless every instance runs on
+        // the level kernel (a batch on kernel_form 0; handles keep them for
+        // f64 cells)
+        bool old_needed = kernel_form != 0;
+        for (uint32_t i = 0; i < count && !old_needed; i++) old_needed = !is_batch && desc[i].mode == kModeF64;
         std::vector<std::vector<uint32_t>> lrec(count), lwt(count);
         std::vector<ie_status> st(count, IE_OK);
         std::vector<std::string> msg(count);
-        parallel_for(count, [&](uint32_t i) {
+        parallel_for(old_needed ? count : 0u, [&](uint32_t i) {
             st[i] = build_records(insts[i], clampf, desc[i].site, lrec[i], desc[i].rec, desc[i].rec_len);
             if (st[i] == IE_OK) st[i] = window_records(insts[i], clampf, desc[i].site, lrec[i], desc[i].rec, desc[i].wrec);
             if (st[i] != IE_OK) {
@@ -751,6 +756,7 @@ struct Engine {
     // shared-memory spin capacity of the instance's class; 0: spins in global memory
     static uint32_t class_cap(const InstDesc& d) { return cap_of(d.n) > kSmemSpinCap ? 0u : cap_of(d.n); }
     bool use_windows = true;
+    bool is_batch = false;        // ie_batch: single-cell instances, no PT cells
     std::vector<uint8_t> active;  // instances in the work classes (empty: all)
 
     // Level kernel (ie_level.cu): kernel_form 0 runs batched instances and
@@ -2520,6 +2526,7 @@ ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint
     b->eng.blocks_per_sm = cfg.blocks_per_sm;
     b->eng.use_windows = cfg.disable_windows == 0;
     b->eng.use_graph = cfg.use_graph != 0;
+    b->eng.is_batch = true;
     if (cfg.kernel_form < 0 || cfg.kernel_form > 1) return fail(IE_ERR_INVALID, "kernel_form must be 0 or 1");
     b->eng.kernel_form = cfg.kernel_form;
     if (cfg.item_sites) {
