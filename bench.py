@@ -67,6 +67,10 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=20.0)
     p.add_argument("--serve-sweeps", type=int, nargs=2, default=[100, 2000])
     p.add_argument("--serve-budget", type=int, default=65536)
+    p.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 4],
+                   help="3: the batched headline workload; 1, 2, 4: the PT configurations alone")
+    p.add_argument("--no-configs", action="store_true", help="skip configs 1, 2, 4 in the headline line")
+    p.add_argument("--c4-steps", type=int, default=500)
     return p.parse_args()
 
 
@@ -320,6 +324,10 @@ def run_ours(args):
     if not args.no_serve and rank == 0:
         serve = run_serve(args, local)
 
+    configs = None
+    if not args.no_configs and rank == 0 and ws == 1:
+        configs = [run_config(c, local, args) for c in (1, 2, 4)]
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -357,6 +365,8 @@ def run_ours(args):
         }
         if parity:
             line["parity"] = parity
+        if configs:
+            line["configs"] = configs
         if serve:
             line["serve"] = serve
         if cpu:
@@ -364,6 +374,86 @@ def run_ours(args):
         print(json.dumps(line))
     eng.close()
     dist.close()
+
+
+def _pt_run(m, temps, steps, interval, seed, device, warm=0, **kw):
+    """Wall time of `steps` PT steps (engine::step with the exchange every
+    `interval` steps) on a fresh handle with its state resident on the
+    device; returns (seconds, engine)."""
+    from ising_engine_b200.engine import Engine
+    eng = Engine(m, num_temps=len(temps), seed=seed, exchange_interval=interval, device=device, **kw)
+    eng.init_random()
+    if warm:
+        eng.step(temps, warm)
+    t0 = time.perf_counter()
+    eng.step(temps, steps)
+    return time.perf_counter() - t0, eng
+
+
+def _pt_parity(m, temps, steps, interval, seed, device, threads):
+    """Spin words, energies, swap statistics and stream position after
+    `steps` steps from the random init, against the oracle."""
+    from oracle import oracle as O
+    ref = O.run_schedule(m, np.tile(temps, (steps, 1)), seed, exchange_interval=interval, collect_stats=True,
+                         threads=threads)
+    _, eng = _pt_run(m, temps, steps, interval, seed, device)
+    w, e = eng.spins(), eng.energies()
+    att, acc = eng.swap_stats()
+    out = {"steps": steps, "mismatched_cells": int((w != ref.words).any(axis=1).sum()),
+           "energies_equal": bool(e.tobytes() == ref.energies.tobytes()),
+           "stream_position_equal": eng.rng_state()[0] == ref.draws,
+           "swap_stats_equal": bool((att == ref.swap_attempts).all() and (acc == ref.swap_accepts).all())
+           if len(temps) > 1 else None}
+    eng.close()
+    return out
+
+
+def run_config(cfg, device, args):
+    """Configs 1, 2, 4 (seeded synthetic instances of their shapes); value =
+    attempts/s of the PT steps on the level kernel (wall clock around
+    ie_step, state resident on the device)."""
+    from ising_engine_b200 import instances as I
+    cores = os.cpu_count() or 1
+    if cfg == 1:
+        m = I.pm_j_lattice(32, 2, seed=2024)
+        temps, steps, interval = np.ones(1), 1000, 1
+        dt, eng = _pt_run(m, temps, steps, interval, 11, device, warm=20)
+        eng.close()
+        lane_dt, eng = _pt_run(m, temps, steps, interval, 11, device, warm=20, kernel_form=1)
+        eng.close()
+        return {"config": 1, "workload": "2D periodic +-J lattice L=32 (N=1024), one cell at beta=1, 1000 sweeps",
+                "value": m.num_vars * 64.0 * steps / dt, "unit": UNIT, "s_per_1000_sweeps": dt,
+                "per_lane_kernel_s_per_1000_sweeps": lane_dt,
+                "parity": _pt_parity(m, temps, steps, interval, 11, device, cores)}
+    if cfg == 2:
+        m = I.maxcut_gnm(800, 19176, seed=3)
+        temps, steps, interval = I.geometric_beta_ladder(32, 0.1, 3.0), 10000, 10
+        dt, eng = _pt_run(m, temps, steps, interval, 12, device, warm=10)
+        e = eng.energies()
+        att, acc = eng.swap_stats()
+        eng.close()
+        return {"config": 2, "workload": "Max-Cut of G(800, 19176) as QUBO, 32 temperatures beta geometric "
+                "0.1..3.0, 64 replicas each, exchange every 10 sweeps, 10^4 sweeps",
+                "value": m.num_vars * 64.0 * len(temps) * steps / dt, "unit": UNIT, "seconds": dt,
+                "best_cut": float(-e.min()), "mean_cut_coldest": float(-e[-1].mean()),
+                "swap_acceptance_per_pair": [round(float(a) / max(int(b), 1), 4) for a, b in zip(acc, att)],
+                "parity": _pt_parity(m, temps, 1000, interval, 12, device, cores)}
+    m = I.pm_j_lattice(64, 3, seed=64)
+    temps, interval = I.geometric_beta_ladder(64, 0.2, 2.0), 5
+    steps = max(args.c4_steps, 10)
+    dt, eng = _pt_run(m, temps, steps, interval, 99, device, warm=5)
+    eng.close()
+    pdt, eng = _pt_run(m, temps, 4, interval, 99, device, warm=1, pt_path=3)
+    eng.close()
+    att = m.num_vars * 64.0 * len(temps)
+    return {"config": 4, "workload": "3D periodic +-J lattice L=64 (N=262144), 64 temperatures beta geometric "
+            "0.2..2.0, 64 replicas each, exchange every 5 sweeps",
+            "value": att * steps / dt, "unit": UNIT, "ms_per_step": dt / steps * 1e3,
+            "timed": f"{steps} of the 5000 sweeps (attempts/s is per step; the full run scales linearly)",
+            "plain": {"value": att * 4 / pdt, "ms_per_step": pdt / 4 * 1e3,
+                      "form": "one launch (one CTA) per temperature cell per step, in sequence"},
+            "batched_over_plain": (att * steps / dt) / (att * 4 / pdt),
+            "parity": _pt_parity(m, temps, 6, interval, 99, device, cores)}
 
 
 def run_serve(args, device):
@@ -494,6 +584,13 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config != 3:
+        ws, rank, local = dist_setup()
+        if rank == 0:
+            out = run_config(args.config, local, args)
+            out.update({"metric": METRIC, "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded)",
+                        "dtype": "i32"})
+            print(json.dumps(out))
     else:
         run_ours(args)
 
