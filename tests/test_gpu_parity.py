@@ -97,10 +97,11 @@ def test_pt_maxcut_exchange(interval, path):
 @pytest.mark.parametrize("path", PT_PATHS)
 def test_maxcut_800_pt32_interval10(path):
     """The G(n=800, m=19176) Max-Cut ladder: 32 temperatures, beta geometric
-    0.1..3.0, exchange every 10 sweeps (a shortened run)."""
+    0.1..3.0, exchange every 10 sweeps, 1000 of the 10^4 sweeps (the level
+    kernel's cells; 100 on the one-CTA kernel, 10x slower)."""
     m = I.maxcut_gnm(800, 19176, seed=42)
     temps = I.geometric_beta_ladder(32, 0.1, 3.0)
-    steps = 100
+    steps = 1000 if path == 2 else 100
     ref = O.run_schedule(m, np.tile(temps, (steps, 1)), 1337, exchange_interval=10,
                          collect_stats=True, threads=8)
     with Engine(m, num_temps=32, seed=1337, exchange_interval=10, pt_path=path) as eng:
@@ -203,14 +204,15 @@ def test_windowed_global_spins_random_graphs():
 
 def test_lattice_3d_L64_64_temperatures_full_size():
     """The 3D +-J lattice at full size (L=64, N=262144, 64 temperatures, beta
-    geometric 0.2..2.0, exchange every 5 sweeps) for 6 steps: spins,
+    geometric 0.2..2.0, exchange every 5 sweeps) for 100 steps: spins,
     energies, swap statistics and stream position equal the oracle's."""
     m = I.pm_j_lattice(64, 3, seed=64)
     temps = I.geometric_beta_ladder(64, 0.2, 2.0)
-    ref = O.run_schedule(m, np.tile(temps, (6, 1)), 99, exchange_interval=5, collect_stats=True, threads=16)
+    ref = O.run_schedule(m, np.tile(temps, (100, 1)), 99, exchange_interval=5, collect_stats=True, threads=16)
     with Engine(m, num_temps=64, seed=99, exchange_interval=5) as eng:
         eng.init_random()
-        eng.step(temps, 6)
+        eng.step(temps, 40)
+        eng.step(temps, 60)
         assert_same_run(eng, ref)
 
 
