@@ -63,10 +63,10 @@ def parse():
     p.add_argument("--threads-per-block", type=int, default=0)
     p.add_argument("--blocks-per-sm", type=int, default=0)
     p.add_argument("--no-serve", action="store_true")
-    p.add_argument("--serve-count", type=int, default=64)
-    p.add_argument("--serve-rate", type=float, default=20.0)
-    p.add_argument("--serve-sweeps", type=int, nargs=2, default=[100, 2000])
-    p.add_argument("--serve-budget", type=int, default=65536)
+    p.add_argument("--serve-count", type=int, default=128)
+    p.add_argument("--serve-rates", type=float, nargs="+", default=[100.0, 300.0, 1000.0])
+    p.add_argument("--serve-sweeps", type=int, nargs=2, default=[1000, 20000])
+    p.add_argument("--serve-budget", type=int, default=1 << 20)
     p.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 4],
                    help="3: the batched headline workload; 1, 2, 4: the PT configurations alone")
     p.add_argument("--no-configs", action="store_true", help="skip configs 1, 2, 4 in the headline line")
@@ -457,29 +457,33 @@ def run_config(cfg, device, args):
 
 
 def run_serve(args, device):
-    """Serving stream: Poisson arrivals at a fixed rate of SA requests with N
+    """Serving streams (config 5): Poisson arrivals of SA requests with N
     log-uniform in [100, 20000], degree 4..32, integer [-8, 8] or float32
-    N(0, 1) couplings (half each), SA lengths uniform in the given range; the
-    pool admits by device-memory footprint and ticks until all are done.
-    Latency = result taken - arrival, on the host clock."""
+    N(0, 1) couplings (half each), SA lengths uniform in [1000, 20000]
+    sweeps, at each of the given rates; the pool admits by device-memory
+    footprint and ticks until all are done. Latency = result taken - arrival,
+    on the host clock. Offered load = rate x mean attempts per request."""
     from ising_engine_b200 import instances as I
     from ising_engine_b200.serve import ServeEngine, serve_stream
     lo, hi = args.serve_sweeps
     reqs = I.serve_requests(args.serve_count, args.seed + 5, sweeps_min=lo, sweeps_max=hi)
     reqs = [(m, s, I.sa_temps(sw)) for (m, s, sw) in reqs]
     attempts = sum(m.num_vars * 64.0 * len(t) for m, _, t in reqs)
-    arrivals = I.poisson_arrivals(len(reqs), args.serve_rate, args.seed + 6)
+    rows = []
     with ServeEngine(device=device, site_budget=args.serve_budget) as srv:
         m0, s0, t0 = reqs[0]
         srv.submit(m0, s0, t0[:2])
         srv.run_all()  # warm-up: kernels loaded, pools touched
-        tr = serve_stream(srv, reqs, arrivals, keep_results=False)
-    s = tr.summary()
-    return {"p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"], "mean_ms": s["mean_ms"],
-            "rate_req_per_s": args.serve_rate, "requests": s["requests"],
-            "attempts_per_s": attempts / s["makespan_s"], "makespan_s": s["makespan_s"],
-            "ticks": s["ticks"], "mean_tick_ms": s["mean_tick_ms"], "gpu_launches": tr.launches,
-            "site_budget": args.serve_budget,
+        for k, rate in enumerate(args.serve_rates):
+            arrivals = I.poisson_arrivals(len(reqs), rate, args.seed + 6 + k)
+            tr = serve_stream(srv, reqs, arrivals, keep_results=False)
+            s = tr.summary()
+            rows.append({"rate_req_per_s": rate, "offered_attempts_per_s": rate * attempts / len(reqs),
+                         "attempts_per_s": attempts / s["makespan_s"], "p50_ms": s["p50_ms"],
+                         "p99_ms": s["p99_ms"], "mean_ms": s["mean_ms"], "makespan_s": s["makespan_s"],
+                         "ticks": s["ticks"], "mean_tick_ms": s["mean_tick_ms"], "gpu_launches": tr.launches})
+    return {"rates": rows, "requests": len(reqs), "site_budget": args.serve_budget,
+            "mean_attempts_per_request": attempts / len(reqs),
             "stream": f"N log-uniform [100, 20000], degree 4..32, int [-8,8] / f32 N(0,1) half each, "
                       f"SA {lo}..{hi} sweeps (beta 0.1 -> 5.0), Poisson arrivals"}
 

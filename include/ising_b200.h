@@ -304,6 +304,7 @@ typedef struct ie_serve_config {
     uint64_t max_sites;          /* summed num_vars of resident requests (0: 2^24) */
     uint64_t max_couplings;      /* summed stored couplings, both triangles (0: 2^27) */
     uint64_t max_schedule_steps; /* summed schedule lengths (0: 2^25) */
+    int32_t kernel_form;         /* 0: the level kernel (default); 1: the per-lane kernels */
 } ie_serve_config;
 
 ie_status ie_serve_create(const ie_serve_config* config, ie_serve** out);

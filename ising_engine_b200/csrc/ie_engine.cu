@@ -1708,11 +1708,12 @@ struct ServeReq {
     std::vector<uint8_t> clampf;
     std::vector<int8_t> clampv;
     std::vector<uint32_t> recs, wtab, draw_idx;
+    std::vector<uint32_t> lrecs, lrecoff, lv_sites, lv_off;  // level kernel: records, offsets, levels
     uint32_t unclamped = 0;
     uint64_t wrec = 0;  // offset of the windowed record stream within recs
     std::vector<double> temps;
     uint32_t key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    uint64_t slot = 0, o_row = 0, o_site = 0, o_ent = 0, o_rec = 0, o_win = 0, o_sched = 0;
+    uint64_t slot = 0, o_row = 0, o_site = 0, o_ent = 0, o_rec = 0, o_win = 0, o_sched = 0, o_lrec = 0;
     uint64_t done = 0;  // steps executed (host mirror of DevArrays::done)
     std::vector<uint64_t> words;
     std::vector<double> energies;
@@ -1725,15 +1726,21 @@ struct ServeReq {
 struct ServeEngine {
     Engine eng;
     ie_serve_config cfg{};
-    RangeAlloc a_slot, a_row, a_site, a_ent, a_rec, a_win, a_sched;
+    RangeAlloc a_slot, a_row, a_site, a_ent, a_rec, a_win, a_sched, a_lrec;
     std::mutex mu;  // guards pending, finished, next_id
     std::deque<std::unique_ptr<ServeReq>> pending;
     std::vector<std::unique_ptr<ServeReq>> slots;
     std::map<uint64_t, std::unique_ptr<ServeReq>> finished;
     uint64_t next_id = 1;
     uint32_t n_active = 0;
+    bool set_changed = true;     // a request was admitted or retired since the work items were built
+    std::vector<uint32_t> unit;  // per slot: sites one unit of the site budget covers
 
-    uint64_t rec_cap() const { return 8 * cfg.max_sites + 4 * cfg.max_couplings + kChunk; }
+    bool level() const { return cfg.kernel_form == 0; }
+    uint64_t rec_cap() const { return level() ? 0 : 8 * cfg.max_sites + 4 * cfg.max_couplings + kChunk; }
+    // level records: 4 header words per site, then per coupling one word
+    // (integer) or three (f64), rows padded to 4
+    uint64_t lrec_cap() const { return level() ? 13 * cfg.max_sites + 3 * cfg.max_couplings + 4 : 0; }
     uint64_t win_cap() const { return (uint64_t)kWT * ((cfg.max_sites + kWin - 1) / kWin + cfg.max_requests); }
 
     ie_status create(const ie_serve_config* c) {
@@ -1746,7 +1753,9 @@ struct ServeEngine {
         if (cfg.max_sites >= (1ull << 32) || cfg.max_couplings >= (1ull << 32))
             return fail(IE_ERR_INVALID, "max_sites and max_couplings must be below 2^32");
         IE_TRY(eng.setup_device(cfg.device));
-        eng.kernel_form = 1;
+        if (cfg.kernel_form < 0 || cfg.kernel_form > 1) return fail(IE_ERR_INVALID, "kernel_form must be 0 or 1");
+        eng.kernel_form = cfg.kernel_form;
+        eng.serving = true;
         const uint32_t S = cfg.max_requests;
         eng.nt = 1;
         eng.count = S;
@@ -1772,7 +1781,14 @@ struct ServeEngine {
         IE_TRY(eng.d_cols.alloc(std::max<uint64_t>(cfg.max_couplings, 1)));
         IE_TRY(eng.d_vals.alloc(std::max<uint64_t>(cfg.max_couplings, 1)));
         IE_TRY(eng.d_recs.alloc(rec_cap() + kChunk));
-        IE_TRY(eng.d_wtab.alloc(win_cap()));
+        IE_TRY(eng.d_wtab.alloc(level() ? 1 : win_cap()));
+        if (level()) {
+            IE_TRY(eng.d_lrecs.alloc(lrec_cap()));
+            IE_TRY(eng.d_recoff.alloc(cfg.max_sites));
+            eng.h_recoff.assign(cfg.max_sites, 0);
+            eng.lv_sites.assign(S, {});
+            eng.lv_off.assign(S, {});
+        }
         IE_TRY(eng.d_temps.alloc(cfg.max_schedule_steps));
         IE_TRY(eng.d_att.alloc(1));
         IE_TRY(eng.d_acc.alloc(1));
@@ -1785,8 +1801,9 @@ struct ServeEngine {
         a_site.reset(cfg.max_sites);
         a_ent.reset(cfg.max_couplings);
         a_rec.reset(rec_cap());
-        a_win.reset(win_cap());
+        a_win.reset(level() ? 0 : win_cap());
         a_sched.reset(cfg.max_schedule_steps);
+        a_lrec.reset(lrec_cap());
         slots.resize(S);
         eng.initialized = true;
         eng.recs_dirty = false;
@@ -1818,14 +1835,22 @@ struct ServeEngine {
             if (!r.clampf[v]) c++;
         }
         r.unclamped = c;
-        uint64_t off = 0, len = 0;
-        IE_TRY(build_records(r.h, r.clampf, 0, r.recs, off, len));
-        IE_TRY(window_records(r.h, r.clampf, 0, r.recs, 0, r.wrec));
-        window_table(r.h, r.wtab);
+        if (level()) {
+            const LvlSource src = Engine::lvl_source(r.h, r.clampf.data());
+            r.lrecoff.assign(n, 0);
+            level_records(src, r.lrecs, r.lrecoff.data());
+            site_levels(src, r.lv_sites, r.lv_off);
+        } else {
+            uint64_t off = 0, len = 0;
+            IE_TRY(build_records(r.h, r.clampf, 0, r.recs, off, len));
+            IE_TRY(window_records(r.h, r.clampf, 0, r.recs, 0, r.wrec));
+            window_table(r.h, r.wtab);
+        }
         chacha_key_from_u64(seed, r.key);
         // capacity checks: the request alone must fit every pool and the
         // shared memory of the kernels that can run it
         if (n + 1 > a_row.cap || n > a_site.cap || r.h.nnz > a_ent.cap || r.recs.size() > a_rec.cap ||
+            r.lrecs.size() > a_lrec.cap ||
             r.wtab.size() > a_win.cap || n_steps > a_sched.cap)
             return fail(IE_ERR_OOM, "request exceeds the serving engine's capacity");
         return IE_OK;
@@ -1833,7 +1858,8 @@ struct ServeEngine {
 
     static uint64_t bytes_of(const ServeReq& r) {
         const uint64_t n = r.h.n;
-        return (n + 1) * 4 + n * (8 + 4 + 1 + 1 + 4 + 8) + r.h.nnz * (4 + 4 + 8) + r.recs.size() * 4 +
+        return (n + 1) * 4 + n * (8 + 4 + 1 + 1 + 4 + 8 + 4) + r.h.nnz * (4 + 4 + 8) + r.recs.size() * 4 +
+               r.lrecs.size() * 4 +
                r.wtab.size() * 4 + r.temps.size() * 8 + sizeof(InstDesc) + 32 + 8 + 4 + 8 + 4 +
                kReplicas * (4 + 8);
     }
@@ -1841,14 +1867,14 @@ struct ServeEngine {
     // Reserves every pool range of r; all or nothing.
     bool place(ServeReq& r) {
         const uint64_t n = r.h.n;
-        uint64_t o[7];
-        RangeAlloc* al[7] = {&a_slot, &a_row, &a_site, &a_ent, &a_rec, &a_win, &a_sched};
-        const uint64_t len[7] = {1, n + 1, n, r.h.nnz, r.recs.size(), r.wtab.size(), r.temps.size()};
-        const uint64_t align[7] = {1, 4, 4, 4, kChunk, 4, 2};
+        uint64_t o[8];
+        RangeAlloc* al[8] = {&a_slot, &a_row, &a_site, &a_ent, &a_rec, &a_win, &a_sched, &a_lrec};
+        const uint64_t len[8] = {1, n + 1, n, r.h.nnz, r.recs.size(), r.wtab.size(), r.temps.size(), r.lrecs.size()};
+        const uint64_t align[8] = {1, 4, 4, 4, kChunk, 4, 2, 4};
         int k = 0;
-        for (; k < 7; k++)
+        for (; k < 8; k++)
             if (!al[k]->alloc(len[k], align[k], o[k])) break;
-        if (k < 7) {
+        if (k < 8) {
             for (int j = 0; j < k; j++) al[j]->release(o[j], len[j]);
             return false;
         }
@@ -1859,6 +1885,7 @@ struct ServeEngine {
         r.o_rec = o[4];
         r.o_win = o[5];
         r.o_sched = o[6];
+        r.o_lrec = o[7];
         return true;
     }
 
@@ -1871,6 +1898,7 @@ struct ServeEngine {
         a_rec.release(r.o_rec, r.recs.size());
         a_win.release(r.o_win, r.wtab.size());
         a_sched.release(r.o_sched, r.temps.size());
+        a_lrec.release(r.o_lrec, r.lrecs.size());
     }
 
     template <typename T>
@@ -1924,6 +1952,14 @@ struct ServeEngine {
         IE_TRY(put(eng.d_recs.p, r.o_rec, r.recs.data(), r.recs.size()));
         IE_TRY(put(eng.d_wtab.p, r.o_win, r.wtab.data(), r.wtab.size()));
         IE_TRY(put(eng.d_temps.p, r.o_sched, r.temps.data(), r.temps.size()));
+        if (level()) {
+            IE_TRY(put(eng.d_lrecs.p, r.o_lrec, r.lrecs.data(), r.lrecs.size()));
+            const uint32_t b16 = (uint32_t)(r.o_lrec / 4);
+            for (uint32_t v = 0; v < h.n; v++) eng.h_recoff[r.o_site + v] = r.lrecoff[v] + b16;
+            IE_TRY(put(eng.d_recoff.p, r.o_site, eng.h_recoff.data() + r.o_site, h.n));
+            eng.lv_sites[s] = r.lv_sites;
+            eng.lv_off[s] = r.lv_off;
+        }
         IE_TRY(put(eng.d_keys.p, 8 * (uint64_t)s, r.key, 8));
         IE_TRY(put(eng.d_unclamped.p, s, &r.unclamped, 1));
         IE_TRY(put(eng.d_desc.p, s, &d, 1));
@@ -1963,6 +1999,10 @@ struct ServeEngine {
         r.h = HostInst();
         r.recs.clear();
         r.wtab.clear();
+        r.lrecs.clear();
+        r.lrecoff.clear();
+        r.lv_sites.clear();
+        r.lv_off.clear();
         r.temps.clear();
         r.clampf.clear();
         r.clampv.clear();
@@ -1990,11 +2030,21 @@ struct ServeEngine {
         for (ServeReq* r : admitted) {
             IE_TRY(upload(*r));
             n_active++;
+            set_changed = true;
         }
         eng.last_ms = 0.0;
         eng.last_launches = 0;
         if (n_active) {
-            IE_TRY(eng.build_quads());
+            if (set_changed || !eng.quads_built) {
+                // the resident set changed: new work items, and per slot the
+                // sites one budget unit covers (its item's sites on the level
+                // kernel, its own on the per-lane kernels)
+                IE_TRY(eng.build_quads());
+                unit.assign(cfg.max_requests, 0);
+                for (const LvlItem& it : eng.lvh.items)
+                    for (uint32_t k = 0; k < it.nmem; k++) unit[eng.lvh.members[it.mem0 + k].inst] = it.sites;
+                set_changed = false;
+            }
             RunArgs R{};
             R.temps = eng.d_temps.p;
             R.temps_per_step = 1;
@@ -2007,12 +2057,14 @@ struct ServeEngine {
                 if (!slots[s] || !eng.active[s]) continue;
                 ServeReq& r = *slots[s];
                 const uint64_t left = r.temps.size() - r.done;
-                const uint64_t want = std::max<uint64_t>(1, cfg.site_budget / std::max<uint32_t>(r.h.n, 1));
+                const uint32_t u = unit[s] ? unit[s] : r.h.n;
+                const uint64_t want = std::max<uint64_t>(1, cfg.site_budget / std::max<uint32_t>(u, 1));
                 r.done += std::min(left, want);
                 if (r.done == r.temps.size()) {
                     IE_TRY(retire(slots[s]));
                     slots[s].reset();
                     n_active--;
+                    set_changed = true;
                 }
             }
         }

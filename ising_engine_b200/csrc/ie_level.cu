@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
         for (uint32_t k = tid; k < I.nmem; k += T) {
             const LvlMember mb = L.members[I.mem0 + k];
             const InstDesc d = A.desc[mb.inst];
-            const StepPlan P = step_plan(A, R, d, mb.inst);
+            const StepPlan P = step_plan(A, R, d, mb.inst, I.sites);
             LvlMem& m = ms[k];
             m.temps = P.temps;
             m.tstride = P.tstride;
