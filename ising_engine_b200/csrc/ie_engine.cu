@@ -709,6 +709,7 @@ struct Engine {
         // level-kernel class: items of the shared item arrays in launch order
         bool level = false;
         bool gsp = false;
+        uint32_t split = 1;  // CTAs per cluster (one item per cluster)
         uint32_t ntab = 1;
         int grid = 0;
         uint64_t keystride = 0, keyoff = 0;
@@ -765,6 +766,7 @@ struct Engine {
     uint32_t lvl_cap = 4096;  // spin words per item (shared memory)
     int lvl_threads = 256;
     uint32_t lvl_tie_shift = 0;
+    bool lvl_split = true;    // large single-member items on thread block clusters
     bool serving = false;     // serving launches: one threshold table per member
     std::vector<std::vector<uint32_t>> lv_sites, lv_off;  // per instance: sites by level, level starts
     std::vector<uint32_t> h_recoff;                       // level-record offset per site
@@ -872,6 +874,17 @@ struct Engine {
         for (int m = 0; m < 2; m++)
             for (int g = 0; g < 2; g++) {
                 if (mem[m][g].empty()) continue;
+                // spins in global memory: few large items spread over clusters
+                // of up to 8 CTAs while that keeps every SM busy
+                uint32_t split = 1;
+                const size_t smem0 = level_smem(m ? kModeF64 : kModeInt, own ? (one_per_item ? 1u : kLvlMaxOwnTables) : 1u,
+                                                0);
+                if (g && !one_per_item && lvl_split && !(cells_view && pt_path == 3)) {
+                    const int occ1 = level_occupancy(m ? kModeF64 : kModeInt, true, lvl_threads, smem0);
+                    while (split < 8 && (uint64_t)mem[m][g].size() * split * 2 <= (uint64_t)occ1 * g_sm_count) split *= 2;
+                    while (split > 1 && level_clusters(m ? kModeF64 : kModeInt, lvl_threads, smem0, split) <= 0)
+                        split /= 2;
+                }
                 std::unique_ptr<WorkClass> wc(new WorkClass());
                 wc->level = true;
                 wc->mode = m ? kModeF64 : kModeInt;
@@ -884,8 +897,8 @@ struct Engine {
                 const uint32_t maxmem = one_per_item ? 1u : own ? kLvlMaxOwnTables : kLvlMaxMembers;
                 std::vector<uint32_t> order;
                 double longest = 0;
-                build_level_items(D, nnz_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem, lvh, order,
-                                  longest);
+                build_level_items(D, nnz_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem, split, lvh,
+                                  order, longest);
                 wc->nitems = (uint32_t)order.size();
                 wc->work = longest;
                 for (uint32_t i : mem[m][g]) wc->site_steps += (double)D[i].n;
@@ -894,10 +907,16 @@ struct Engine {
                 int occ = level_occupancy(wc->mode, g != 0, lvl_threads, smem);
                 if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "level kernel does not fit on an SM");
                 if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
-                wc->grid = std::max(1, std::min<int>((int)wc->nitems, occ * g_sm_count));
+                wc->split = split;
+                if (split > 1) {
+                    const int nc = level_clusters(wc->mode, lvl_threads, smem, split);
+                    wc->grid = (int)split * std::max(1, std::min<int>((int)wc->nitems, nc));
+                } else {
+                    wc->grid = std::max(1, std::min<int>((int)wc->nitems, occ * g_sm_count));
+                }
                 wc->keystride = 64ull * (g ? maxn : lvl_cap);
                 wc->keyoff = keytotal;
-                keytotal += wc->keystride * (uint64_t)wc->grid;
+                keytotal += wc->keystride * (uint64_t)(wc->grid / split);
                 IE_TRY(wc->order.upload(order, stream));
                 classes.push_back(std::move(wc));
             }
@@ -1216,7 +1235,7 @@ struct Engine {
                 launches--;
             } else if (wc.level)
                 IE_CUDA(launch_level(A, R, level_args(wc, d_queue.p + k), wc.mode, wc.gsp, lvl_threads, grids[k],
-                                     cstreams[k]));
+                                     cstreams[k], wc.split));
             else if (wc.tpl == 8) IE_CUDA(launch_window(A, R, wc.mode, wc.cap, grids[k], cstreams[k]));
             else if (wc.tpl == kChain) IE_CUDA(launch_chain(A, R, wc.mode, wc.cap, grids[k], cstreams[k]));
             else IE_CUDA(launch_batch(A, R, wc.mode, wc.tpl, wc.cap, grids[k], cstreams[k]));

@@ -41,8 +41,10 @@ cudaError_t launch_one_opt(const DevArrays& A, uint32_t inst, int8_t* state, con
                            double* improvement, uint64_t* flips, uint64_t max_flips, cudaStream_t st);
 size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap);
 int level_occupancy(uint32_t mode, bool gsp, int threads, size_t smem);
+// resident clusters of `split` CTAs of the split (cluster) form, GPU-wide
+int level_clusters(uint32_t mode, int threads, size_t smem, uint32_t split);
 cudaError_t launch_level(const DevArrays& A, const RunArgs& R, const LvlArgs& L, uint32_t mode, bool gsp, int threads,
-                         int grid, cudaStream_t st);
+                         int grid, cudaStream_t st, uint32_t split = 1);
 void set_last_error(const char* msg);
 cudaError_t probe_peaks(int sm_count, double* int_ops_per_s, double* xoshiro_per_s);
 }  // namespace ie

@@ -29,12 +29,15 @@
 // request's schedule) they are computed from the spins, integer exactly and
 // f64 in the reference's summation order (engine.rs:333-368), which is the
 // value the reference's periodic re-sync (ultimate.rs:316-324) takes.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "ie_device.cuh"
 #include "ie_kernels.cuh"
 #include "ie_level.cuh"
 #include "ie_sweep.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace ie {
 
@@ -76,6 +79,18 @@ __device__ __forceinline__ LvlEntry load_entry(const LvlEntry* p) {
 
 __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// A spin byte; CG: from L2 (another CTA of the cluster may have written it).
+template <bool CG>
+__device__ __forceinline__ uint32_t ld_spin(const uint8_t* p) {
+    if constexpr (CG) {
+        uint32_t v;
+        asm volatile("ld.global.cg.u8 %0, [%1];" : "=r"(v) : "l"(p));
+        return v;
+    } else {
+        return *p;
+    }
 }
 
 __device__ __forceinline__ float ex2_approx(float a) {
@@ -137,13 +152,14 @@ __device__ __noinline__ uint32_t exact_flips_f64(uint32_t ties, uint64_t base, i
 // Integer energies of one member (hubo.rs:176-189 restricted to QUBO, each
 // edge once from its lower end): thread (site, lane) adds x_v (lin_v +
 // sum_{j > v} w x_j) for its 8 replicas, by SWAR byte sums as in the sweep.
+template <bool CG>
 __device__ __forceinline__ void member_energy_int(const LvlArgs& L, const LvlMem& m, const uint8_t* spb,
                                                   const uint2* lut, int tid, int T, int32_t* sE) {
     int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t i = tid; i < 8u * m.n; i += T) {
         const uint32_t v = i >> 3;
         const uint32_t f = m.flat + v;
-        const uint32_t xb = spb[8u * f];
+        const uint32_t xb = ld_spin<CG>(spb + 8u * f);
         if (!xb) continue;
         const uint32_t* rec = L.lrecs + 4ull * __ldg(L.recoff + m.site + v);
         const uint4 hd = __ldg(reinterpret_cast<const uint4*>(rec));
@@ -160,7 +176,7 @@ __device__ __forceinline__ void member_energy_int(const LvlArgs& L, const LvlMem
                 const uint32_t col = en[e] & 0xFFFFFFu;
                 const uint32_t w = (en[e] >> 24) & 0x7Fu;
                 if (col > v && w) {
-                    const uint2 sv = lut[spb[8u * (m.flat + col)] | ((en[e] >> 23) & 0x100u)];
+                    const uint2 sv = lut[ld_spin<CG>(spb + 8u * (m.flat + col)) | ((en[e] >> 23) & 0x100u)];
                     aL += w * sv.x;
                     aH += w * sv.y;
                     if (en[e] >> 31) nsum += (int)w;
@@ -180,6 +196,7 @@ __device__ __forceinline__ void member_energy_int(const LvlArgs& L, const LvlMem
 // f64 energies of one (member, lane): calculate_replica_energies_local
 // (engine.rs:333-368) in its order: site order, lin then the CSR entries with
 // v < j, each added with one rounding.
+template <bool CG>
 __device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uint8_t* spb, double* out) {
     const InstDesc d = A.desc[m.inst];
     const uint32_t* rows = A.rows + d.row;
@@ -190,7 +207,7 @@ __device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uin
 #pragma unroll
     for (int k = 0; k < 8; k++) E[k] = 0.0;
     for (uint32_t v = 0; v < d.n; v++) {
-        const uint32_t xb = spb[8u * (m.flat + v)];
+        const uint32_t xb = ld_spin<CG>(spb + 8u * (m.flat + v));
         if (!xb) continue;
         const double wl = lin[v];
 #pragma unroll
@@ -199,7 +216,7 @@ __device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uin
         for (uint32_t e = rows[v]; e < rows[v + 1]; e++) {
             const uint32_t j = cols[e];
             if (v < j) {
-                const uint32_t mk = xb & spb[8u * (m.flat + j)];
+                const uint32_t mk = xb & ld_spin<CG>(spb + 8u * (m.flat + j));
                 if (mk) {
                     const double w = vals[e];
 #pragma unroll
@@ -213,7 +230,11 @@ __device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uin
     for (int k = 0; k < 8; k++) out[8 * k] = E[k];
 }
 
-template <uint32_t MODE, bool GSP>
+// SPLIT: the item (one member, spins in global memory) is run by a thread
+// block cluster; CTA r of C generates and decides the sites of segments s
+// with s % C == r, reads spins from L2 and meets the other CTAs at a cluster
+// barrier (release / acquire) after every level.
+template <uint32_t MODE, bool GSP, bool SPLIT>
 __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
     extern __shared__ __align__(16) uint64_t dsm[];
     __shared__ LvlMem ms[kLvlMaxMembers];
@@ -226,7 +247,13 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
     uint32_t* const tabs = reinterpret_cast<uint32_t*>(dsm);
     uint2* const lut = reinterpret_cast<uint2*>(tabs + (size_t)L.ntab * kLvlTab);
     uint64_t* const ssw = reinterpret_cast<uint64_t*>(lut + (MODE == kModeInt ? 512 : 0));
-    uint32_t* const kb = L.keybuf + (size_t)blockIdx.x * L.keystride;
+    uint32_t crank = 0, csize = 1;
+    if constexpr (SPLIT) {
+        crank = cg::this_cluster().block_rank();
+        csize = cg::this_cluster().num_blocks();
+    }
+    // one output buffer per CTA, or per cluster (its CTAs write disjoint segments)
+    uint32_t* const kb = L.keybuf + (size_t)(blockIdx.x / csize) * L.keystride;
     if constexpr (MODE == kModeInt) {
         // spread table: entry b (256 + b for a negative coupling, which
         // contributes |w| (1 - x_j)) holds bit k of b (~b) in byte k
@@ -236,17 +263,31 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
         }
     }
     for (;;) {
-        __syncthreads();
-        if (tid == 0) {
-            const uint32_t q = atomicAdd(L.queue, 1u);
-            s_item = q < L.nitems ? L.order[q] : 0xffffffffu;
+        uint32_t it;
+        if constexpr (SPLIT) {
+            // the cluster's first CTA takes the item, the others read it from
+            // its shared memory
+            cg::this_cluster().sync();
+            if (crank == 0 && tid == 0) {
+                const uint32_t q = atomicAdd(L.queue, 1u);
+                s_item = q < L.nitems ? L.order[q] : 0xffffffffu;
+            }
+            cg::this_cluster().sync();
+            it = *cg::this_cluster().map_shared_rank(&s_item, 0);
+        } else {
+            __syncthreads();
+            if (tid == 0) {
+                const uint32_t q = atomicAdd(L.queue, 1u);
+                s_item = q < L.nitems ? L.order[q] : 0xffffffffu;
+            }
+            __syncthreads();
+            it = s_item;
         }
-        __syncthreads();
-        const uint32_t it = s_item;
         if (it == 0xffffffffu) break;
         const LvlItem I = L.items[it];
         if ((!GSP && I.sites > L.spin_cap) || I.nmem > kLvlMaxMembers || I.nmem == 0 ||
-            (own_tab && I.nmem > L.ntab) || (uint64_t)I.sites * 64 > L.keystride || (GSP && I.nmem != 1)) {
+            (own_tab && I.nmem > L.ntab) || (uint64_t)I.sites * 64 > L.keystride || (GSP && I.nmem != 1) ||
+            I.split != csize) {
             if (tid == 0) atomicExch(A.err, 2);  // host sizing error: report, skip the item
             continue;
         }
@@ -305,9 +346,11 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     if (s < ms[k].steps) tabs[k * kLvlTab + idx] = q_threshold((int)idx - H, ms[k].beta);
                 }
             }
-            // generator phase: chain c = (segment c / 8, lane c % 8)
-            for (uint32_t c = tid; c < 8u * I.nseg; c += T) {
-                const uint32_t sd = __ldg(L.segs + I.seg0 + (c >> 3));
+            // generator phase: chain j = (this CTA's segment j / 8, lane j % 8)
+            for (uint32_t j = tid;; j += T) {
+                const uint32_t sg = crank + csize * (j >> 3);
+                if (sg >= I.nseg) break;
+                const uint32_t sd = __ldg(L.segs + I.seg0 + sg);
                 const uint32_t slot = sd >> 24, seg = sd & 0xFFFFFFu;
                 const LvlMem& m = ms[slot];
                 if (s >= m.steps) continue;
@@ -330,11 +373,11 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
             // thread loads its first entry of the next level and prefetches
             // that site's record and outputs (read-only during the phase)
             const uint32_t sh = L.tie_shift;
-            uint32_t e1 = I.nlvl ? __ldg(L.lvloff + I.lvl0) : 0u;
+            // this CTA's entries of level l: lvloff[lvl0 + l C + r .. + 1]
+            const uint32_t* const lo = L.lvloff + I.lvl0 + crank;
+            uint32_t e0 = I.nlvl ? __ldg(lo) : 0u, e1 = I.nlvl ? __ldg(lo + 1) : 0u;
             LvlEntry nxt{0, 0};
             for (uint32_t l = 0; l < I.nlvl; l++) {
-                const uint32_t e0 = e1;
-                e1 = __ldg(L.lvloff + I.lvl0 + l + 1);
                 for (uint32_t i = tid; i < 8u * (e1 - e0); i += T) {
                     const LvlEntry en = (i == (uint32_t)tid && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + (i >> 3));
                     const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
@@ -345,7 +388,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     const uint4 hd = __ldg(reinterpret_cast<const uint4*>(rec));
                     const uint32_t deg = hd.x & 0x7FFFFFFFu;
                     const uint32_t fb = m.flat;
-                    const uint32_t xb = spb[8u * f];
+                    const uint32_t xb = ld_spin<SPLIT>(spb + 8u * f);
                     const uint4* kp = reinterpret_cast<const uint4*>(kb + (size_t)f * 64 + lane * 8);
                     const uint4 k0 = kp[0], k1 = kp[1];
                     const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
@@ -360,7 +403,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                             uint32_t li[4];
 #pragma unroll
                             for (int e = 0; e < 4; e++)
-                                li[e] = spb[8u * (fb + (en[e] & 0xFFFFFFu))] | ((en[e] >> 23) & 0x100u);
+                                li[e] = ld_spin<SPLIT>(spb + 8u * (fb + (en[e] & 0xFFFFFFu))) | ((en[e] >> 23) & 0x100u);
 #pragma unroll
                             for (int e = 0; e < 4; e++) {
                                 const uint2 sv = lut[li[e]];
@@ -410,7 +453,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                             const double ww[4] = {w01.x, w01.y, w23.x, w23.y};
                             uint32_t bj[4];
 #pragma unroll
-                            for (int e = 0; e < 4; e++) bj[e] = spb[8u * (fb + cc[e])];
+                            for (int e = 0; e < 4; e++) bj[e] = ld_spin<SPLIT>(spb + 8u * (fb + cc[e]));
 #pragma unroll
                             for (int e = 0; e < 4; e++) {
                                 if (q + e < deg) {
@@ -439,15 +482,22 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     spb[8u * f] = (uint8_t)(xb ^ flips);
                 }
                 if (l + 1 < I.nlvl) {
-                    const uint32_t e2 = __ldg(L.lvloff + I.lvl0 + l + 2);
-                    if ((uint32_t)tid < 8u * (e2 - e1)) {
-                        nxt = load_entry(L.entries + I.ent0 + e1 + (tid >> 3));
+                    e0 = __ldg(lo + (l + 1) * csize);
+                    e1 = __ldg(lo + (l + 1) * csize + 1);
+                    if ((uint32_t)tid < 8u * (e1 - e0)) {
+                        nxt = load_entry(L.entries + I.ent0 + e0 + (tid >> 3));
                         prefetch_l1(L.lrecs + 4ull * nxt.rec);
                         prefetch_l1(kb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64 + lane * 8);
                     }
                 }
-                __syncthreads();
+                if constexpr (SPLIT) cg::this_cluster().sync();
+                else __syncthreads();
             }
+        }
+        if constexpr (SPLIT) {
+            // every CTA's last level is done; the first CTA finishes the item
+            cg::this_cluster().sync();
+            if (crank != 0) continue;
         }
         __syncthreads();
         // energies, spins and stream state of every member
@@ -457,7 +507,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
             if constexpr (MODE == kModeInt) {
                 if (tid < kReplicas) sE[tid] = 0;
                 __syncthreads();
-                member_energy_int(L, m, spb, lut, tid, T, sE);
+                member_energy_int<SPLIT>(L, m, spb, lut, tid, T, sE);
                 __syncthreads();
                 if (tid < kReplicas) A.Ei[m.energy + tid] = sE[tid];
             }
@@ -466,7 +516,8 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
             for (uint32_t p = tid; p < 8u * I.nmem; p += T) {
                 const LvlMem& m = ms[p >> 3];
                 if (!m.fin || m.steps == 0) continue;
-                member_energy_f64(A, m, reinterpret_cast<const uint8_t*>(sw) + (p & 7), A.Ef + m.energy + (p & 7));
+                member_energy_f64<SPLIT>(A, m, reinterpret_cast<const uint8_t*>(sw) + (p & 7),
+                                         A.Ef + m.energy + (p & 7));
             }
         }
         if (!GSP) {
@@ -486,39 +537,79 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
     }
 }
 
-template __global__ void level_kernel<kModeInt, false>(DevArrays, RunArgs, LvlArgs);
-template __global__ void level_kernel<kModeInt, true>(DevArrays, RunArgs, LvlArgs);
-template __global__ void level_kernel<kModeF64, false>(DevArrays, RunArgs, LvlArgs);
-template __global__ void level_kernel<kModeF64, true>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeInt, false, false>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeInt, true, false>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeInt, true, true>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeF64, false, false>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeF64, true, false>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModeF64, true, true>(DevArrays, RunArgs, LvlArgs);
 
 size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap) {
     return (size_t)ntab * kLvlTab * 4 + (mode == kModeInt ? 512 * 8 : 0) + (size_t)spin_cap * 8;
 }
 
-template <uint32_t MODE, bool GSP>
-static int level_occ_of(int threads, size_t smem) {
-    auto k = level_kernel<MODE, GSP>;
+template <uint32_t MODE, bool GSP, bool SPLIT>
+static void* level_fn() {
+    return reinterpret_cast<void*>(level_kernel<MODE, GSP, SPLIT>);
+}
+
+static void* level_fn_of(uint32_t mode, bool gsp, bool split) {
+    if (mode == kModeInt)
+        return split ? level_fn<kModeInt, true, true>() : gsp ? level_fn<kModeInt, true, false>()
+                                                              : level_fn<kModeInt, false, false>();
+    return split ? level_fn<kModeF64, true, true>() : gsp ? level_fn<kModeF64, true, false>()
+                                                          : level_fn<kModeF64, false, false>();
+}
+
+static cudaLaunchConfig_t level_config(int grid, int threads, size_t smem, cudaStream_t st, uint32_t split,
+                                       cudaLaunchAttribute* attr) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr->id = cudaLaunchAttributeClusterDimension;
+    attr->val.clusterDim.x = split;
+    attr->val.clusterDim.y = 1;
+    attr->val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+int level_occupancy(uint32_t mode, bool gsp, int threads, size_t smem) {
+    const void* k = level_fn_of(mode, gsp, false);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) return 0;
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess) return 0;
     return occ;
 }
 
-int level_occupancy(uint32_t mode, bool gsp, int threads, size_t smem) {
-    if (mode == kModeInt)
-        return gsp ? level_occ_of<kModeInt, true>(threads, smem) : level_occ_of<kModeInt, false>(threads, smem);
-    return gsp ? level_occ_of<kModeF64, true>(threads, smem) : level_occ_of<kModeF64, false>(threads, smem);
+int level_clusters(uint32_t mode, int threads, size_t smem, uint32_t split) {
+    const void* k = level_fn_of(mode, true, true);
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) return 0;
+    cudaLaunchAttribute attr;
+    cudaLaunchConfig_t cfg = level_config((int)split, threads, smem, nullptr, split, &attr);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) return 0;
+    return n;
 }
 
 cudaError_t launch_level(const DevArrays& A, const RunArgs& R, const LvlArgs& L, uint32_t mode, bool gsp, int threads,
-                         int grid, cudaStream_t st) {
+                         int grid, cudaStream_t st, uint32_t split) {
     const size_t smem = level_smem(mode, L.ntab, gsp ? 0 : L.spin_cap);
+    if (split > 1) {
+        cudaLaunchAttribute attr;
+        const cudaLaunchConfig_t cfg = level_config(grid, threads, smem, st, split, &attr);
+        if (mode == kModeInt) return cudaLaunchKernelEx(&cfg, level_kernel<kModeInt, true, true>, A, R, L);
+        return cudaLaunchKernelEx(&cfg, level_kernel<kModeF64, true, true>, A, R, L);
+    }
     if (mode == kModeInt) {
-        if (gsp) level_kernel<kModeInt, true><<<grid, threads, smem, st>>>(A, R, L);
-        else level_kernel<kModeInt, false><<<grid, threads, smem, st>>>(A, R, L);
+        if (gsp) level_kernel<kModeInt, true, false><<<grid, threads, smem, st>>>(A, R, L);
+        else level_kernel<kModeInt, false, false><<<grid, threads, smem, st>>>(A, R, L);
     } else {
-        if (gsp) level_kernel<kModeF64, true><<<grid, threads, smem, st>>>(A, R, L);
-        else level_kernel<kModeF64, false><<<grid, threads, smem, st>>>(A, R, L);
+        if (gsp) level_kernel<kModeF64, true, false><<<grid, threads, smem, st>>>(A, R, L);
+        else level_kernel<kModeF64, false, false><<<grid, threads, smem, st>>>(A, R, L);
     }
     return cudaGetLastError();
 }

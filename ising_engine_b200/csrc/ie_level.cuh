@@ -35,6 +35,8 @@ struct LvlItem {
     uint32_t sites;  // flat spin words of the item
     int32_t H;       // integer mode: largest H of the members
     uint32_t gsp;    // 1: one member whose spins stay in global memory
+    uint32_t split;  // CTAs (a cluster) running the item; lvloff holds nlvl * split + 1 offsets,
+                     // level l's sites for CTA r (segment % split == r) at [l split + r]
 };
 
 struct LvlMember {

@@ -222,8 +222,9 @@ void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_
                        const std::vector<std::vector<uint32_t>>& lv_sites,
                        const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& recoff,
                        const std::vector<uint32_t>& mem,
-                       bool gsp, uint32_t cap, uint32_t max_mem, LvlHost& out, std::vector<uint32_t>& order,
-                       double& longest) {
+                       bool gsp, uint32_t cap, uint32_t max_mem, uint32_t split, LvlHost& out,
+                       std::vector<uint32_t>& order, double& longest) {
+    if (!gsp || split < 1) split = 1;
     std::vector<uint32_t> m = mem;
     std::stable_sort(m.begin(), m.end(), [&](uint32_t a, uint32_t b) { return D[a].n > D[b].n; });
     std::vector<std::vector<uint32_t>> groups;
@@ -252,6 +253,7 @@ void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_
         it.lvl0 = (uint32_t)out.lvloff.size();
         it.seg0 = (uint32_t)out.segs.size();
         it.gsp = gsp ? 1u : 0u;
+        it.split = split;
         uint32_t flat = 0, depth = 0;
         double w = 0;
         for (uint32_t slot = 0; slot < g.size(); slot++) {
@@ -269,18 +271,21 @@ void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_
         }
         it.sites = flat;
         it.nlvl = depth;
-        for (uint32_t l = 0; l < depth; l++) {
-            out.lvloff.push_back((uint32_t)(out.entries.size() - it.ent0));
-            for (uint32_t slot = 0; slot < g.size(); slot++) {
-                const InstDesc& d = D[g[slot]];
-                const std::vector<uint32_t>& off = lv_off[d.owner];
-                if (l + 1 >= off.size()) continue;
-                const std::vector<uint32_t>& st = lv_sites[d.owner];
-                const uint32_t f0 = out.members[it.mem0 + slot].flat;
-                for (uint32_t q = off[l]; q < off[l + 1]; q++)
-                    out.entries.push_back(LvlEntry{slot << kLvlFlatBits | (f0 + st[q]), recoff[d.site + st[q]]});
+        for (uint32_t l = 0; l < depth; l++)
+            for (uint32_t r = 0; r < split; r++) {
+                out.lvloff.push_back((uint32_t)(out.entries.size() - it.ent0));
+                for (uint32_t slot = 0; slot < g.size(); slot++) {
+                    const InstDesc& d = D[g[slot]];
+                    const std::vector<uint32_t>& off = lv_off[d.owner];
+                    if (l + 1 >= off.size()) continue;
+                    const std::vector<uint32_t>& st = lv_sites[d.owner];
+                    const uint32_t f0 = out.members[it.mem0 + slot].flat;
+                    for (uint32_t q = off[l]; q < off[l + 1]; q++)
+                        if (split == 1 || (st[q] / kLvlSeg) % split == r)
+                            out.entries.push_back(
+                                LvlEntry{slot << kLvlFlatBits | (f0 + st[q]), recoff[d.site + st[q]]});
+                }
             }
-        }
         out.lvloff.push_back((uint32_t)(out.entries.size() - it.ent0));
         // per-level barrier and latency, in site-work units
         w += (double)depth * 400.0;

@@ -44,7 +44,9 @@ void site_levels(const LvlSource& s, std::vector<uint32_t>& sites, std::vector<u
 // grouped into items of at most cap spin words and max_mem members (gsp: one
 // member per item, spins in global memory). Level lists of member i are
 // lv_sites / lv_off of instance D[i].owner; recoff[D[i].site + v] is site v's
-// level-record offset. Appends to the item arrays and
+// level-record offset. split > 1 (gsp only): each item runs on a cluster of
+// split CTAs, CTA r taking the sites of segments s with s % split == r.
+// Appends to the item arrays and
 // returns the class's item ids ordered longest first.
 struct LvlHost {
     std::vector<LvlItem> items;
@@ -65,7 +67,7 @@ void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_
                        const std::vector<std::vector<uint32_t>>& lv_sites,
                        const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& recoff,
                        const std::vector<uint32_t>& mem,
-                       bool gsp, uint32_t cap, uint32_t max_mem, LvlHost& out, std::vector<uint32_t>& order,
-                       double& longest);
+                       bool gsp, uint32_t cap, uint32_t max_mem, uint32_t split, LvlHost& out,
+                       std::vector<uint32_t>& order, double& longest);
 
 }  // namespace ie
