@@ -274,6 +274,9 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
             }
             cg::this_cluster().sync();
             it = *cg::this_cluster().map_shared_rank(&s_item, 0);
+            // every CTA has read the leader's shared memory before the leader
+            // can overwrite it or exit
+            cg::this_cluster().sync();
         } else {
             __syncthreads();
             if (tid == 0) {
