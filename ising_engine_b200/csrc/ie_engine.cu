@@ -2061,7 +2061,8 @@ struct ServeEngine {
                 IE_TRY(eng.build_quads());
                 unit.assign(cfg.max_requests, 0);
                 for (const LvlItem& it : eng.lvh.items)
-                    for (uint32_t k = 0; k < it.nmem; k++) unit[eng.lvh.members[it.mem0 + k].inst] = it.sites;
+                    for (uint32_t k = 0; k < it.nmem; k++)
+                        unit[eng.lvh.members[it.mem0 + k].inst] = (it.sites + it.split - 1) / it.split;
                 set_changed = false;
             }
             RunArgs R{};

@@ -299,7 +299,8 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
         for (uint32_t k = tid; k < I.nmem; k += T) {
             const LvlMember mb = L.members[I.mem0 + k];
             const InstDesc d = A.desc[mb.inst];
-            const StepPlan P = step_plan(A, R, d, mb.inst, I.sites);
+            // serving: the site budget is per CTA, so a cluster's item gets split times as many steps
+            const StepPlan P = step_plan(A, R, d, mb.inst, (I.sites + I.split - 1) / I.split);
             LvlMem& m = ms[k];
             m.temps = P.temps;
             m.tstride = P.tstride;
