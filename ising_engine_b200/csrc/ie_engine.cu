@@ -875,13 +875,13 @@ struct Engine {
             for (int g = 0; g < 2; g++) {
                 if (mem[m][g].empty()) continue;
                 // spins in global memory: few large items spread over clusters
-                // of up to 8 CTAs while that keeps every SM busy
+                // of up to 16 CTAs while that keeps every SM busy
                 uint32_t split = 1;
                 const size_t smem0 = level_smem(m ? kModeF64 : kModeInt, own ? (one_per_item ? 1u : kLvlMaxOwnTables) : 1u,
                                                 0);
                 if (g && !one_per_item && lvl_split && !(cells_view && pt_path == 3)) {
                     const int occ1 = level_occupancy(m ? kModeF64 : kModeInt, true, lvl_threads, smem0);
-                    while (split < 8 && (uint64_t)mem[m][g].size() * split * 2 <= (uint64_t)occ1 * g_sm_count) split *= 2;
+                    while (split < 16 && (uint64_t)mem[m][g].size() * split * 2 <= (uint64_t)occ1 * g_sm_count) split *= 2;
                     while (split > 1 && level_clusters(m ? kModeF64 : kModeInt, lvl_threads, smem0, split) <= 0)
                         split /= 2;
                 }

@@ -592,6 +592,11 @@ int level_occupancy(uint32_t mode, bool gsp, int threads, size_t smem) {
 int level_clusters(uint32_t mode, int threads, size_t smem, uint32_t split) {
     const void* k = level_fn_of(mode, true, true);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) return 0;
+    // clusters of 16 CTAs are beyond the portable 8
+    if (split > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
     cudaLaunchAttribute attr;
     cudaLaunchConfig_t cfg = level_config((int)split, threads, smem, nullptr, split, &attr);
     int n = 0;
