@@ -865,8 +865,10 @@ struct Engine {
         for (size_t i = 0; i < D.size(); i++) nnz_of[i] = HI[i].nnz;
         const bool own = cells_view || serving;
         std::vector<uint32_t> mem[2][2];
+        uint64_t live_count = 0;
         for (uint32_t i = 0; i < (uint32_t)D.size(); i++) {
             if (!live(i) || !level_ok(D[i], cells_view)) continue;
+            live_count++;
             const bool gsp = D[i].n > lvl_cap;
             mem[D[i].mode == kModeF64 ? 1 : 0][gsp ? 1 : 0].push_back(i);
         }
@@ -882,6 +884,7 @@ struct Engine {
                 if (g && !one_per_item && lvl_split && !(cells_view && pt_path == 3)) {
                     const int occ1 = level_occupancy(m ? kModeF64 : kModeInt, true, lvl_threads, smem0);
                     while (split < 16 && (uint64_t)mem[m][g].size() * split * 2 <= (uint64_t)occ1 * g_sm_count) split *= 2;
+                    if (serving) split = std::min<uint32_t>(16, split * 2);
                     while (split > 1 && level_clusters(m ? kModeF64 : kModeInt, lvl_threads, smem0, split) <= 0)
                         split /= 2;
                 }
@@ -894,7 +897,10 @@ struct Engine {
                 uint32_t cap = lvl_cap, maxn = 0;
                 for (uint32_t i : mem[m][g]) maxn = std::max(maxn, D[i].n);
                 if (cells_view && maxn >= 512) cap = std::min(cap, maxn);
-                const uint32_t maxmem = one_per_item ? 1u : own ? kLvlMaxOwnTables : kLvlMaxMembers;
+                // serving: one request per CTA while the requests fit the GPU's
+                // CTA slots (a packed item advances all its requests at the rate of one)
+                const bool alone = one_per_item || (serving && live_count <= (uint64_t)4 * g_sm_count);
+                const uint32_t maxmem = alone ? 1u : own ? kLvlMaxOwnTables : kLvlMaxMembers;
                 std::vector<uint32_t> order;
                 double longest = 0;
                 build_level_items(D, nnz_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem, split, lvh,
