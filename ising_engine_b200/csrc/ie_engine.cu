@@ -1781,6 +1781,9 @@ struct ServeEngine {
         if (cfg.kernel_form < 0 || cfg.kernel_form > 1) return fail(IE_ERR_INVALID, "kernel_form must be 0 or 1");
         eng.kernel_form = cfg.kernel_form;
         eng.serving = true;
+        // requests above 1024 sites keep their spins in global memory, so a
+        // request can run on a cluster of CTAs
+        eng.lvl_cap = 1024;
         const uint32_t S = cfg.max_requests;
         eng.nt = 1;
         eng.count = S;
