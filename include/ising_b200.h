@@ -232,7 +232,8 @@ ie_status ie_batch_recompute_energies(ie_batch* b, double* energies /* [count][6
 /* Device time of the last run call in milliseconds (CUDA events on its stream). */
 ie_status ie_batch_last_run_ms(ie_batch* b, double* ms);
 /* Work classes of the last batched run: for class k < min(max_classes, *n_classes),
- * info[5k..5k+4] = {mode (0 integer, 1 f64), threads per lane (8 = windowed kernel),
+ * info[5k..5k+4] = {mode (0 integer, 1 f64, 2 the level kernel's bit-sliced +-J form),
+ * threads per lane (8 = windowed kernel, 16 = chain kernel, 32 = level kernel),
  * shared-memory spin capacity, work items, valid}, ms[k] = its device time. */
 ie_status ie_batch_class_report(ie_batch* b, uint32_t max_classes, uint32_t* n_classes, uint32_t* info,
                                 double* ms);

@@ -145,6 +145,7 @@ struct HostInst {
     std::vector<double> vals;
     std::vector<double> lin;
     std::vector<uint32_t> recpos, reclen;  // first record of each site: word offset and length in its stream
+    uint32_t pmj = 0;                      // +-J form for the level kernel: c | D << 16 (0: not)
     bool windowed_ok = false;              // the windowed kernel is preferred (parallel windows)
     bool has_wtab = false;                 // has a window table (the windowed kernel can run it)
     uint64_t nnz = 0;
@@ -219,6 +220,22 @@ ie_status ingest(const ie_problem* p, bool force_f64, HostInst& out) {
         out.mode = kModeInt;
         out.H = H;
         out.linp = std::move(linp);
+        // +-J form: one coupling magnitude c, lin_v = -sum_j w_vj / 2 and one
+        // degree D <= 8 at every site (the Ising lowering of a +-J lattice)
+        bool pm = n > 0 && nnz > 0;
+        const double c = pm ? std::fabs(p->values[0]) : 0.0;
+        const uint64_t D = pm ? p->row_offsets[1] - p->row_offsets[0] : 0;
+        pm = pm && D >= 1 && D <= 8 && c >= 1.0;
+        for (uint64_t i = 0; pm && i < n; i++) {
+            if (p->row_offsets[i + 1] - p->row_offsets[i] != D) pm = false;
+            double sw = 0.0;
+            for (uint64_t k = p->row_offsets[i]; pm && k < p->row_offsets[i + 1]; k++) {
+                if (std::fabs(p->values[k]) != c) pm = false;
+                sw += p->values[k];
+            }
+            if (pm && 2.0 * p->linear[i] != -sw) pm = false;
+        }
+        out.pmj = pm ? ((uint32_t)c | (uint32_t)D << 16) : 0u;
         out.ents.resize(nnz);
         for (uint64_t k = 0; k < nnz; k++) {
             const double w = p->values[k];
@@ -767,6 +784,7 @@ struct Engine {
     int lvl_threads = 256;
     uint32_t lvl_tie_shift = 0;
     bool lvl_split = true;    // large single-member items on thread block clusters
+    bool use_pmj = true;      // +-J instances on the bit-sliced form
     bool serving = false;     // serving launches: one threshold table per member
     std::vector<std::vector<uint32_t>> lv_sites, lv_off;  // per instance: sites by level, level starts
     std::vector<uint32_t> h_recoff;                       // level-record offset per site
@@ -862,35 +880,42 @@ struct Engine {
                                   Live live, bool one_per_item = false) {
         lvh.clear();
         std::vector<uint64_t> nnz_of(D.size());
+        std::vector<uint32_t> pmj_of(D.size());
         for (size_t i = 0; i < D.size(); i++) nnz_of[i] = HI[i].nnz;
         const bool own = cells_view || serving;
-        std::vector<uint32_t> mem[2][2];
+        // classes: integer, f64, +-J form (one magnitude c per launch)
+        std::vector<uint32_t> mem[3][2];
         uint64_t live_count = 0;
+        uint32_t c0 = 0;
         for (uint32_t i = 0; i < (uint32_t)D.size(); i++) {
             if (!live(i) || !level_ok(D[i], cells_view)) continue;
             live_count++;
             const bool gsp = D[i].n > lvl_cap;
-            mem[D[i].mode == kModeF64 ? 1 : 0][gsp ? 1 : 0].push_back(i);
+            const uint32_t pm = use_pmj ? HI[i].pmj : 0u;
+            if (pm && !c0) c0 = pm & 0xFFFFu;
+            const bool as_pmj = pm && (pm & 0xFFFFu) == c0;
+            pmj_of[i] = as_pmj ? pm : 0u;
+            mem[as_pmj ? 2 : D[i].mode == kModeF64 ? 1 : 0][gsp ? 1 : 0].push_back(i);
         }
         uint64_t keytotal = 0;
-        for (int m = 0; m < 2; m++)
+        for (int m = 0; m < 3; m++)
             for (int g = 0; g < 2; g++) {
                 if (mem[m][g].empty()) continue;
                 // spins in global memory: few large items spread over clusters
                 // of up to 16 CTAs while that keeps every SM busy
                 uint32_t split = 1;
-                const size_t smem0 = level_smem(m ? kModeF64 : kModeInt, own ? (one_per_item ? 1u : kLvlMaxOwnTables) : 1u,
-                                                0);
+                const uint32_t kmode = m == 2 ? kModePmJ : m ? kModeF64 : kModeInt;
+                const size_t smem0 = level_smem(kmode, own ? (one_per_item ? 1u : kLvlMaxOwnTables) : 1u, 0);
                 if (g && !one_per_item && lvl_split && !(cells_view && pt_path == 3)) {
-                    const int occ1 = level_occupancy(m ? kModeF64 : kModeInt, true, lvl_threads, smem0);
+                    const int occ1 = level_occupancy(kmode, true, lvl_threads, smem0);
                     while (split < 16 && (uint64_t)mem[m][g].size() * split * 2 <= (uint64_t)occ1 * g_sm_count) split *= 2;
                     if (serving) split = std::min<uint32_t>(16, split * 2);
-                    while (split > 1 && level_clusters(m ? kModeF64 : kModeInt, lvl_threads, smem0, split) <= 0)
+                    while (split > 1 && level_clusters(kmode, lvl_threads, smem0, split) <= 0)
                         split /= 2;
                 }
                 std::unique_ptr<WorkClass> wc(new WorkClass());
                 wc->level = true;
-                wc->mode = m ? kModeF64 : kModeInt;
+                wc->mode = kmode;
                 wc->gsp = g != 0;
                 wc->tpl = kLevelForm;
                 wc->cap = g ? 0u : lvl_cap;
@@ -903,8 +928,8 @@ struct Engine {
                 const uint32_t maxmem = alone ? 1u : own ? kLvlMaxOwnTables : kLvlMaxMembers;
                 std::vector<uint32_t> order;
                 double longest = 0;
-                build_level_items(D, nnz_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem, split, lvh,
-                                  order, longest);
+                build_level_items(D, nnz_of, pmj_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem, split,
+                                  lvh, order, longest);
                 wc->nitems = (uint32_t)order.size();
                 wc->work = longest;
                 for (uint32_t i : mem[m][g]) wc->site_steps += (double)D[i].n;
@@ -1075,6 +1100,7 @@ struct Engine {
                 l.nnz = insts[i].nnz;
                 l.windowed_ok = insts[i].windowed_ok;
                 l.has_wtab = insts[i].has_wtab;
+                l.pmj = insts[i].pmj;
                 cinsts.push_back(l);
             }
         IE_TRY(d_cdesc.upload(cdesc, stream));

@@ -47,6 +47,7 @@ struct LvlMem {
     double beta;
     uint32_t key[8];
     uint32_t inst, flat, n, steps, tstride, cell, owner, fin;
+    uint32_t pmj;  // +-J form: c | degree << 16
 };
 
 // Top 32 bits of the integer threshold: accept iff m < T with T =
@@ -79,6 +80,18 @@ __device__ __forceinline__ LvlEntry load_entry(const LvlEntry* p) {
 
 __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// A spin word (+-J form); CG: from L2.
+template <bool CG>
+__device__ __forceinline__ uint64_t ld_word(const uint64_t* p) {
+    if constexpr (CG) {
+        uint64_t v;
+        asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(v) : "l"(p));
+        return v;
+    } else {
+        return *p;
+    }
 }
 
 // A spin byte; CG: from L2 (another CTA of the cluster may have written it).
@@ -246,7 +259,8 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
     const bool own_tab = R.serve != 0 || R.cells != 0;
     uint32_t* const tabs = reinterpret_cast<uint32_t*>(dsm);
     uint2* const lut = reinterpret_cast<uint2*>(tabs + (size_t)L.ntab * kLvlTab);
-    uint64_t* const ssw = reinterpret_cast<uint64_t*>(lut + (MODE == kModeInt ? 512 : 0));
+    uint64_t* const ssw = reinterpret_cast<uint64_t*>(lut + (MODE != kModeF64 ? 512 : 0));
+    uint64_t* const tabs64 = reinterpret_cast<uint64_t*>(tabs);  // +-J form: thresholds per level
     uint32_t crank = 0, csize = 1;
     if constexpr (SPLIT) {
         crank = cg::this_cluster().block_rank();
@@ -254,7 +268,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
     }
     // one output buffer per CTA, or per cluster (its CTAs write disjoint segments)
     uint32_t* const kb = L.keybuf + (size_t)(blockIdx.x / csize) * L.keystride;
-    if constexpr (MODE == kModeInt) {
+    if constexpr (MODE != kModeF64) {
         // spread table: entry b (256 + b for a negative coupling, which
         // contributes |w| (1 - x_j)) holds bit k of b (~b) in byte k
         for (int i = tid; i < 512; i += T) {
@@ -312,6 +326,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
             m.n = d.n;
             m.flat = mb.flat;
             m.inst = mb.inst;
+            m.pmj = mb.pmj;
             m.cell = d.cell;
             m.owner = d.owner;
             m.pos0 = A.pos[d.owner];
@@ -350,6 +365,16 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     if (s < ms[k].steps) tabs[k * kLvlTab + idx] = q_threshold((int)idx - H, ms[k].beta);
                 }
             }
+            if constexpr (MODE == kModePmJ) {
+                // threshold of dE = c e / 2 for e = 1..15 (the odd e only occur
+                // for even c); the full 64-bit form, decided exactly in the generator
+                const uint32_t nt = own_tab ? I.nmem : 1u;
+                for (uint32_t i = tid; i < nt * 16u; i += T) {
+                    const uint32_t k = i >> 4, e = i & 15u, c = ms[k].pmj & 0xFFFFu;
+                    if (s < ms[k].steps && e && (c * e) % 2 == 0)
+                        tabs64[k * (kLvlTab / 2) + e] = metropolis_threshold((int)(c * e / 2), ms[k].beta);
+                }
+            }
             // generator phase: chain j = (this CTA's segment j / 8, lane j % 8)
             for (uint32_t j = tid;; j += T) {
                 const uint32_t sg = crank + csize * (j >> 3);
@@ -362,14 +387,39 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                 x.seed_lane(m.base, lane);
                 if (seg) x.jump(L.jpoly + 4ull * seg);
                 const uint32_t v0 = seg * kLvlSeg, v1 = min(m.n, v0 + kLvlSeg);
-                uint4* out = reinterpret_cast<uint4*>(kb + (size_t)(m.flat + v0) * 64 + lane * 8);
-                for (uint32_t v = v0; v < v1; v++) {
-                    uint32_t h[8];
+                if constexpr (MODE == kModePmJ) {
+                    // acceptance masks: byte `lane` of word i of the site's row
+                    // holds [output <= U(dE of uphill level i + 1)] for the lane's
+                    // 8 calls, exactly (engine.rs:665-666)
+                    const uint32_t D = m.pmj >> 16, odd = D & 1u, nl = (D + 1) >> 1;
+                    const uint64_t* U = tabs64 + (own_tab ? slot * (kLvlTab / 2) : 0u);
+                    uint64_t ul[4];
 #pragma unroll
-                    for (int k = 0; k < 8; k++) h[k] = x.next_hi();
-                    out[0] = make_uint4(h[0], h[1], h[2], h[3]);
-                    out[1] = make_uint4(h[4], h[5], h[6], h[7]);
-                    out += 16;
+                    for (int i = 0; i < 4; i++) ul[i] = (uint32_t)i < nl ? U[2 * (i + 1) - odd] : 0ull;
+                    uint8_t* out8 = reinterpret_cast<uint8_t*>(kb + (size_t)(m.flat + v0) * 64) + lane;
+                    for (uint32_t v = v0; v < v1; v++) {
+                        uint32_t a[4] = {0, 0, 0, 0};
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            const uint64_t res = x.next();
+#pragma unroll
+                            for (int i = 0; i < 4; i++) a[i] |= (uint32_t)(res <= ul[i]) << k;
+                        }
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            if ((uint32_t)i < nl) out8[8 * i] = (uint8_t)a[i];
+                        out8 += 256;
+                    }
+                } else {
+                    uint4* out = reinterpret_cast<uint4*>(kb + (size_t)(m.flat + v0) * 64 + lane * 8);
+                    for (uint32_t v = v0; v < v1; v++) {
+                        uint32_t h[8];
+#pragma unroll
+                        for (int k = 0; k < 8; k++) h[k] = x.next_hi();
+                        out[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                        out[1] = make_uint4(h[4], h[5], h[6], h[7]);
+                        out += 16;
+                    }
                 }
             }
             __syncthreads();
@@ -382,6 +432,58 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
             uint32_t e0 = I.nlvl ? __ldg(lo) : 0u, e1 = I.nlvl ? __ldg(lo + 1) : 0u;
             LvlEntry nxt{0, 0};
             for (uint32_t l = 0; l < I.nlvl; l++) {
+                if constexpr (MODE == kModePmJ) {
+                    // one thread per site, all 64 replicas at once: cnt = number of
+                    // neighbours j with x_j ^ (w_j < 0) = 1, kept as 4 bit planes;
+                    // dE = (c/2)(2 cnt - D) for x_v = 0 and (c/2)(D - 2 cnt) for
+                    // x_v = 1 (|w| = c, lin = -sum w / 2), uphill level i at cnt =
+                    // floor(D/2) + i resp. ceil(D/2) - i; flip unless an uphill
+                    // level's acceptance bit is clear
+                    for (uint32_t i = tid; i < e1 - e0; i += T) {
+                        const LvlEntry en = load_entry(L.entries + I.ent0 + e0 + i);
+                        const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
+                        const LvlMem& m = ms[slot];
+                        if (s >= m.steps) continue;
+                        const uint32_t* rec = L.lrecs + 4ull * en.rec;
+                        const uint32_t D = __ldg(rec) & 0x7FFFFFFFu;
+                        const uint64_t xw = ld_word<SPLIT>(sw + f);
+                        uint64_t p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+                        const uint4* e4p = reinterpret_cast<const uint4*>(rec + 4);
+                        for (uint32_t q = 0; q < D; q += 4) {
+                            const uint4 e4 = __ldg(e4p + (q >> 2));
+                            const uint32_t ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+                            for (int e = 0; e < 4; e++) {
+                                if (q + e < D) {
+                                    uint64_t b = ld_word<SPLIT>(sw + m.flat + (ev[e] & 0xFFFFFFu));
+                                    if (ev[e] >> 31) b = ~b;
+                                    uint64_t c = p0 & b;
+                                    p0 ^= b;
+                                    const uint64_t c1 = p1 & c;
+                                    p1 ^= c;
+                                    c = p2 & c1;
+                                    p2 ^= c1;
+                                    p3 ^= c;
+                                }
+                            }
+                        }
+                        const uint64_t* A = reinterpret_cast<const uint64_t*>(kb + (size_t)f * 64);
+                        const uint32_t nl = (D + 1) >> 1, hD = D >> 1, cD = (D + 1) >> 1;
+                        uint64_t bad = 0;
+                        for (uint32_t lv = 1; lv <= nl; lv++) {
+                            const uint32_t K0 = hD + lv, K1 = cD - lv;
+                            uint64_t eq = ~0ull;
+                            const uint64_t pl[4] = {p0, p1, p2, p3};
+#pragma unroll
+                            for (int b = 0; b < 4; b++) {
+                                const uint64_t t = (((K1 >> b) & 1u) ? xw : 0ull) | (((K0 >> b) & 1u) ? ~xw : 0ull);
+                                eq &= ~(pl[b] ^ t);
+                            }
+                            bad |= eq & ~A[lv - 1];
+                        }
+                        sw[f] = xw ^ ~bad;
+                    }
+                } else
                 for (uint32_t i = tid; i < 8u * (e1 - e0); i += T) {
                     const LvlEntry en = (i == (uint32_t)tid && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + (i >> 3));
                     const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
@@ -488,7 +590,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                 if (l + 1 < I.nlvl) {
                     e0 = __ldg(lo + (l + 1) * csize);
                     e1 = __ldg(lo + (l + 1) * csize + 1);
-                    if ((uint32_t)tid < 8u * (e1 - e0)) {
+                    if (MODE != kModePmJ && (uint32_t)tid < 8u * (e1 - e0)) {
                         nxt = load_entry(L.entries + I.ent0 + e0 + (tid >> 3));
                         prefetch_l1(L.lrecs + 4ull * nxt.rec);
                         prefetch_l1(kb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64 + lane * 8);
@@ -508,7 +610,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
         for (uint32_t k = 0; k < I.nmem; k++) {
             const LvlMem& m = ms[k];
             if (!m.fin || m.steps == 0) continue;
-            if constexpr (MODE == kModeInt) {
+            if constexpr (MODE != kModeF64) {
                 if (tid < kReplicas) sE[tid] = 0;
                 __syncthreads();
                 member_energy_int<SPLIT>(L, m, spb, lut, tid, T, sE);
@@ -547,9 +649,12 @@ template __global__ void level_kernel<kModeInt, true, true>(DevArrays, RunArgs, 
 template __global__ void level_kernel<kModeF64, false, false>(DevArrays, RunArgs, LvlArgs);
 template __global__ void level_kernel<kModeF64, true, false>(DevArrays, RunArgs, LvlArgs);
 template __global__ void level_kernel<kModeF64, true, true>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModePmJ, false, false>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModePmJ, true, false>(DevArrays, RunArgs, LvlArgs);
+template __global__ void level_kernel<kModePmJ, true, true>(DevArrays, RunArgs, LvlArgs);
 
 size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap) {
-    return (size_t)ntab * kLvlTab * 4 + (mode == kModeInt ? 512 * 8 : 0) + (size_t)spin_cap * 8;
+    return (size_t)ntab * kLvlTab * 4 + (mode != kModeF64 ? 512 * 8 : 0) + (size_t)spin_cap * 8;
 }
 
 template <uint32_t MODE, bool GSP, bool SPLIT>
@@ -558,6 +663,9 @@ static void* level_fn() {
 }
 
 static void* level_fn_of(uint32_t mode, bool gsp, bool split) {
+    if (mode == kModePmJ)
+        return split ? level_fn<kModePmJ, true, true>() : gsp ? level_fn<kModePmJ, true, false>()
+                                                              : level_fn<kModePmJ, false, false>();
     if (mode == kModeInt)
         return split ? level_fn<kModeInt, true, true>() : gsp ? level_fn<kModeInt, true, false>()
                                                               : level_fn<kModeInt, false, false>();
@@ -611,9 +719,13 @@ cudaError_t launch_level(const DevArrays& A, const RunArgs& R, const LvlArgs& L,
         cudaLaunchAttribute attr;
         const cudaLaunchConfig_t cfg = level_config(grid, threads, smem, st, split, &attr);
         if (mode == kModeInt) return cudaLaunchKernelEx(&cfg, level_kernel<kModeInt, true, true>, A, R, L);
+        if (mode == kModePmJ) return cudaLaunchKernelEx(&cfg, level_kernel<kModePmJ, true, true>, A, R, L);
         return cudaLaunchKernelEx(&cfg, level_kernel<kModeF64, true, true>, A, R, L);
     }
-    if (mode == kModeInt) {
+    if (mode == kModePmJ) {
+        if (gsp) level_kernel<kModePmJ, true, false><<<grid, threads, smem, st>>>(A, R, L);
+        else level_kernel<kModePmJ, false, false><<<grid, threads, smem, st>>>(A, R, L);
+    } else if (mode == kModeInt) {
         if (gsp) level_kernel<kModeInt, true, false><<<grid, threads, smem, st>>>(A, R, L);
         else level_kernel<kModeInt, false, false><<<grid, threads, smem, st>>>(A, R, L);
     } else {

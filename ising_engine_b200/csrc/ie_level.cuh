@@ -18,6 +18,10 @@
 namespace ie {
 
 constexpr uint32_t kLvlSeg = 128;          // sites per generator segment
+// Kernel mode of the +-J form (integer couplings of one magnitude c, lin_v =
+// -sum_j w_vj / 2, every site of degree D <= 8): bit-sliced decisions, one
+// thread per site (the instances' InstDesc mode stays the integer mode).
+constexpr uint32_t kModePmJ = 2;
 constexpr uint32_t kLvlMaxMembers = 64;    // instances per item
 constexpr uint32_t kLvlMaxOwnTables = 16;  // members per item when each has its own threshold table
 constexpr uint32_t kLvlFlatBits = 26;      // entry = slot << 26 | flat site index within the item
@@ -42,6 +46,7 @@ struct LvlItem {
 struct LvlMember {
     uint32_t inst;  // index into the launch's InstDesc array
     uint32_t flat;  // first flat spin word of the member
+    uint32_t pmj;   // +-J form: c | D << 16 (0: not)
 };
 
 // One site of a level: slot << 26 | flat site index, and its level record's

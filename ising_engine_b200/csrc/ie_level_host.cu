@@ -219,6 +219,7 @@ void site_levels(const LvlSource& s, std::vector<uint32_t>& sites, std::vector<u
 }
 
 void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_t>& nnz_of,
+                       const std::vector<uint32_t>& pmj_of,
                        const std::vector<std::vector<uint32_t>>& lv_sites,
                        const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& recoff,
                        const std::vector<uint32_t>& mem,
@@ -258,7 +259,7 @@ void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_
         double w = 0;
         for (uint32_t slot = 0; slot < g.size(); slot++) {
             const InstDesc& d = D[g[slot]];
-            out.members.push_back(LvlMember{g[slot], flat});
+            out.members.push_back(LvlMember{g[slot], flat, pmj_of[g[slot]]});
             const uint32_t ns = (d.n + kLvlSeg - 1) / kLvlSeg;
             for (uint32_t sg = 0; sg < ns; sg++) out.segs.push_back(slot << 24 | sg);
             out.max_segs = std::max(out.max_segs, ns);

@@ -278,13 +278,14 @@ class BatchEngine:
     def class_report(self):
         """Per work class of the last run: (mode, threads per lane, capacity,
         items, device ms); threads per lane 8 marks the windowed kernel, 16 the
-        chain kernel."""
+        chain kernel, 32 the level kernel (mode "pmj": its bit-sliced +-J
+        form; capacity 0: spins in global memory)."""
         n = np.zeros(1, dtype=np.uint32)
         info = np.zeros(5 * 64, dtype=np.uint32)
         ms = np.zeros(64, dtype=np.float64)
         _ffi.check(self._L.ie_batch_class_report(self._h, 64, _p(n), _p(info), _p(ms)))
         k = int(min(n[0], 64))
-        return [(("int", "f64")[info[5 * i]], int(info[5 * i + 1]), int(info[5 * i + 2]),
+        return [(("int", "f64", "pmj")[info[5 * i]], int(info[5 * i + 1]), int(info[5 * i + 2]),
                  int(info[5 * i + 3]), float(ms[i])) for i in range(k)]
 
     def last_launches(self) -> int:

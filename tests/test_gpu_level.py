@@ -124,3 +124,48 @@ def test_lattice_ladders_on_level_cells(L, dim, nt, steps, interval):
             if nt > 1:
                 att, acc = eng.swap_stats()
                 assert (att == ref.swap_attempts).all() and (acc == ref.swap_accepts).all()
+
+
+def pm_j_regular(n, d, c, rng):
+    """Random d-regular graph with couplings +-c and lin_v = -sum_j w_vj / 2:
+    the Ising lowering of a +-J spin glass, the level kernel's bit-sliced
+    form (odd d with even c, or any d)."""
+    from ising_engine_b200.core import QuboModel
+    e = I.random_regular_edges(n, d, rng)
+    w = (c * rng.choice(np.array([-1, 1]), size=len(e))).astype(np.float64)
+    lin = np.zeros(n)
+    np.add.at(lin, e[:, 0], -w / 2)
+    np.add.at(lin, e[:, 1], -w / 2)
+    return QuboModel.from_edges(n, lin, np.concatenate([e.astype(np.float64), w[:, None]], axis=1), 0.0)
+
+
+def test_bit_sliced_pm_j_form_batch():
+    """+-J instances (lattices and random regular graphs of degree 3..8, one
+    coupling magnitude) run on the bit-sliced form, one thread per site for
+    all 64 replicas; spins, energies and stream positions equal the oracle's,
+    with clamps too."""
+    rng = np.random.default_rng(404)
+    models = [I.pm_j_lattice(16, 2, seed=1), I.pm_j_lattice(8, 3, seed=2), I.pm_j_lattice(40, 2, seed=3)]
+    models += [pm_j_regular(n, d, 2, rng) for n, d in [(300, 3), (500, 5), (240, 7), (1000, 8), (5000, 4)]]
+    seeds = np.arange(len(models), dtype=np.uint64) * 31 + 7
+    temps = I.sa_temps(80, 0.2, 3.0)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
+    b = BatchEngine(models, seeds)
+    b.init_random()
+    b.run_schedule(temps[:33])
+    b.run_schedule(temps[33:])
+    check_batch(b, models, words_ref, ref_e)
+    assert any(c[0] == "pmj" for c in b.class_report())
+    b.close()
+    m = I.pm_j_lattice(24, 2, seed=9)
+    f = np.zeros(m.num_vars, np.uint8)
+    f[::7] = 1
+    v = (np.arange(m.num_vars) % 3 == 0).astype(np.int8)
+    temps = I.geometric_beta_ladder(6, 0.3, 1.5)
+    ref = O.run_schedule(m, np.tile(temps, (25, 1)), 3, clamped=f, clamp_val=v, collect_stats=True)
+    with Engine(m, num_temps=6, seed=3, pt_path=2) as eng:
+        eng.set_clamps(f, v)
+        eng.init_random()
+        eng.step(temps, 25)
+        assert (eng.spins() == ref.words).all()
+        assert eng.energies().tobytes() == ref.energies.tobytes()
