@@ -76,6 +76,8 @@ typedef struct ie_config {
     int32_t kernel_form; /* 0: integer-mode cells run on the level kernel (generator and
                             decision phases, all cells of the ladder in flight); 1: the
                             per-lane kernels only (same results) */
+    uint32_t max_cluster; /* level kernel: most CTAs (a thread block cluster) running one
+                             large cell, 1, 2, 4, 8 or 16; 0: chosen by size (at most 16) */
 } ie_config;
 
 typedef struct ie_handle ie_handle;

@@ -38,7 +38,7 @@ class ie_config(C.Structure):
                 ("seed", C.c_uint64), ("num_temps", C.c_uint32), ("num_pops", C.c_uint32),
                 ("num_slices", C.c_uint32), ("exchange_interval", C.c_uint32),
                 ("force_f64", C.c_int32), ("device", C.c_int32), ("pt_path", C.c_int32),
-                ("use_icm", C.c_int32), ("kernel_form", C.c_int32)]
+                ("use_icm", C.c_int32), ("kernel_form", C.c_int32), ("max_cluster", C.c_uint32)]
 
 
 class ie_problem_device(C.Structure):

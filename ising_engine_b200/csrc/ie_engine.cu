@@ -784,6 +784,7 @@ struct Engine {
     int lvl_threads = 256;
     uint32_t lvl_tie_shift = 0;
     bool lvl_split = true;    // large single-member items on thread block clusters
+    uint32_t lvl_cluster_max = 0;  // most CTAs per cluster (0: 16)
     bool use_pmj = true;      // +-J instances on the bit-sliced form
     bool serving = false;     // serving launches: one threshold table per member
     std::vector<std::vector<uint32_t>> lv_sites, lv_off;  // per instance: sites by level, level starts
@@ -908,8 +909,10 @@ struct Engine {
                 const size_t smem0 = level_smem(kmode, own ? (one_per_item ? 1u : kLvlMaxOwnTables) : 1u, 0);
                 if (g && !one_per_item && lvl_split && !(cells_view && pt_path == 3)) {
                     const int occ1 = level_occupancy(kmode, true, lvl_threads, smem0);
-                    while (split < 16 && (uint64_t)mem[m][g].size() * split * 2 <= (uint64_t)occ1 * g_sm_count) split *= 2;
-                    if (serving) split = std::min<uint32_t>(16, split * 2);
+                    const uint32_t cmax = lvl_cluster_max ? lvl_cluster_max : 16u;
+                    while (split < cmax && (uint64_t)mem[m][g].size() * split * 2 <= (uint64_t)occ1 * g_sm_count)
+                        split *= 2;
+                    if (serving) split = std::min<uint32_t>(cmax, split * 2);
                     while (split > 1 && level_clusters(kmode, lvl_threads, smem0, split) <= 0)
                         split /= 2;
                 }
@@ -2224,6 +2227,9 @@ ie_status ie_create(const ie_problem* problem, const ie_config* config, ie_handl
     IE_TRY(h->eng.setup_device(config->device));
     h->eng.pt_path = h->cfg.pt_path;
     h->eng.kernel_form = h->cfg.kernel_form;
+    if (h->cfg.max_cluster > 16 || (h->cfg.max_cluster & (h->cfg.max_cluster - 1)))
+        return fail(IE_ERR_INVALID, "max_cluster must be 0, 1, 2, 4, 8 or 16");
+    h->eng.lvl_cluster_max = h->cfg.max_cluster;
     const uint32_t pops = std::max<uint32_t>(h->cfg.num_pops, 1);
     if (pops > 1) {
         // QuantumField::new(n, 1, num_temps, num_pops): cell t + num_temps * p,

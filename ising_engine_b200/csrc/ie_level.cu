@@ -85,25 +85,15 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
 // A spin word (+-J form); CG: from L2.
 template <bool CG>
 __device__ __forceinline__ uint64_t ld_word(const uint64_t* p) {
-    if constexpr (CG) {
-        uint64_t v;
-        asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(v) : "l"(p));
-        return v;
-    } else {
-        return *p;
-    }
+    if constexpr (CG) return __ldcg(reinterpret_cast<const unsigned long long*>(p));
+    else return *p;
 }
 
 // A spin byte; CG: from L2 (another CTA of the cluster may have written it).
 template <bool CG>
 __device__ __forceinline__ uint32_t ld_spin(const uint8_t* p) {
-    if constexpr (CG) {
-        uint32_t v;
-        asm volatile("ld.global.cg.u8 %0, [%1];" : "=r"(v) : "l"(p));
-        return v;
-    } else {
-        return *p;
-    }
+    if constexpr (CG) return __ldcg(p);
+    else return *p;
 }
 
 __device__ __forceinline__ float ex2_approx(float a) {
@@ -440,7 +430,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     // floor(D/2) + i resp. ceil(D/2) - i; flip unless an uphill
                     // level's acceptance bit is clear
                     for (uint32_t i = tid; i < e1 - e0; i += T) {
-                        const LvlEntry en = load_entry(L.entries + I.ent0 + e0 + i);
+                        const LvlEntry en = (i == (uint32_t)tid && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + i);
                         const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
                         const LvlMem& m = ms[slot];
                         if (s >= m.steps) continue;
@@ -594,6 +584,11 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                         nxt = load_entry(L.entries + I.ent0 + e0 + (tid >> 3));
                         prefetch_l1(L.lrecs + 4ull * nxt.rec);
                         prefetch_l1(kb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64 + lane * 8);
+                    }
+                    if (MODE == kModePmJ && (uint32_t)tid < e1 - e0) {
+                        nxt = load_entry(L.entries + I.ent0 + e0 + tid);
+                        prefetch_l1(L.lrecs + 4ull * nxt.rec);
+                        prefetch_l1(kb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64);
                     }
                 }
                 if constexpr (SPLIT) cg::this_cluster().sync();

@@ -43,7 +43,7 @@ class Engine:
                  exchange_interval: int = 1, temp_max: float = 1.0, temp_min: float = 0.1,
                  sweeps_per_exchange: int = 1, total_exchanges: int = 1, force_f64: bool = False,
                  device: int = 0, pt_path: int = 0, num_pops: int = 1, use_icm: bool = False,
-                 kernel_form: int = 0):
+                 kernel_form: int = 0, max_cluster: int = 0):
         self._L = _ffi.lib()
         self.model = model
         self.num_temps = int(num_temps)
@@ -54,7 +54,8 @@ class Engine:
         prob = _problem(model, keep)
         cfg = _ffi.ie_config(temp_max, temp_min, sweeps_per_exchange, total_exchanges,
                              seed & 0xFFFFFFFFFFFFFFFF, self.num_temps, self.num_pops, 1, exchange_interval,
-                             int(force_f64), device, pt_path, int(use_icm), int(kernel_form))
+                             int(force_f64), device, pt_path, int(use_icm), int(kernel_form),
+                             int(max_cluster))
         h = C.c_void_p()
         _ffi.check(self._L.ie_create(C.byref(prob), C.byref(cfg), C.byref(h)))
         self._h = h
