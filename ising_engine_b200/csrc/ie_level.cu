@@ -107,6 +107,19 @@ __device__ __forceinline__ float ex2_approx(float a) {
 // m 2^-52 lies in [lo 2^-32, (lo + 2^sh) 2^-32), lo = mh with its low sh bits
 // cleared. fast_exp(x) >= exp(x) (the alternating Taylor tail is negative) and
 // <= 1.054 exp(x) on [-20, 0]; ex2.approx is within 3e-6 of exp here.
+// Out of line (the rare case: u within the ex2 bracket): the f32 form of
+// fast_exp with its 2^-10 band, then the exact f64 value.
+__device__ __noinline__ int f64_decide_slow(double x, uint32_t lo, uint32_t sh, float ulo, float uhi) {
+    const float f = fast_exp_f32(__double2float_rn(x));
+    if (uhi < __fmul_rn(f, 0.9990234375f)) return 1;
+    if (ulo > __fmul_rn(f, 1.0009765625f)) return -1;
+    const uint64_t T = (uint64_t)ceil(__dmul_rn(fast_exp_rn(x), 4503599627370496.0));
+    const uint64_t mlo = (uint64_t)lo << 20, mhi = ((uint64_t)lo + (1ull << sh)) << 20;
+    if (mhi <= T) return 1;
+    if (mlo >= T) return -1;
+    return 0;
+}
+
 __device__ __forceinline__ int f64_decide(double de, double beta, uint32_t mh, uint32_t sh) {
     const double x = __dmul_rn(-de, beta);
     const uint32_t lo = (mh >> sh) << sh;
@@ -117,14 +130,7 @@ __device__ __forceinline__ int f64_decide(double de, double beta, uint32_t mh, u
     const float ex = ex2_approx(__fmul_rn(xf, 1.4426950408889634f));
     if (uhi <= __fmul_rn(ex, 0.99998f)) return 1;
     if (ulo >= __fmul_rn(ex, 1.0625f)) return -1;
-    const float f = fast_exp_f32(__double2float_rn(x));
-    if (uhi < __fmul_rn(f, 0.9990234375f)) return 1;
-    if (ulo > __fmul_rn(f, 1.0009765625f)) return -1;
-    const uint64_t T = (uint64_t)ceil(__dmul_rn(fast_exp_rn(x), 4503599627370496.0));
-    const uint64_t mlo = (uint64_t)lo << 20, mhi = ((uint64_t)lo + (1ull << sh)) << 20;
-    if (mhi <= T) return 1;
-    if (mlo >= T) return -1;
-    return 0;
+    return f64_decide_slow(x, lo, sh, ulo, uhi);
 }
 
 // Exact decisions of the undecided calls (bit k of `ties`): the outputs are
@@ -141,15 +147,11 @@ __device__ __noinline__ uint32_t exact_flips_int(uint32_t ties, uint64_t base, i
     return f;
 }
 
-__device__ __noinline__ uint32_t exact_flips_f64(uint32_t ties, uint64_t base, int lane, uint32_t v,
-                                                 const double* dl, double beta, const uint64_t* jpoly) {
-    uint32_t f = 0;
-    for (int k = 0; k < 8; k++) {
-        if (!((ties >> k) & 1u)) continue;
-        const uint64_t res = lane_output(base, lane, v, k, jpoly);
-        if (metropolis_exact_f64(__dmul_rn(-dl[k], beta), res >> 12)) f |= 1u << k;
-    }
-    return f;
+// x = -dE beta of one undecided call k
+__device__ __noinline__ uint32_t exact_flip_f64(uint64_t base, int lane, uint32_t v, int k, double x,
+                                                const uint64_t* jpoly) {
+    const uint64_t res = lane_output(base, lane, v, k, jpoly);
+    return metropolis_exact_f64(x, res >> 12) ? 1u : 0u;
 }
 
 // Integer energies of one member (hubo.rs:176-189 restricted to QUBO, each
@@ -238,7 +240,7 @@ __device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uin
 // with s % C == r, reads spins from L2 and meets the other CTAs at a cluster
 // barrier (release / acquire) after every level.
 template <uint32_t MODE, bool GSP, bool SPLIT>
-__global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
+__global__ void __launch_bounds__(256, MODE == kModeF64 ? 3 : 4) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
     extern __shared__ __align__(16) uint64_t dsm[];
     __shared__ LvlMem ms[kLvlMaxMembers];
     __shared__ uint32_t s_item, s_steps;
@@ -571,7 +573,11 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                             ties |= (uint32_t)(r == 0) << k;
                         }
                         if (ties) {
-                            flips |= exact_flips_f64(ties, m.base, lane, v, dl, m.beta, L.jpoly);
+#pragma unroll
+                            for (int k = 0; k < 8; k++)
+                                if ((ties >> k) & 1u)
+                                    flips |= exact_flip_f64(m.base, lane, v, k, __dmul_rn(-dl[k], m.beta), L.jpoly)
+                                             << k;
                             if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
                         }
                     }
