@@ -240,7 +240,7 @@ __device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uin
 // with s % C == r, reads spins from L2 and meets the other CTAs at a cluster
 // barrier (release / acquire) after every level.
 template <uint32_t MODE, bool GSP, bool SPLIT>
-__global__ void __launch_bounds__(256, MODE == kModeF64 ? 3 : 4) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
+__global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
     extern __shared__ __align__(16) uint64_t dsm[];
     __shared__ LvlMem ms[kLvlMaxMembers];
     __shared__ uint32_t s_item, s_steps;
