@@ -886,13 +886,18 @@ struct Engine {
         const bool own = cells_view || serving;
         // classes: integer, f64, +-J form (one magnitude c per launch)
         std::vector<uint32_t> mem[3][2];
-        uint64_t live_count = 0;
+        uint64_t live_count = 0, pm_count = 0;
         uint32_t c0 = 0;
+        for (uint32_t i = 0; i < (uint32_t)D.size(); i++)
+            if (live(i) && level_ok(D[i], cells_view) && HI[i].pmj) pm_count++;
         for (uint32_t i = 0; i < (uint32_t)D.size(); i++) {
             if (!live(i) || !level_ok(D[i], cells_view)) continue;
             live_count++;
             const bool gsp = D[i].n > lvl_cap;
-            const uint32_t pm = use_pmj ? HI[i].pmj : 0u;
+            // the +-J form trades a dearer generator (exact masks per level) for
+            // far cheaper decisions: taken for large instances and for enough
+            // instances to fill the GPU, not for a few small latency-bound ones
+            const uint32_t pm = use_pmj && (gsp || pm_count >= (uint64_t)g_sm_count) ? HI[i].pmj : 0u;
             if (pm && !c0) c0 = pm & 0xFFFFu;
             const bool as_pmj = pm && (pm & 0xFFFFu) == c0;
             pmj_of[i] = as_pmj ? pm : 0u;
