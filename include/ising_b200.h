@@ -78,6 +78,11 @@ typedef struct ie_config {
                             per-lane kernels only (same results) */
     uint32_t max_cluster; /* level kernel: most CTAs (a thread block cluster) running one
                              large cell, 1, 2, 4, 8 or 16; 0: chosen by size (at most 16) */
+    int32_t bit_sliced;   /* level kernel, +-J problems (one coupling magnitude, lin = -sum w / 2,
+                             degree <= 8): 0 the bit-sliced form (one thread per site for all 64
+                             replicas) for problems too large for one CTA's shared memory and for
+                             runs of at least one such cell per SM; 1 always; -1 never. Same
+                             results either way */
 } ie_config;
 
 typedef struct ie_handle ie_handle;
@@ -203,6 +208,7 @@ typedef struct ie_batch_config {
     uint32_t tie_shift;         /* test hook, 0 in normal use: level-kernel decisions compare only
                                    the top 32 - tie_shift bits of the stored outputs, so the exact
                                    path (outputs recomputed from the lane seed) runs often */
+    int32_t bit_sliced;         /* as ie_config::bit_sliced */
 } ie_batch_config;
 
 /* count problems, each run as one cell of 64 replicas with its own seed. */

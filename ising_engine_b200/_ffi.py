@@ -38,7 +38,8 @@ class ie_config(C.Structure):
                 ("seed", C.c_uint64), ("num_temps", C.c_uint32), ("num_pops", C.c_uint32),
                 ("num_slices", C.c_uint32), ("exchange_interval", C.c_uint32),
                 ("force_f64", C.c_int32), ("device", C.c_int32), ("pt_path", C.c_int32),
-                ("use_icm", C.c_int32), ("kernel_form", C.c_int32), ("max_cluster", C.c_uint32)]
+                ("use_icm", C.c_int32), ("kernel_form", C.c_int32), ("max_cluster", C.c_uint32),
+                ("bit_sliced", C.c_int32)]
 
 
 class ie_problem_device(C.Structure):
@@ -62,7 +63,8 @@ class ie_batch_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("force_f64", C.c_int32),
                 ("threads_per_block", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("disable_windows", C.c_int32), ("use_graph", C.c_int32),
-                ("kernel_form", C.c_int32), ("item_sites", C.c_uint32), ("tie_shift", C.c_uint32)]
+                ("kernel_form", C.c_int32), ("item_sites", C.c_uint32), ("tie_shift", C.c_uint32),
+                ("bit_sliced", C.c_int32)]
 
 
 class ie_serve_config(C.Structure):

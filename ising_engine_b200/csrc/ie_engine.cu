@@ -785,7 +785,7 @@ struct Engine {
     uint32_t lvl_tie_shift = 0;
     bool lvl_split = true;    // large single-member items on thread block clusters
     uint32_t lvl_cluster_max = 0;  // most CTAs per cluster (0: 16)
-    bool use_pmj = true;      // +-J instances on the bit-sliced form
+    int32_t pmj_policy = 0;   // +-J instances on the bit-sliced form: 0 auto, 1 always, -1 never
     bool serving = false;     // serving launches: one threshold table per member
     std::vector<std::vector<uint32_t>> lv_sites, lv_off;  // per instance: sites by level, level starts
     std::vector<uint32_t> h_recoff;                       // level-record offset per site
@@ -881,8 +881,13 @@ struct Engine {
                                   Live live, bool one_per_item = false) {
         lvh.clear();
         std::vector<uint64_t> nnz_of(D.size());
-        std::vector<uint32_t> pmj_of(D.size());
-        for (size_t i = 0; i < D.size(); i++) nnz_of[i] = HI[i].nnz;
+        std::vector<uint32_t> pmj_of(D.size()), dmax_of(D.size(), 0);
+        for (size_t i = 0; i < D.size(); i++) {
+            nnz_of[i] = HI[i].nnz;
+            if (!live(i)) continue;
+            const std::vector<uint32_t>& rw = HI[i].rows;
+            for (size_t v = 0; v + 1 < rw.size(); v++) dmax_of[i] = std::max(dmax_of[i], rw[v + 1] - rw[v]);
+        }
         const bool own = cells_view || serving;
         // classes: integer, f64, +-J form (one magnitude c per launch)
         std::vector<uint32_t> mem[3][2];
@@ -897,7 +902,8 @@ struct Engine {
             // the +-J form trades a dearer generator (exact masks per level) for
             // far cheaper decisions: taken for large instances and for enough
             // instances to fill the GPU, not for a few small latency-bound ones
-            const uint32_t pm = use_pmj && (gsp || pm_count >= (uint64_t)g_sm_count) ? HI[i].pmj : 0u;
+            const bool want = pmj_policy > 0 || (pmj_policy == 0 && (gsp || pm_count >= (uint64_t)g_sm_count));
+            const uint32_t pm = want ? HI[i].pmj : 0u;
             if (pm && !c0) c0 = pm & 0xFFFFu;
             const bool as_pmj = pm && (pm & 0xFFFFu) == c0;
             pmj_of[i] = as_pmj ? pm : 0u;
@@ -936,8 +942,8 @@ struct Engine {
                 const uint32_t maxmem = alone ? 1u : own ? kLvlMaxOwnTables : kLvlMaxMembers;
                 std::vector<uint32_t> order;
                 double longest = 0;
-                build_level_items(D, nnz_of, pmj_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem, split,
-                                  lvh, order, longest);
+                build_level_items(D, nnz_of, dmax_of, pmj_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem,
+                                  split, lvh, order, longest);
                 wc->nitems = (uint32_t)order.size();
                 wc->work = longest;
                 for (uint32_t i : mem[m][g]) wc->site_steps += (double)D[i].n;
@@ -2235,6 +2241,8 @@ ie_status ie_create(const ie_problem* problem, const ie_config* config, ie_handl
     if (h->cfg.max_cluster > 16 || (h->cfg.max_cluster & (h->cfg.max_cluster - 1)))
         return fail(IE_ERR_INVALID, "max_cluster must be 0, 1, 2, 4, 8 or 16");
     h->eng.lvl_cluster_max = h->cfg.max_cluster;
+    if (h->cfg.bit_sliced < -1 || h->cfg.bit_sliced > 1) return fail(IE_ERR_INVALID, "bit_sliced must be -1, 0 or 1");
+    h->eng.pmj_policy = h->cfg.bit_sliced;
     const uint32_t pops = std::max<uint32_t>(h->cfg.num_pops, 1);
     if (pops > 1) {
         // QuantumField::new(n, 1, num_temps, num_pops): cell t + num_temps * p,
@@ -2299,16 +2307,18 @@ ie_status ie_step(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t 
     if (!h || !temps) return fail(IE_ERR_INVALID, "NULL argument");
     if (n_temps != h->cfg.num_temps) return fail(IE_ERR_INVALID, "n_temps must equal the handle's num_temps");
     IE_CUDA(cudaSetDevice(h->eng.device));
-    if (!h->eng.pop_len) return h->eng.run_pt(temps, n_steps, false, h->cfg.exchange_interval);
-    return h->eng.run_pt(ladder_rows(h->eng, temps, 1).data(), n_steps, false, h->cfg.exchange_interval);
+    if (!h->eng.pop_len) IE_TRY(h->eng.run_pt(temps, n_steps, false, h->cfg.exchange_interval));
+    else IE_TRY(h->eng.run_pt(ladder_rows(h->eng, temps, 1).data(), n_steps, false, h->cfg.exchange_interval));
+    return h->eng.check_err();
 }
 
 ie_status ie_run_schedule(ie_handle* h, const double* temps, uint32_t n_temps, uint64_t n_steps) {
     if (!h || !temps) return fail(IE_ERR_INVALID, "NULL argument");
     if (n_temps != h->cfg.num_temps) return fail(IE_ERR_INVALID, "n_temps must equal the handle's num_temps");
     IE_CUDA(cudaSetDevice(h->eng.device));
-    if (!h->eng.pop_len) return h->eng.run_pt(temps, n_steps, true, h->cfg.exchange_interval);
-    return h->eng.run_pt(ladder_rows(h->eng, temps, n_steps).data(), n_steps, true, h->cfg.exchange_interval);
+    if (!h->eng.pop_len) IE_TRY(h->eng.run_pt(temps, n_steps, true, h->cfg.exchange_interval));
+    else IE_TRY(h->eng.run_pt(ladder_rows(h->eng, temps, n_steps).data(), n_steps, true, h->cfg.exchange_interval));
+    return h->eng.check_err();
 }
 
 ie_status ie_run_pt(ie_handle* h) {
@@ -2326,7 +2336,7 @@ ie_status ie_run_pt(ie_handle* h) {
     }
     IE_CUDA(cudaStreamSynchronize(h->eng.stream));
     h->have_incumbent = true;
-    return IE_OK;
+    return h->eng.check_err();
 }
 
 // UltimateSolver::solve_population_annealing_diag (ultimate.rs:576-852) with
@@ -2654,6 +2664,8 @@ ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint
     }
     if (cfg.tie_shift > 31) return fail(IE_ERR_INVALID, "tie_shift must be below 32");
     b->eng.lvl_tie_shift = cfg.tie_shift;
+    if (cfg.bit_sliced < -1 || cfg.bit_sliced > 1) return fail(IE_ERR_INVALID, "bit_sliced must be -1, 0 or 1");
+    b->eng.pmj_policy = cfg.bit_sliced;
     if (cfg.threads_per_block && (cfg.threads_per_block % 32 || cfg.threads_per_block > 256))
         return fail(IE_ERR_INVALID, "threads_per_block must be a multiple of 32, at most 256");
     if (cfg.threads_per_block) b->eng.lvl_threads = (int)cfg.threads_per_block;

@@ -366,6 +366,8 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     if (s < ms[k].steps && e && (c * e) % 2 == 0)
                         tabs64[k * (kLvlTab / 2) + e] = metropolis_threshold((int)(c * e / 2), ms[k].beta);
                 }
+                // the generator reads these thresholds
+                __syncthreads();
             }
             // generator phase: chain j = (this CTA's segment j / 8, lane j % 8)
             for (uint32_t j = tid;; j += T) {
@@ -424,6 +426,33 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
             uint32_t e0 = I.nlvl ? __ldg(lo) : 0u, e1 = I.nlvl ? __ldg(lo + 1) : 0u;
             LvlEntry nxt{0, 0};
             for (uint32_t l = 0; l < I.nlvl; l++) {
+                // items of high degree (records of several lines): threads
+                // without a task on this level bring into L1 the entries of
+                // level l + 3 and the records and output rows of level l + 2
+                // (whose entries came a level earlier); all are read-only
+                // during the phase. (With short records the first task's
+                // prefetch before each barrier covers them, and this would only
+                // take issue slots from the level's chains.)
+                if (I.dmax > 8) {
+                    const uint32_t busy = (MODE == kModePmJ ? 1u : 8u) * (e1 - e0);
+                    if ((uint32_t)tid >= busy && l + 2 < I.nlvl) {
+                        const uint32_t stride = (uint32_t)T - busy, t0 = (uint32_t)tid - busy;
+                        if (l + 3 < I.nlvl) {
+                            const uint32_t b0 = __ldg(lo + (l + 3) * csize), b1 = __ldg(lo + (l + 3) * csize + 1);
+                            for (uint32_t j = 16u * t0; j < b1 - b0; j += 16u * stride)
+                                prefetch_l1(L.entries + I.ent0 + b0 + j);
+                        }
+                        const uint32_t a0 = __ldg(lo + (l + 2) * csize), a1 = __ldg(lo + (l + 2) * csize + 1);
+                        for (uint32_t j = t0; j < a1 - a0; j += stride) {
+                            const LvlEntry en = load_entry(L.entries + I.ent0 + a0 + j);
+                            prefetch_l1(L.lrecs + 4ull * en.rec);
+                            prefetch_l1(L.lrecs + 4ull * en.rec + 32);
+                            const uint32_t* kr = kb + (size_t)(en.site & ((1u << kLvlFlatBits) - 1u)) * 64;
+                            prefetch_l1(kr);
+                            if (MODE != kModePmJ) prefetch_l1(kr + 32);
+                        }
+                    }
+                }
                 if constexpr (MODE == kModePmJ) {
                     // one thread per site, all 64 replicas at once: cnt = number of
                     // neighbours j with x_j ^ (w_j < 0) = 1, kept as 4 bit planes;

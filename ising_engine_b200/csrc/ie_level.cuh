@@ -41,6 +41,7 @@ struct LvlItem {
     uint32_t gsp;    // 1: one member whose spins stay in global memory
     uint32_t split;  // CTAs (a cluster) running the item; lvloff holds nlvl * split + 1 offsets,
                      // level l's sites for CTA r (segment % split == r) at [l split + r]
+    uint32_t dmax;   // largest site degree of the members
 };
 
 struct LvlMember {

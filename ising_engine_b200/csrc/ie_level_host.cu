@@ -219,7 +219,7 @@ void site_levels(const LvlSource& s, std::vector<uint32_t>& sites, std::vector<u
 }
 
 void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_t>& nnz_of,
-                       const std::vector<uint32_t>& pmj_of,
+                       const std::vector<uint32_t>& dmax_of, const std::vector<uint32_t>& pmj_of,
                        const std::vector<std::vector<uint32_t>>& lv_sites,
                        const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& recoff,
                        const std::vector<uint32_t>& mem,
@@ -265,6 +265,7 @@ void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_
             out.max_segs = std::max(out.max_segs, ns);
             it.nseg += ns;
             it.H = std::max(it.H, d.H);
+            it.dmax = std::max(it.dmax, dmax_of[g[slot]]);
             depth = std::max(depth, (uint32_t)lv_off[d.owner].size() - 1);
             const double deg = d.n ? (double)nnz_of[g[slot]] / d.n : 0.0;
             w += (double)d.n * (deg + 12.0) * (d.mode == kModeF64 ? 2.5 : 1.0);

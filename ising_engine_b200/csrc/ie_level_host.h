@@ -64,7 +64,7 @@ struct LvlHost {
     }
 };
 void build_level_items(const std::vector<InstDesc>& D, const std::vector<uint64_t>& nnz_of,
-                       const std::vector<uint32_t>& pmj_of,
+                       const std::vector<uint32_t>& dmax_of, const std::vector<uint32_t>& pmj_of,
                        const std::vector<std::vector<uint32_t>>& lv_sites,
                        const std::vector<std::vector<uint32_t>>& lv_off, const std::vector<uint32_t>& recoff,
                        const std::vector<uint32_t>& mem,

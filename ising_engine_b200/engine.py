@@ -43,7 +43,7 @@ class Engine:
                  exchange_interval: int = 1, temp_max: float = 1.0, temp_min: float = 0.1,
                  sweeps_per_exchange: int = 1, total_exchanges: int = 1, force_f64: bool = False,
                  device: int = 0, pt_path: int = 0, num_pops: int = 1, use_icm: bool = False,
-                 kernel_form: int = 0, max_cluster: int = 0):
+                 kernel_form: int = 0, max_cluster: int = 0, bit_sliced: int = 0):
         self._L = _ffi.lib()
         self.model = model
         self.num_temps = int(num_temps)
@@ -55,7 +55,7 @@ class Engine:
         cfg = _ffi.ie_config(temp_max, temp_min, sweeps_per_exchange, total_exchanges,
                              seed & 0xFFFFFFFFFFFFFFFF, self.num_temps, self.num_pops, 1, exchange_interval,
                              int(force_f64), device, pt_path, int(use_icm), int(kernel_form),
-                             int(max_cluster))
+                             int(max_cluster), int(bit_sliced))
         h = C.c_void_p()
         _ffi.check(self._L.ie_create(C.byref(prob), C.byref(cfg), C.byref(h)))
         self._h = h
@@ -192,7 +192,8 @@ class BatchEngine:
 
     def __init__(self, models, seeds, device: int = 0, force_f64: bool = False,
                  threads_per_block: int = 0, blocks_per_sm: int = 0, windows: bool = True,
-                 graph: bool = False, kernel_form: int = 0, item_sites: int = 0, tie_shift: int = 0):
+                 graph: bool = False, kernel_form: int = 0, item_sites: int = 0, tie_shift: int = 0,
+                 bit_sliced: int = 0):
         self._L = _ffi.lib()
         self.kernel_form = int(kernel_form)
         self.models = list(models)
@@ -204,7 +205,7 @@ class BatchEngine:
             raise ValueError("one seed per problem")
         cfg = _ffi.ie_batch_config(device, int(force_f64), threads_per_block, blocks_per_sm,
                                    0 if windows else 1, 1 if graph else 0, int(kernel_form),
-                                   int(item_sites), int(tie_shift))
+                                   int(item_sites), int(tie_shift), int(bit_sliced))
         h = C.c_void_p()
         _ffi.check(self._L.ie_batch_create(probs, self.count, _p(self.seeds), C.byref(cfg),
                                            C.byref(h)))

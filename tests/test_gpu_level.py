@@ -150,7 +150,7 @@ def test_bit_sliced_pm_j_form_batch():
     seeds = np.arange(len(models), dtype=np.uint64) * 31 + 7
     temps = I.sa_temps(80, 0.2, 3.0)
     words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
-    b = BatchEngine(models, seeds)
+    b = BatchEngine(models, seeds, bit_sliced=1)
     b.init_random()
     b.run_schedule(temps[:33])
     b.run_schedule(temps[33:])
@@ -163,7 +163,7 @@ def test_bit_sliced_pm_j_form_batch():
     v = (np.arange(m.num_vars) % 3 == 0).astype(np.int8)
     temps = I.geometric_beta_ladder(6, 0.3, 1.5)
     ref = O.run_schedule(m, np.tile(temps, (25, 1)), 3, clamped=f, clamp_val=v, collect_stats=True)
-    with Engine(m, num_temps=6, seed=3, pt_path=2) as eng:
+    with Engine(m, num_temps=6, seed=3, pt_path=2, bit_sliced=1) as eng:
         eng.set_clamps(f, v)
         eng.init_random()
         eng.step(temps, 25)
