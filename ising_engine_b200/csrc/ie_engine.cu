@@ -730,6 +730,7 @@ struct Engine {
         uint32_t ntab = 1;
         int grid = 0;
         uint64_t keystride = 0, keyoff = 0;
+        uint32_t ov = 0;  // > 0: sweeps overlapped, a generator group of ov threads per CTA
         DevBuf<uint32_t> order;
     };
     static constexpr int kLevelForm = 32;  // tpl tag of a level-kernel class
@@ -784,6 +785,7 @@ struct Engine {
     int lvl_threads = 256;
     uint32_t lvl_tie_shift = 0;
     bool lvl_split = true;    // large single-member items on thread block clusters
+    bool lvl_overlap = true;  // latency-bound launches overlap the generator and decision phases
     uint32_t lvl_cluster_max = 0;  // most CTAs per cluster (0: 16)
     int32_t pmj_policy = 0;   // +-J instances on the bit-sliced form: 0 auto, 1 always, -1 never
     bool serving = false;     // serving launches: one threshold table per member
@@ -942,14 +944,32 @@ struct Engine {
                 const uint32_t maxmem = alone ? 1u : own ? kLvlMaxOwnTables : kLvlMaxMembers;
                 std::vector<uint32_t> order;
                 double longest = 0;
+                const size_t item_begin = lvh.items.size();
                 build_level_items(D, nnz_of, dmax_of, pmj_of, lv_sites, lv_off, h_recoff, mem[m][g], g != 0, cap, maxmem,
                                   split, lvh, order, longest);
                 wc->nitems = (uint32_t)order.size();
                 wc->work = longest;
                 for (uint32_t i : mem[m][g]) wc->site_steps += (double)D[i].n;
                 wc->ntab = own ? std::max<uint32_t>(maxmem, 1u) : 1u;
-                const size_t smem = level_smem(wc->mode, wc->ntab, g ? 0 : lvl_cap);
-                int occ = level_occupancy(wc->mode, g != 0, lvl_threads, smem);
+                // latency-bound launches (an item per CTA, narrow levels): the
+                // generator half of each CTA runs one sweep ahead of the decider half
+                {
+                    double sites = 0, levels = 0;
+                    for (size_t q = item_begin; q < lvh.items.size(); q++) {
+                        sites += (double)lvh.items[q].sites;
+                        levels += (double)std::max<uint32_t>(lvh.items[q].nlvl, 1);
+                    }
+                    const double width = (kmode == kModePmJ ? 1.0 : 8.0) * sites / std::max(levels, 1.0);
+                    const uint32_t gen = kLvlOverlapGen;
+                    const int occ0 = level_occupancy(wc->mode, g != 0, lvl_threads + (int)gen,
+                                                     level_smem(wc->mode, wc->ntab, g ? 0 : lvl_cap, true));
+                    wc->ov = lvl_overlap && split == 1 && occ0 > 0 && wc->nitems <= (uint32_t)(occ0 * g_sm_count) &&
+                                     width <= lvl_threads
+                                 ? gen
+                                 : 0u;
+                }
+                const size_t smem = level_smem(wc->mode, wc->ntab, g ? 0 : lvl_cap, wc->ov != 0);
+                int occ = level_occupancy(wc->mode, g != 0, lvl_threads + (int)wc->ov, smem);
                 if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "level kernel does not fit on an SM");
                 if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
                 wc->split = split;
@@ -959,7 +979,7 @@ struct Engine {
                 } else {
                     wc->grid = std::max(1, std::min<int>((int)wc->nitems, occ * g_sm_count));
                 }
-                wc->keystride = 64ull * (g ? maxn : lvl_cap);
+                wc->keystride = 64ull * (g ? maxn : lvl_cap) * (wc->ov ? 2 : 1);
                 wc->keyoff = keytotal;
                 keytotal += wc->keystride * (uint64_t)(wc->grid / split);
                 IE_TRY(wc->order.upload(order, stream));
@@ -998,6 +1018,8 @@ struct Engine {
         L.lrecs = d_lrecs.p;
         L.keybuf = d_keybuf.p + wc.keyoff;
         L.keystride = wc.keystride;
+        L.ov = wc.ov;
+        L.keyhalf = wc.ov ? wc.keystride / 2 : 0;
         L.spin_cap = wc.gsp ? 0u : lvl_cap;
         L.ntab = wc.ntab;
         L.tie_shift = lvl_tie_shift;

@@ -39,7 +39,7 @@ cudaError_t launch_best_extract(const DevArrays& A, uint32_t inst, const double*
                                 double* best, int32_t* found, cudaStream_t st);
 cudaError_t launch_one_opt(const DevArrays& A, uint32_t inst, int8_t* state, const uint8_t* clamped, double* gains,
                            double* improvement, uint64_t* flips, uint64_t max_flips, cudaStream_t st);
-size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap);
+size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap, bool ov = false);
 int level_occupancy(uint32_t mode, bool gsp, int threads, size_t smem);
 // resident clusters of `split` CTAs of the split (cluster) form, GPU-wide
 int level_clusters(uint32_t mode, int threads, size_t smem, uint32_t split);

@@ -43,8 +43,9 @@ namespace ie {
 
 struct LvlMem {
     const double* temps;
-    uint64_t site, spin, energy, pos0, step0, base;
-    double beta;
+    uint64_t site, spin, energy, pos0, step0;
+    uint64_t base[2];  // lane seed base of the sweep in buffer b (two sweeps in flight when overlapped)
+    double beta[2];
     uint32_t key[8];
     uint32_t inst, flat, n, steps, tstride, cell, owner, fin;
     uint32_t pmj;  // +-J form: c | degree << 16
@@ -240,7 +241,9 @@ __device__ void member_energy_f64(const DevArrays& A, const LvlMem& m, const uin
 // with s % C == r, reads spins from L2 and meets the other CTAs at a cluster
 // barrier (release / acquire) after every level.
 template <uint32_t MODE, bool GSP, bool SPLIT>
-__global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
+// 64 registers: four CTAs of 256 threads per SM; overlapped launches add a
+// generator group to the 256 decider threads (at most 384 threads)
+__global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) {
     extern __shared__ __align__(16) uint64_t dsm[];
     __shared__ LvlMem ms[kLvlMaxMembers];
     __shared__ uint32_t s_item, s_steps;
@@ -250,7 +253,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
     const int lane = tid & 7;
     const bool own_tab = R.serve != 0 || R.cells != 0;
     uint32_t* const tabs = reinterpret_cast<uint32_t*>(dsm);
-    uint2* const lut = reinterpret_cast<uint2*>(tabs + (size_t)L.ntab * kLvlTab);
+    uint2* const lut = reinterpret_cast<uint2*>(tabs + (size_t)L.ntab * kLvlTab * (L.ov ? 2u : 1u));
     uint64_t* const ssw = reinterpret_cast<uint64_t*>(lut + (MODE != kModeF64 ? 512 : 0));
     uint64_t* const tabs64 = reinterpret_cast<uint64_t*>(tabs);  // +-J form: thresholds per level
     uint32_t crank = 0, csize = 1;
@@ -295,8 +298,8 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
         if (it == 0xffffffffu) break;
         const LvlItem I = L.items[it];
         if ((!GSP && I.sites > L.spin_cap) || I.nmem > kLvlMaxMembers || I.nmem == 0 ||
-            (own_tab && I.nmem > L.ntab) || (uint64_t)I.sites * 64 > L.keystride || (GSP && I.nmem != 1) ||
-            I.split != csize) {
+            (own_tab && I.nmem > L.ntab) || (uint64_t)I.sites * 64 > (L.ov ? L.keyhalf : L.keystride) ||
+            (GSP && I.nmem != 1) || I.split != csize || (L.ov && !SPLIT && (L.ov % 32 || L.ov >= (uint32_t)T))) {
             if (tid == 0) atomicExch(A.err, 2);  // host sizing error: report, skip the item
             continue;
         }
@@ -339,38 +342,46 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                 for (uint32_t i = tid; i < ms[k].n; i += T) ssw[ms[k].flat + i] = gw[i];
             }
         }
-        for (uint32_t s = 0; s < nsteps; s++) {
-            __syncthreads();
-            for (uint32_t k = tid; k < I.nmem; k += T) {
+        // Sweep s uses buffer b = s & 1 when overlapped (L.ov: the generator
+        // warps produce sweep s + 1 while the decider warps decide sweep s),
+        // else buffer 0. prep: seed bases and betas; tables: thresholds.
+        auto prep = [&](uint32_t s, uint32_t b, uint32_t t0, uint32_t TT) {
+            for (uint32_t k = t0; k < I.nmem; k += TT) {
                 LvlMem& m = ms[k];
                 if (s < m.steps) {
-                    m.base = chacha8_draw(m.key, m.pos0 + s) + m.cell;
-                    m.beta = __ddiv_rn(1.0, m.temps[(size_t)m.tstride * s]);
+                    m.base[b] = chacha8_draw(m.key, m.pos0 + s) + m.cell;
+                    m.beta[b] = __ddiv_rn(1.0, m.temps[(size_t)m.tstride * s]);
                 }
             }
-            __syncthreads();
+        };
+        auto tables = [&](uint32_t s, uint32_t b, uint32_t t0, uint32_t TT) {
             if constexpr (MODE == kModeInt) {
                 const int H = I.H, W = 2 * H + 1;
                 const uint32_t nt = own_tab ? I.nmem : 1u;
-                for (uint32_t i = tid; i < nt * (uint32_t)W; i += T) {
+                uint32_t* const tb = tabs + (size_t)b * L.ntab * kLvlTab;
+                for (uint32_t i = t0; i < nt * (uint32_t)W; i += TT) {
                     const uint32_t k = i / (uint32_t)W, idx = i % (uint32_t)W;
-                    if (s < ms[k].steps) tabs[k * kLvlTab + idx] = q_threshold((int)idx - H, ms[k].beta);
+                    if (s < ms[k].steps) tb[k * kLvlTab + idx] = q_threshold((int)idx - H, ms[k].beta[b]);
                 }
             }
             if constexpr (MODE == kModePmJ) {
                 // threshold of dE = c e / 2 for e = 1..15 (the odd e only occur
                 // for even c); the full 64-bit form, decided exactly in the generator
                 const uint32_t nt = own_tab ? I.nmem : 1u;
-                for (uint32_t i = tid; i < nt * 16u; i += T) {
+                uint64_t* const tb = tabs64 + (size_t)b * L.ntab * (kLvlTab / 2);
+                for (uint32_t i = t0; i < nt * 16u; i += TT) {
                     const uint32_t k = i >> 4, e = i & 15u, c = ms[k].pmj & 0xFFFFu;
                     if (s < ms[k].steps && e && (c * e) % 2 == 0)
-                        tabs64[k * (kLvlTab / 2) + e] = metropolis_threshold((int)(c * e / 2), ms[k].beta);
+                        tb[k * (kLvlTab / 2) + e] = metropolis_threshold((int)(c * e / 2), ms[k].beta[b]);
                 }
-                // the generator reads these thresholds
-                __syncthreads();
             }
-            // generator phase: chain j = (this CTA's segment j / 8, lane j % 8)
-            for (uint32_t j = tid;; j += T) {
+        };
+        // generator phase of sweep s into buffer b by threads t0 .. t0 + TT:
+        // chain j = (this CTA's segment j / 8, lane j % 8)
+        auto generate = [&](uint32_t s, uint32_t b, uint32_t t0, uint32_t TT) {
+            uint32_t* const kbb = kb + (size_t)b * L.keyhalf;
+            const uint64_t* const tb64 = tabs64 + (size_t)b * L.ntab * (kLvlTab / 2);
+            for (uint32_t j = t0;; j += TT) {
                 const uint32_t sg = crank + csize * (j >> 3);
                 if (sg >= I.nseg) break;
                 const uint32_t sd = __ldg(L.segs + I.seg0 + sg);
@@ -378,7 +389,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                 const LvlMem& m = ms[slot];
                 if (s >= m.steps) continue;
                 Xoshiro x;
-                x.seed_lane(m.base, lane);
+                x.seed_lane(m.base[b], lane);
                 if (seg) x.jump(L.jpoly + 4ull * seg);
                 const uint32_t v0 = seg * kLvlSeg, v1 = min(m.n, v0 + kLvlSeg);
                 if constexpr (MODE == kModePmJ) {
@@ -386,11 +397,11 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     // holds [output <= U(dE of uphill level i + 1)] for the lane's
                     // 8 calls, exactly (engine.rs:665-666)
                     const uint32_t D = m.pmj >> 16, odd = D & 1u, nl = (D + 1) >> 1;
-                    const uint64_t* U = tabs64 + (own_tab ? slot * (kLvlTab / 2) : 0u);
+                    const uint64_t* U = tb64 + (own_tab ? slot * (kLvlTab / 2) : 0u);
                     uint64_t ul[4];
 #pragma unroll
                     for (int i = 0; i < 4; i++) ul[i] = (uint32_t)i < nl ? U[2 * (i + 1) - odd] : 0ull;
-                    uint8_t* out8 = reinterpret_cast<uint8_t*>(kb + (size_t)(m.flat + v0) * 64) + lane;
+                    uint8_t* out8 = reinterpret_cast<uint8_t*>(kbb + (size_t)(m.flat + v0) * 64) + lane;
                     for (uint32_t v = v0; v < v1; v++) {
                         uint32_t a[4] = {0, 0, 0, 0};
 #pragma unroll
@@ -405,7 +416,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                         out8 += 256;
                     }
                 } else {
-                    uint4* out = reinterpret_cast<uint4*>(kb + (size_t)(m.flat + v0) * 64 + lane * 8);
+                    uint4* out = reinterpret_cast<uint4*>(kbb + (size_t)(m.flat + v0) * 64 + lane * 8);
                     for (uint32_t v = v0; v < v1; v++) {
                         uint32_t h[8];
 #pragma unroll
@@ -416,10 +427,15 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     }
                 }
             }
-            __syncthreads();
-            // decision phase, level by level; before each level barrier a
-            // thread loads its first entry of the next level and prefetches
-            // that site's record and outputs (read-only during the phase)
+        };
+        // decision phase of sweep s from buffer b by threads t0 .. t0 + TT
+        // (thread t0 + i serves lane i % 8), level by level; before each level
+        // barrier a thread loads its first entry of the next level and
+        // prefetches that site's record and outputs (read-only during the phase)
+        auto decide = [&](uint32_t s, uint32_t b, uint32_t t0, uint32_t TT) {
+            const uint32_t* const kbb = kb + (size_t)b * L.keyhalf;
+            const uint32_t* const tabb = tabs + (size_t)b * L.ntab * kLvlTab;
+            const uint32_t dt = (uint32_t)tid - t0;
             const uint32_t sh = L.tie_shift;
             // this CTA's entries of level l: lvloff[lvl0 + l C + r .. + 1]
             const uint32_t* const lo = L.lvloff + I.lvl0 + crank;
@@ -435,19 +451,19 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                 // take issue slots from the level's chains.)
                 if (I.dmax > 8) {
                     const uint32_t busy = (MODE == kModePmJ ? 1u : 8u) * (e1 - e0);
-                    if ((uint32_t)tid >= busy && l + 2 < I.nlvl) {
-                        const uint32_t stride = (uint32_t)T - busy, t0 = (uint32_t)tid - busy;
+                    if (dt >= busy && l + 2 < I.nlvl) {
+                        const uint32_t stride = TT - busy, q0 = dt - busy;
                         if (l + 3 < I.nlvl) {
                             const uint32_t b0 = __ldg(lo + (l + 3) * csize), b1 = __ldg(lo + (l + 3) * csize + 1);
-                            for (uint32_t j = 16u * t0; j < b1 - b0; j += 16u * stride)
+                            for (uint32_t j = 16u * q0; j < b1 - b0; j += 16u * stride)
                                 prefetch_l1(L.entries + I.ent0 + b0 + j);
                         }
                         const uint32_t a0 = __ldg(lo + (l + 2) * csize), a1 = __ldg(lo + (l + 2) * csize + 1);
-                        for (uint32_t j = t0; j < a1 - a0; j += stride) {
+                        for (uint32_t j = q0; j < a1 - a0; j += stride) {
                             const LvlEntry en = load_entry(L.entries + I.ent0 + a0 + j);
                             prefetch_l1(L.lrecs + 4ull * en.rec);
                             prefetch_l1(L.lrecs + 4ull * en.rec + 32);
-                            const uint32_t* kr = kb + (size_t)(en.site & ((1u << kLvlFlatBits) - 1u)) * 64;
+                            const uint32_t* kr = kbb + (size_t)(en.site & ((1u << kLvlFlatBits) - 1u)) * 64;
                             prefetch_l1(kr);
                             if (MODE != kModePmJ) prefetch_l1(kr + 32);
                         }
@@ -460,8 +476,8 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     // x_v = 1 (|w| = c, lin = -sum w / 2), uphill level i at cnt =
                     // floor(D/2) + i resp. ceil(D/2) - i; flip unless an uphill
                     // level's acceptance bit is clear
-                    for (uint32_t i = tid; i < e1 - e0; i += T) {
-                        const LvlEntry en = (i == (uint32_t)tid && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + i);
+                    for (uint32_t i = dt; i < e1 - e0; i += TT) {
+                        const LvlEntry en = (i == dt && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + i);
                         const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
                         const LvlMem& m = ms[slot];
                         if (s >= m.steps) continue;
@@ -488,7 +504,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                                 }
                             }
                         }
-                        const uint64_t* A = reinterpret_cast<const uint64_t*>(kb + (size_t)f * 64);
+                        const uint64_t* A = reinterpret_cast<const uint64_t*>(kbb + (size_t)f * 64);
                         const uint32_t nl = (D + 1) >> 1, hD = D >> 1, cD = (D + 1) >> 1;
                         uint64_t bad = 0;
                         for (uint32_t lv = 1; lv <= nl; lv++) {
@@ -504,9 +520,9 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                         }
                         sw[f] = xw ^ ~bad;
                     }
-                } else
-                for (uint32_t i = tid; i < 8u * (e1 - e0); i += T) {
-                    const LvlEntry en = (i == (uint32_t)tid && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + (i >> 3));
+                } else {
+                for (uint32_t i = dt; i < 8u * (e1 - e0); i += TT) {
+                    const LvlEntry en = (i == dt && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + (i >> 3));
                     const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
                     const LvlMem& m = ms[slot];
                     if (s >= m.steps) continue;
@@ -516,7 +532,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                     const uint32_t deg = hd.x & 0x7FFFFFFFu;
                     const uint32_t fb = m.flat;
                     const uint32_t xb = ld_spin<SPLIT>(spb + 8u * f);
-                    const uint4* kp = reinterpret_cast<const uint4*>(kb + (size_t)f * 64 + lane * 8);
+                    const uint4* kp = reinterpret_cast<const uint4*>(kbb + (size_t)f * 64 + lane * 8);
                     const uint4 k0 = kp[0], k1 = kp[1];
                     const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
                     uint32_t flips = 0, ties = 0;
@@ -547,7 +563,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                         // byte k of iL / iH = dE_k + H for replica lane + 8k
                         const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
                         const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
-                        const uint32_t* tb = tabs + (own_tab ? slot * kLvlTab : 0u);
+                        const uint32_t* tb = tabb + (own_tab ? slot * kLvlTab : 0u);
 #pragma unroll
                         for (int k = 0; k < 8; k++) {
                             const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
@@ -556,7 +572,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                             ties |= (uint32_t)(a == b) << k;
                         }
                         if (ties) {
-                            flips |= exact_flips_int(ties, m.base, lane, v, iL, iH, H, m.beta, L.jpoly);
+                            flips |= exact_flips_int(ties, m.base[b], lane, v, iL, iH, H, m.beta[b], L.jpoly);
                             if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
                         }
                     } else {
@@ -597,7 +613,7 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
                                 flips |= 1u << k;
                                 continue;
                             }
-                            const int r = f64_decide(dl[k], m.beta, mh[k], sh);
+                            const int r = f64_decide(dl[k], m.beta[b], mh[k], sh);
                             flips |= (uint32_t)(r > 0) << k;
                             ties |= (uint32_t)(r == 0) << k;
                         }
@@ -605,29 +621,74 @@ __global__ void __launch_bounds__(256, 4) level_kernel(DevArrays A, RunArgs R, L
 #pragma unroll
                             for (int k = 0; k < 8; k++)
                                 if ((ties >> k) & 1u)
-                                    flips |= exact_flip_f64(m.base, lane, v, k, __dmul_rn(-dl[k], m.beta), L.jpoly)
+                                    flips |= exact_flip_f64(m.base[b], lane, v, k, __dmul_rn(-dl[k], m.beta[b]), L.jpoly)
                                              << k;
                             if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
                         }
                     }
                     spb[8u * f] = (uint8_t)(xb ^ flips);
                 }
+                }
                 if (l + 1 < I.nlvl) {
                     e0 = __ldg(lo + (l + 1) * csize);
                     e1 = __ldg(lo + (l + 1) * csize + 1);
-                    if (MODE != kModePmJ && (uint32_t)tid < 8u * (e1 - e0)) {
-                        nxt = load_entry(L.entries + I.ent0 + e0 + (tid >> 3));
+                    if (MODE != kModePmJ && dt < 8u * (e1 - e0)) {
+                        nxt = load_entry(L.entries + I.ent0 + e0 + (dt >> 3));
                         prefetch_l1(L.lrecs + 4ull * nxt.rec);
-                        prefetch_l1(kb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64 + lane * 8);
+                        prefetch_l1(kbb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64 + lane * 8);
                     }
-                    if (MODE == kModePmJ && (uint32_t)tid < e1 - e0) {
-                        nxt = load_entry(L.entries + I.ent0 + e0 + tid);
+                    if (MODE == kModePmJ && dt < e1 - e0) {
+                        nxt = load_entry(L.entries + I.ent0 + e0 + dt);
                         prefetch_l1(L.lrecs + 4ull * nxt.rec);
-                        prefetch_l1(kb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64);
+                        prefetch_l1(kbb + (size_t)(nxt.site & ((1u << kLvlFlatBits) - 1u)) * 64);
                     }
                 }
-                if constexpr (SPLIT) cg::this_cluster().sync();
-                else __syncthreads();
+                if constexpr (SPLIT) {
+                    cg::this_cluster().sync();
+                } else {
+                    if (TT == (uint32_t)T) __syncthreads();
+                    else asm volatile("bar.sync 1, %0;" ::"r"(TT) : "memory");
+                }
+            }
+        };
+        // the sweeps: overlapped (generator warps t < L.ov one sweep ahead of
+        // the decider warps t >= L.ov) or in sequence with every thread on each phase
+        const bool ov = L.ov && !SPLIT;
+        if (!ov) {
+            for (uint32_t s = 0; s < nsteps; s++) {
+                __syncthreads();
+                prep(s, 0, tid, T);
+                __syncthreads();
+                tables(s, 0, tid, T);
+                __syncthreads();
+                generate(s, 0, tid, T);
+                __syncthreads();
+                decide(s, 0, 0, T);
+            }
+        } else if (nsteps) {
+            const uint32_t gn = L.ov, dn = (uint32_t)T - L.ov;
+            __syncthreads();
+            prep(0, 0, tid, T);
+            __syncthreads();
+            tables(0, 0, tid, T);
+            __syncthreads();
+            generate(0, 0, tid, T);
+            for (uint32_t s = 0; s < nsteps; s++) {
+                // sweep s's outputs, tables and bases are complete; buffer
+                // (s + 1) & 1 is free (sweep s - 1 is decided)
+                __syncthreads();
+                const uint32_t nb = (s + 1) & 1u;
+                if ((uint32_t)tid < gn) {
+                    if (s + 1 < nsteps) {
+                        prep(s + 1, nb, tid, gn);
+                        asm volatile("bar.sync 2, %0;" ::"r"(gn) : "memory");
+                        tables(s + 1, nb, tid, gn);
+                        asm volatile("bar.sync 2, %0;" ::"r"(gn) : "memory");
+                        generate(s + 1, nb, tid, gn);
+                    }
+                } else {
+                    decide(s, s & 1u, gn, dn);
+                }
             }
         }
         if constexpr (SPLIT) {
@@ -683,8 +744,8 @@ template __global__ void level_kernel<kModePmJ, false, false>(DevArrays, RunArgs
 template __global__ void level_kernel<kModePmJ, true, false>(DevArrays, RunArgs, LvlArgs);
 template __global__ void level_kernel<kModePmJ, true, true>(DevArrays, RunArgs, LvlArgs);
 
-size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap) {
-    return (size_t)ntab * kLvlTab * 4 + (mode != kModeF64 ? 512 * 8 : 0) + (size_t)spin_cap * 8;
+size_t level_smem(uint32_t mode, uint32_t ntab, uint32_t spin_cap, bool ov) {
+    return (size_t)ntab * kLvlTab * 4 * (ov ? 2 : 1) + (mode != kModeF64 ? 512 * 8 : 0) + (size_t)spin_cap * 8;
 }
 
 template <uint32_t MODE, bool GSP, bool SPLIT>
@@ -744,7 +805,8 @@ int level_clusters(uint32_t mode, int threads, size_t smem, uint32_t split) {
 
 cudaError_t launch_level(const DevArrays& A, const RunArgs& R, const LvlArgs& L, uint32_t mode, bool gsp, int threads,
                          int grid, cudaStream_t st, uint32_t split) {
-    const size_t smem = level_smem(mode, L.ntab, gsp ? 0 : L.spin_cap);
+    if (L.ov && split <= 1) threads += (int)L.ov;  // the generator group of an overlapped launch
+    const size_t smem = level_smem(mode, L.ntab, gsp ? 0 : L.spin_cap, L.ov != 0);
     if (split > 1) {
         cudaLaunchAttribute attr;
         const cudaLaunchConfig_t cfg = level_config(grid, threads, smem, st, split, &attr);

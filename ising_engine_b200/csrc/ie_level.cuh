@@ -26,6 +26,7 @@ constexpr uint32_t kLvlMaxMembers = 64;    // instances per item
 constexpr uint32_t kLvlMaxOwnTables = 16;  // members per item when each has its own threshold table
 constexpr uint32_t kLvlFlatBits = 26;      // entry = slot << 26 | flat site index within the item
 constexpr uint32_t kLvlTab = 256;          // u32 per threshold table (indices 0 .. 2H <= 254)
+constexpr uint32_t kLvlOverlapGen = 128;   // generator threads of an overlapped launch
 
 // One item: members[mem0 .. mem0 + nmem) share a CTA; their spin words are
 // laid out one after another (member slot s at flat offset members[s].flat).
@@ -73,8 +74,13 @@ struct LvlArgs {
     const uint64_t* jpoly;     // [j][4]: x^(8 kLvlSeg j) mod P(x), bit i = coefficient of x^i
     const uint32_t* recoff;    // per site (InstDesc::site + v): record offset in 16-byte units
     const uint32_t* lrecs;
-    uint32_t* keybuf;          // per CTA: keystride u32 (64 per flat site)
+    uint32_t* keybuf;          // per CTA: keystride u32 (64 per flat site, twice when overlapped)
     uint64_t keystride;
+    // > 0: each CTA overlaps sweeps, its first ov threads generating sweep
+    // s + 1 while the others decide sweep s; outputs, thresholds and seeds
+    // double-buffered (second output buffer at keyhalf)
+    uint32_t ov;
+    uint64_t keyhalf;
     uint32_t spin_cap;         // shared-memory spin words per CTA (0: global spins)
     uint32_t ntab;             // threshold tables per CTA (own tables: one per member)
     // Test hook: decisions compare only the top 32 - tie_shift bits of the
