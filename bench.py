@@ -67,6 +67,7 @@ def parse():
     p.add_argument("--serve-rates", type=float, nargs="+", default=[100.0, 300.0, 1000.0])
     p.add_argument("--serve-sweeps", type=int, nargs=2, default=[1000, 20000])
     p.add_argument("--serve-budget", type=int, default=1 << 20)
+    p.add_argument("--serve-tick-ms", type=float, default=200.0)
     p.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 4],
                    help="3: the batched headline workload; 1, 2, 4: the PT configurations alone")
     p.add_argument("--no-configs", action="store_true", help="skip configs 1, 2, 4 in the headline line")
@@ -470,7 +471,7 @@ def run_serve(args, device):
     reqs = [(m, s, I.sa_temps(sw)) for (m, s, sw) in reqs]
     attempts = sum(m.num_vars * 64.0 * len(t) for m, _, t in reqs)
     rows = []
-    with ServeEngine(device=device, site_budget=args.serve_budget) as srv:
+    with ServeEngine(device=device, site_budget=args.serve_budget, tick_us=int(args.serve_tick_ms * 1e3)) as srv:
         m0, s0, t0 = reqs[0]
         srv.submit(m0, s0, t0[:2])
         srv.run_all()  # warm-up: kernels loaded, pools touched
@@ -482,7 +483,7 @@ def run_serve(args, device):
                          "attempts_per_s": attempts / s["makespan_s"], "p50_ms": s["p50_ms"],
                          "p99_ms": s["p99_ms"], "mean_ms": s["mean_ms"], "makespan_s": s["makespan_s"],
                          "ticks": s["ticks"], "mean_tick_ms": s["mean_tick_ms"], "gpu_launches": tr.launches})
-    return {"rates": rows, "requests": len(reqs), "site_budget": args.serve_budget,
+    return {"rates": rows, "requests": len(reqs), "site_budget": args.serve_budget, "tick_ms": args.serve_tick_ms,
             "mean_attempts_per_request": attempts / len(reqs),
             "stream": f"N log-uniform [100, 20000], degree 4..32, int [-8,8] / f32 N(0,1) half each, "
                       f"SA {lo}..{hi} sweeps (beta 0.1 -> 5.0), Poisson arrivals"}

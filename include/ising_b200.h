@@ -296,9 +296,12 @@ ie_status ie_sa_run_static(const ie_problem_device* problem, uint64_t seed, cons
  * is admitted, first come first served, once a slot and room in every device
  * pool (sites, couplings, records, schedule) are free; it stays resident
  * (spins, energies, generator position) until its schedule is done, and
- * every tick advances each resident request by up to max(1, site_budget / N)
- * steps in one group of persistent launches, so requests of different sizes
- * and arrival times share the GPU. A request's result does not depend on
+ * every tick advances each resident request in one group of persistent
+ * launches, so requests of different sizes and arrival times share the GPU.
+ * On the level kernel a tick gives each request the steps that its work item
+ * runs in about tick_us of device time, from the cycles per step that item
+ * measured in the previous tick (a request's first tick: at most 64 steps);
+ * on the per-lane kernels up to max(1, site_budget / N) steps. A request's result does not depend on
  * what else is resident: it equals ie_batch_run_schedule of the same problem,
  * seed and temperatures alone.
  * ie_serve_submit, ie_serve_poll and ie_serve_result may be called from any
@@ -314,6 +317,8 @@ typedef struct ie_serve_config {
     uint64_t max_couplings;      /* summed stored couplings, both triangles (0: 2^27) */
     uint64_t max_schedule_steps; /* summed schedule lengths (0: 2^25) */
     int32_t kernel_form;         /* 0: the level kernel (default); 1: the per-lane kernels */
+    uint32_t tick_us;            /* level kernel: device time per tick to plan for, microseconds
+                                    (0: 200000) */
 } ie_serve_config;
 
 ie_status ie_serve_create(const ie_serve_config* config, ie_serve** out);

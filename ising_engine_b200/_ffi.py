@@ -70,7 +70,7 @@ class ie_batch_config(C.Structure):
 class ie_serve_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("force_f64", C.c_int32), ("max_requests", C.c_uint32),
                 ("site_budget", C.c_uint32), ("max_sites", C.c_uint64), ("max_couplings", C.c_uint64),
-                ("max_schedule_steps", C.c_uint64), ("kernel_form", C.c_int32)]
+                ("max_schedule_steps", C.c_uint64), ("kernel_form", C.c_int32), ("tick_us", C.c_uint32)]
 
 
 _vp = C.c_void_p

@@ -1822,6 +1822,14 @@ struct ServeEngine {
     uint32_t n_active = 0;
     bool set_changed = true;     // a request was admitted or retired since the work items were built
     std::vector<uint32_t> unit;  // per slot: sites one unit of the site budget covers
+    // level kernel: per slot the steps of this tick, and the device cycles per
+    // step its work item measured in the last tick (0: not yet run)
+    std::vector<uint32_t> plan;
+    std::vector<float> cost;
+    DevBuf<uint32_t> d_plan;
+    DevBuf<float> d_cost;
+    double tick_cycles = 0;
+    static constexpr uint32_t kProbeSteps = 64;  // a request's first tick on the level kernel
 
     bool level() const { return cfg.kernel_form == 0; }
     uint64_t rec_cap() const { return level() ? 0 : 8 * cfg.max_sites + 4 * cfg.max_couplings + kChunk; }
@@ -1837,6 +1845,7 @@ struct ServeEngine {
         if (!cfg.max_sites) cfg.max_sites = 1ull << 24;
         if (!cfg.max_couplings) cfg.max_couplings = 1ull << 27;
         if (!cfg.max_schedule_steps) cfg.max_schedule_steps = 1ull << 25;
+        if (!cfg.tick_us) cfg.tick_us = 200000;
         if (cfg.max_sites >= (1ull << 32) || cfg.max_couplings >= (1ull << 32))
             return fail(IE_ERR_INVALID, "max_sites and max_couplings must be below 2^32");
         IE_TRY(eng.setup_device(cfg.device));
@@ -1857,6 +1866,15 @@ struct ServeEngine {
         IE_TRY(eng.d_pos.alloc(S));
         IE_TRY(eng.d_deo.alloc(S));
         IE_TRY(eng.d_done.alloc(S));
+        IE_TRY(d_plan.alloc(S));
+        IE_TRY(d_cost.upload(std::vector<float>(S, 0.0f), eng.stream));
+        plan.assign(S, 0);
+        cost.assign(S, 0.0f);
+        {
+            int khz = 0;
+            IE_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, eng.device));
+            tick_cycles = (double)cfg.tick_us * (double)khz / 1000.0;
+        }
         IE_TRY(eng.d_unclamped.alloc(S));
         IE_TRY(eng.d_Ei.alloc((size_t)kReplicas * S));
         IE_TRY(eng.d_Ef.alloc((size_t)kReplicas * S));
@@ -2056,6 +2074,8 @@ struct ServeEngine {
         IE_CUDA(cudaMemsetAsync(eng.d_pos.p + s, 0, sizeof(uint64_t), eng.stream));
         IE_CUDA(cudaMemsetAsync(eng.d_deo.p + s, 0, sizeof(int32_t), eng.stream));
         IE_CUDA(cudaMemsetAsync(eng.d_done.p + s, 0, sizeof(uint64_t), eng.stream));
+        IE_CUDA(cudaMemsetAsync(d_cost.p + s, 0, sizeof(float), eng.stream));
+        cost[s] = 0.0f;
         const DevArrays A = eng.arrays();
         IE_CUDA(launch_init(A, s, 1, eng.d_draw_idx.p, eng.d_unclamped.p, eng.stream));
         IE_CUDA(launch_energy(A, s, 1, eng.stream));
@@ -2142,15 +2162,32 @@ struct ServeEngine {
             R.exchange_interval = 1;
             R.serve = 1;
             R.site_budget = cfg.site_budget;
+            // the tick's plan: about tick_us of device time per work item
+            for (uint32_t s = 0; s < cfg.max_requests; s++) {
+                plan[s] = 0;
+                if (!slots[s] || !eng.active[s]) continue;
+                const ServeReq& r = *slots[s];
+                const uint64_t left = r.temps.size() - r.done;
+                const uint32_t u = unit[s] ? unit[s] : r.h.n;
+                uint64_t want = std::max<uint64_t>(1, cfg.site_budget / std::max<uint32_t>(u, 1));
+                if (level()) {
+                    want = cost[s] > 0.0f ? std::max<uint64_t>(1, (uint64_t)(tick_cycles / (double)cost[s]))
+                                          : std::min<uint64_t>(want, kProbeSteps);
+                }
+                plan[s] = (uint32_t)std::min<uint64_t>({left, want, 0xFFFFFFFFull});
+            }
+            IE_CUDA(cudaMemcpyAsync(d_plan.p, plan.data(), plan.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                    eng.stream));
+            R.plan = d_plan.p;
+            R.cost = level() ? d_cost.p : nullptr;
             IE_TRY(eng.launch_classes(R));
             IE_TRY(eng.check_err());
+            if (level())
+                IE_CUDA(cudaMemcpy(cost.data(), d_cost.p, cost.size() * sizeof(float), cudaMemcpyDeviceToHost));
             for (uint32_t s = 0; s < cfg.max_requests; s++) {
                 if (!slots[s] || !eng.active[s]) continue;
                 ServeReq& r = *slots[s];
-                const uint64_t left = r.temps.size() - r.done;
-                const uint32_t u = unit[s] ? unit[s] : r.h.n;
-                const uint64_t want = std::max<uint64_t>(1, cfg.site_budget / std::max<uint32_t>(u, 1));
-                r.done += std::min(left, want);
+                r.done += plan[s];
                 if (r.done == r.temps.size()) {
                     IE_TRY(retire(slots[s]));
                     slots[s].reset();

@@ -103,10 +103,13 @@ struct RunArgs {
     uint32_t nquads;
     uint32_t* queue;          // atomic counter
     // serving: every instance runs its own schedule (InstDesc::sched) from
-    // its next unexecuted step (DevArrays::done) for up to
-    // max(1, site_budget / n) steps in this launch
+    // its next unexecuted step (DevArrays::done) for plan[inst] steps in this
+    // launch (without a plan: up to max(1, site_budget / n)); the level kernel
+    // writes each instance's device cycles per step of its item to cost[inst]
     uint32_t serve;
     uint32_t site_budget;
+    const uint32_t* plan;
+    float* cost;
     // PT cells: every work item is one cell (InstDesc::owner, ::cell) of a
     // ladder of `ladder` temperatures; the launch runs steps that end at an
     // exchange or resync step at the latest, and leaves the stream position,

@@ -654,6 +654,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
         // the sweeps: overlapped (generator warps t < L.ov one sweep ahead of
         // the decider warps t >= L.ov) or in sequence with every thread on each phase
         const bool ov = L.ov && !SPLIT;
+        const long long t_item = clock64();
         if (!ov) {
             for (uint32_t s = 0; s < nsteps; s++) {
                 __syncthreads();
@@ -695,6 +696,11 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
             // every CTA's last level is done; the first CTA finishes the item
             cg::this_cluster().sync();
             if (crank != 0) continue;
+        }
+        // serving: the item's cycles per step, for the host's next plan
+        if (R.serve && R.cost && tid == 0 && nsteps) {
+            const float c = (float)(clock64() - t_item) / (float)nsteps;
+            for (uint32_t k = 0; k < I.nmem; k++) R.cost[ms[k].inst] = c;
         }
         __syncthreads();
         // energies, spins and stream state of every member

@@ -16,8 +16,9 @@ __device__ __forceinline__ uint32_t exchanges_in(uint64_t base, uint32_t steps, 
 
 // The steps one instance runs in a batched launch: the launch's own schedule,
 // or in a serving launch the instance's schedule from its next unexecuted
-// step, at most max(1, site_budget / unit) steps, unit = the sites of the
-// work item the instance is in (n for the per-lane kernels). Step s of the
+// step, for the host's plan of the tick or else at most max(1, site_budget /
+// unit) steps, unit = the sites of the work item the instance is in (n for
+// the per-lane kernels). Step s of the
 // launch is global step base + s of the instance and runs at temperature
 // temps[tstride * s].
 struct StepPlan {
@@ -33,7 +34,7 @@ __device__ __forceinline__ StepPlan step_plan(const DevArrays& A, const RunArgs&
     if (R.serve) {
         P.base = A.done[d.owner];
         const uint64_t left = d.sched_len > P.base ? d.sched_len - P.base : 0;
-        const uint64_t want = max(1u, R.site_budget / max(unit ? unit : d.n, 1u));
+        const uint64_t want = R.plan ? (uint64_t)R.plan[inst] : max(1u, R.site_budget / max(unit ? unit : d.n, 1u));
         P.steps = (uint32_t)min(left, want);
         P.tstride = 1;
         P.temps = R.temps + d.sched + P.base;

@@ -40,10 +40,10 @@ class ServeEngine:
 
     def __init__(self, device: int = 0, force_f64: bool = False, max_requests: int = 4096,
                  site_budget: int = 65536, max_sites: int = 1 << 24, max_couplings: int = 1 << 27,
-                 max_schedule_steps: int = 1 << 25, kernel_form: int = 0):
+                 max_schedule_steps: int = 1 << 25, kernel_form: int = 0, tick_us: int = 0):
         self._L = _ffi.lib()
         cfg = _ffi.ie_serve_config(device, int(force_f64), max_requests, site_budget, max_sites,
-                                   max_couplings, max_schedule_steps, int(kernel_form))
+                                   max_couplings, max_schedule_steps, int(kernel_form), int(tick_us))
         h = C.c_void_p()
         _ffi.check(self._L.ie_serve_create(C.byref(cfg), C.byref(h)))
         self._h = h
