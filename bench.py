@@ -64,7 +64,7 @@ def parse():
     p.add_argument("--blocks-per-sm", type=int, default=0)
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-count", type=int, default=128)
-    p.add_argument("--serve-rates", type=float, nargs="+", default=[100.0, 300.0, 1000.0])
+    p.add_argument("--serve-rates", type=float, nargs="+", default=[5.0, 100.0, 300.0, 1000.0, 5000.0])
     p.add_argument("--serve-sweeps", type=int, nargs=2, default=[1000, 20000])
     p.add_argument("--serve-budget", type=int, default=1 << 20)
     p.add_argument("--serve-tick-ms", type=float, default=200.0)
@@ -483,7 +483,10 @@ def run_serve(args, device):
                          "attempts_per_s": attempts / s["makespan_s"], "p50_ms": s["p50_ms"],
                          "p99_ms": s["p99_ms"], "mean_ms": s["mean_ms"], "makespan_s": s["makespan_s"],
                          "ticks": s["ticks"], "mean_tick_ms": s["mean_tick_ms"], "gpu_launches": tr.launches})
+    cap = max(r["attempts_per_s"] for r in rows)
     return {"rates": rows, "requests": len(reqs), "site_budget": args.serve_budget, "tick_ms": args.serve_tick_ms,
+            # the arrival rate the measured throughput sustains: above it the queue grows
+            "saturation_req_per_s": cap / (attempts / len(reqs)),
             "mean_attempts_per_request": attempts / len(reqs),
             "stream": f"N log-uniform [100, 20000], degree 4..32, int [-8,8] / f32 N(0,1) half each, "
                       f"SA {lo}..{hi} sweeps (beta 0.1 -> 5.0), Poisson arrivals"}

@@ -209,6 +209,10 @@ typedef struct ie_batch_config {
                                    the top 32 - tie_shift bits of the stored outputs, so the exact
                                    path (outputs recomputed from the lane seed) runs often */
     int32_t bit_sliced;         /* as ie_config::bit_sliced */
+    int32_t bulk_ring;          /* per-lane kernels (kernel_form 1): nonzero streams the site-record
+                                   chunks by 1D bulk copies completing on mbarriers instead of
+                                   16-byte cp.async copies (same results; cp.async is the default,
+                                   measured faster on these kernels) */
 } ie_batch_config;
 
 /* count problems, each run as one cell of 64 replicas with its own seed. */

@@ -64,7 +64,7 @@ class ie_batch_config(C.Structure):
                 ("threads_per_block", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("disable_windows", C.c_int32), ("use_graph", C.c_int32),
                 ("kernel_form", C.c_int32), ("item_sites", C.c_uint32), ("tie_shift", C.c_uint32),
-                ("bit_sliced", C.c_int32)]
+                ("bit_sliced", C.c_int32), ("bulk_ring", C.c_int32)]
 
 
 class ie_serve_config(C.Structure):

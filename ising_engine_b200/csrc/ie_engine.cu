@@ -786,6 +786,7 @@ struct Engine {
     uint32_t lvl_tie_shift = 0;
     bool lvl_split = true;    // large single-member items on thread block clusters
     bool lvl_overlap = true;  // latency-bound launches overlap the generator and decision phases
+    bool bulk_ring = false;   // per-lane kernels: record chunks by bulk copies (cp.async measured faster)
     uint32_t lvl_cluster_max = 0;  // most CTAs per cluster (0: 16)
     int32_t pmj_policy = 0;   // +-J instances on the bit-sliced form: 0 auto, 1 always, -1 never
     bool serving = false;     // serving launches: one threshold table per member
@@ -1284,6 +1285,7 @@ struct Engine {
             if (!wc.nitems) continue;
             IE_CUDA(cudaStreamWaitEvent(cstreams[k], evfork, 0));
             RunArgs R = base;
+            R.bulk_ring = bulk_ring ? 1u : 0u;
             R.quads = wc.items.p;
             R.quad_h = wc.itemh.p;
             R.nquads = wc.nitems;
@@ -1567,6 +1569,7 @@ struct Engine {
         IE_CUDA(cudaEventRecord(ev0, stream));
         for (uint32_t i = 0; i < n_inst; i++) {
             RunArgs R = sa_args(steps);
+            R.bulk_ring = bulk_ring ? 1u : 0u;
             R.quads = dq.p + 4 * (size_t)i;
             R.quad_h = dh.p + i;
             R.nquads = 1;
@@ -2725,6 +2728,7 @@ ie_status ie_batch_create(const ie_problem* problems, uint32_t count, const uint
     b->eng.lvl_tie_shift = cfg.tie_shift;
     if (cfg.bit_sliced < -1 || cfg.bit_sliced > 1) return fail(IE_ERR_INVALID, "bit_sliced must be -1, 0 or 1");
     b->eng.pmj_policy = cfg.bit_sliced;
+    b->eng.bulk_ring = cfg.bulk_ring != 0;
     if (cfg.threads_per_block && (cfg.threads_per_block % 32 || cfg.threads_per_block > 256))
         return fail(IE_ERR_INVALID, "threads_per_block must be a multiple of 32, at most 256");
     if (cfg.threads_per_block) b->eng.lvl_threads = (int)cfg.threads_per_block;

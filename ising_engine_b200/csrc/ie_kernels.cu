@@ -194,8 +194,10 @@ __device__ __forceinline__ unsigned group_mask(int tid) { return 0xFFu << (8 * (
 // replicas. A warp holds 4/TPL instances; in a batched run they run the same
 // schedule in step and share one threshold table per sweep, in a serving or
 // PT-cells run each has its own schedule and table. Each instance streams its
-// site records through a 3-slot shared-memory ring with cp.async (two 512-byte
-// chunks in flight ahead of the sweep); its spin words stay in shared memory
+// site records through a 3-slot shared-memory ring (two 512-byte chunks in
+// flight ahead of the sweep: 16-byte cp.async copies spread over the group, or
+// with RunArgs::bulk_ring one 1D bulk copy by the group's first thread
+// completing on the slot's mbarrier); its spin words stay in shared memory
 // for the whole run. Every thread of a lane writes the same combined byte, so
 // each thread's later reads see the update in program order.
 // ---------------------------------------------------------------------------
@@ -208,19 +210,73 @@ __device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_g
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
-// Copies chunk k of a stream into its ring slot (32 x 16 bytes spread over
-// the G threads of the group) and commits a group; beyond the stream end
-// only an empty group is committed.
+// Record ring of the per-lane kernels, two forms. cp.async: the group's
+// threads copy a chunk 16 bytes each and commit one group per chunk (an empty
+// one beyond the stream end); chunk k is complete once at most two newer
+// groups are pending. Bulk: slot s has its own mbarrier bar[s] (arrival count
+// 1); the group's first thread arms it with the chunk's 512 bytes and issues
+// the 1D bulk copy (cp.async.bulk, no multicast), every thread of the group
+// waits for the slot's phase. Every fetched chunk is waited for exactly once
+// and in order, so the phase parity of slot s is bit s of ph. Bulk waits give
+// up after kRingWaitCycles, set the error word and stop waiting (the results
+// are void, the launch still ends).
+constexpr long long kRingWaitCycles = 1ll << 31;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ring_init(uint64_t* bar) {
+    for (uint32_t s = 0; s < kSlots; s++)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + s)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Chunk k of a stream into its ring slot (beyond the stream end: no copy).
 template <int G>
-__device__ __forceinline__ void ring_fetch(uint32_t* ring, const uint32_t* stream, uint32_t nchunks,
-                                           uint32_t k, int t) {
-    if (k < nchunks) {
-        uint32_t* dst = ring + (k % kSlots) * kChunk;
-        const uint32_t* src = stream + (size_t)k * kChunk;
+__device__ __forceinline__ void ring_fetch(bool bulk, uint32_t* ring, uint64_t* bar, const uint32_t* stream,
+                                           uint32_t nchunks, uint32_t k, int t) {
+    if (!bulk) {
+        if (k < nchunks) {
+            uint32_t* dst = ring + (k % kSlots) * kChunk;
+            const uint32_t* src = stream + (size_t)k * kChunk;
 #pragma unroll
-        for (int i = 0; i < 32 / G; i++) cp_async16(dst + 4 * (t + G * i), src + 4 * (t + G * i));
+            for (int i = 0; i < 32 / G; i++) cp_async16(dst + 4 * (t + G * i), src + 4 * (t + G * i));
+        }
+        cp_async_commit();
+        return;
     }
-    cp_async_commit();
+    if (k < nchunks && t == 0) {
+        const uint32_t b = smem_u32(bar + k % kSlots);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kChunk * 4u) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_u32(ring + (k % kSlots) * kChunk)),
+                     "l"(stream + (size_t)k * kChunk), "r"(kChunk * 4u), "r"(b)
+                     : "memory");
+    }
+}
+
+// Waits for chunk k (fetched, two newer fetches issued, not yet waited for).
+__device__ __forceinline__ void ring_wait(bool bulk, uint64_t* bar, uint32_t k, uint32_t& ph, bool& bad, int32_t* err) {
+    if (!bulk) {
+        cp_async_wait2();
+        return;
+    }
+    const uint32_t s = k % kSlots, b = smem_u32(bar + s), parity = (ph >> s) & 1u;
+    ph ^= 1u << s;
+    if (bad) return;
+    uint32_t ok = 0;
+    long long t0 = 0;
+    for (bool first = true;; first = false) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(b), "r"(parity)
+            : "memory");
+        if (ok) return;
+        if (first) t0 = clock64();
+        else if (clock64() - t0 > kRingWaitCycles) break;
+    }
+    bad = true;
+    atomicExch(err, 5);
 }
 
 // The reference decision dE <= 0 || u < fast_exp(-dE * beta) (engine.rs:665-666),
@@ -294,7 +350,8 @@ using ETypeT = typename std::conditional<MODE == kModeInt, int32_t, double>::typ
 // PROD: the uniforms come from a generator warp through rngb (produce_windows;
 // barrier count 64), window by window, instead of the thread's own generator.
 template <uint32_t MODE, int TPL, bool PROD = false>
-__device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc& d, uint32_t* ring, uint8_t* sp,
+__device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc& d, bool bulk, uint32_t* ring,
+                                             uint64_t* bar, uint32_t& ph, bool& bad, uint8_t* sp,
                                              const uint2* __restrict__ lut, int lane, int h, unsigned gmask,
                                              const uint64_t* __restrict__ tab,
                                              int H, double beta, uint64_t cell_seed,
@@ -312,10 +369,10 @@ __device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc&
     }
     const uint32_t* stream = A.recs + d.rec;
     const uint32_t nchunks = (uint32_t)(d.rec_len / kChunk);
-    ring_fetch<G>(ring, stream, nchunks, 0, t);
-    ring_fetch<G>(ring, stream, nchunks, 1, t);
-    ring_fetch<G>(ring, stream, nchunks, 2, t);
-    cp_async_wait2();
+    ring_fetch<G>(bulk, ring, bar, stream, nchunks, 0, t);
+    ring_fetch<G>(bulk, ring, bar, stream, nchunks, 1, t);
+    ring_fetch<G>(bulk, ring, bar, stream, nchunks, 2, t);
+    if (nchunks) ring_wait(bulk, bar, 0, ph, bad, A.err);
     __syncwarp(gmask);
     uint32_t k = 0, c = 0;
     const uint32_t* chunk = ring;
@@ -330,8 +387,8 @@ __device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc&
             __syncwarp(gmask);
             k++;
             c = 0;
-            ring_fetch<G>(ring, stream, nchunks, k + 2, t);
-            cp_async_wait2();
+            ring_fetch<G>(bulk, ring, bar, stream, nchunks, k + 2, t);
+            ring_wait(bulk, bar, k, ph, bad, A.err);
             __syncwarp(gmask);
             chunk = ring + (k % kSlots) * kChunk;
             continue;
@@ -461,7 +518,7 @@ __device__ __forceinline__ void sweep_stream(const DevArrays& A, const InstDesc&
         }
         v++;
     }
-    cp_async_wait0();
+    if (!bulk) cp_async_wait0();
     __syncwarp(gmask);
 }
 
@@ -523,6 +580,11 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
     }
     uint8_t* sp = reinterpret_cast<uint8_t*>(sw) + lane;
     const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (G * g));
+    __shared__ __align__(8) uint64_t s_bar[NG][kSlots];
+    if (t == 0) ring_init(s_bar[g]);
+    __syncwarp();
+    uint32_t ph = 0;
+    bool bad = false;
     typedef ETypeT<MODE, TPL> EType;
     for (;;) {
         uint32_t q = 0;
@@ -575,7 +637,7 @@ __global__ void __launch_bounds__(32) batch_kernel(DevArrays A, RunArgs R, uint3
             }
             if (active) {
                 const uint64_t base = chacha8_draw(key, pos0 + s) + d.cell;
-                sweep_stream<MODE, TPL>(A, d, ring, sp, lut, lane, h, gmask, tab, H, beta, base, E);
+                sweep_stream<MODE, TPL>(A, d, R.bulk_ring != 0, ring, s_bar[g], ph, bad, sp, lut, lane, h, gmask, tab, H, beta, base, E);
                 if constexpr (MODE == kModeF64) {
                     if (!R.cells && (P.base + s + 1) % kResyncEvery == 0) {
                         __syncwarp(gmask);
@@ -630,6 +692,10 @@ __global__ void __launch_bounds__(64, 1) chain_kernel(DevArrays A, RunArgs R, ui
     const bool producer = tid < 32;
     const int t = tid & 31;
     const int lane = t >> 2, h = t & 3;
+    __shared__ __align__(8) uint64_t s_bar[kSlots];
+    if (tid == 32) ring_init(s_bar);
+    uint32_t ph = 0;
+    bool bad = false;
     typedef ETypeT<MODE, 4> EType;
     if constexpr (MODE == kModeInt) {
         for (int i = tid; i < 512; i += 64) {
@@ -684,7 +750,8 @@ __global__ void __launch_bounds__(64, 1) chain_kernel(DevArrays A, RunArgs R, ui
                     for (int i = t; i < 2 * H + 1; i += 32) tab[i] = metropolis_threshold(i - H, beta);
                     __syncwarp();
                 }
-                sweep_stream<MODE, 4, true>(A, d, ring, sp, lut, lane, h, 0xffffffffu, tab, H, beta, base, E, rngb);
+                sweep_stream<MODE, 4, true>(A, d, R.bulk_ring != 0, ring, s_bar, ph, bad, sp, lut, lane, h, 0xffffffffu, tab, H, beta, base,
+                                            E, rngb);
                 if constexpr (MODE == kModeF64) {
                     if (!R.cells && (P.base + s + 1) % kResyncEvery == 0) {
                         __syncwarp();

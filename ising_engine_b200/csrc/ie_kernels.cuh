@@ -110,6 +110,8 @@ struct RunArgs {
     uint32_t site_budget;
     const uint32_t* plan;
     float* cost;
+    // per-lane kernels: record chunks by 1D bulk copies on mbarriers (else cp.async)
+    uint32_t bulk_ring;
     // PT cells: every work item is one cell (InstDesc::owner, ::cell) of a
     // ladder of `ladder` temperatures; the launch runs steps that end at an
     // exchange or resync step at the latest, and leaves the stream position,

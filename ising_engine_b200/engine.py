@@ -193,7 +193,7 @@ class BatchEngine:
     def __init__(self, models, seeds, device: int = 0, force_f64: bool = False,
                  threads_per_block: int = 0, blocks_per_sm: int = 0, windows: bool = True,
                  graph: bool = False, kernel_form: int = 0, item_sites: int = 0, tie_shift: int = 0,
-                 bit_sliced: int = 0):
+                 bit_sliced: int = 0, bulk_ring: bool = False):
         self._L = _ffi.lib()
         self.kernel_form = int(kernel_form)
         self.models = list(models)
@@ -205,7 +205,7 @@ class BatchEngine:
             raise ValueError("one seed per problem")
         cfg = _ffi.ie_batch_config(device, int(force_f64), threads_per_block, blocks_per_sm,
                                    0 if windows else 1, 1 if graph else 0, int(kernel_form),
-                                   int(item_sites), int(tie_shift), int(bit_sliced))
+                                   int(item_sites), int(tie_shift), int(bit_sliced), int(bool(bulk_ring)))
         h = C.c_void_p()
         _ffi.check(self._L.ie_batch_create(probs, self.count, _p(self.seeds), C.byref(cfg),
                                            C.byref(h)))

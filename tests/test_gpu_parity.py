@@ -340,6 +340,29 @@ def test_batch_long_rows_and_thread_classes():
     b.close()
 
 
+@pytest.mark.parametrize("bulk", [False, True])
+def test_per_lane_record_ring_forms(bulk):
+    """The per-lane kernels (kernel_form 1) with the site-record ring fed by
+    16-byte cp.async copies or by 1D bulk copies on mbarriers: spins and
+    energies equal the oracle's for rows longer than one record, every thread
+    class and lattices (the chain kernel)."""
+    rng = np.random.default_rng(35)
+    models = [I.maxcut_gnm(160, 2600, seed=5), I.random_regular_qubo(300, 20, rng, integer=False),
+              I.pm_j_lattice(32, 2, seed=6), I.pm_j_lattice(12, 3, seed=8)]
+    models += [I.random_regular_qubo(int(n), 6, rng, integer=bool(i % 2))
+               for i, n in enumerate(rng.integers(40, 700, size=9) * 2)]
+    seeds = np.arange(len(models), dtype=np.uint64) * 5 + 1
+    temps = I.sa_temps(25, 0.2, 3.0)
+    words_ref, _, ref_e = O.run_sa_batch(models, seeds, temps, threads=8)
+    b = BatchEngine(models, seeds, kernel_form=1, bulk_ring=bulk)
+    b.init_random()
+    b.run_schedule(temps[:9])
+    b.run_schedule(temps[9:])
+    assert (b.spins() == words_ref).all()
+    assert_batch_energies(b, models, ref_e)
+    b.close()
+
+
 def test_autotune_restores_state():
     """The autotuner's trial runs leave no trace: after tuning, the run equals
     the oracle's from the same initial state."""
