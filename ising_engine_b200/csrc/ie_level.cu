@@ -564,12 +564,21 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                         const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
                         const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
                         const uint32_t* tb = tabb + (own_tab ? slot * kLvlTab : 0u);
+                        if (sh == 0) {
 #pragma unroll
-                        for (int k = 0; k < 8; k++) {
-                            const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
-                            const uint32_t a = mh[k] >> sh, b = tb[idx] >> sh;
-                            flips |= (uint32_t)(a < b) << k;
-                            ties |= (uint32_t)(a == b) << k;
+                            for (int k = 0; k < 8; k++) {
+                                const uint32_t qa = mh[k], qb = tb[((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu];
+                                flips |= (uint32_t)(qa < qb) << k;
+                                ties |= (uint32_t)(qa == qb) << k;
+                            }
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < 8; k++) {
+                                const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
+                                const uint32_t qa = mh[k] >> sh, qb = tb[idx] >> sh;
+                                flips |= (uint32_t)(qa < qb) << k;
+                                ties |= (uint32_t)(qa == qb) << k;
+                            }
                         }
                         if (ties) {
                             flips |= exact_flips_int(ties, m.base[b], lane, v, iL, iH, H, m.beta[b], L.jpoly);
