@@ -533,10 +533,10 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                     const uint32_t fb = m.flat;
                     const uint32_t xb = ld_spin<SPLIT>(spb + 8u * f);
                     const uint4* kp = reinterpret_cast<const uint4*>(kbb + (size_t)f * 64 + lane * 8);
-                    const uint4 k0 = kp[0], k1 = kp[1];
-                    const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
                     uint32_t flips = 0, ties = 0;
                     if constexpr (MODE == kModeInt) {
+                        const uint4 k0 = kp[0], k1 = kp[1];
+                        const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
                         const int lp = (int)hd.y;
                         uint32_t aL = 0, aH = 0;
                         const uint4* e4p = reinterpret_cast<const uint4*>(rec + 4);
@@ -594,6 +594,8 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                         // x_v) = s_k w or a zero term, and round-to-nearest is symmetric
                         // (fl(-a - b) = -fl(a + b)), so the sum of signed terms is s_k
                         // times the sum of the weights; zero terms change no nonzero sum.
+                        // the outputs are read after the sum (fewer live registers), from L1
+                        prefetch_l1(kp);
                         double dl[8];
 #pragma unroll
                         for (int k = 0; k < 8; k++) dl[k] = wl;
@@ -615,6 +617,8 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                                 }
                             }
                         }
+                        const uint4 k0 = kp[0], k1 = kp[1];
+                        const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
 #pragma unroll
                         for (int k = 0; k < 8; k++) {
                             if ((xb >> k) & 1u) dl[k] = -dl[k];
