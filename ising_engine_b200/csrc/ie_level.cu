@@ -521,126 +521,128 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                         sw[f] = xw ^ ~bad;
                     }
                 } else {
-                for (uint32_t i = dt; i < 8u * (e1 - e0); i += TT) {
-                    const LvlEntry en = (i == dt && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + (i >> 3));
-                    const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
-                    const LvlMem& m = ms[slot];
-                    if (s >= m.steps) continue;
-                    const uint32_t v = f - m.flat;
-                    const uint32_t* rec = L.lrecs + 4ull * en.rec;
-                    const uint4 hd = __ldg(reinterpret_cast<const uint4*>(rec));
-                    const uint32_t deg = hd.x & 0x7FFFFFFFu;
-                    const uint32_t fb = m.flat;
-                    const uint32_t xb = ld_spin<SPLIT>(spb + 8u * f);
-                    const uint4* kp = reinterpret_cast<const uint4*>(kbb + (size_t)f * 64 + lane * 8);
-                    uint32_t flips = 0, ties = 0;
-                    if constexpr (MODE == kModeInt) {
-                        const uint4 k0 = kp[0], k1 = kp[1];
-                        const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
-                        const int lp = (int)hd.y;
-                        uint32_t aL = 0, aH = 0;
-                        const uint4* e4p = reinterpret_cast<const uint4*>(rec + 4);
-                        for (uint32_t q = 0; q < deg; q += 4) {
-                            const uint4 e4 = __ldg(e4p + (q >> 2));
-                            const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
-                            uint32_t li[4];
-#pragma unroll
-                            for (int e = 0; e < 4; e++)
-                                li[e] = ld_spin<SPLIT>(spb + 8u * (fb + (en[e] & 0xFFFFFFu))) | ((en[e] >> 23) & 0x100u);
-#pragma unroll
-                            for (int e = 0; e < 4; e++) {
-                                const uint2 sv = lut[li[e]];
-                                const uint32_t w = (en[e] >> 24) & 0x7Fu;
-                                aL += w * sv.x;
-                                aH += w * sv.y;
-                            }
-                        }
-                        const int H = I.H;
-                        const uint32_t cA = (uint32_t)(H + lp) * 0x01010101u;
-                        const uint32_t cB = (uint32_t)(H - lp) * 0x01010101u;
-                        const uint32_t xL = spread4(xb) * 0xFFu;
-                        const uint32_t xH = spread4(xb >> 4) * 0xFFu;
-                        // byte k of iL / iH = dE_k + H for replica lane + 8k
-                        const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
-                        const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
-                        const uint32_t* tb = tabb + (own_tab ? slot * kLvlTab : 0u);
-                        if (sh == 0) {
-#pragma unroll
-                            for (int k = 0; k < 8; k++) {
-                                const uint32_t qa = mh[k], qb = tb[((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu];
-                                flips |= (uint32_t)(qa < qb) << k;
-                                ties |= (uint32_t)(qa == qb) << k;
-                            }
-                        } else {
-#pragma unroll
-                            for (int k = 0; k < 8; k++) {
-                                const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
-                                const uint32_t qa = mh[k] >> sh, qb = tb[idx] >> sh;
-                                flips |= (uint32_t)(qa < qb) << k;
-                                ties |= (uint32_t)(qa == qb) << k;
-                            }
-                        }
-                        if (ties) {
-                            flips |= exact_flips_int(ties, m.base[b], lane, v, iL, iH, H, m.beta[b], L.jpoly);
-                            if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
-                        }
-                    } else {
-                        const double wl = __hiloint2double((int)hd.w, (int)hd.z);
-                        const uint32_t deg4 = (deg + 3u) & ~3u;
-                        const uint4* c4p = reinterpret_cast<const uint4*>(rec + 4);
-                        const double2* w2p = reinterpret_cast<const double2*>(rec + 4 + deg4);
-                        // dE_k = s_k (lin + sum of w over the neighbours with x_j = 1, in
-                        // CSR order), s_k = 1 - 2 x_v: the reference adds w ((x_j ^ x_v) -
-                        // x_v) = s_k w or a zero term, and round-to-nearest is symmetric
-                        // (fl(-a - b) = -fl(a + b)), so the sum of signed terms is s_k
-                        // times the sum of the weights; zero terms change no nonzero sum.
-                        // the outputs are read after the sum (fewer live registers), from L1
-                        prefetch_l1(kp);
-                        double dl[8];
-#pragma unroll
-                        for (int k = 0; k < 8; k++) dl[k] = wl;
-                        for (uint32_t q = 0; q < deg; q += 4) {
-                            const uint4 c4 = __ldg(c4p + (q >> 2));
-                            const double2 w01 = __ldg(w2p + (q >> 1));
-                            const double2 w23 = __ldg(w2p + (q >> 1) + 1);
-                            const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
-                            const double ww[4] = {w01.x, w01.y, w23.x, w23.y};
-                            uint32_t bj[4];
-#pragma unroll
-                            for (int e = 0; e < 4; e++) bj[e] = ld_spin<SPLIT>(spb + 8u * (fb + cc[e]));
-#pragma unroll
-                            for (int e = 0; e < 4; e++) {
-                                if (q + e < deg) {
-#pragma unroll
-                                    for (int k = 0; k < 8; k++)
-                                        if ((bj[e] >> k) & 1u) dl[k] = __dadd_rn(dl[k], ww[e]);
+                    for (uint32_t i = dt; i < 8u * (e1 - e0); i += TT) {
+                        const LvlEntry en = (i == dt && l) ? nxt : load_entry(L.entries + I.ent0 + e0 + (i >> 3));
+                        const uint32_t slot = en.site >> kLvlFlatBits, f = en.site & ((1u << kLvlFlatBits) - 1u);
+                        const LvlMem& m = ms[slot];
+                        if (s >= m.steps) continue;
+                        const uint32_t v = f - m.flat;
+                        const uint32_t* rec = L.lrecs + 4ull * en.rec;
+                        const uint4 hd = __ldg(reinterpret_cast<const uint4*>(rec));
+                        const uint32_t deg = hd.x & 0x7FFFFFFFu;
+                        const uint32_t fb = m.flat;
+                        const uint32_t xb = ld_spin<SPLIT>(spb + 8u * f);
+                        const uint4* kp = reinterpret_cast<const uint4*>(kbb + (size_t)f * 64 + lane * 8);
+                        uint32_t flips = 0, ties = 0;
+                        if constexpr (MODE == kModeInt) {
+                            const uint4 k0 = kp[0], k1 = kp[1];
+                            const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+                            const int lp = (int)hd.y;
+                            uint32_t aL = 0, aH = 0;
+                            const uint4* e4p = reinterpret_cast<const uint4*>(rec + 4);
+                            for (uint32_t q = 0; q < deg; q += 4) {
+                                const uint4 e4 = __ldg(e4p + (q >> 2));
+                                const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
+                                uint32_t li[4];
+    #pragma unroll
+                                for (int e = 0; e < 4; e++)
+                                    li[e] = ld_spin<SPLIT>(spb + 8u * (fb + (en[e] & 0xFFFFFFu))) |
+                                            ((en[e] >> 23) & 0x100u);
+    #pragma unroll
+                                for (int e = 0; e < 4; e++) {
+                                    const uint2 sv = lut[li[e]];
+                                    const uint32_t w = (en[e] >> 24) & 0x7Fu;
+                                    aL += w * sv.x;
+                                    aH += w * sv.y;
                                 }
                             }
-                        }
-                        const uint4 k0 = kp[0], k1 = kp[1];
-                        const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
-#pragma unroll
-                        for (int k = 0; k < 8; k++) {
-                            if ((xb >> k) & 1u) dl[k] = -dl[k];
-                            if (dl[k] <= 0.0) {
-                                flips |= 1u << k;
-                                continue;
+                            const int H = I.H;
+                            const uint32_t cA = (uint32_t)(H + lp) * 0x01010101u;
+                            const uint32_t cB = (uint32_t)(H - lp) * 0x01010101u;
+                            const uint32_t xL = spread4(xb) * 0xFFu;
+                            const uint32_t xH = spread4(xb >> 4) * 0xFFu;
+                            // byte k of iL / iH = dE_k + H for replica lane + 8k
+                            const uint32_t iL = ((aL + cA) & ~xL) | ((cB - aL) & xL);
+                            const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
+                            const uint32_t* tb = tabb + (own_tab ? slot * kLvlTab : 0u);
+                            if (sh == 0) {
+    #pragma unroll
+                                for (int k = 0; k < 8; k++) {
+                                    const uint32_t qa = mh[k], qb = tb[((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu];
+                                    flips |= (uint32_t)(qa < qb) << k;
+                                    ties |= (uint32_t)(qa == qb) << k;
+                                }
+                            } else {
+    #pragma unroll
+                                for (int k = 0; k < 8; k++) {
+                                    const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
+                                    const uint32_t qa = mh[k] >> sh, qb = tb[idx] >> sh;
+                                    flips |= (uint32_t)(qa < qb) << k;
+                                    ties |= (uint32_t)(qa == qb) << k;
+                                }
                             }
-                            const int r = f64_decide(dl[k], m.beta[b], mh[k], sh);
-                            flips |= (uint32_t)(r > 0) << k;
-                            ties |= (uint32_t)(r == 0) << k;
+                            if (ties) {
+                                flips |= exact_flips_int(ties, m.base[b], lane, v, iL, iH, H, m.beta[b], L.jpoly);
+                                if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
+                            }
+                        } else {
+                            const double wl = __hiloint2double((int)hd.w, (int)hd.z);
+                            const uint32_t deg4 = (deg + 3u) & ~3u;
+                            const uint4* c4p = reinterpret_cast<const uint4*>(rec + 4);
+                            const double2* w2p = reinterpret_cast<const double2*>(rec + 4 + deg4);
+                            // dE_k = s_k (lin + sum of w over the neighbours with x_j = 1, in
+                            // CSR order), s_k = 1 - 2 x_v: the reference adds w ((x_j ^ x_v) -
+                            // x_v) = s_k w or a zero term, and round-to-nearest is symmetric
+                            // (fl(-a - b) = -fl(a + b)), so the sum of signed terms is s_k
+                            // times the sum of the weights; zero terms change no nonzero sum.
+                            // the outputs are read after the sum (fewer live registers), from L1
+                            prefetch_l1(kp);
+                            double dl[8];
+    #pragma unroll
+                            for (int k = 0; k < 8; k++) dl[k] = wl;
+                            for (uint32_t q = 0; q < deg; q += 4) {
+                                const uint4 c4 = __ldg(c4p + (q >> 2));
+                                const double2 w01 = __ldg(w2p + (q >> 1));
+                                const double2 w23 = __ldg(w2p + (q >> 1) + 1);
+                                const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+                                const double ww[4] = {w01.x, w01.y, w23.x, w23.y};
+                                uint32_t bj[4];
+    #pragma unroll
+                                for (int e = 0; e < 4; e++) bj[e] = ld_spin<SPLIT>(spb + 8u * (fb + cc[e]));
+    #pragma unroll
+                                for (int e = 0; e < 4; e++) {
+                                    if (q + e < deg) {
+    #pragma unroll
+                                        for (int k = 0; k < 8; k++)
+                                            if ((bj[e] >> k) & 1u) dl[k] = __dadd_rn(dl[k], ww[e]);
+                                    }
+                                }
+                            }
+                            const uint4 k0 = kp[0], k1 = kp[1];
+                            const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+    #pragma unroll
+                            for (int k = 0; k < 8; k++) {
+                                if ((xb >> k) & 1u) dl[k] = -dl[k];
+                                if (dl[k] <= 0.0) {
+                                    flips |= 1u << k;
+                                    continue;
+                                }
+                                const int r = f64_decide(dl[k], m.beta[b], mh[k], sh);
+                                flips |= (uint32_t)(r > 0) << k;
+                                ties |= (uint32_t)(r == 0) << k;
+                            }
+                            if (ties) {
+    #pragma unroll
+                                for (int k = 0; k < 8; k++)
+                                    if ((ties >> k) & 1u)
+                                        flips |= exact_flip_f64(m.base[b], lane, v, k, __dmul_rn(-dl[k], m.beta[b]),
+                                                                L.jpoly)
+                                                 << k;
+                                if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
+                            }
                         }
-                        if (ties) {
-#pragma unroll
-                            for (int k = 0; k < 8; k++)
-                                if ((ties >> k) & 1u)
-                                    flips |= exact_flip_f64(m.base[b], lane, v, k, __dmul_rn(-dl[k], m.beta[b]), L.jpoly)
-                                             << k;
-                            if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
-                        }
+                        spb[8u * f] = (uint8_t)(xb ^ flips);
                     }
-                    spb[8u * f] = (uint8_t)(xb ^ flips);
-                }
                 }
                 if (l + 1 < I.nlvl) {
                     e0 = __ldg(lo + (l + 1) * csize);
