@@ -731,7 +731,6 @@ struct Engine {
         int grid = 0;
         uint64_t keystride = 0, keyoff = 0;
         uint32_t ov = 0;  // > 0: sweeps overlapped, a generator group of ov threads per CTA
-        uint32_t slice = 0;  // cluster class: spin words per CTA kept in shared memory (0: read from L2)
         DevBuf<uint32_t> order;
     };
     static constexpr int kLevelForm = 32;  // tpl tag of a level-kernel class
@@ -787,7 +786,6 @@ struct Engine {
     uint32_t lvl_tie_shift = 0;
     bool lvl_split = true;    // large single-member items on thread block clusters
     bool lvl_overlap = true;  // latency-bound launches overlap the generator and decision phases
-    bool lvl_dsm = true;      // cluster items keep their spin words in distributed shared memory
     bool bulk_ring = false;   // per-lane kernels: record chunks by bulk copies (cp.async measured faster)
     uint32_t lvl_cluster_max = 0;  // most CTAs per cluster (0: 16)
     int32_t pmj_policy = 0;   // +-J instances on the bit-sliced form: 0 auto, 1 always, -1 never
@@ -971,15 +969,7 @@ struct Engine {
                                  ? gen
                                  : 0u;
                 }
-                // clusters: the spin words of each CTA's segments in its shared
-                // memory when the largest slice fits (64 KiB)
-                if (g && split > 1 && lvl_dsm) {
-                    uint32_t seg = 0;
-                    for (size_t q = item_begin; q < lvh.items.size(); q++) seg = std::max(seg, lvh.items[q].nseg);
-                    const uint64_t words = (uint64_t)((seg + split - 1) / split) * kLvlSeg;
-                    if (words * 8 <= 64 * 1024) wc->slice = (uint32_t)words;
-                }
-                const size_t smem = level_smem(wc->mode, wc->ntab, g ? wc->slice : lvl_cap, wc->ov != 0);
+                const size_t smem = level_smem(wc->mode, wc->ntab, g ? 0 : lvl_cap, wc->ov != 0);
                 int occ = level_occupancy(wc->mode, g != 0, lvl_threads + (int)wc->ov, smem);
                 if (occ <= 0) return fail(IE_ERR_UNSUPPORTED, "level kernel does not fit on an SM");
                 if (blocks_per_sm) occ = std::min<int>(occ, (int)blocks_per_sm);
@@ -1031,8 +1021,7 @@ struct Engine {
         L.keystride = wc.keystride;
         L.ov = wc.ov;
         L.keyhalf = wc.ov ? wc.keystride / 2 : 0;
-        L.spin_cap = wc.gsp ? wc.slice : lvl_cap;
-        L.dsm = wc.slice ? 1u : 0u;
+        L.spin_cap = wc.gsp ? 0u : lvl_cap;
         L.ntab = wc.ntab;
         L.tie_shift = lvl_tie_shift;
         L.exact_count = d_exact.p;

@@ -299,8 +299,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
         const LvlItem I = L.items[it];
         if ((!GSP && I.sites > L.spin_cap) || I.nmem > kLvlMaxMembers || I.nmem == 0 ||
             (own_tab && I.nmem > L.ntab) || (uint64_t)I.sites * 64 > (L.ov ? L.keyhalf : L.keystride) ||
-            (GSP && I.nmem != 1) || I.split != csize || (L.ov && !SPLIT && (L.ov % 32 || L.ov >= (uint32_t)T)) ||
-            (SPLIT && L.dsm && (uint64_t)((I.nseg + csize - 1) / csize) * kLvlSeg > L.spin_cap)) {
+            (GSP && I.nmem != 1) || I.split != csize || (L.ov && !SPLIT && (L.ov % 32 || L.ov >= (uint32_t)T))) {
             if (tid == 0) atomicExch(A.err, 2);  // host sizing error: report, skip the item
             continue;
         }
@@ -337,26 +336,6 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
         const uint32_t nsteps = s_steps;
         uint64_t* const sw = GSP ? A.spins + ms[0].spin : ssw;
         uint8_t* const spb = reinterpret_cast<uint8_t*>(sw) + lane;
-        // cluster items whose slices fit (L.dsm): each CTA keeps the spin words
-        // of its own segments (s % C == rank) in shared memory, word j at
-        // sidx(j) of rank (j / 128) % C, and reads the other CTAs' words through
-        // distributed shared memory instead of L2
-        const bool dsm = SPLIT && L.dsm;
-        const uint32_t lc = (uint32_t)__ffs((int)csize) - 1u;
-        auto sidx = [&](uint32_t j) -> uint32_t { return (((j >> 7) >> lc) << 7) | (j & 127u); };
-        auto wptr = [&](uint32_t j) -> const uint64_t* {
-            return cg::this_cluster().map_shared_rank(ssw, (j >> 7) & (csize - 1u)) + sidx(j);
-        };
-        if constexpr (SPLIT) {
-            if (dsm) {
-                for (uint32_t i = tid; i < L.spin_cap; i += T) {
-                    const uint32_t j = ((crank + csize * (i >> 7)) << 7) | (i & 127u);
-                    if (j < ms[0].n) ssw[i] = sw[j];
-                }
-                // every slice is loaded before any CTA reads another's
-                cg::this_cluster().sync();
-            }
-        }
         if (!GSP) {
             for (uint32_t k = 0; k < I.nmem; k++) {
                 const uint64_t* gw = A.spins + ms[k].spin;
@@ -504,7 +483,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                         if (s >= m.steps) continue;
                         const uint32_t* rec = L.lrecs + 4ull * en.rec;
                         const uint32_t D = __ldg(rec) & 0x7FFFFFFFu;
-                        const uint64_t xw = dsm ? ssw[sidx(f)] : ld_word<SPLIT>(sw + f);
+                        const uint64_t xw = ld_word<SPLIT>(sw + f);
                         uint64_t p0 = 0, p1 = 0, p2 = 0, p3 = 0;
                         const uint4* e4p = reinterpret_cast<const uint4*>(rec + 4);
                         for (uint32_t q = 0; q < D; q += 4) {
@@ -513,8 +492,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
 #pragma unroll
                             for (int e = 0; e < 4; e++) {
                                 if (q + e < D) {
-                                    const uint32_t j = m.flat + (ev[e] & 0xFFFFFFu);
-                                    uint64_t b = dsm ? *wptr(j) : ld_word<SPLIT>(sw + j);
+                                    uint64_t b = ld_word<SPLIT>(sw + m.flat + (ev[e] & 0xFFFFFFu));
                                     if (ev[e] >> 31) b = ~b;
                                     uint64_t c = p0 & b;
                                     p0 ^= b;
@@ -540,8 +518,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                             }
                             bad |= eq & ~A[lv - 1];
                         }
-                        if (dsm) ssw[sidx(f)] = xw ^ ~bad;
-                        else sw[f] = xw ^ ~bad;
+                        sw[f] = xw ^ ~bad;
                     }
                 } else {
                     for (uint32_t i = dt; i < 8u * (e1 - e0); i += TT) {
@@ -554,8 +531,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                         const uint4 hd = __ldg(reinterpret_cast<const uint4*>(rec));
                         const uint32_t deg = hd.x & 0x7FFFFFFFu;
                         const uint32_t fb = m.flat;
-                        const uint32_t xb = dsm ? reinterpret_cast<const uint8_t*>(ssw + sidx(f))[lane]
-                                                : ld_spin<SPLIT>(spb + 8u * f);
+                        const uint32_t xb = ld_spin<SPLIT>(spb + 8u * f);
                         const uint4* kp = reinterpret_cast<const uint4*>(kbb + (size_t)f * 64 + lane * 8);
                         uint32_t flips = 0, ties = 0;
                         if constexpr (MODE == kModeInt) {
@@ -570,8 +546,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                                 uint32_t li[4];
     #pragma unroll
                                 for (int e = 0; e < 4; e++)
-                                    li[e] = (dsm ? reinterpret_cast<const uint8_t*>(wptr(fb + (en[e] & 0xFFFFFFu)))[lane]
-                                                 : ld_spin<SPLIT>(spb + 8u * (fb + (en[e] & 0xFFFFFFu)))) |
+                                    li[e] = ld_spin<SPLIT>(spb + 8u * (fb + (en[e] & 0xFFFFFFu))) |
                                             ((en[e] >> 23) & 0x100u);
     #pragma unroll
                                 for (int e = 0; e < 4; e++) {
@@ -633,9 +608,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                                 const double ww[4] = {w01.x, w01.y, w23.x, w23.y};
                                 uint32_t bj[4];
     #pragma unroll
-                                for (int e = 0; e < 4; e++)
-                                    bj[e] = dsm ? reinterpret_cast<const uint8_t*>(wptr(fb + cc[e]))[lane]
-                                                : ld_spin<SPLIT>(spb + 8u * (fb + cc[e]));
+                                for (int e = 0; e < 4; e++) bj[e] = ld_spin<SPLIT>(spb + 8u * (fb + cc[e]));
     #pragma unroll
                                 for (int e = 0; e < 4; e++) {
                                     if (q + e < deg) {
@@ -668,8 +641,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                                 if (L.exact_count) atomicAdd(L.exact_count, __popc(ties));
                             }
                         }
-                        if (dsm) reinterpret_cast<uint8_t*>(ssw + sidx(f))[lane] = (uint8_t)(xb ^ flips);
-                        else spb[8u * f] = (uint8_t)(xb ^ flips);
+                        spb[8u * f] = (uint8_t)(xb ^ flips);
                     }
                 }
                 if (l + 1 < I.nlvl) {
@@ -736,14 +708,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
             }
         }
         if constexpr (SPLIT) {
-            // every CTA's last level is done (its slice back in global memory
-            // first); the first CTA finishes the item
-            if (dsm) {
-                for (uint32_t i = tid; i < L.spin_cap; i += T) {
-                    const uint32_t j = ((crank + csize * (i >> 7)) << 7) | (i & 127u);
-                    if (j < ms[0].n) sw[j] = ssw[i];
-                }
-            }
+            // every CTA's last level is done; the first CTA finishes the item
             cg::this_cluster().sync();
             if (crank != 0) continue;
         }
@@ -862,7 +827,7 @@ int level_clusters(uint32_t mode, int threads, size_t smem, uint32_t split) {
 cudaError_t launch_level(const DevArrays& A, const RunArgs& R, const LvlArgs& L, uint32_t mode, bool gsp, int threads,
                          int grid, cudaStream_t st, uint32_t split) {
     if (L.ov && split <= 1) threads += (int)L.ov;  // the generator group of an overlapped launch
-    const size_t smem = level_smem(mode, L.ntab, (gsp && !L.dsm) ? 0 : L.spin_cap, L.ov != 0);
+    const size_t smem = level_smem(mode, L.ntab, gsp ? 0 : L.spin_cap, L.ov != 0);
     if (split > 1) {
         cudaLaunchAttribute attr;
         const cudaLaunchConfig_t cfg = level_config(grid, threads, smem, st, split, &attr);

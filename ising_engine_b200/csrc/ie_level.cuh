@@ -81,10 +81,6 @@ struct LvlArgs {
     // double-buffered (second output buffer at keyhalf)
     uint32_t ov;
     uint64_t keyhalf;
-    // cluster launches: 1 when each CTA keeps its segments' spin words in
-    // shared memory (spin_cap words: the largest slice) and reads the other
-    // CTAs' through distributed shared memory
-    uint32_t dsm;
     uint32_t spin_cap;         // shared-memory spin words per CTA (0: global spins)
     uint32_t ntab;             // threshold tables per CTA (own tables: one per member)
     // Test hook: decisions compare only the top 32 - tie_shift bits of the
