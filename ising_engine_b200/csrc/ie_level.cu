@@ -544,11 +544,11 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                                 const uint4 e4 = __ldg(e4p + (q >> 2));
                                 const uint32_t en[4] = {e4.x, e4.y, e4.z, e4.w};
                                 uint32_t li[4];
-    #pragma unroll
+#pragma unroll
                                 for (int e = 0; e < 4; e++)
                                     li[e] = ld_spin<SPLIT>(spb + 8u * (fb + (en[e] & 0xFFFFFFu))) |
                                             ((en[e] >> 23) & 0x100u);
-    #pragma unroll
+#pragma unroll
                                 for (int e = 0; e < 4; e++) {
                                     const uint2 sv = lut[li[e]];
                                     const uint32_t w = (en[e] >> 24) & 0x7Fu;
@@ -566,14 +566,14 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                             const uint32_t iH = ((aH + cA) & ~xH) | ((cB - aH) & xH);
                             const uint32_t* tb = tabb + (own_tab ? slot * kLvlTab : 0u);
                             if (sh == 0) {
-    #pragma unroll
+#pragma unroll
                                 for (int k = 0; k < 8; k++) {
                                     const uint32_t qa = mh[k], qb = tb[((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu];
                                     flips |= (uint32_t)(qa < qb) << k;
                                     ties |= (uint32_t)(qa == qb) << k;
                                 }
                             } else {
-    #pragma unroll
+#pragma unroll
                                 for (int k = 0; k < 8; k++) {
                                     const uint32_t idx = ((k < 4 ? iL : iH) >> (8 * (k & 3))) & 0xFFu;
                                     const uint32_t qa = mh[k] >> sh, qb = tb[idx] >> sh;
@@ -598,7 +598,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                             // the outputs are read after the sum (fewer live registers), from L1
                             prefetch_l1(kp);
                             double dl[8];
-    #pragma unroll
+#pragma unroll
                             for (int k = 0; k < 8; k++) dl[k] = wl;
                             for (uint32_t q = 0; q < deg; q += 4) {
                                 const uint4 c4 = __ldg(c4p + (q >> 2));
@@ -607,20 +607,21 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                                 const uint32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
                                 const double ww[4] = {w01.x, w01.y, w23.x, w23.y};
                                 uint32_t bj[4];
-    #pragma unroll
+#pragma unroll
                                 for (int e = 0; e < 4; e++) bj[e] = ld_spin<SPLIT>(spb + 8u * (fb + cc[e]));
-    #pragma unroll
+                                // branch-free: a clear bit (or a padding entry, w = 0) adds +0.0,
+                                // which leaves every sum but -0.0 unchanged, and -0.0 and +0.0
+                                // take the same decision (dE <= 0 accepts)
+#pragma unroll
                                 for (int e = 0; e < 4; e++) {
-                                    if (q + e < deg) {
-    #pragma unroll
-                                        for (int k = 0; k < 8; k++)
-                                            if ((bj[e] >> k) & 1u) dl[k] = __dadd_rn(dl[k], ww[e]);
-                                    }
+#pragma unroll
+                                    for (int k = 0; k < 8; k++)
+                                        dl[k] = __dadd_rn(dl[k], ((bj[e] >> k) & 1u) ? ww[e] : 0.0);
                                 }
                             }
                             const uint4 k0 = kp[0], k1 = kp[1];
                             const uint32_t mh[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
-    #pragma unroll
+#pragma unroll
                             for (int k = 0; k < 8; k++) {
                                 if ((xb >> k) & 1u) dl[k] = -dl[k];
                                 if (dl[k] <= 0.0) {
@@ -632,7 +633,7 @@ __global__ void __maxnreg__(64) level_kernel(DevArrays A, RunArgs R, LvlArgs L) 
                                 ties |= (uint32_t)(r == 0) << k;
                             }
                             if (ties) {
-    #pragma unroll
+#pragma unroll
                                 for (int k = 0; k < 8; k++)
                                     if ((ties >> k) & 1u)
                                         flips |= exact_flip_f64(m.base[b], lane, v, k, __dmul_rn(-dl[k], m.beta[b]),
