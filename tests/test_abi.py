@@ -40,3 +40,28 @@ def test_suggested_temp_range_matches_definition():
     mn = min(np.abs(lin[lin != 0]).min(), np.abs(va[va != 0]).min())
     assert tmax == ml / np.log(2.0)
     assert tmin == min(mn / np.log(100.0), tmax * 0.5)
+
+
+def _header_struct_fields(name):
+    """Field names, in order, of `typedef struct name { ... } name;` in the header."""
+    import os
+    import re
+    txt = open(os.path.join(os.path.dirname(_build.HERE), "include", "ising_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    m = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), txt, flags=re.S)
+    assert m, name
+    fields = []
+    for decl in m.group(1).split(";"):
+        decl = decl.strip()
+        if decl:
+            fields += [v.strip().lstrip("*") for v in decl.split()[-1].split(",")]
+    return fields
+
+
+def test_config_structs_match_the_header():
+    """The ctypes mirrors of the config structs list the header's fields in
+    the header's order (callers zero-initialise and set fields by name, so a
+    field out of place would shift every later one)."""
+    for name in ["ie_config", "ie_batch_config", "ie_serve_config", "ie_pa_config", "ie_problem"]:
+        ours = [f[0] for f in getattr(_ffi, name)._fields_]
+        assert ours == _header_struct_fields(name), name
