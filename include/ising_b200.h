@@ -175,6 +175,21 @@ ie_status ie_read_swap_stats(ie_handle* h, uint64_t* attempts, uint64_t* accepts
 ie_status ie_read_rng_state(ie_handle* h, uint64_t* draws, int32_t* deo_odd_phase);
 /* Incumbent of ie_run_pt: energy (model energy incl. offset) and state [num_vars]. */
 ie_status ie_read_incumbent(ie_handle* h, double* energy, int8_t* state);
+
+/* Checkpoint of a handle's device state (handles with num_pops = 1): spin
+ * words, replica energies, swap statistics, master-stream position, DEO
+ * phase, steps run and the incumbent, as one blob. Loading it into a handle
+ * created with the same problem and config continues the trajectory exactly
+ * (the blob checks sites, cells, mode and its own spin digest).
+ * The reference's replay anchor is the FNV-1a digest of the state
+ * (src/engine_v2/state.rs:55-67); ie_state_digest is FNV-1a over the
+ * little-endian bytes of the spin words in the reference layout (cell-major,
+ * bit r = replica r), ie_fnv1a the same hash of any host buffer. */
+ie_status ie_state_size(ie_handle* h, uint64_t* bytes);
+ie_status ie_save_state(ie_handle* h, void* blob, uint64_t bytes);
+ie_status ie_load_state(ie_handle* h, const void* blob, uint64_t bytes);
+ie_status ie_state_digest(ie_handle* h, uint64_t* digest);
+ie_status ie_fnv1a(const void* bytes, uint64_t n, uint64_t* digest);
 /* Best replica of the final field in (t, r) order with strict < on the model
  * energy (ultimate.rs:345-368), merged with the incumbent (ultimate.rs:371-373). */
 ie_status ie_read_best(ie_handle* h, double* energy, int8_t* state);

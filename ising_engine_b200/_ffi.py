@@ -103,6 +103,11 @@ _SIGS = {
     "ie_read_energies": ([_vp, _vp], C.c_int),
     "ie_read_swap_stats": ([_vp, _vp, _vp], C.c_int),
     "ie_read_rng_state": ([_vp, _vp, _vp], C.c_int),
+    "ie_state_size": ([_vp, _vp], C.c_int),
+    "ie_save_state": ([_vp, _vp, C.c_uint64], C.c_int),
+    "ie_load_state": ([_vp, _vp, C.c_uint64], C.c_int),
+    "ie_state_digest": ([_vp, _vp], C.c_int),
+    "ie_fnv1a": ([_vp, C.c_uint64, _vp], C.c_int),
     "ie_read_incumbent": ([_vp, _vp, _vp], C.c_int),
     "ie_read_best": ([_vp, _vp, _vp], C.c_int),
     "ie_one_opt": ([_vp, _vp, _vp, _vp], C.c_int),

@@ -2626,6 +2626,163 @@ ie_status ie_read_rng_state(ie_handle* h, uint64_t* draws, int32_t* deo) {
     return IE_OK;
 }
 
+// ---- checkpoint ----
+namespace {
+constexpr uint64_t kStateMagic = 0x3154534232424549ull;  // "IEB2BST1"
+
+struct StateHeader {
+    uint64_t magic;
+    uint32_t version, mode;
+    uint64_t n, cells, npairs, steps_done, draws;
+    int32_t deo, have_inc;
+    double inc_e;
+    uint64_t digest, inc_words;
+};
+
+uint64_t fnv1a_bytes(const uint8_t* b, uint64_t n, uint64_t h = 0xcbf29ce484222325ull) {
+    for (uint64_t i = 0; i < n; i++) {
+        h ^= b[i];
+        h *= 0x100000001b3ull;
+    }
+    return h;
+}
+
+// FNV-1a over the reference-layout words of lane-major device words (little-endian bytes)
+uint64_t spin_digest(const std::vector<uint64_t>& lane_major) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    for (uint64_t w : lane_major) {
+        const uint64_t r = transpose8x8(w);
+        uint8_t b[8];
+        for (int i = 0; i < 8; i++) b[i] = (uint8_t)(r >> (8 * i));
+        h = fnv1a_bytes(b, 8, h);
+    }
+    return h;
+}
+
+uint64_t state_bytes(const Engine& E, uint64_t inc_words) {
+    const InstDesc& d = E.desc[0];
+    const uint32_t L = E.nt;
+    const uint64_t np = L > 1 ? L - 1 : 0;
+    return sizeof(StateHeader) + 8ull * d.nt * d.n + (d.mode == kModeInt ? 4ull : 8ull) * d.nt * kReplicas +
+           16ull * np + 8ull * inc_words;
+}
+}  // namespace
+
+ie_status ie_state_size(ie_handle* h, uint64_t* bytes) {
+    if (!h || !bytes) return fail(IE_ERR_INVALID, "NULL argument");
+    if (h->eng.pop_len) return fail(IE_ERR_UNSUPPORTED, "checkpoints cover handles with num_pops = 1");
+    *bytes = state_bytes(h->eng, h->d_inc_state.n);
+    return IE_OK;
+}
+
+ie_status ie_state_digest(ie_handle* h, uint64_t* digest) {
+    if (!h || !digest) return fail(IE_ERR_INVALID, "NULL argument");
+    IE_CUDA(cudaSetDevice(h->eng.device));
+    const InstDesc& d = h->eng.desc[0];
+    std::vector<uint64_t> w((size_t)d.nt * d.n);
+    if (!w.empty())
+        IE_CUDA(cudaMemcpy(w.data(), h->eng.d_spins.p + d.spin, w.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    *digest = spin_digest(w);
+    return IE_OK;
+}
+
+ie_status ie_fnv1a(const void* bytes, uint64_t n, uint64_t* digest) {
+    if ((!bytes && n) || !digest) return fail(IE_ERR_INVALID, "NULL argument");
+    *digest = fnv1a_bytes(static_cast<const uint8_t*>(bytes), n);
+    return IE_OK;
+}
+
+ie_status ie_save_state(ie_handle* h, void* blob, uint64_t bytes) {
+    if (!h || !blob) return fail(IE_ERR_INVALID, "NULL argument");
+    Engine& E = h->eng;
+    if (E.pop_len) return fail(IE_ERR_UNSUPPORTED, "checkpoints cover handles with num_pops = 1");
+    if (!E.initialized) return fail(IE_ERR_INVALID, "the handle's state is not initialised");
+    const uint64_t iw = h->d_inc_state.n;
+    if (bytes < state_bytes(E, iw)) return fail(IE_ERR_INVALID, "blob smaller than ie_state_size");
+    IE_CUDA(cudaSetDevice(E.device));
+    IE_CUDA(cudaStreamSynchronize(E.stream));
+    const InstDesc& d = E.desc[0];
+    const uint64_t nw = (uint64_t)d.nt * d.n, ne = (uint64_t)d.nt * kReplicas, np = E.nt > 1 ? E.nt - 1 : 0;
+    uint8_t* p = static_cast<uint8_t*>(blob);
+    StateHeader hd{};
+    hd.magic = kStateMagic;
+    hd.version = 1;
+    hd.mode = d.mode;
+    hd.n = d.n;
+    hd.cells = d.nt;
+    hd.npairs = np;
+    hd.steps_done = E.steps_done;
+    hd.have_inc = h->have_incumbent ? 1 : 0;
+    hd.inc_words = iw;
+    IE_CUDA(cudaMemcpy(&hd.draws, E.d_pos.p, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    IE_CUDA(cudaMemcpy(&hd.deo, E.d_deo.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (h->d_inc_e.p) IE_CUDA(cudaMemcpy(&hd.inc_e, h->d_inc_e.p, sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<uint64_t> w(nw);
+    if (nw) IE_CUDA(cudaMemcpy(w.data(), E.d_spins.p + d.spin, nw * 8, cudaMemcpyDeviceToHost));
+    hd.digest = spin_digest(w);
+    std::memcpy(p, &hd, sizeof(hd));
+    p += sizeof(hd);
+    std::memcpy(p, w.data(), nw * 8);
+    p += nw * 8;
+    if (d.mode == kModeInt) {
+        IE_CUDA(cudaMemcpy(p, E.d_Ei.p + d.energy, ne * 4, cudaMemcpyDeviceToHost));
+        p += ne * 4;
+    } else {
+        IE_CUDA(cudaMemcpy(p, E.d_Ef.p + d.energy, ne * 8, cudaMemcpyDeviceToHost));
+        p += ne * 8;
+    }
+    if (np) {
+        IE_CUDA(cudaMemcpy(p, E.d_att.p, np * 8, cudaMemcpyDeviceToHost));
+        IE_CUDA(cudaMemcpy(p + np * 8, E.d_acc.p, np * 8, cudaMemcpyDeviceToHost));
+        p += 16 * np;
+    }
+    if (iw) IE_CUDA(cudaMemcpy(p, h->d_inc_state.p, iw * 8, cudaMemcpyDeviceToHost));
+    return IE_OK;
+}
+
+ie_status ie_load_state(ie_handle* h, const void* blob, uint64_t bytes) {
+    if (!h || !blob) return fail(IE_ERR_INVALID, "NULL argument");
+    Engine& E = h->eng;
+    if (E.pop_len) return fail(IE_ERR_UNSUPPORTED, "checkpoints cover handles with num_pops = 1");
+    if (bytes < sizeof(StateHeader)) return fail(IE_ERR_INVALID, "blob too small");
+    StateHeader hd;
+    std::memcpy(&hd, blob, sizeof(hd));
+    const InstDesc& d = E.desc[0];
+    const uint64_t nw = (uint64_t)d.nt * d.n, ne = (uint64_t)d.nt * kReplicas, np = E.nt > 1 ? E.nt - 1 : 0;
+    if (hd.magic != kStateMagic || hd.version != 1) return fail(IE_ERR_INVALID, "not a state blob of this version");
+    if (hd.n != d.n || hd.cells != d.nt || hd.mode != d.mode || hd.npairs != np || hd.inc_words != h->d_inc_state.n)
+        return fail(IE_ERR_INVALID, "state blob of another problem or config (sites, cells, mode)");
+    if (bytes < state_bytes(E, hd.inc_words)) return fail(IE_ERR_INVALID, "blob truncated");
+    const uint8_t* p = static_cast<const uint8_t*>(blob) + sizeof(hd);
+    std::vector<uint64_t> w(nw);
+    std::memcpy(w.data(), p, nw * 8);
+    p += nw * 8;
+    if (spin_digest(w) != hd.digest) return fail(IE_ERR_INVALID, "state blob digest mismatch");
+    IE_CUDA(cudaSetDevice(E.device));
+    IE_CUDA(cudaStreamSynchronize(E.stream));
+    if (nw) IE_CUDA(cudaMemcpy(E.d_spins.p + d.spin, w.data(), nw * 8, cudaMemcpyHostToDevice));
+    if (d.mode == kModeInt) {
+        IE_CUDA(cudaMemcpy(E.d_Ei.p + d.energy, p, ne * 4, cudaMemcpyHostToDevice));
+        p += ne * 4;
+    } else {
+        IE_CUDA(cudaMemcpy(E.d_Ef.p + d.energy, p, ne * 8, cudaMemcpyHostToDevice));
+        p += ne * 8;
+    }
+    if (np) {
+        IE_CUDA(cudaMemcpy(E.d_att.p, p, np * 8, cudaMemcpyHostToDevice));
+        IE_CUDA(cudaMemcpy(E.d_acc.p, p + np * 8, np * 8, cudaMemcpyHostToDevice));
+        p += 16 * np;
+    }
+    if (hd.inc_words) IE_CUDA(cudaMemcpy(h->d_inc_state.p, p, hd.inc_words * 8, cudaMemcpyHostToDevice));
+    if (h->d_inc_e.p) IE_CUDA(cudaMemcpy(h->d_inc_e.p, &hd.inc_e, sizeof(double), cudaMemcpyHostToDevice));
+    IE_CUDA(cudaMemcpy(E.d_pos.p, &hd.draws, sizeof(uint64_t), cudaMemcpyHostToDevice));
+    IE_CUDA(cudaMemcpy(E.d_deo.p, &hd.deo, sizeof(int32_t), cudaMemcpyHostToDevice));
+    E.steps_done = hd.steps_done;
+    E.initialized = true;
+    h->have_incumbent = hd.have_inc != 0;
+    return IE_OK;
+}
+
 ie_status ie_read_incumbent(ie_handle* h, double* energy, int8_t* state) {
     if (!h || !energy || !state) return fail(IE_ERR_INVALID, "NULL argument");
     IE_CUDA(cudaSetDevice(h->eng.device));

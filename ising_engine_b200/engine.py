@@ -164,6 +164,27 @@ class Engine:
         _ffi.check(self._L.ie_read_rng_state(self._h, _p(d), _p(p)))
         return int(d[0]), int(p[0])
 
+    def save_state(self) -> bytes:
+        """The device state as one blob (spins, energies, swap statistics,
+        stream position, DEO phase, steps run, incumbent)."""
+        n = C.c_uint64()
+        _ffi.check(self._L.ie_state_size(self._h, C.byref(n)))
+        buf = (C.c_uint8 * n.value)()
+        _ffi.check(self._L.ie_save_state(self._h, buf, n.value))
+        return bytes(buf)
+
+    def load_state(self, blob: bytes) -> None:
+        """Restores a blob of save_state into this handle (same problem and
+        config); the run continues as the saved one would have."""
+        buf = (C.c_uint8 * len(blob)).from_buffer_copy(blob)
+        _ffi.check(self._L.ie_load_state(self._h, buf, len(blob)))
+
+    def digest(self) -> int:
+        """FNV-1a over the spin words in the reference layout (state.rs:60-67)."""
+        d = C.c_uint64()
+        _ffi.check(self._L.ie_state_digest(self._h, C.byref(d)))
+        return d.value
+
     def incumbent(self):
         e = np.zeros(1, dtype=np.float64)
         s = np.zeros(self.n, dtype=np.int8)

@@ -65,3 +65,19 @@ def test_config_structs_match_the_header():
     for name in ["ie_config", "ie_batch_config", "ie_serve_config", "ie_pa_config", "ie_problem"]:
         ours = [f[0] for f in getattr(_ffi, name)._fields_]
         assert ours == _header_struct_fields(name), name
+
+
+def test_fnv1a_matches_the_reference_definition():
+    """ie_fnv1a is FNV-1a 64 (src/engine_v2/state.rs:60-67): offset basis
+    0xcbf29ce484222325, prime 0x100000001b3, xor then multiply per byte."""
+    rng = np.random.default_rng(5)
+    for n in (0, 1, 7, 64, 1000):
+        data = rng.integers(0, 256, size=n, dtype=np.uint8)
+        h = 0xcbf29ce484222325
+        for b in data.tobytes():
+            h = ((h ^ b) * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+        out = C.c_uint64()
+        buf = data.ctypes.data if n else None
+        assert _ffi.lib().ie_fnv1a(buf, n, C.byref(out)) == 0
+        assert out.value == h
+    assert _ffi.lib().ie_fnv1a(None, 0, C.byref(out)) == 0 and out.value == 0xcbf29ce484222325
